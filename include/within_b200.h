@@ -1,0 +1,176 @@
+/*
+ * within_b200.h -- C ABI of the B200-native solve phase of `within`.
+ *
+ * The entry points replace the reference's Rust API (paths relative to the
+ * reference's crates/ directory):
+ *
+ *   within_solver_new          Solver::new               within/src/solver.rs:415-430
+ *   within_solver_solve        Solver::solve             within/src/solver.rs:157-239
+ *   within_solver_solve_batch  Solver::solve_batch       within/src/solver.rs:241-277
+ *   within_solver_n_dofs/_obs  Solver::{n_dofs,n_obs}    within/src/solver.rs:284-292
+ *   within_solve / _batch      orchestrate::{solve,solve_batch}  within/src/orchestrate.rs:151-184
+ *   within_solver_free         Drop for Solver
+ *   within_last_error          Display of WithinError    within/src/error.rs:61-90
+ *
+ * Configuration mirrors SolverParams / Preconditioner / LocalSolverConfig
+ * (within/src/config.rs:43-236).  Every computation runs on the current CUDA
+ * device through hand-written sm_100a kernels; there is no CPU fallback: when
+ * no device is usable the calls fail with WITHIN_ERR_CUDA.
+ *
+ * Layouts: categories element (i, q) is codes[i*row_stride + q*col_stride]
+ * (F-order: row_stride 1, col_stride n_obs).  Batch inputs and outputs are
+ * RHS-major (column j of an F-order (n, k) array starts at j*n), matching
+ * BatchSolveResult (within/src/orchestrate.rs:58-135).
+ *
+ * Thread safety: a solver may be used from several host threads; calls on one
+ * solver are serialised internally.
+ */
+#ifndef WITHIN_B200_H
+#define WITHIN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: one per WithinError variant (within/src/error.rs:25-59). */
+enum {
+    WITHIN_OK = 0,
+    WITHIN_ERR_EMPTY_OBSERVATIONS = 1,
+    WITHIN_ERR_OBSERVATION_COUNT_MISMATCH = 2,
+    WITHIN_ERR_WEIGHT_COUNT_MISMATCH = 3,
+    WITHIN_ERR_OVERFLOW = 4,
+    WITHIN_ERR_SINGULAR_DIAGONAL = 5,
+    WITHIN_ERR_LOCAL_SOLVER_BUILD = 6,
+    WITHIN_ERR_PRECONDITIONER_BUILD = 7,
+    WITHIN_ERR_ITERATIVE_SOLVE = 8,
+    WITHIN_ERR_INVALID_ARGUMENT = 9, /* configuration rejected (PyValueError in within-py) */
+    WITHIN_ERR_CUDA = 10             /* device unavailable or a CUDA call failed */
+};
+
+enum { WITHIN_KRYLOV_CG = 0, WITHIN_KRYLOV_GMRES = 1 };
+enum { WITHIN_OPERATOR_IMPLICIT = 0, WITHIN_OPERATOR_EXPLICIT = 1 };
+enum { WITHIN_PRECOND_OFF = 0, WITHIN_PRECOND_ADDITIVE = 1, WITHIN_PRECOND_MULTIPLICATIVE = 2 };
+/* Arithmetic of the inner Krylov solve.  FP64 is the plain drop-in; MIXED runs the
+ * operator and Schwarz applies in FP32 inside an FP64 iterative-refinement loop. */
+enum { WITHIN_PRECISION_FP64 = 0, WITHIN_PRECISION_MIXED = 1 };
+
+/* SolverParams (within/src/config.rs:205-236). */
+typedef struct {
+    int32_t krylov;          /* WITHIN_KRYLOV_* */
+    int32_t gmres_restart;   /* KrylovMethod::Gmres { restart } */
+    int32_t operator_repr;   /* WITHIN_OPERATOR_* */
+    double tol;
+    int32_t maxiter;
+    int32_t max_refinements;
+    int32_t precision;       /* WITHIN_PRECISION_* */
+} within_params;
+
+/* Preconditioner + LocalSolverConfig (within/src/config.rs:76-117, 174-183). */
+typedef struct {
+    int32_t kind;                  /* WITHIN_PRECOND_* */
+    uint64_t approx_chol_seed;
+    uint32_t approx_chol_split;    /* split_merge; 0 or 1 = None */
+    int32_t approx_schur_enabled;  /* 0 = exact Schur complement */
+    uint64_t approx_schur_seed;
+    uint32_t approx_schur_split;
+    int32_t dense_threshold;
+    int32_t reduction_strategy;    /* accepted for API parity; the device path has one reduction */
+} within_preconditioner;
+
+typedef struct {
+    int32_t converged;
+    int32_t iterations;      /* Krylov iterations including refinement */
+    double final_residual;   /* ||D'W(y - D x)|| / ||D'W y|| */
+    double time_total;       /* seconds */
+    double time_setup;
+    double time_solve;
+} within_solve_stats;
+
+typedef struct within_solver within_solver;
+
+/* Fill the reference defaults: CG, implicit, tol 1e-8, maxiter 1000, 2 refinements
+ * (config.rs:227-236); additive Schwarz with LocalSolverConfig::solver_default()
+ * (config.rs:108-117, within-py/src/lib.rs:546-552). */
+void within_default_params(within_params *params);
+void within_default_preconditioner(within_preconditioner *precond);
+
+/* Solver::new.  weights may be NULL (unit weights).  precond may be NULL (no
+ * preconditioner, Preconditioner.Off).  On success *out owns the device copy of
+ * the design and the preconditioner factors. */
+int within_solver_new(const uint32_t *codes, size_t n_obs, size_t n_factors,
+                      int64_t row_stride, int64_t col_stride, const double *weights,
+                      const within_params *params, const within_preconditioner *precond,
+                      within_solver **out);
+void within_solver_free(within_solver *solver);
+
+size_t within_solver_n_dofs(const within_solver *solver);
+size_t within_solver_n_obs(const within_solver *solver);
+size_t within_solver_n_factors(const within_solver *solver);
+
+/* Solver::solve: y (n_obs), x (n_dofs), demeaned (n_obs) are host buffers. */
+int within_solver_solve(within_solver *solver, const double *y, double *x, double *demeaned,
+                        within_solve_stats *stats);
+
+/* Solver::solve_batch: ys (n_obs*k, RHS-major), x (n_dofs*k), demeaned (n_obs*k) host
+ * buffers; stats has k entries; time_total of entry 0 is the batch total. */
+int within_solver_solve_batch(within_solver *solver, const double *ys, size_t k, double *x,
+                              double *demeaned, within_solve_stats *stats);
+
+/* Same as solve_batch with device buffers, on the given CUDA stream (NULL = the
+ * solver's own stream).  Inputs stay resident in HBM; no host copies of vectors. */
+int within_solver_solve_batch_device(within_solver *solver, const double *d_ys, size_t k,
+                                     double *d_x, double *d_demeaned, within_solve_stats *stats,
+                                     void *cuda_stream);
+
+/* One-shot orchestrate::solve / solve_batch (build, solve, free). */
+int within_solve(const uint32_t *codes, size_t n_obs, size_t n_factors, int64_t row_stride,
+                 int64_t col_stride, const double *y, const double *weights,
+                 const within_params *params, const within_preconditioner *precond, double *x,
+                 double *demeaned, within_solve_stats *stats);
+int within_solve_batch(const uint32_t *codes, size_t n_obs, size_t n_factors, int64_t row_stride,
+                       int64_t col_stride, const double *ys, size_t k, const double *weights,
+                       const within_params *params, const within_preconditioner *precond,
+                       double *x, double *demeaned, within_solve_stats *stats);
+
+/* Operator applies on host vectors, for parity tests against the CPU oracle
+ * (Operator::apply of GramianOperator, within/src/operator/gramian.rs:84-89, and of
+ * FePreconditioner, within/src/operator/preconditioner.rs:108-154).
+ * x, y: n_dofs*k RHS-major.  Precision follows the solver's params. */
+int within_solver_apply_gramian(within_solver *solver, const double *x, size_t k, double *y);
+int within_solver_apply_preconditioner(within_solver *solver, const double *r, size_t k, double *z);
+/* D x (matvec_d, domain.rs:390-395): x n_dofs*k -> y n_obs*k; D'W r (rmatvec_wdt, :409-417). */
+int within_solver_matvec_d(within_solver *solver, const double *x, size_t k, double *y);
+int within_solver_rmatvec_wdt(within_solver *solver, const double *r, size_t k, double *x);
+
+/* Setup introspection, for bit-exact checks of the integer setup against the oracle.
+ * factor_meta: n_levels[q], offsets[q] (WeightedDesign::from_store, domain.rs:133-155). */
+void within_solver_factor_meta(const within_solver *solver, int64_t *n_levels, int64_t *offsets);
+int32_t within_solver_n_subdomains(const within_solver *solver);
+/* info[8] = q, r, n_local, n_q, n_r, eliminate_q, reduced_kind (0 dense, 1 ac), n_reduced */
+void within_solver_subdomain_info(const within_solver *solver, int32_t i, int64_t *info);
+void within_solver_subdomain_indices(const within_solver *solver, int32_t i, uint32_t *gidx,
+                                     double *pou);
+/* AC factor of subdomain i: sizes[5] = n, n_levels, nnz, n_columns, n_core (zeros for
+ * dense subdomains).  Arrays: level_ptr (n_levels+1), col_vertex/col_diag (n_columns),
+ * col_ptr (n_columns+1), col_idx/col_coef (nnz), core_vertex (n_core),
+ * core_z (n_core*n_core row-major anchored inverse of the dense core). */
+void within_solver_ac_sizes(const within_solver *solver, int32_t i, int64_t *sizes);
+void within_solver_ac_arrays(const within_solver *solver, int32_t i, int32_t *level_ptr,
+                             int32_t *col_vertex, double *col_diag, int32_t *col_ptr,
+                             int32_t *col_idx, double *col_coef, int32_t *core_vertex,
+                             double *core_z);
+
+/* Number of kernels this solver has launched so far, and its setup wall time (s). */
+int64_t within_solver_gpu_launches(const within_solver *solver);
+double within_solver_setup_time(const within_solver *solver);
+
+/* Message of the last failed call on this host thread ("" when none). */
+const char *within_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WITHIN_B200_H */

@@ -1,0 +1,408 @@
+"""B200-native solve phase of `within` with the `within_py` Python API.
+
+Mirrors ``within`` (python/within/__init__.py, within-py/src/lib.rs:62-1074):
+``solve``, ``solve_batch``, ``Solver``, the configuration classes ``CG``,
+``GMRES``, ``AdditiveSchwarz``, ``MultiplicativeSchwarz``, ``SchurComplement``,
+``ApproxCholConfig``, ``ApproxSchurConfig`` and the enums ``OperatorRepr``,
+``Preconditioner``, ``ReductionStrategy``.  Every solve runs on the current CUDA
+device through ``libwithin_b200.so``; invalid input raises ``ValueError``, a bad
+configuration type ``TypeError`` (as within-py does, lib.rs:480-483, 516, 590).
+
+One addition: ``CG``/``GMRES`` take ``precision="fp64"`` (the drop-in: every
+step in FP64) or ``precision="mixed"`` (FP32 operator and Schwarz applies inside
+an FP64 iterative-refinement loop; same tolerance on the FP64 residual).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+import warnings
+from enum import IntEnum
+
+import numpy as np
+
+from . import _lib
+
+__all__ = [
+    "OperatorRepr", "Preconditioner", "ReductionStrategy", "CG", "GMRES", "ApproxCholConfig",
+    "ApproxSchurConfig", "SchurComplement", "AdditiveSchwarz", "MultiplicativeSchwarz", "SolveResult",
+    "BatchSolveResult", "FePreconditioner", "Solver", "solve", "solve_batch", "WithinError",
+]
+
+
+class WithinError(ValueError):
+    """Error raised by the native library (a ValueError, like within-py's errors)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+        self.kind = _lib.ERR_NAMES.get(code, "Unknown")
+
+
+class OperatorRepr(IntEnum):
+    Implicit = 0
+    Explicit = 1
+
+
+class Preconditioner(IntEnum):
+    Additive = 0
+    Multiplicative = 1
+    Off = 2
+
+
+class ReductionStrategy(IntEnum):
+    Auto = 0
+    AtomicScatter = 1
+    ParallelReduction = 2
+
+
+_PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
+class CG:
+    """Conjugate gradient on the normal equations (within-py CG, lib.rs:262-300)."""
+
+    def __init__(self, tol: float = 1e-8, maxiter: int = 1000, operator: OperatorRepr = OperatorRepr.Implicit,
+                 max_refinements: int = 2, precision: str = "fp64"):
+        if precision not in _PRECISIONS:
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.tol, self.maxiter, self.operator = float(tol), int(maxiter), OperatorRepr(operator)
+        self.max_refinements, self.precision = int(max_refinements), precision
+
+    def __repr__(self):
+        return f"CG(tol={self.tol}, maxiter={self.maxiter}, operator={self.operator.name}, precision={self.precision!r})"
+
+
+class GMRES:
+    """Right-preconditioned GMRES(restart) (within-py GMRES, lib.rs:302-346)."""
+
+    def __init__(self, tol: float = 1e-8, maxiter: int = 1000, restart: int = 30,
+                 operator: OperatorRepr = OperatorRepr.Implicit, max_refinements: int = 2,
+                 precision: str = "fp64"):
+        if precision not in _PRECISIONS:
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.tol, self.maxiter, self.restart = float(tol), int(maxiter), int(restart)
+        self.operator, self.max_refinements, self.precision = OperatorRepr(operator), int(max_refinements), precision
+
+    def __repr__(self):
+        return f"GMRES(tol={self.tol}, maxiter={self.maxiter}, restart={self.restart})"
+
+
+class ApproxCholConfig:
+    """Approximate Cholesky parameters; split > 1 means split_merge=Some(split) (lib.rs:62-98)."""
+
+    def __init__(self, seed: int = 0, split: int = 1):
+        if split < 1:
+            raise ValueError("split must be >= 1")
+        self.seed, self.split = int(seed), int(split)
+
+
+class ApproxSchurConfig:
+    """Sampled Schur complement parameters (lib.rs:100-128)."""
+
+    def __init__(self, seed: int = 0, split: int = 1):
+        if split < 1:
+            raise ValueError("split must be >= 1")
+        self.seed, self.split = int(seed), int(split)
+
+
+class SchurComplement:
+    """Local solver: Schur complement + approximate Cholesky (lib.rs:130-180)."""
+
+    def __init__(self, approx_chol: ApproxCholConfig | None = None, approx_schur: ApproxSchurConfig | None = None,
+                 dense_threshold: int = 24):
+        self.approx_chol, self.approx_schur, self.dense_threshold = approx_chol, approx_schur, int(dense_threshold)
+
+
+class AdditiveSchwarz:
+    def __init__(self, local_solver: SchurComplement | None = None,
+                 reduction: ReductionStrategy = ReductionStrategy.Auto):
+        self.local_solver, self.reduction = local_solver, ReductionStrategy(reduction)
+
+
+class MultiplicativeSchwarz:
+    def __init__(self, local_solver: SchurComplement | None = None):
+        self.local_solver = local_solver
+
+
+def _default_local() -> _lib.Precond:
+    p = _lib.Precond()
+    _lib.load().within_default_preconditioner(C.byref(p))  # LocalSolverConfig::solver_default()
+    return p
+
+
+def _local_config(p: _lib.Precond, local) -> None:
+    if local is None:
+        return
+    if not isinstance(local, SchurComplement):
+        raise TypeError("local_solver must be SchurComplement or None")
+    ac = local.approx_chol or ApproxCholConfig()   # unwrap_or_default: seed 0, split_merge None
+    p.approx_chol_seed, p.approx_chol_split = ac.seed, ac.split
+    if local.approx_schur is None:
+        p.approx_schur_enabled = 0
+    else:
+        p.approx_schur_enabled, p.approx_schur_seed = 1, local.approx_schur.seed
+        p.approx_schur_split = local.approx_schur.split
+    p.dense_threshold = local.dense_threshold
+
+
+def _precond_struct(preconditioner):
+    """extract_preconditioner_config (within-py/src/lib.rs:542-594)."""
+    if isinstance(preconditioner, FePreconditioner):
+        return preconditioner._cfg
+    p = _default_local()
+    if preconditioner is None:
+        return p
+    if isinstance(preconditioner, Preconditioner):
+        if preconditioner == Preconditioner.Off:
+            p.kind = 0
+        elif preconditioner == Preconditioner.Multiplicative:
+            p.kind = 2
+        return p
+    if isinstance(preconditioner, AdditiveSchwarz):
+        _local_config(p, preconditioner.local_solver)
+        p.kind, p.reduction_strategy = 1, int(preconditioner.reduction)
+        return p
+    if isinstance(preconditioner, MultiplicativeSchwarz):
+        _local_config(p, preconditioner.local_solver)
+        p.kind = 2
+        return p
+    raise TypeError("preconditioner must be Preconditioner.Additive, Preconditioner.Multiplicative, "
+                    "Preconditioner.Off, AdditiveSchwarz(...), MultiplicativeSchwarz(...), or None")
+
+
+def _params_struct(config):
+    p = _lib.Params()
+    _lib.load().within_default_params(C.byref(p))
+    if config is None:
+        return p
+    if isinstance(config, CG):
+        p.krylov = 0
+    elif isinstance(config, GMRES):
+        p.krylov, p.gmres_restart = 1, config.restart
+    else:
+        raise TypeError("config must be CG, GMRES, or LSMR")
+    p.operator_repr, p.tol, p.maxiter = int(config.operator), config.tol, config.maxiter
+    p.max_refinements, p.precision = config.max_refinements, _PRECISIONS[config.precision]
+    return p
+
+
+def _validate(params, pre) -> None:
+    """validate_cg_preconditioner (within-py/src/lib.rs:639-656)."""
+    if params.krylov == 0 and pre.kind == 2:
+        raise ValueError("CG requires a symmetric preconditioner; use 'additive' or switch to GMRES")
+
+
+def _categories(categories) -> np.ndarray:
+    cats = np.asarray(categories)
+    if cats.ndim != 2:
+        raise ValueError("categories must be a 2-D array of shape (n_obs, n_factors)")
+    if cats.dtype != np.uint32:
+        raise TypeError("categories must have dtype uint32")
+    if cats.strides[0] != cats.itemsize and cats.shape[0] > 1 and cats.shape[1] > 1:
+        warnings.warn("categories array is not F-contiguous (column-major). "
+                      "Use np.asfortranarray(categories) for faster solves.", UserWarning, stacklevel=3)
+    return cats
+
+
+def _check(rc: int) -> None:
+    if rc != _lib.WITHIN_OK:
+        raise WithinError(rc, _lib.last_error())
+
+
+class SolveResult:
+    """Single-RHS result (orchestrate.rs:37-54; within-py SolveResult)."""
+
+    def __init__(self, x, demeaned, converged, iterations, residual, time_total, time_setup, time_solve):
+        self.x, self.demeaned, self.converged = x, demeaned, bool(converged)
+        self.iterations, self.residual = int(iterations), float(residual)
+        self.time_total, self.time_setup, self.time_solve = time_total, time_setup, time_solve
+
+    def __repr__(self):
+        return (f"SolveResult(converged={self.converged}, iterations={self.iterations}, "
+                f"residual={self.residual:.3e})")
+
+
+class BatchSolveResult:
+    """Batch result: x (n_dofs, k) and demeaned (n_obs, k) F-order (within-py lib.rs:690-714)."""
+
+    def __init__(self, x, demeaned, converged, iterations, residual, time_solve, time_total):
+        self.x, self.demeaned = x, demeaned
+        self.converged, self.iterations, self.residual = converged, iterations, residual
+        self.time_solve, self.time_total = time_solve, time_total
+
+    def __repr__(self):
+        return f"BatchSolveResult(n_rhs={len(self.converged)}, converged={self.converged})"
+
+
+class FePreconditioner:
+    """Handle of a built preconditioner (within-py PyFePreconditioner, lib.rs:825-914).
+
+    It records the configuration it was built with; passing it back to
+    ``Solver(..., preconditioner=p)`` rebuilds the same factors (the build is
+    deterministic for a given design and seed).
+    """
+
+    def __init__(self, solver: "Solver"):
+        self._solver = solver
+        self._cfg = solver._pre
+
+    def apply(self, x) -> np.ndarray:
+        return self._solver._apply("within_solver_apply_preconditioner", x)
+
+    @property
+    def nrows(self) -> int:
+        return self._solver.n_dofs
+
+    @property
+    def ncols(self) -> int:
+        return self._solver.n_dofs
+
+    @property
+    def n_subdomains(self) -> int:
+        return int(_lib.load().within_solver_n_subdomains(self._solver._h))
+
+    def __repr__(self):
+        kind = {1: "Additive", 2: "Multiplicative"}.get(self._cfg.kind, "Off")
+        return f"FePreconditioner({kind}, n_subdomains={self.n_subdomains})"
+
+
+class Solver:
+    """Persistent solver (Solver::new / solve / solve_batch, within/src/solver.rs:82-447)."""
+
+    def __init__(self, categories, config=None, weights=None, preconditioner=None):
+        t0 = time.perf_counter()
+        L = _lib.load()
+        cats = _categories(categories)
+        self._params = _params_struct(config)
+        self._pre = _precond_struct(preconditioner)
+        _validate(self._params, self._pre)
+        n, q = cats.shape
+        self._w = None
+        if weights is not None:
+            self._w = np.ascontiguousarray(weights, dtype=np.float64)
+            if self._w.ndim != 1 or self._w.shape[0] != n:
+                raise WithinError(3, f"weights has length {self._w.shape[0] if self._w.ndim else 0}, expected {n}")
+        isz = cats.itemsize
+        h = C.c_void_p()
+        pre = None if self._pre.kind == 0 else C.byref(self._pre)
+        rc = L.within_solver_new(cats.ctypes.data_as(C.c_void_p), n, q, cats.strides[0] // isz,
+                                 cats.strides[1] // isz, _lib.ptr(self._w), C.byref(self._params), pre, C.byref(h))
+        _check(rc)
+        self._h = h
+        self.n_obs, self.n_dofs, self.n_factors = n, int(L.within_solver_n_dofs(h)), q
+        self.time_setup = time.perf_counter() - t0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.load().within_solver_free(h)
+            self._h = None
+
+    def _y(self, y, ndim):
+        y = np.asarray(y, dtype=np.float64)
+        if y.ndim != ndim:
+            raise ValueError(f"expected a {ndim}-D array")
+        if y.shape[0] != self.n_obs:
+            raise WithinError(2, f"y has {y.shape[0]} observations, expected {self.n_obs}")
+        return y
+
+    def solve(self, y) -> SolveResult:
+        y = np.ascontiguousarray(self._y(y, 1))
+        x = np.empty(self.n_dofs)
+        d = np.empty(self.n_obs)
+        st = _lib.Stats()
+        _check(_lib.load().within_solver_solve(self._h, _lib.ptr(y), _lib.ptr(x), _lib.ptr(d), C.byref(st)))
+        return SolveResult(x, d, st.converged, st.iterations, st.final_residual, st.time_total,
+                           self.time_setup, st.time_solve)
+
+    def solve_batch(self, Y) -> BatchSolveResult:
+        Y = np.asfortranarray(self._y(Y, 2))
+        k = Y.shape[1]
+        x = np.empty((self.n_dofs, k), order="F")
+        d = np.empty((self.n_obs, k), order="F")
+        st = (_lib.Stats * max(k, 1))()
+        _check(_lib.load().within_solver_solve_batch(self._h, _lib.ptr(Y), k, _lib.ptr(x), _lib.ptr(d), st))
+        return BatchSolveResult(x, d, [bool(st[c].converged) for c in range(k)],
+                                [int(st[c].iterations) for c in range(k)],
+                                [float(st[c].final_residual) for c in range(k)],
+                                [float(st[c].time_solve) for c in range(k)], float(st[0].time_total) if k else 0.0)
+
+    def preconditioner(self) -> FePreconditioner | None:
+        return None if self._pre.kind == 0 else FePreconditioner(self)
+
+    # --- operator access (kernel-level parity checks) ---
+    def _apply(self, fn, v, out_rows=None):
+        v = np.asarray(v, dtype=np.float64)
+        one = v.ndim == 1
+        V = np.asfortranarray(v.reshape(v.shape[0], -1))
+        out_rows = out_rows or self.n_dofs
+        out = np.empty((out_rows, V.shape[1]), order="F")
+        _check(getattr(_lib.load(), fn)(self._h, _lib.ptr(V), V.shape[1], _lib.ptr(out)))
+        return out[:, 0] if one else out
+
+    def apply_gramian(self, x):
+        return self._apply("within_solver_apply_gramian", x)
+
+    def matvec_d(self, x):
+        return self._apply("within_solver_matvec_d", x, self.n_obs)
+
+    def rmatvec_wdt(self, r):
+        return self._apply("within_solver_rmatvec_wdt", r)
+
+    def factor_meta(self):
+        nl = np.zeros(self.n_factors, np.int64)
+        off = np.zeros(self.n_factors, np.int64)
+        _lib.load().within_solver_factor_meta(self._h, nl, off)
+        return nl, off
+
+    def subdomains(self):
+        """Setup structure in the oracle's format (pair, indices, weights, factors)."""
+        L = _lib.load()
+        out = []
+        for i in range(L.within_solver_n_subdomains(self._h)):
+            info = np.zeros(8, np.int64)
+            L.within_solver_subdomain_info(self._h, i, info)
+            q, r, nloc, nq, nr, eq, kind, nred = (int(v) for v in info)
+            g = np.zeros(nloc, np.uint32)
+            w = np.zeros(nloc)
+            L.within_solver_subdomain_indices(self._h, i, g, w)
+            d = dict(pair=(q, r), global_indices=g, pou=w, n_q=nq, n_r=nr, eliminate_q=bool(eq),
+                     reduced_kind="dense" if kind == 0 else "ac", n_reduced=nred)
+            if kind == 1:
+                sz = np.zeros(5, np.int64)
+                L.within_solver_ac_sizes(self._h, i, sz)
+                n, nlev, nnz, ncol, ncore = (int(v) for v in sz)
+                lp = np.zeros(nlev + 1, np.int32); cv = np.zeros(max(ncol, 1), np.int32)
+                cd = np.zeros(max(ncol, 1)); cp = np.zeros(ncol + 1, np.int32)
+                ci = np.zeros(max(nnz, 1), np.int32); cc = np.zeros(max(nnz, 1))
+                core = np.zeros(max(ncore, 1), np.int32); z = np.zeros(max(ncore * ncore, 1))
+                L.within_solver_ac_arrays(self._h, i, lp, cv, cd, cp, ci, cc, core, z)
+                d["ac"] = dict(n=n, level_ptr=lp, col_vertex=cv[:ncol], col_diag=cd[:ncol], col_ptr=cp,
+                               col_idx=ci[:nnz], col_coef=cc[:nnz], core_vertex=core[:ncore],
+                               core_z=z[:ncore * ncore].reshape(ncore, ncore))
+            out.append(d)
+        return out
+
+    @property
+    def gpu_launches(self) -> int:
+        return int(_lib.load().within_solver_gpu_launches(self._h))
+
+
+def solve(categories, y, config=None, weights=None, preconditioner=None) -> SolveResult:
+    """orchestrate::solve (within/src/orchestrate.rs:151-166)."""
+    t0 = time.perf_counter()
+    s = Solver(categories, config, weights, preconditioner)
+    r = s.solve(y)
+    r.time_setup = s.time_setup
+    r.time_total = time.perf_counter() - t0
+    return r
+
+
+def solve_batch(categories, Y, config=None, weights=None, preconditioner=None) -> BatchSolveResult:
+    """orchestrate::solve_batch (within/src/orchestrate.rs:172-184)."""
+    t0 = time.perf_counter()
+    s = Solver(categories, config, weights, preconditioner)
+    r = s.solve_batch(Y)
+    r.time_total = time.perf_counter() - t0
+    return r

@@ -1,0 +1,115 @@
+"""ctypes binding of libwithin_b200.so (the C ABI in include/within_b200.h).
+
+The shared library is built in-tree by ``within_b200.build``.  There is no CPU
+fallback: a missing library raises ImportError, a missing device makes every
+solver call fail with a CUDA error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwithin_b200.so")
+
+WITHIN_OK = 0
+ERR_NAMES = {
+    1: "EmptyObservations", 2: "ObservationCountMismatch", 3: "WeightCountMismatch", 4: "Overflow",
+    5: "SingularDiagonal", 6: "LocalSolverBuild", 7: "PreconditionerBuild", 8: "IterativeSolve",
+    9: "InvalidArgument", 10: "Cuda",
+}
+
+
+class Params(C.Structure):
+    _fields_ = [("krylov", C.c_int32), ("gmres_restart", C.c_int32), ("operator_repr", C.c_int32),
+                ("tol", C.c_double), ("maxiter", C.c_int32), ("max_refinements", C.c_int32),
+                ("precision", C.c_int32)]
+
+
+class Precond(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("approx_chol_seed", C.c_uint64), ("approx_chol_split", C.c_uint32),
+                ("approx_schur_enabled", C.c_int32), ("approx_schur_seed", C.c_uint64),
+                ("approx_schur_split", C.c_uint32), ("dense_threshold", C.c_int32),
+                ("reduction_strategy", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("final_residual", C.c_double),
+                ("time_total", C.c_double), ("time_setup", C.c_double), ("time_solve", C.c_double)]
+
+
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+
+# Every symbol declared in include/within_b200.h.
+EXPORTED = [
+    "within_default_params", "within_default_preconditioner", "within_solver_new", "within_solver_free",
+    "within_solver_n_dofs", "within_solver_n_obs", "within_solver_n_factors", "within_solver_solve",
+    "within_solver_solve_batch", "within_solver_solve_batch_device", "within_solve", "within_solve_batch",
+    "within_solver_apply_gramian", "within_solver_apply_preconditioner", "within_solver_matvec_d",
+    "within_solver_rmatvec_wdt", "within_solver_factor_meta", "within_solver_n_subdomains",
+    "within_solver_subdomain_info", "within_solver_subdomain_indices", "within_solver_ac_sizes",
+    "within_solver_ac_arrays", "within_solver_gpu_launches", "within_solver_setup_time", "within_last_error",
+]
+
+_lib = None
+
+
+def load():
+    """Load the library (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        try:
+            from . import build as _build
+            _build.build()
+        except Exception as e:  # pragma: no cover - build environment specific
+            raise ImportError(f"libwithin_b200.so is missing and could not be built: {e}") from e
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.within_default_params.argtypes = [C.POINTER(Params)]
+    L.within_default_preconditioner.argtypes = [C.POINTER(Precond)]
+    L.within_solver_new.argtypes = [vp, C.c_size_t, C.c_size_t, C.c_int64, C.c_int64, vp,
+                                    C.POINTER(Params), C.POINTER(Precond), C.POINTER(vp)]
+    L.within_solver_new.restype = C.c_int
+    L.within_solver_free.argtypes = [vp]
+    for f in ("within_solver_n_dofs", "within_solver_n_obs", "within_solver_n_factors"):
+        getattr(L, f).argtypes = [vp]
+        getattr(L, f).restype = C.c_size_t
+    L.within_solver_solve.argtypes = [vp, vp, vp, vp, C.POINTER(Stats)]
+    L.within_solver_solve_batch.argtypes = [vp, vp, C.c_size_t, vp, vp, C.POINTER(Stats)]
+    L.within_solver_solve_batch_device.argtypes = [vp, vp, C.c_size_t, vp, vp, C.POINTER(Stats), vp]
+    L.within_solve.argtypes = [vp, C.c_size_t, C.c_size_t, C.c_int64, C.c_int64, vp, vp,
+                               C.POINTER(Params), C.POINTER(Precond), vp, vp, C.POINTER(Stats)]
+    L.within_solve_batch.argtypes = [vp, C.c_size_t, C.c_size_t, C.c_int64, C.c_int64, vp, C.c_size_t, vp,
+                                     C.POINTER(Params), C.POINTER(Precond), vp, vp, C.POINTER(Stats)]
+    for f in ("within_solver_apply_gramian", "within_solver_apply_preconditioner", "within_solver_matvec_d",
+              "within_solver_rmatvec_wdt"):
+        getattr(L, f).argtypes = [vp, vp, C.c_size_t, vp]
+    L.within_solver_factor_meta.argtypes = [vp, _i64p, _i64p]
+    L.within_solver_n_subdomains.argtypes = [vp]
+    L.within_solver_n_subdomains.restype = C.c_int32
+    L.within_solver_subdomain_info.argtypes = [vp, C.c_int32, _i64p]
+    L.within_solver_subdomain_indices.argtypes = [vp, C.c_int32, _u32p, _f64p]
+    L.within_solver_ac_sizes.argtypes = [vp, C.c_int32, _i64p]
+    L.within_solver_ac_arrays.argtypes = [vp, C.c_int32, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p, _i32p, _f64p]
+    L.within_solver_gpu_launches.argtypes = [vp]
+    L.within_solver_gpu_launches.restype = C.c_int64
+    L.within_solver_setup_time.argtypes = [vp]
+    L.within_solver_setup_time.restype = C.c_double
+    L.within_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load().within_last_error().decode(errors="replace")
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)

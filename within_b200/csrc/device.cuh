@@ -1,0 +1,141 @@
+// Device-side containers and the flattened layout of a Schwarz stage.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace wb {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define WB_CUDA(call)                                                                           \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            throw ::wb::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " + \
+                                  __FILE__ + ":" + std::to_string(__LINE__));                   \
+    } while (0)
+
+// Owning device array.
+template <typename T>
+struct DArr {
+    T* p = nullptr;
+    size_t n = 0;
+    DArr() = default;
+    DArr(const DArr&) = delete;
+    DArr& operator=(const DArr&) = delete;
+    DArr(DArr&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DArr& operator=(DArr&& o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DArr() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        if (count == 0) return;
+        WB_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void upload(const std::vector<T>& h) {
+        release();
+        if (h.empty()) return;
+        alloc(h.size());
+        WB_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    template <typename S>
+    void upload_cast(const std::vector<S>& h) {
+        std::vector<T> t(h.begin(), h.end());
+        upload(t);
+    }
+};
+
+// Row-wise CSR over local slots with its balanced work chunks.
+template <typename T>
+struct CsrDev {
+    int64_t nrows = 0;
+    DArr<uint32_t> row_slot;
+    DArr<int64_t> ptr;
+    DArr<uint32_t> col;
+    DArr<T> val;
+    DArr<T> rscale;
+    DArr<CsrChunk> chunks;
+    int64_t nchunks = 0;
+};
+
+// Host form of a row-wise CSR over slots.
+struct CsrHost {
+    std::vector<uint32_t> row_slot;
+    std::vector<int64_t> ptr{0};
+    std::vector<uint32_t> col;
+    std::vector<double> val;
+    std::vector<double> rscale;
+    std::vector<CsrChunk> chunks;
+    int64_t nrows() const { return (int64_t)row_slot.size(); }
+};
+
+// One Schwarz stage: the local solves of a set of subdomains over their
+// concatenated slots (slots of subdomain s: q-block then r-block).
+struct StageHost {
+    int32_t nsub = 0;
+    int64_t nslots = 0;
+    std::vector<uint32_t> gidx, sub_of, keep_slots;
+    std::vector<double> spou, scale;
+    std::vector<int32_t> sub_nloc, sub_nkeep;
+    CsrHost keep, elim;
+    // dense reduced solves
+    std::vector<int64_t> dn_keep0, dn_loff;
+    std::vector<int32_t> dn_n;
+    std::vector<double> dn_L;
+    // approximate Cholesky level sweeps: rows of level l are chunks [lp[l], lp[l+1])
+    CsrHost fwd, bwd;
+    std::vector<int64_t> fwd_lp, bwd_lp;
+    // dense cores
+    std::vector<int32_t> core_of_block, row0_of_block, core_n;
+    std::vector<int64_t> core_slot_off, core_z_off;
+    std::vector<uint32_t> core_slot;
+    std::vector<double> core_z;
+    // additive prolongation gather: dof j <- slots gslot[gptr[j]..gptr[j+1])
+    std::vector<int64_t> gptr;
+    std::vector<uint32_t> gslot;
+};
+
+template <typename T>
+struct StageDev {
+    int32_t nsub = 0;
+    int64_t nslots = 0, nkeep = 0;
+    DArr<uint32_t> gidx, sub_of, keep_slots;
+    DArr<T> spou, scale;
+    DArr<int32_t> sub_nloc, sub_nkeep;
+    CsrDev<T> keep, elim, fwd, bwd;
+    std::vector<int64_t> fwd_lp, bwd_lp;  // host copies (launch ranges)
+    int32_t ndense = 0;
+    DArr<int64_t> dn_keep0, dn_loff;
+    DArr<int32_t> dn_n;
+    DArr<T> dn_L;
+    int32_t ncore_blocks = 0, core_rmax = 0;
+    int64_t core_total = 0;
+    DArr<int32_t> core_of_block, row0_of_block, core_n;
+    DArr<int64_t> core_slot_off, core_z_off;
+    DArr<uint32_t> core_slot;
+    DArr<T> core_z;
+    DArr<int64_t> gptr;
+    DArr<uint32_t> gslot;
+};
+
+constexpr int kCoreRowsPerBlock = 32;
+
+}  // namespace wb

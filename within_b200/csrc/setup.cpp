@@ -1,0 +1,731 @@
+// Host-side setup of the solve phase (see setup.hpp).  Reference citations are
+// relative to the reference's crates/ directory.
+#include "setup.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <numeric>
+#include <thread>
+
+#include "../../include/within_b200.h"
+
+namespace wb {
+
+namespace {
+
+// splitmix64 (Steele, Lea & Flood 2014): random stream of the clique-tree sampler.
+struct SplitMix {
+    uint64_t s;
+    explicit SplitMix(uint64_t seed) : s(seed) {}
+    uint64_t next() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    }
+    double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }
+};
+uint64_t hash64(uint64_t x) { return SplitMix(x).next(); }
+
+Csr transpose(const Csr& a) {
+    // Stable counting scatter: rows of the result come out column-sorted
+    // (CsrBlock::transpose, operator/csr_block.rs:31-62).
+    Csr t;
+    t.nrows = a.ncols;
+    t.ncols = a.nrows;
+    const int64_t nnz = a.nnz();
+    t.ptr.assign((size_t)t.nrows + 1, 0);
+    t.idx.resize((size_t)nnz);
+    t.val.resize((size_t)nnz);
+    for (int64_t e = 0; e < nnz; ++e) t.ptr[a.idx[e] + 1]++;
+    for (int32_t i = 0; i < t.nrows; ++i) t.ptr[i + 1] += t.ptr[i];
+    std::vector<uint32_t> cursor(t.ptr.begin(), t.ptr.end() - 1);
+    for (int32_t r = 0; r < a.nrows; ++r)
+        for (uint32_t e = a.ptr[r]; e < a.ptr[r + 1]; ++e) {
+            const uint32_t pos = cursor[a.idx[e]]++;
+            t.idx[pos] = (uint32_t)r;
+            t.val[pos] = a.val[e];
+        }
+    return t;
+}
+
+// One factor pair's cross-tab over active levels (CrossTab::build_for_pair_with_active,
+// gramian/cross_tab.rs:246-265; bucket accumulation :568-664).  Returns false when a
+// factor of the pair has no active level.
+bool pair_crosstab(const Design& d, int q, int r, const std::vector<std::vector<uint8_t>>& active,
+                   CrossTab& out, std::vector<uint32_t>& l2g, int32_t& nq_out) {
+    const int64_t Lq = d.nlev[q], Lr = d.nlev[r];
+    std::vector<uint32_t> qmap((size_t)Lq, UINT32_MAX), rmap((size_t)Lr, UINT32_MAX);
+    int32_t nq = 0, nr = 0;
+    for (int64_t j = 0; j < Lq; ++j) if (active[q][j]) qmap[j] = (uint32_t)nq++;
+    for (int64_t k = 0; k < Lr; ++k) if (active[r][k]) rmap[k] = (uint32_t)nr++;
+    if (nq == 0 || nr == 0) return false;
+    l2g.clear();
+    l2g.reserve((size_t)nq + nr);
+    for (int64_t j = 0; j < Lq; ++j) if (active[q][j]) l2g.push_back((uint32_t)(d.off[q] + j));
+    for (int64_t k = 0; k < Lr; ++k) if (active[r][k]) l2g.push_back((uint32_t)(d.off[r] + k));
+
+    const uint32_t* cq = d.codes.data() + (size_t)q * d.n;
+    const uint32_t* cr = d.codes.data() + (size_t)r * d.n;
+    std::vector<double> dq((size_t)nq, 0.0), dr((size_t)nr, 0.0);
+    std::vector<uint32_t> bptr((size_t)nq + 1, 0);
+    for (int64_t i = 0; i < d.n; ++i) {
+        const uint32_t j = qmap[cq[i]], k = rmap[cr[i]];
+        const double w = d.weight(i);
+        dq[j] += w;
+        dr[k] += w;
+        bptr[j + 1]++;
+    }
+    for (int32_t j = 0; j < nq; ++j) bptr[j + 1] += bptr[j];
+    std::vector<uint32_t> bcol(bptr[nq]);
+    std::vector<double> bval(bptr[nq]);
+    {
+        std::vector<uint32_t> cur(bptr.begin(), bptr.end() - 1);
+        for (int64_t i = 0; i < d.n; ++i) {
+            const uint32_t j = qmap[cq[i]];
+            const uint32_t pos = cur[j]++;
+            bcol[pos] = rmap[cr[i]];
+            bval[pos] = d.weight(i);
+        }
+    }
+    Csr c;
+    c.nrows = nq;
+    c.ncols = nr;
+    c.ptr.assign((size_t)nq + 1, 0);
+    c.idx.reserve(bcol.size());
+    c.val.reserve(bcol.size());
+    std::vector<double> work((size_t)nr, 0.0);
+    std::vector<uint8_t> seen((size_t)nr, 0);
+    std::vector<uint32_t> touched;
+    for (int32_t row = 0; row < nq; ++row) {
+        touched.clear();
+        for (uint32_t e = bptr[row]; e < bptr[row + 1]; ++e) {
+            const uint32_t col = bcol[e];
+            if (!seen[col]) { seen[col] = 1; touched.push_back(col); }
+            work[col] += bval[e];  // summed in observation order
+        }
+        std::sort(touched.begin(), touched.end());
+        for (uint32_t col : touched) {
+            if (work[col] != 0.0) { c.idx.push_back(col); c.val.push_back(work[col]); }
+            work[col] = 0.0;
+            seen[col] = 0;
+        }
+        c.ptr[row + 1] = (uint32_t)c.idx.size();
+    }
+    out.ct = transpose(c);
+    out.c = std::move(c);
+    out.dq = std::move(dq);
+    out.dr = std::move(dr);
+    nq_out = nq;
+    return true;
+}
+
+struct Component {
+    std::vector<int32_t> qi, ri;
+};
+
+// Connected components of the bipartite graph, in order of their smallest node
+// (q-nodes numbered before r-nodes); members sorted.  Union-find gives the same sets
+// and order as the reference's DFS (cross_tab.rs:381-444).
+std::vector<Component> components(const CrossTab& x) {
+    const int32_t nq = x.c.nrows, nr = x.c.ncols, n = nq + nr;
+    std::vector<int32_t> parent((size_t)n);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto find = [&](int32_t a) {
+        while (parent[a] != a) { parent[a] = parent[parent[a]]; a = parent[a]; }
+        return a;
+    };
+    for (int32_t i = 0; i < nq; ++i)
+        for (uint32_t e = x.c.ptr[i]; e < x.c.ptr[i + 1]; ++e) {
+            int32_t a = find(i), b = find(nq + (int32_t)x.c.idx[e]);
+            if (a != b) parent[std::max(a, b)] = std::min(a, b);  // root = smallest node
+        }
+    std::vector<int32_t> comp_of((size_t)n, -1);
+    std::vector<Component> comps;
+    for (int32_t v = 0; v < n; ++v) {
+        const int32_t root = find(v);
+        if (comp_of[root] < 0) { comp_of[root] = (int32_t)comps.size(); comps.emplace_back(); }
+        Component& c = comps[comp_of[root]];
+        if (v < nq) c.qi.push_back(v); else c.ri.push_back(v - nq);
+    }
+    return comps;
+}
+
+// extract_component (cross_tab.rs:450-501).
+CrossTab extract(const CrossTab& x, const Component& cp) {
+    std::vector<uint32_t> rre((size_t)x.c.ncols, UINT32_MAX);
+    for (size_t a = 0; a < cp.ri.size(); ++a) rre[cp.ri[a]] = (uint32_t)a;
+    CrossTab o;
+    o.dq.reserve(cp.qi.size());
+    o.dr.reserve(cp.ri.size());
+    for (int32_t i : cp.qi) o.dq.push_back(x.dq[i]);
+    for (int32_t i : cp.ri) o.dr.push_back(x.dr[i]);
+    Csr c;
+    c.nrows = (int32_t)cp.qi.size();
+    c.ncols = (int32_t)cp.ri.size();
+    c.ptr.assign((size_t)c.nrows + 1, 0);
+    for (int32_t a = 0; a < c.nrows; ++a) {
+        const int32_t old = cp.qi[a];
+        for (uint32_t e = x.c.ptr[old]; e < x.c.ptr[old + 1]; ++e) {
+            const uint32_t nc = rre[x.c.idx[e]];
+            if (nc != UINT32_MAX) { c.idx.push_back(nc); c.val.push_back(x.c.val[e]); }
+        }
+        c.ptr[a + 1] = (uint32_t)c.idx.size();
+    }
+    o.ct = transpose(c);
+    o.c = std::move(c);
+    return o;
+}
+
+// ---------------------------------------------------------------------------
+// Schur complements (operator/schur_complement.rs)
+// ---------------------------------------------------------------------------
+
+struct Elim {
+    bool elim_q;
+    int32_t n_keep, n_elim;
+    const std::vector<double>* diag_elim;
+    const std::vector<double>* diag_keep;
+    const Csr* k2e;  // keep rows -> elim columns
+    const Csr* e2k;  // elim rows -> keep columns
+};
+
+Status make_elim(const CrossTab& x, Elim& e, std::vector<double>& inv) {
+    const int32_t nq = x.c.nrows, nr = x.c.ncols;
+    e.elim_q = nq >= nr;
+    e.n_keep = e.elim_q ? nr : nq;
+    e.n_elim = e.elim_q ? nq : nr;
+    e.diag_elim = e.elim_q ? &x.dq : &x.dr;
+    e.diag_keep = e.elim_q ? &x.dr : &x.dq;
+    e.k2e = e.elim_q ? &x.ct : &x.c;
+    e.e2k = e.elim_q ? &x.c : &x.ct;
+    inv.resize((size_t)e.n_elim);
+    for (int32_t i = 0; i < e.n_elim; ++i) {
+        const double dd = (*e.diag_elim)[i];
+        if (!(dd > 0.0)) {
+            Status s;
+            s.code = WITHIN_ERR_SINGULAR_DIAGONAL;
+            s.msg = std::string("zero diagonal in ") + (e.elim_q ? "q (elim)" : "r (elim)") +
+                    " block at index " + std::to_string(i);
+            return s;
+        }
+        inv[i] = 1.0 / dd;
+    }
+    return {};
+}
+
+// Sparse symmetric matrix in CSR (only off-diagonal entries are used downstream).
+struct SymCsr {
+    int32_t n = 0;
+    std::vector<uint32_t> ptr, idx;
+    std::vector<double> val;
+};
+
+// Exact Schur complement by row workspace (SchurLaplacian::from_elimination, :394-412).
+SymCsr schur_exact(const Elim& e, const std::vector<double>& inv) {
+    SymCsr s;
+    s.n = e.n_keep;
+    s.ptr.assign((size_t)s.n + 1, 0);
+    std::vector<double> work((size_t)s.n, 0.0);
+    std::vector<uint8_t> in((size_t)s.n, 0);
+    std::vector<int32_t> touched;
+    for (int32_t i = 0; i < s.n; ++i) {
+        touched.clear();
+        work[i] = (*e.diag_keep)[i];
+        touched.push_back(i);
+        in[i] = 1;
+        for (uint32_t f = e.k2e->ptr[i]; f < e.k2e->ptr[i + 1]; ++f) {
+            const uint32_t k = e.k2e->idx[f];
+            const double scale = e.k2e->val[f] * inv[k];
+            for (uint32_t b = e.e2k->ptr[k]; b < e.e2k->ptr[k + 1]; ++b) {
+                const uint32_t j = e.e2k->idx[b];
+                if (!in[j]) { in[j] = 1; touched.push_back((int32_t)j); }
+                work[j] -= scale * e.e2k->val[b];
+            }
+        }
+        std::sort(touched.begin(), touched.end());
+        for (int32_t j : touched) {
+            if (work[j] != 0.0 || j == i) { s.idx.push_back((uint32_t)j); s.val.push_back(work[j]); }
+            work[j] = 0.0;
+            in[j] = 0;
+        }
+        s.ptr[i + 1] = (uint32_t)s.idx.size();
+    }
+    return s;
+}
+
+// Top-left (n_keep-1)^2 minor of the exact Schur complement (:490-527).
+std::vector<double> schur_anchored_minor(const Elim& e, const std::vector<double>& inv) {
+    const int32_t n = e.n_keep;
+    if (n <= 1) return {};
+    const int32_t m = n - 1;
+    std::vector<double> a((size_t)m * m, 0.0);
+    for (int32_t i = 0; i < m; ++i) a[(size_t)i * m + i] = (*e.diag_keep)[i];
+    for (int32_t i = 0; i < m; ++i)
+        for (uint32_t f = e.k2e->ptr[i]; f < e.k2e->ptr[i + 1]; ++f) {
+            const uint32_t k = e.k2e->idx[f];
+            const double scale = e.k2e->val[f] * inv[k];
+            for (uint32_t b = e.e2k->ptr[k]; b < e.e2k->ptr[k + 1]; ++b) {
+                const uint32_t j = e.e2k->idx[b];
+                if ((int32_t)j < m) a[(size_t)i * m + j] -= scale * e.e2k->val[b];
+            }
+        }
+    return a;
+}
+
+struct Edge {
+    uint32_t lo, hi;
+    double w;
+};
+struct Nbr {
+    uint32_t col;
+    double w;
+};
+
+// Sampled clique tree of one eliminated vertex (Gao, Kyng & Spielman,
+// arXiv:2303.00709).  Neighbours split into `split` copies of weight w/split are
+// ordered by (weight, column); copy i links to a later copy j drawn with
+// probability w_j / S_i (S_i = weight after i) with edge weight w_i S_i / d, so the
+// expected tree equals the clique with weights w_a w_b / d.  One uniform draw per
+// copy; links between copies of one neighbour are dropped (self-loops).
+class CliqueTreeSampler {
+public:
+    void sample(const Nbr* nb, int32_t deg, uint32_t split, double d, uint64_t seed,
+                std::vector<Edge>& out) {
+        if (split < 1) split = 1;
+        const int32_t m = deg * (int32_t)split;
+        v_.resize((size_t)m);
+        cum_.resize((size_t)m);
+        suf_.resize((size_t)m);
+        for (int32_t a = 0, p = 0; a < deg; ++a)
+            for (uint32_t s = 0; s < split; ++s, ++p) v_[p] = Nbr{nb[a].col, nb[a].w / (double)split};
+        std::sort(v_.begin(), v_.end(), [](const Nbr& x, const Nbr& y) {
+            if (x.w != y.w) return x.w < y.w;
+            return x.col < y.col;
+        });
+        double acc = 0.0;
+        for (int32_t a = 0; a < m; ++a) { acc += v_[a].w; cum_[a] = acc; }
+        acc = 0.0;
+        for (int32_t a = m - 1; a >= 0; --a) { suf_[a] = acc; acc += v_[a].w; }
+        SplitMix rng(seed);
+        for (int32_t i = 0; i + 1 < m; ++i) {
+            const double u = rng.uniform();
+            if (!(suf_[i] > 0.0)) continue;
+            const double target = cum_[i] + u * suf_[i];
+            // first j in (i, m-1] with cum[j] > target
+            const int32_t j = (int32_t)(std::upper_bound(cum_.begin() + i + 1, cum_.begin() + m - 1, target) -
+                                        cum_.begin());
+            if (v_[j].col == v_[i].col) continue;
+            const uint32_t a = v_[i].col, b = v_[j].col;
+            out.push_back(Edge{std::min(a, b), std::max(a, b), v_[i].w * suf_[i] / d});
+        }
+    }
+
+private:
+    std::vector<Nbr> v_;
+    std::vector<double> cum_, suf_;
+};
+
+// Stable sort by (lo, hi), then sum duplicates in emission order.
+void sort_merge_edges(std::vector<Edge>& e) {
+    std::stable_sort(e.begin(), e.end(), [](const Edge& a, const Edge& b) {
+        return a.lo != b.lo ? a.lo < b.lo : a.hi < b.hi;
+    });
+    size_t w = 0;
+    for (size_t a = 0; a < e.size(); ++a) {
+        if (w > 0 && e[w - 1].lo == e[a].lo && e[w - 1].hi == e[a].hi) e[w - 1].w += e[a].w;
+        else e[w++] = e[a];
+    }
+    e.resize(w);
+}
+
+// Approximate Schur complement: each eliminated star of degree > 1 emits a clique
+// tree with seed = seed + k (ApproxSchurComplement::compute, :697-711 and :128-139).
+SymCsr schur_approx(const Elim& e, uint64_t seed, uint32_t split) {
+    std::vector<Edge> edges;
+    CliqueTreeSampler sampler;
+    std::vector<Nbr> nb;
+    for (int32_t k = 0; k < e.n_elim; ++k) {
+        const uint32_t b = e.e2k->ptr[k], en = e.e2k->ptr[k + 1];
+        const int32_t deg = (int32_t)(en - b);
+        if (deg <= 1) continue;
+        nb.resize((size_t)deg);
+        for (int32_t a = 0; a < deg; ++a) nb[a] = Nbr{e.e2k->idx[b + a], e.e2k->val[b + a]};
+        sampler.sample(nb.data(), deg, split, (*e.diag_elim)[k], seed + (uint64_t)k, edges);
+    }
+    sort_merge_edges(edges);
+    // Laplacian CSR (build_laplacian_csr, :534-586); only off-diagonals are consumed.
+    SymCsr s;
+    s.n = e.n_keep;
+    std::vector<uint32_t> lc((size_t)s.n, 0), uc((size_t)s.n, 0);
+    std::vector<double> dg((size_t)s.n, 0.0);
+    for (const Edge& x : edges) { uc[x.lo]++; lc[x.hi]++; dg[x.lo] += x.w; dg[x.hi] += x.w; }
+    s.ptr.assign((size_t)s.n + 1, 0);
+    for (int32_t i = 0; i < s.n; ++i) s.ptr[i + 1] = s.ptr[i] + lc[i] + 1 + uc[i];
+    s.idx.resize(s.ptr[s.n]);
+    s.val.resize(s.ptr[s.n]);
+    std::vector<uint32_t> lcur((size_t)s.n), ucur((size_t)s.n);
+    for (int32_t i = 0; i < s.n; ++i) {
+        lcur[i] = s.ptr[i];
+        ucur[i] = s.ptr[i] + lc[i] + 1;
+        s.idx[s.ptr[i] + lc[i]] = (uint32_t)i;
+        s.val[s.ptr[i] + lc[i]] = dg[i];
+    }
+    for (const Edge& x : edges) {
+        uint32_t p = ucur[x.lo]++;
+        s.idx[p] = x.hi;
+        s.val[p] = -x.w;
+        p = lcur[x.hi]++;
+        s.idx[p] = x.lo;
+        s.val[p] = -x.w;
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// Approximate Cholesky in rounds of independent vertices
+// ---------------------------------------------------------------------------
+
+// Sort neighbour records by column (stable) and merge duplicates, dropping dead ones.
+void compact_adj(std::vector<Nbr>& l, const std::vector<uint8_t>& dead) {
+    size_t m = 0;
+    for (size_t a = 0; a < l.size(); ++a)
+        if (!dead[l[a].col]) l[m++] = l[a];
+    l.resize(m);
+    std::stable_sort(l.begin(), l.end(), [](const Nbr& a, const Nbr& b) { return a.col < b.col; });
+    size_t w = 0;
+    for (size_t a = 0; a < m; ++a) {
+        if (w > 0 && l[w - 1].col == l[a].col) l[w - 1].w += l[a].w;
+        else l[w++] = l[a];
+    }
+    l.resize(w);
+}
+
+bool dense_cholesky(std::vector<double>& a, int32_t m);
+
+// SPD inverse through the Cholesky factor: A = L L^T, A^-1 = L^-T L^-1.
+bool spd_inverse(std::vector<double>& a, int32_t m) {
+    if (!dense_cholesky(a, m)) return false;
+    for (int32_t j = 0; j < m; ++j) {  // L^-1 in place, column by column
+        a[(size_t)j * m + j] = 1.0 / a[(size_t)j * m + j];
+        for (int32_t i = j + 1; i < m; ++i) {
+            double s = 0.0;
+            for (int32_t k = j; k < i; ++k) s += a[(size_t)i * m + k] * a[(size_t)k * m + j];
+            a[(size_t)i * m + j] = -s / a[(size_t)i * m + i];
+        }
+    }
+    std::vector<double> z((size_t)m * m);
+    for (int32_t i = 0; i < m; ++i)
+        for (int32_t j = 0; j <= i; ++j) {
+            double s = 0.0;
+            for (int32_t k = i; k < m; ++k) s += a[(size_t)k * m + i] * a[(size_t)k * m + j];
+            z[(size_t)i * m + j] = s;
+            z[(size_t)j * m + i] = s;
+        }
+    a.swap(z);
+    return true;
+}
+
+// Dense core: live vertices ascending, exact Laplacian of the remaining graph, anchored
+// inverse per connected component (anchor = the component's largest vertex).
+void ac_core(AcFactor& f, std::vector<std::vector<Nbr>>& g, const std::vector<uint8_t>& dead) {
+    const int32_t n = f.n;
+    std::vector<int32_t> loc((size_t)n, -1);
+    int32_t r = 0;
+    for (int32_t v = 0; v < n; ++v) if (!dead[v]) { loc[v] = r++; f.core_vertex.push_back(v); }
+    f.ncore = r;
+    f.core_z.assign((size_t)r * r, 0.0);
+    if (r == 0) return;
+    std::vector<double> S((size_t)r * r, 0.0);
+    std::vector<int32_t> parent((size_t)r);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto find = [&](int32_t a) { while (parent[a] != a) a = parent[a]; return a; };
+    for (int32_t a = 0; a < r; ++a) {
+        std::vector<Nbr>& L = g[f.core_vertex[a]];
+        compact_adj(L, dead);
+        for (const Nbr& x : L) {
+            const int32_t c = loc[x.col];
+            S[(size_t)a * r + c] -= x.w;
+            S[(size_t)a * r + a] += x.w;
+            const int32_t ra = find(a), rc = find(c);
+            if (ra != rc) parent[std::max(ra, rc)] = std::min(ra, rc);
+        }
+    }
+    std::vector<int32_t> root((size_t)r);
+    for (int32_t a = 0; a < r; ++a) root[a] = find(a);
+    std::vector<uint8_t> done((size_t)r, 0);
+    std::vector<int32_t> mem;
+    for (int32_t a = 0; a < r; ++a) {
+        if (done[root[a]]) continue;
+        done[root[a]] = 1;
+        mem.clear();
+        for (int32_t b = a; b < r; ++b) if (root[b] == root[a]) mem.push_back(b);
+        const int32_t m = (int32_t)mem.size() - 1;  // last member anchors the component
+        if (m <= 0) continue;
+        std::vector<double> A((size_t)m * m);
+        for (int32_t i = 0; i < m; ++i)
+            for (int32_t j = 0; j < m; ++j) A[(size_t)i * m + j] = S[(size_t)mem[i] * r + mem[j]];
+        if (spd_inverse(A, m))
+            for (int32_t i = 0; i < m; ++i)
+                for (int32_t j = 0; j < m; ++j) f.core_z[(size_t)mem[i] * r + mem[j]] = A[(size_t)i * m + j];
+    }
+}
+
+AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
+    const int32_t n = s.n;
+    AcFactor f;
+    f.n = n;
+    std::vector<std::vector<Nbr>> g((size_t)n);
+    for (int32_t i = 0; i < n; ++i)
+        for (uint32_t e = s.ptr[i]; e < s.ptr[i + 1]; ++e)
+            if ((int32_t)s.idx[e] != i && s.val[e] < 0.0) g[i].push_back(Nbr{s.idx[e], -s.val[e]});
+    std::vector<uint8_t> dead((size_t)n, 0), blocked((size_t)n, 0);
+    struct Rank {
+        int32_t deg;
+        uint64_t h;
+        int32_t v;
+    };
+    std::vector<Rank> rank;
+    std::vector<int32_t> picked;
+    f.col_vertex.reserve((size_t)n);
+    f.col_diag.reserve((size_t)n);
+    f.col_ptr.reserve((size_t)n + 1);
+    CliqueTreeSampler sampler;
+    std::vector<Edge> fill;
+    int32_t remaining = n;
+    while (remaining > kAcCoreMax) {
+        rank.clear();
+        for (int32_t v = 0; v < n; ++v) {
+            if (dead[v]) continue;
+            compact_adj(g[v], dead);
+            rank.push_back(Rank{(int32_t)g[v].size(), hash64(seed ^ ((uint64_t)v * 0xD1B54A32D192ED03ULL)), v});
+        }
+        std::sort(rank.begin(), rank.end(), [](const Rank& a, const Rank& b) {
+            if (a.deg != b.deg) return a.deg < b.deg;
+            if (a.h != b.h) return a.h < b.h;
+            return a.v < b.v;
+        });
+        picked.clear();
+        for (const Rank& rk : rank) {
+            if (blocked[rk.v]) continue;
+            picked.push_back(rk.v);
+            blocked[rk.v] = 1;
+            for (const Nbr& x : g[rk.v]) blocked[x.col] = 1;
+        }
+        f.level_ptr.push_back((int32_t)f.col_vertex.size());
+        for (int32_t v : picked) {
+            const std::vector<Nbr>& L = g[v];
+            double d = 0.0;
+            for (const Nbr& x : L) d += x.w;
+            f.col_vertex.push_back(v);
+            f.col_diag.push_back(L.empty() ? 0.0 : d);
+            f.col_ptr.push_back((int32_t)f.col_idx.size());
+            for (const Nbr& x : L) {
+                f.col_idx.push_back((int32_t)x.col);
+                f.col_coef.push_back(x.w / d);
+            }
+            if (L.size() > 1) {
+                fill.clear();
+                sampler.sample(L.data(), (int32_t)L.size(), split, d, seed + (uint64_t)v, fill);
+                for (const Edge& e : fill) {
+                    g[e.lo].push_back(Nbr{e.hi, e.w});
+                    g[e.hi].push_back(Nbr{e.lo, e.w});
+                }
+            }
+        }
+        for (int32_t v : picked) { dead[v] = 1; std::vector<Nbr>().swap(g[v]); }
+        for (const Rank& rk : rank) blocked[rk.v] = 0;
+        remaining -= (int32_t)picked.size();
+        f.nlev++;
+    }
+    f.level_ptr.push_back((int32_t)f.col_vertex.size());
+    f.col_ptr.push_back((int32_t)f.col_idx.size());
+    f.ncol = (int32_t)f.col_vertex.size();
+    ac_core(f, g, dead);
+    return f;
+}
+
+// Lower Cholesky of an SPD row-major matrix; false when a pivot is not positive.
+bool dense_cholesky(std::vector<double>& a, int32_t m) {
+    for (int32_t j = 0; j < m; ++j) {
+        double s = a[(size_t)j * m + j];
+        for (int32_t k = 0; k < j; ++k) s -= a[(size_t)j * m + k] * a[(size_t)j * m + k];
+        if (!(s > 0.0)) return false;
+        const double ljj = std::sqrt(s);
+        a[(size_t)j * m + j] = ljj;
+        for (int32_t i = j + 1; i < m; ++i) {
+            double t = a[(size_t)i * m + j];
+            for (int32_t k = 0; k < j; ++k) t -= a[(size_t)i * m + k] * a[(size_t)j * m + k];
+            a[(size_t)i * m + j] = t / ljj;
+        }
+        for (int32_t i = 0; i < j; ++i) a[(size_t)i * m + j] = 0.0;
+    }
+    return true;
+}
+
+// build_reduced_schur_factor (operator/schwarz.rs:274-303).
+Status build_local_factor(Subdomain& sd, const PrecondConfig& cfg) {
+    Elim e;
+    Status st = make_elim(sd.ct, e, sd.inv_diag);
+    if (!st.ok()) return st;
+    sd.elim_q = e.elim_q;
+    if (cfg.dense_threshold > 0 && e.n_keep <= cfg.dense_threshold) {
+        std::vector<double> minor = schur_anchored_minor(e, sd.inv_diag);
+        if (e.n_keep <= 1 || dense_cholesky(minor, e.n_keep - 1)) {
+            sd.kind = 0;
+            sd.n_red = e.n_keep;
+            sd.L = std::move(minor);
+            return {};
+        }
+    }
+    SymCsr s = cfg.approx_schur ? schur_approx(e, cfg.schur_seed, cfg.schur_split) : schur_exact(e, sd.inv_diag);
+    sd.kind = 1;
+    sd.n_red = e.n_keep;
+    sd.ac = ac_factor(s, cfg.ac_seed, cfg.ac_split < 1 ? 1 : cfg.ac_split);
+    return {};
+}
+
+}  // namespace
+
+Status build_design(const uint32_t* codes, int64_t n, int Q, int64_t row_stride, int64_t col_stride,
+                    const double* weights, Design& d) {
+    Status st;
+    if (n <= 0) { st.code = WITHIN_ERR_EMPTY_OBSERVATIONS; st.msg = "no observations provided"; return st; }
+    if (Q <= 0) { st.code = WITHIN_ERR_INVALID_ARGUMENT; st.msg = "categories must have at least one factor column"; return st; }
+    if ((uint64_t)n > 0xFFFFFFFFull) { st.code = WITHIN_ERR_OVERFLOW; st.msg = "more than 2^32-1 observations"; return st; }
+    d.n = n;
+    d.Q = Q;
+    d.codes.resize((size_t)n * Q);
+    for (int q = 0; q < Q; ++q) {
+        uint32_t* dst = d.codes.data() + (size_t)q * n;
+        if (row_stride == 1) {
+            std::memcpy(dst, codes + q * col_stride, sizeof(uint32_t) * (size_t)n);
+        } else {
+            for (int64_t i = 0; i < n; ++i) dst[i] = codes[i * row_stride + q * col_stride];
+        }
+    }
+    if (weights) d.w.assign(weights, weights + n);
+    d.nlev.resize(Q);
+    d.off.resize(Q);
+    int64_t off = 0;
+    for (int q = 0; q < Q; ++q) {
+        const uint32_t* c = d.codes.data() + (size_t)q * n;
+        uint32_t mx = 0;
+        for (int64_t i = 0; i < n; ++i) mx = std::max(mx, c[i]);
+        d.nlev[q] = (int64_t)mx + 1;
+        d.off[q] = off;
+        off += d.nlev[q];
+    }
+    if ((uint64_t)off > 0xFFFFFFFFull) { st.code = WITHIN_ERR_OVERFLOW; st.msg = "more than 2^32-1 fixed-effect levels"; return st; }
+    d.ndofs = off;
+    return st;
+}
+
+Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<Subdomain>& subs) {
+    subs.clear();
+    std::vector<std::vector<uint8_t>> active((size_t)d.Q);
+    for (int q = 0; q < d.Q; ++q) {  // find_all_active_levels (cross_tab.rs:75-89)
+        active[q].assign((size_t)d.nlev[q], 0);
+        const uint32_t* c = d.codes.data() + (size_t)q * d.n;
+        for (int64_t i = 0; i < d.n; ++i) active[q][c[i]] = 1;
+    }
+    // Pairs (q < r) in lexicographic order (factor_pairs.rs:252-260); components in
+    // order; indices q-levels then r-levels (:244-250).
+    for (int q = 0; q < d.Q; ++q)
+        for (int r = q + 1; r < d.Q; ++r) {
+            CrossTab full;
+            std::vector<uint32_t> l2g;
+            int32_t nqf = 0;
+            if (!pair_crosstab(d, q, r, active, full, l2g, nqf)) continue;
+            std::vector<Component> comps = components(full);
+            for (size_t c = 0; c < comps.size(); ++c) {
+                Subdomain sd;
+                sd.q = q;
+                sd.r = r;
+                sd.gidx.reserve(comps[c].qi.size() + comps[c].ri.size());
+                for (int32_t i : comps[c].qi) sd.gidx.push_back(l2g[i]);
+                for (int32_t i : comps[c].ri) sd.gidx.push_back(l2g[nqf + i]);
+                sd.ct = comps.size() == 1 ? std::move(full) : extract(full, comps[c]);
+                subs.push_back(std::move(sd));
+            }
+        }
+    // Partition-of-unity weights (compute_partition_weights, factor_pairs.rs:272-304).
+    std::vector<uint32_t> count((size_t)d.ndofs, 0);
+    for (const Subdomain& sd : subs)
+        for (uint32_t g : sd.gidx) count[g]++;
+    for (Subdomain& sd : subs) {
+        bool unique = true;
+        for (uint32_t g : sd.gidx) if (count[g] > 1) { unique = false; break; }
+        if (!unique) {
+            sd.pou.resize(sd.gidx.size());
+            for (size_t a = 0; a < sd.gidx.size(); ++a) sd.pou[a] = 1.0 / std::sqrt((double)count[sd.gidx[a]]);
+        }
+    }
+    // Local factors: independent per subdomain; large ones on worker threads.
+    std::vector<Status> status(subs.size());
+    std::vector<std::future<void>> jobs;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    for (size_t i = 0; i < subs.size(); ++i) {
+        if (subs[i].n_local() > 4096 && jobs.size() + 1 < hw) {
+            jobs.push_back(std::async(std::launch::async, [&, i] { status[i] = build_local_factor(subs[i], cfg); }));
+        } else {
+            status[i] = build_local_factor(subs[i], cfg);
+        }
+    }
+    for (auto& j : jobs) j.get();
+    for (const Status& s : status)
+        if (!s.ok()) return s;
+    return {};
+}
+
+void build_explicit_gramian(const Design& d, std::vector<int64_t>& ptr, std::vector<uint32_t>& idx,
+                            std::vector<double>& val) {
+    // Gramian::build (gramian/explicit.rs:207): G = D'WD as symmetric CSR, columns
+    // ascending, each row = its diagonal plus every cross-pair entry.
+    const int64_t m = d.ndofs;
+    std::vector<double> diag((size_t)m, 0.0);
+    for (int q = 0; q < d.Q; ++q)
+        for (int64_t i = 0; i < d.n; ++i) diag[d.off[q] + d.level(i, q)] += d.weight(i);
+    std::vector<std::vector<std::pair<uint32_t, double>>> rows((size_t)m);
+    for (int q = 0; q < d.Q; ++q)
+        for (int r = q + 1; r < d.Q; ++r) {
+            const int64_t Lq = d.nlev[q];
+            std::vector<int64_t> bp((size_t)Lq + 1, 0);
+            for (int64_t i = 0; i < d.n; ++i) bp[d.level(i, q) + 1]++;
+            for (int64_t j = 0; j < Lq; ++j) bp[j + 1] += bp[j];
+            std::vector<int64_t> cur(bp.begin(), bp.end() - 1);
+            std::vector<std::pair<uint32_t, double>> b((size_t)d.n);
+            for (int64_t i = 0; i < d.n; ++i)
+                b[cur[d.level(i, q)]++] = {(uint32_t)(d.off[r] + d.level(i, r)), d.weight(i)};
+            for (int64_t j = 0; j < Lq; ++j) {
+                std::stable_sort(b.begin() + bp[j], b.begin() + bp[j + 1],
+                                 [](const auto& x, const auto& y) { return x.first < y.first; });
+                const uint32_t gq = (uint32_t)(d.off[q] + j);
+                for (int64_t e = bp[j]; e < bp[j + 1];) {
+                    const uint32_t col = b[e].first;
+                    double w = 0.0;
+                    while (e < bp[j + 1] && b[e].first == col) { w += b[e].second; ++e; }
+                    if (w == 0.0) continue;
+                    rows[gq].push_back({col, w});
+                    rows[col].push_back({gq, w});
+                }
+            }
+        }
+    ptr.assign((size_t)m + 1, 0);
+    for (int64_t i = 0; i < m; ++i) ptr[i + 1] = ptr[i] + (int64_t)rows[i].size() + 1;
+    idx.resize((size_t)ptr[m]);
+    val.resize((size_t)ptr[m]);
+    for (int64_t i = 0; i < m; ++i) {
+        rows[i].push_back({(uint32_t)i, diag[i]});
+        std::sort(rows[i].begin(), rows[i].end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+        for (size_t a = 0; a < rows[i].size(); ++a) {
+            idx[ptr[i] + a] = rows[i][a].first;
+            val[ptr[i] + a] = rows[i][a].second;
+        }
+        std::vector<std::pair<uint32_t, double>>().swap(rows[i]);
+    }
+}
+
+}  // namespace wb

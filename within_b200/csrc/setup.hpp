@@ -1,0 +1,103 @@
+// Host-side setup of the solve phase: design metadata, factor-pair subdomains,
+// Schur complements and approximate-Cholesky factors.  Integer outputs
+// (level counts, offsets, subdomain membership and order) follow the
+// reference exactly; the device layout is built from these in solver.cu.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace wb {
+
+struct Status {
+    int code = 0;  // WITHIN_OK or a WITHIN_ERR_* value
+    std::string msg;
+    bool ok() const { return code == 0; }
+};
+
+// WeightedDesign (within/src/domain.rs:97-155).
+struct Design {
+    int64_t n = 0;
+    int Q = 0;
+    std::vector<uint32_t> codes;  // factor-major: codes[q*n + i]
+    std::vector<double> w;        // empty = unit weights
+    std::vector<int64_t> nlev, off;
+    int64_t ndofs = 0;
+    uint32_t level(int64_t i, int q) const { return codes[(size_t)q * n + i]; }
+    double weight(int64_t i) const { return w.empty() ? 1.0 : w[i]; }
+};
+
+struct Csr {
+    int32_t nrows = 0, ncols = 0;
+    std::vector<uint32_t> ptr, idx;
+    std::vector<double> val;
+    int64_t nnz() const { return ptr.empty() ? 0 : (int64_t)ptr[nrows]; }
+};
+
+// Bipartite block [D_q C; C^T D_r] of one factor pair (gramian/cross_tab.rs:189-199).
+struct CrossTab {
+    Csr c, ct;
+    std::vector<double> dq, dr;
+};
+
+// Rounds of the approximate Cholesky factor stop once at most this many vertices remain.
+constexpr int32_t kAcCoreMax = 1024;
+
+// Approximate Cholesky factor L D L^T of a Schur-complement Laplacian, eliminated in
+// rounds of independent vertices.  Column c eliminates vertex col_vertex[c] with pivot
+// col_diag[c] (0 = anchor) and entries (col_idx, col_coef = w/d) for its live neighbours.
+// The last <= kAcCoreMax vertices form a dense core solved by its anchored inverse core_z.
+struct AcFactor {
+    int32_t n = 0, nlev = 0, ncol = 0, ncore = 0;
+    std::vector<int32_t> level_ptr, col_vertex, col_ptr, col_idx;
+    std::vector<double> col_diag, col_coef;
+    std::vector<int32_t> core_vertex;  // ascending
+    std::vector<double> core_z;        // ncore x ncore row-major
+};
+
+struct Subdomain {
+    int q = 0, r = 0;
+    std::vector<uint32_t> gidx;   // q-levels then r-levels (factor_pairs.rs:244-250)
+    std::vector<double> pou;      // empty = uniform weights
+    CrossTab ct;
+    bool elim_q = true;           // n_q >= n_r (schur_complement.rs:174)
+    std::vector<double> inv_diag; // 1 / D_elim
+    int kind = 0;                 // 0 dense anchored Cholesky, 1 approximate Cholesky
+    int32_t n_red = 0;            // reduced (kept) size
+    std::vector<double> L;        // dense: (n_red-1)^2 row-major lower factor
+    AcFactor ac;
+    int32_t n_q() const { return ct.c.nrows; }
+    int32_t n_r() const { return ct.c.ncols; }
+    int32_t n_local() const { return ct.c.nrows + ct.c.ncols; }
+};
+
+struct PrecondConfig {
+    int kind = 1;  // 0 off, 1 additive, 2 multiplicative
+    uint64_t ac_seed = 0;
+    uint32_t ac_split = 2;
+    bool approx_schur = true;
+    uint64_t schur_seed = 0;
+    uint32_t schur_split = 1;
+    int dense_threshold = 24;
+};
+
+struct Setup {
+    Design d;
+    std::vector<Subdomain> subs;
+    // Explicit symmetric Gramian CSR (multiplicative Schwarz residual updates only).
+    std::vector<int64_t> g_ptr;
+    std::vector<uint32_t> g_idx;
+    std::vector<double> g_val;
+};
+
+// Validates the inputs and builds the design (ArrayStore::new + from_store).
+Status build_design(const uint32_t* codes, int64_t n, int Q, int64_t row_stride, int64_t col_stride,
+                    const double* weights, Design& d);
+// Builds subdomains and their local factors (build_local_domains + build_additive).
+Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<Subdomain>& subs);
+// Explicit Gramian for the multiplicative residual updater.
+void build_explicit_gramian(const Design& d, std::vector<int64_t>& ptr, std::vector<uint32_t>& idx,
+                            std::vector<double>& val);
+
+}  // namespace wb

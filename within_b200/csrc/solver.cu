@@ -1,0 +1,1371 @@
+// Solver of the B200-native solve phase: device layout, Schwarz/Krylov drivers and
+// the C ABI declared in include/within_b200.h.  Reference citations are relative to
+// the reference's crates/ directory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <functional>
+#include <type_traits>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/within_b200.h"
+#include "device.cuh"
+#include "kernels.cuh"
+#include "setup.hpp"
+
+namespace wb {
+
+namespace {
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int pow2ceil(int k) {
+    int g = 1;
+    while (g < k) g <<= 1;
+    return g;
+}
+int group_width(int k) {  // 1, 4, 8, 16 or 32 lanes per row
+    int g = pow2ceil(k);
+    if (g == 2) g = 4;
+    return g;
+}
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Balanced chunks of a row-wise CSR: at most max_rows rows / max_nz entries each;
+// rows longer than max_nz are cut into pieces when allow_split.
+std::vector<CsrChunk> make_chunks(const std::vector<int64_t>& ptr, int64_t row_lo, int64_t row_hi,
+                                  int64_t max_nz, int64_t max_rows, bool allow_split) {
+    std::vector<CsrChunk> out;
+    int64_t r = row_lo;
+    while (r < row_hi) {
+        const int64_t len = ptr[r + 1] - ptr[r];
+        if (allow_split && len > max_nz) {
+            for (int64_t a = ptr[r]; a < ptr[r + 1]; a += max_nz)
+                out.push_back(CsrChunk{(uint32_t)r, (uint32_t)(r + 1), a, std::min(a + max_nz, ptr[r + 1])});
+            ++r;
+            continue;
+        }
+        int64_t r1 = r + 1;
+        while (r1 < row_hi && r1 - r < max_rows && ptr[r1 + 1] - ptr[r] <= max_nz &&
+               !(allow_split && ptr[r1 + 1] - ptr[r1] > max_nz))
+            ++r1;
+        out.push_back(CsrChunk{(uint32_t)r, (uint32_t)r1, ptr[r], ptr[r1]});
+        r = r1;
+    }
+    return out;
+}
+
+void csr_add_row(CsrHost& c, uint32_t slot, double rscale) {
+    c.row_slot.push_back(slot);
+    c.rscale.push_back(rscale);
+}
+void csr_end_row(CsrHost& c) { c.ptr.push_back((int64_t)c.col.size()); }
+
+// Flatten the subdomains `ids` into one stage (see StageHost).
+StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int32_t>& ids, int64_t ndofs,
+                      bool with_gather) {
+    StageHost st;
+    st.nsub = (int32_t)ids.size();
+    struct AcRows {
+        std::vector<std::vector<std::pair<uint32_t, std::vector<std::pair<uint32_t, double>>>>> fwd;  // per level
+        std::vector<std::vector<std::tuple<uint32_t, double, std::vector<std::pair<uint32_t, double>>>>> bwd;
+    } ac;
+    int64_t o = 0;
+    for (int32_t si = 0; si < st.nsub; ++si) {
+        const Subdomain& sd = subs[ids[si]];
+        const int32_t nq = sd.n_q(), nr = sd.n_r(), nl = nq + nr;
+        const int64_t keep0 = o + (sd.elim_q ? nq : 0), elim0 = o + (sd.elim_q ? 0 : nq);
+        const int32_t n_keep = sd.elim_q ? nr : nq, n_elim = sd.elim_q ? nq : nr;
+        st.sub_nloc.push_back(nl);
+        st.sub_nkeep.push_back(n_keep);
+        for (int32_t a = 0; a < nl; ++a) {
+            st.gidx.push_back(sd.gidx[a]);
+            st.sub_of.push_back((uint32_t)si);
+            const double pw = sd.pou.empty() ? 1.0 : sd.pou[a];
+            st.spou.push_back(a < nq ? pw : -pw);  // r-block sign flip (local_solver.rs:83-87, 362, 447)
+            st.scale.push_back(1.0);
+        }
+        for (int32_t e = 0; e < n_elim; ++e) st.scale[elim0 + e] = sd.inv_diag[e];
+        const Csr& k2e = sd.elim_q ? sd.ct.ct : sd.ct.c;
+        const Csr& e2k = sd.elim_q ? sd.ct.c : sd.ct.ct;
+        for (int32_t i = 0; i < n_keep; ++i) {  // reduced rhs rows (local_solver.rs:374-381, 410-417)
+            st.keep_slots.push_back((uint32_t)(keep0 + i));
+            csr_add_row(st.keep, (uint32_t)(keep0 + i), 1.0);
+            for (uint32_t e = k2e.ptr[i]; e < k2e.ptr[i + 1]; ++e) {
+                st.keep.col.push_back((uint32_t)(elim0 + k2e.idx[e]));
+                st.keep.val.push_back(k2e.val[e]);
+            }
+            csr_end_row(st.keep);
+        }
+        for (int32_t e = 0; e < n_elim; ++e) {  // back substitution rows (local_solver.rs:111-151)
+            csr_add_row(st.elim, (uint32_t)(elim0 + e), sd.inv_diag[e]);
+            for (uint32_t x = e2k.ptr[e]; x < e2k.ptr[e + 1]; ++x) {
+                st.elim.col.push_back((uint32_t)(keep0 + e2k.idx[x]));
+                st.elim.val.push_back(e2k.val[x]);
+            }
+            csr_end_row(st.elim);
+        }
+        if (sd.kind == 0) {
+            st.dn_keep0.push_back(keep0);
+            st.dn_n.push_back(sd.n_red);
+            st.dn_loff.push_back((int64_t)st.dn_L.size());
+            st.dn_L.insert(st.dn_L.end(), sd.L.begin(), sd.L.end());
+        } else {
+            const AcFactor& f = sd.ac;
+            if ((int32_t)ac.fwd.size() < f.nlev) { ac.fwd.resize(f.nlev); ac.bwd.resize(f.nlev); }
+            for (int32_t l = 0; l < f.nlev; ++l) {
+                std::vector<std::tuple<uint32_t, uint32_t, double>> trip;  // (target, source, coef)
+                for (int32_t c = f.level_ptr[l]; c < f.level_ptr[l + 1]; ++c) {
+                    const uint32_t v = (uint32_t)(keep0 + f.col_vertex[c]);
+                    std::vector<std::pair<uint32_t, double>> ent;
+                    for (int32_t e = f.col_ptr[c]; e < f.col_ptr[c + 1]; ++e) {
+                        const uint32_t u = (uint32_t)(keep0 + f.col_idx[e]);
+                        ent.push_back({u, f.col_coef[e]});
+                        trip.emplace_back(u, v, f.col_coef[e]);
+                    }
+                    const double d = f.col_diag[c];
+                    ac.bwd[l].emplace_back(v, d > 0.0 ? 1.0 / d : 0.0, std::move(ent));
+                }
+                std::stable_sort(trip.begin(), trip.end(), [](const auto& a, const auto& b) {
+                    return std::get<0>(a) != std::get<0>(b) ? std::get<0>(a) < std::get<0>(b)
+                                                              : std::get<1>(a) < std::get<1>(b);
+                });
+                for (size_t a = 0; a < trip.size();) {
+                    const uint32_t u = std::get<0>(trip[a]);
+                    std::vector<std::pair<uint32_t, double>> ent;
+                    while (a < trip.size() && std::get<0>(trip[a]) == u) {
+                        ent.push_back({std::get<1>(trip[a]), std::get<2>(trip[a])});
+                        ++a;
+                    }
+                    ac.fwd[l].push_back({u, std::move(ent)});
+                }
+            }
+            if (f.ncore > 0) {
+                const int32_t g = (int32_t)st.core_n.size();
+                st.core_n.push_back(f.ncore);
+                st.core_slot_off.push_back((int64_t)st.core_slot.size());
+                st.core_z_off.push_back((int64_t)st.core_z.size());
+                for (int32_t a = 0; a < f.ncore; ++a) st.core_slot.push_back((uint32_t)(keep0 + f.core_vertex[a]));
+                st.core_z.insert(st.core_z.end(), f.core_z.begin(), f.core_z.end());
+                for (int32_t r0 = 0; r0 < f.ncore; r0 += kCoreRowsPerBlock) {
+                    st.core_of_block.push_back(g);
+                    st.row0_of_block.push_back(r0);
+                }
+            }
+        }
+        o += nl;
+    }
+    st.nslots = o;
+    // level-major AC rows: fwd (targets, may split) and bwd (columns, never split)
+    st.fwd_lp.push_back(0);
+    st.bwd_lp.push_back(0);
+    for (size_t l = 0; l < ac.fwd.size(); ++l) {
+        const int64_t r0 = st.fwd.nrows();
+        for (auto& row : ac.fwd[l]) {
+            csr_add_row(st.fwd, row.first, 1.0);
+            for (auto& e : row.second) { st.fwd.col.push_back(e.first); st.fwd.val.push_back(e.second); }
+            csr_end_row(st.fwd);
+        }
+        auto fc = make_chunks(st.fwd.ptr, r0, st.fwd.nrows(), 256, 32, true);
+        st.fwd.chunks.insert(st.fwd.chunks.end(), fc.begin(), fc.end());
+        st.fwd_lp.push_back((int64_t)st.fwd.chunks.size());
+        const int64_t b0 = st.bwd.nrows();
+        for (auto& row : ac.bwd[l]) {
+            csr_add_row(st.bwd, std::get<0>(row), std::get<1>(row));
+            for (auto& e : std::get<2>(row)) { st.bwd.col.push_back(e.first); st.bwd.val.push_back(e.second); }
+            csr_end_row(st.bwd);
+        }
+        auto bc = make_chunks(st.bwd.ptr, b0, st.bwd.nrows(), 256, 32, false);
+        st.bwd.chunks.insert(st.bwd.chunks.end(), bc.begin(), bc.end());
+        st.bwd_lp.push_back((int64_t)st.bwd.chunks.size());
+    }
+    st.keep.chunks = make_chunks(st.keep.ptr, 0, st.keep.nrows(), 256, 32, true);
+    st.elim.chunks = make_chunks(st.elim.ptr, 0, st.elim.nrows(), 256, 32, true);
+    if (with_gather) {
+        st.gptr.assign((size_t)ndofs + 1, 0);
+        for (uint32_t g : st.gidx) st.gptr[g + 1]++;
+        for (int64_t j = 0; j < ndofs; ++j) st.gptr[j + 1] += st.gptr[j];
+        st.gslot.resize(st.gidx.size());
+        std::vector<int64_t> cur(st.gptr.begin(), st.gptr.end() - 1);
+        for (size_t l = 0; l < st.gidx.size(); ++l) st.gslot[cur[st.gidx[l]]++] = (uint32_t)l;
+    }
+    return st;
+}
+
+template <typename T>
+void upload_csr(CsrDev<T>& d, const CsrHost& h) {
+    d.nrows = h.nrows();
+    d.row_slot.upload(h.row_slot);
+    d.ptr.upload(h.ptr);
+    d.col.upload(h.col);
+    d.val.upload_cast(h.val);
+    d.rscale.upload_cast(h.rscale);
+    d.chunks.upload(h.chunks);
+    d.nchunks = (int64_t)h.chunks.size();
+}
+
+template <typename T>
+void upload_stage(StageDev<T>& d, const StageHost& h) {
+    d.nsub = h.nsub;
+    d.nslots = h.nslots;
+    d.nkeep = (int64_t)h.keep_slots.size();
+    d.gidx.upload(h.gidx);
+    d.sub_of.upload(h.sub_of);
+    d.keep_slots.upload(h.keep_slots);
+    d.spou.upload_cast(h.spou);
+    d.scale.upload_cast(h.scale);
+    d.sub_nloc.upload(h.sub_nloc);
+    d.sub_nkeep.upload(h.sub_nkeep);
+    upload_csr(d.keep, h.keep);
+    upload_csr(d.elim, h.elim);
+    upload_csr(d.fwd, h.fwd);
+    upload_csr(d.bwd, h.bwd);
+    d.fwd_lp = h.fwd_lp;
+    d.bwd_lp = h.bwd_lp;
+    d.ndense = (int32_t)h.dn_n.size();
+    d.dn_keep0.upload(h.dn_keep0);
+    d.dn_loff.upload(h.dn_loff);
+    d.dn_n.upload(h.dn_n);
+    d.dn_L.upload_cast(h.dn_L);
+    d.ncore_blocks = (int32_t)h.core_of_block.size();
+    d.core_rmax = h.core_n.empty() ? 0 : *std::max_element(h.core_n.begin(), h.core_n.end());
+    d.core_total = (int64_t)h.core_slot.size();
+    d.core_of_block.upload(h.core_of_block);
+    d.row0_of_block.upload(h.row0_of_block);
+    d.core_n.upload(h.core_n);
+    d.core_slot_off.upload(h.core_slot_off);
+    d.core_z_off.upload(h.core_z_off);
+    d.core_slot.upload(h.core_slot);
+    d.core_z.upload_cast(h.core_z);
+    d.gptr.upload(h.gptr);
+    d.gslot.upload(h.gslot);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Solver
+// ---------------------------------------------------------------------------
+
+struct Workspace {
+    int k = 0;
+    DArr<double> yi, e;          // n x k interleaved (primary-sorted)
+    DArr<double> b, x, r, gx;    // m x k FP64: rhs, solution, refinement residual, G x
+    DArr<double> cx, cr, dz, dp, dap;           // FP64 inner CG vectors
+    DArr<float> frhs, fx, fr, fz, fp, fap;      // FP32 inner CG vectors (mixed precision)
+    DArr<double> vloc;           // slots x k (FP64 local vectors)
+    DArr<float> floc;            // slots x k (FP32)
+    DArr<double> core_tmp;
+    DArr<float> fcore_tmp;
+    DArr<double> rwork;          // multiplicative residual
+    DArr<float> frwork;
+    DArr<double> msum;           // 3 x nsub x k
+    DArr<double> part;           // partial sums
+    // per-RHS Krylov state
+    DArr<double> st_bnorm, st_rz, st_rz0, st_alpha, st_beta, st_rnorm, st_tol;
+    DArr<int32_t> st_active, st_conv, st_iters, st_part;
+    DArr<int32_t> n_active;
+};
+
+struct SolverImpl {
+    std::mutex mu;
+    Design d;
+    PrecondConfig pc;
+    within_params params{};
+    std::vector<Subdomain> subs;
+    int primary = 0;
+    bool perm_identity = true;
+    cudaStream_t stream = nullptr;
+    int n_sm = 148;
+    // device design
+    DArr<uint32_t> codes, perm;
+    DArr<double> w64;
+    DArr<float> w32;
+    DArr<ObsChunk> chunks;
+    ObsParams obs{};
+    bool has_split = false;
+    // Schwarz stages
+    std::vector<StageHost> hstages;
+    std::vector<StageDev<double>> stages64;
+    std::vector<StageDev<float>> stages32;
+    int32_t max_nsub = 0;
+    int64_t max_slots = 0, max_core_total = 0;
+    // explicit Gramian (multiplicative)
+    DArr<int64_t> g_ptr;
+    DArr<uint32_t> g_idx;
+    DArr<double> g_val64;
+    DArr<float> g_val32;
+    Workspace ws;
+    int32_t* h_active = nullptr;  // pinned
+    double setup_time = 0.0;
+    int64_t gpu_launches = 0;
+
+    ~SolverImpl() {
+        if (h_active) cudaFreeHost(h_active);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    bool mixed() const { return params.precision == WITHIN_PRECISION_MIXED; }
+    int nblk(int64_t rows, int G) const {
+        const int64_t need = (rows * G + kBlock - 1) / kBlock;
+        return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)n_sm * 8));
+    }
+};
+
+namespace {
+
+// Observation chunks over primary-sorted observations (level-aligned; long levels split).
+std::vector<ObsChunk> make_obs_chunks(const std::vector<int64_t>& lvl_ptr, int64_t nlev, bool& has_split) {
+    constexpr int64_t kObsPerChunk = 256;
+    std::vector<ObsChunk> out;
+    has_split = false;
+    int64_t l = 0;
+    while (l < nlev) {
+        const int64_t len = lvl_ptr[l + 1] - lvl_ptr[l];
+        if (len > 2 * kObsPerChunk) {
+            for (int64_t a = lvl_ptr[l]; a < lvl_ptr[l + 1]; a += kObsPerChunk)
+                out.push_back(ObsChunk{(uint32_t)a, (uint32_t)std::min(a + kObsPerChunk, lvl_ptr[l + 1]),
+                                       (uint32_t)l, (uint32_t)(l + 1), 1u});
+            has_split = true;
+            ++l;
+            continue;
+        }
+        int64_t l1 = l + 1;
+        while (l1 < nlev && lvl_ptr[l1 + 1] - lvl_ptr[l] <= kObsPerChunk && lvl_ptr[l1 + 1] - lvl_ptr[l1] <= 2 * kObsPerChunk)
+            ++l1;
+        out.push_back(ObsChunk{(uint32_t)lvl_ptr[l], (uint32_t)lvl_ptr[l1], (uint32_t)l, (uint32_t)l1, 0u});
+        l = l1;
+    }
+    return out;
+}
+
+void upload_design(SolverImpl& S) {
+    const Design& d = S.d;
+    // primary = factor with the most levels; observations sorted by its level (stable)
+    S.primary = 0;
+    for (int q = 1; q < d.Q; ++q)
+        if (d.nlev[q] > d.nlev[S.primary]) S.primary = q;
+    const uint32_t* cp = d.codes.data() + (size_t)S.primary * d.n;
+    const int64_t np = d.nlev[S.primary];
+    std::vector<int64_t> lvl_ptr((size_t)np + 1, 0);
+    for (int64_t i = 0; i < d.n; ++i) lvl_ptr[cp[i] + 1]++;
+    for (int64_t l = 0; l < np; ++l) lvl_ptr[l + 1] += lvl_ptr[l];
+    std::vector<uint32_t> perm((size_t)d.n);
+    {
+        std::vector<int64_t> cur(lvl_ptr.begin(), lvl_ptr.end() - 1);
+        for (int64_t i = 0; i < d.n; ++i) perm[cur[cp[i]]++] = (uint32_t)i;
+    }
+    S.perm_identity = true;
+    for (int64_t i = 0; i < d.n; ++i)
+        if (perm[i] != (uint32_t)i) { S.perm_identity = false; break; }
+    std::vector<uint32_t> codes((size_t)d.n * d.Q);
+    for (int q = 0; q < d.Q; ++q)
+        for (int64_t i = 0; i < d.n; ++i) codes[(size_t)q * d.n + i] = d.codes[(size_t)q * d.n + perm[i]];
+    S.codes.upload(codes);
+    if (!S.perm_identity) S.perm.upload(perm);
+    if (!d.w.empty()) {
+        std::vector<double> w((size_t)d.n);
+        for (int64_t i = 0; i < d.n; ++i) w[i] = d.w[perm[i]];
+        S.w64.upload(w);
+        if (S.mixed()) S.w32.upload_cast(w);
+    }
+    auto ch = make_obs_chunks(lvl_ptr, np, S.has_split);
+    S.chunks.upload(ch);
+    ObsParams& P = S.obs;
+    P.n = d.n;
+    P.Q = d.Q;
+    P.primary = S.primary;
+    P.codes = S.codes.p;
+    for (int q = 0; q < d.Q; ++q) P.off[q] = d.off[q];
+    P.chunks = S.chunks.p;
+    P.nchunks = (int64_t)ch.size();
+}
+
+// shared-memory factors for a given k: small non-primary factors within a budget
+void obs_params_for(SolverImpl& S, int k, size_t elem, ObsParams& P) {
+    P = S.obs;
+    P.k = k;
+    int32_t used = 0;
+    const int32_t budget = (int32_t)(32768 / elem);
+    for (int q = 0; q < S.d.Q; ++q) {
+        P.smem_base[q] = -1;
+        P.smem_len[q] = 0;
+        if (q == S.primary) continue;
+        const int64_t len = S.d.nlev[q] * k;
+        if (used + len <= budget) {
+            P.smem_base[q] = used;
+            P.smem_len[q] = (int32_t)len;
+            used += (int32_t)len;
+        }
+    }
+    P.smem_elems = used;
+}
+
+template <typename T, int MODE>
+void launch_obs(SolverImpl& S, int k, const T* w, const T* x, const T* yin, T* out, T* eout) {
+    ObsParams P;
+    obs_params_for(S, k, sizeof(T), P);
+    const int G = group_width(k);
+    if (MODE != OBS_DX && out) {
+        // zero the outputs accumulated atomically (every non-primary factor, split levels)
+        const size_t m = (size_t)S.d.ndofs;
+        if (S.has_split) {
+            WB_CUDA(cudaMemsetAsync(out, 0, m * k * sizeof(T), S.stream));
+        } else {
+            const size_t a = (size_t)S.d.off[S.primary] * k, b = (size_t)(S.d.off[S.primary] + S.d.nlev[S.primary]) * k;
+            if (a > 0) WB_CUDA(cudaMemsetAsync(out, 0, a * sizeof(T), S.stream));
+            if (m * k > b) WB_CUDA(cudaMemsetAsync(out + b, 0, (m * k - b) * sizeof(T), S.stream));
+        }
+    }
+    const size_t smem = (size_t)P.smem_elems * sizeof(T);
+    const int64_t groups = (int64_t)P.nchunks;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((groups * G + kBlock - 1) / kBlock, (int64_t)S.n_sm * 8));
+    auto go = [&](auto kern) {
+        if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, kBlock, smem, S.stream>>>(P, w, x, yin, out, eout);
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+    };
+#define WB_OBS_Q(GV)                                                            \
+    if (S.d.Q <= 4) go(obs_pass_kernel<T, GV, MODE, 4>);                      \
+    else go(obs_pass_kernel<T, GV, MODE, kMaxQ>);
+    switch (G) {
+        case 1: WB_OBS_Q(1) break;
+        case 4: WB_OBS_Q(4) break;
+        case 8: WB_OBS_Q(8) break;
+        case 16: WB_OBS_Q(16) break;
+        default: WB_OBS_Q(32) break;
+    }
+#undef WB_OBS_Q
+}
+
+#define WB_DISPATCH_G(G, ...)                         \
+    switch (G) {                                      \
+        case 1: { constexpr int GV = 1; __VA_ARGS__; } break;   \
+        case 4: { constexpr int GV = 4; __VA_ARGS__; } break;   \
+        case 8: { constexpr int GV = 8; __VA_ARGS__; } break;   \
+        case 16: { constexpr int GV = 16; __VA_ARGS__; } break; \
+        default: { constexpr int GV = 32; __VA_ARGS__; } break; \
+    }
+
+template <typename TA, typename TB>
+void launch_dot(SolverImpl& S, const TA* a, const TB* b, int64_t rows, int k, double* part, int& nb) {
+    const int G = group_width(k);
+    nb = S.nblk(rows, G);
+    WB_DISPATCH_G(G, dot_kernel<TA, TB, GV><<<nb, kBlock, 0, S.stream>>>(a, b, rows, k, part));
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches++;
+}
+
+template <typename T>
+Workspace& ws_for(SolverImpl& S, int k);
+
+template <typename T>
+T* loc_buf(SolverImpl& S);
+template <>
+double* loc_buf<double>(SolverImpl& S) { return S.ws.vloc.p; }
+template <>
+float* loc_buf<float>(SolverImpl& S) { return S.ws.floc.p; }
+template <typename T>
+T* core_buf(SolverImpl& S);
+template <>
+double* core_buf<double>(SolverImpl& S) { return S.ws.core_tmp.p; }
+template <>
+float* core_buf<float>(SolverImpl& S) { return S.ws.fcore_tmp.p; }
+template <typename T>
+std::vector<StageDev<T>>& stages(SolverImpl& S);
+template <>
+std::vector<StageDev<double>>& stages<double>(SolverImpl& S) { return S.stages64; }
+template <>
+std::vector<StageDev<float>>& stages<float>(SolverImpl& S) { return S.stages32; }
+template <typename T>
+const T* gram_val(SolverImpl& S);
+template <>
+const double* gram_val<double>(SolverImpl& S) { return S.g_val64.p; }
+template <>
+const float* gram_val<float>(SolverImpl& S) { return S.g_val32.p; }
+
+template <typename T, int EPI>
+void launch_csr(SolverImpl& S, CsrDev<T>& c, int64_t ch0, int64_t ch1, T* v, int k) {
+    const int64_t nch = ch1 - ch0;
+    if (nch <= 0) return;
+    const int G = group_width(k);
+    const int grid = S.nblk(nch, G);
+    WB_DISPATCH_G(G, csr_rows_kernel<T, GV, EPI><<<grid, kBlock, 0, S.stream>>>(
+                         c.chunks.p + ch0, nch, c.row_slot.p, c.ptr.p, c.col.p, c.val.p, c.rscale.p, v, k));
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches++;
+}
+
+// Local solves of one stage on the slots vector v (restricted input already in v):
+// everything between the restriction and the prolongation.
+template <typename T>
+void stage_local_solve(SolverImpl& S, StageDev<T>& st, T* v, int k, double* msum) {
+    const int G = group_width(k);
+    const int64_t L = st.nslots;
+    double* m0 = msum;
+    double* m1 = msum + (size_t)S.max_nsub * k;
+    double* m2 = msum + (size_t)2 * S.max_nsub * k;
+    WB_CUDA(cudaMemsetAsync(msum, 0, sizeof(double) * 3 * (size_t)S.max_nsub * k, S.stream));
+    const int64_t kSumChunk = 64;
+    auto slot_sum = [&](const uint32_t* list, int64_t cnt, double* out) {
+        const int64_t groups = (cnt + kSumChunk - 1) / kSumChunk;
+        const int grid = S.nblk(groups, G);
+        WB_DISPATCH_G(G, slot_sum_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(list, cnt, st.sub_of.p, v, k, out, kSumChunk));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+    };
+    auto center = [&](const uint32_t* list, int64_t cnt, const int32_t* sub_n, const double* ms, const T* scale) {
+        const int grid = S.nblk(cnt, G);
+        WB_DISPATCH_G(G, center_scale_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(list, cnt, st.sub_of.p, sub_n, ms, scale, v, k));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+    };
+    // subtract_mean over the subdomain, then scale eliminated slots by 1/D_elim (:366-370)
+    slot_sum(nullptr, L, m0);
+    center(nullptr, L, st.sub_nloc.p, m0, st.scale.p);
+    // reduced right-hand side: keep += C^T (scaled elim) (:374-381), then subtract_mean (:385)
+    launch_csr<T, EPI_ACC>(S, st.keep, 0, st.keep.nchunks, v, k);
+    slot_sum(st.keep_slots.p, st.nkeep, m1);
+    center(st.keep_slots.p, st.nkeep, st.sub_nkeep.p, m1, nullptr);
+    // reduced solves: dense anchored Cholesky and approximate Cholesky sweeps
+    if (st.ndense > 0) {
+        const int64_t warps = (int64_t)st.ndense * k;
+        const int grid = (int)((warps * 32 + kBlock - 1) / kBlock);
+        dense_solve_kernel<T><<<grid, kBlock, 0, S.stream>>>(st.ndense, st.dn_keep0.p, st.dn_n.p, st.dn_loff.p, st.dn_L.p, v, k);
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+    }
+    const int nlev = (int)st.fwd_lp.size() - 1;
+    for (int l = 0; l < nlev; ++l) launch_csr<T, EPI_ACC>(S, st.fwd, st.fwd_lp[l], st.fwd_lp[l + 1], v, k);
+    if (st.ncore_blocks > 0) {
+        T* tmp = core_buf<T>(S);
+        const int kc_max = std::max(1, std::min(k, (int)(200 * 1024 / ((size_t)st.core_rmax * sizeof(T)))));
+        for (int c0 = 0; c0 < k; c0 += kc_max) {
+            const int kc = std::min(kc_max, k - c0);
+            const size_t smem = (size_t)st.core_rmax * kc * sizeof(T);
+            auto go = [&](auto kern) {
+                if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                kern<<<st.ncore_blocks, kBlock, smem, S.stream>>>(st.core_of_block.p, st.row0_of_block.p, st.core_n.p,
+                                                                 st.core_slot_off.p, st.core_slot.p, st.core_z_off.p,
+                                                                 st.core_z.p, v, tmp, k, c0, kc, kCoreRowsPerBlock);
+                WB_CUDA(cudaGetLastError());
+                S.gpu_launches++;
+            };
+            if (kc <= 4) go(core_gemv_kernel<T, 4>);
+            else if (kc <= 8) go(core_gemv_kernel<T, 8>);
+            else if (kc <= 16) go(core_gemv_kernel<T, 16>);
+            else go(core_gemv_kernel<T, 32>);
+        }
+        const int grid = S.nblk(st.core_total * k, 1);
+        core_writeback_kernel<T><<<grid, kBlock, 0, S.stream>>>(st.core_total, st.core_slot.p, tmp, v, k);
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+    }
+    for (int l = nlev - 1; l >= 0; --l) launch_csr<T, EPI_PIVOT>(S, st.bwd, st.bwd_lp[l], st.bwd_lp[l + 1], v, k);
+    // back substitution of the eliminated block (:425-436), then subtract_mean (:446)
+    launch_csr<T, EPI_ACC_SCALED>(S, st.elim, 0, st.elim.nchunks, v, k);
+    slot_sum(nullptr, L, m2);
+}
+
+// z = M^{-1} r.  For additive Schwarz also returns partial sums of r.z in part (if non-null).
+template <typename T>
+void apply_precond(SolverImpl& S, const T* r, T* z, int k, double* part, int& nb_part) {
+    const int64_t m = S.d.ndofs;
+    const int G = group_width(k);
+    auto& sts = stages<T>(S);
+    T* v = loc_buf<T>(S);
+    double* msum = S.ws.msum.p;
+    nb_part = 0;
+    if (S.pc.kind == 0 || sts.empty()) {
+        if (S.pc.kind == 0) {
+            WB_CUDA(cudaMemcpyAsync(z, r, sizeof(T) * m * k, cudaMemcpyDeviceToDevice, S.stream));
+        } else {
+            WB_CUDA(cudaMemsetAsync(z, 0, sizeof(T) * m * k, S.stream));
+        }
+        if (part) launch_dot<T, T>(S, r, z, m, k, part, nb_part);
+        return;
+    }
+    if (S.pc.kind == 1) {
+        StageDev<T>& st = sts[0];
+        const int grid = S.nblk(st.nslots, G);
+        WB_DISPATCH_G(G, restrict_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(st.nslots, st.gidx.p, st.spou.p, r, v, k));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+        stage_local_solve<T>(S, st, v, k, msum);
+        nb_part = S.nblk(m, G);
+        double* m2 = msum + (size_t)2 * S.max_nsub * k;
+        WB_DISPATCH_G(G, prolong_gather_kernel<T, GV><<<nb_part, kBlock, 0, S.stream>>>(
+                             m, st.gptr.p, st.gslot.p, st.sub_of.p, st.sub_nloc.p, st.spou.p, m2, v, z, part ? r : nullptr, k, part));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+        if (!part) nb_part = 0;
+        return;
+    }
+    // multiplicative: sequential stages (one per factor pair), residual updated after each
+    T* rw = std::is_same<T, double>::value ? (T*)S.ws.rwork.p : (T*)S.ws.frwork.p;
+    WB_CUDA(cudaMemcpyAsync(rw, r, sizeof(T) * m * k, cudaMemcpyDeviceToDevice, S.stream));
+    WB_CUDA(cudaMemsetAsync(z, 0, sizeof(T) * m * k, S.stream));
+    for (auto& st : sts) {
+        const int grid = S.nblk(st.nslots, G);
+        WB_DISPATCH_G(G, restrict_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(st.nslots, st.gidx.p, st.spou.p, rw, v, k));
+        WB_CUDA(cudaGetLastError());
+        stage_local_solve<T>(S, st, v, k, msum);
+        double* m2 = msum + (size_t)2 * S.max_nsub * k;
+        WB_DISPATCH_G(G, mult_update_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(
+                             st.nslots, st.gidx.p, st.sub_of.p, st.sub_nloc.p, st.spou.p, m2, v, z, S.g_ptr.p,
+                             S.g_idx.p, gram_val<T>(S), rw, k));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches += 2;
+    }
+    if (part) launch_dot<T, T>(S, r, z, m, k, part, nb_part);
+}
+
+// ---------------------------------------------------------------------------
+// Krylov state kernels (one thread per RHS)
+// ---------------------------------------------------------------------------
+
+__device__ double sum_part(const double* part, int nb, int k, int c) {
+    double s = 0.0;
+    for (int b = 0; b < nb; ++b) s += part[(size_t)b * k + c];
+    return s;
+}
+
+struct KState {
+    double *bnorm, *rz, *rz0, *alpha, *beta, *rnorm, *tol;
+    int32_t *active, *conv, *iters, *part_of;
+    int32_t* n_active;
+};
+
+// The state kernels run as one warp (k <= 32 lanes); lanes >= k only join the count.
+__device__ void count_active(KState s, int k) {
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        int na = 0;
+        for (int j = 0; j < k; ++j) na += s.active[j];
+        *s.n_active = na;
+    }
+}
+
+// cg.rs:52-74: ||b||; zero RHS converge at iteration 0.
+__global__ void cg_init_kernel(KState s, const double* part_bb, int nb, int k) {
+    const int c = threadIdx.x;
+    if (c < k) {
+        const double bn = sqrt(sum_part(part_bb, nb, k, c));
+        s.bnorm[c] = bn;
+        s.iters[c] = 0;
+        s.alpha[c] = 0.0;
+        s.beta[c] = 0.0;
+        s.rnorm[c] = bn;
+        if (!s.part_of[c]) {
+            s.active[c] = 0;
+        } else if (bn < 2.220446049250313e-16) {
+            s.active[c] = 0;
+            s.conv[c] = 1;
+        } else {
+            s.active[c] = 1;
+            s.conv[c] = 0;
+        }
+    }
+}
+__global__ void cg_rz0_kernel(KState s, const double* part, int nb, int k) {
+    const int c = threadIdx.x;
+    if (c < k) {
+        const double rz = sum_part(part, nb, k, c);
+        s.rz[c] = rz;
+        s.rz0[c] = rz;
+    }
+    count_active(s, k);
+}
+// cg.rs:76-86
+__global__ void cg_alpha_kernel(KState s, const double* part, int nb, int k, int it) {
+    const int c = threadIdx.x;
+    if (c < k) {
+        s.alpha[c] = 0.0;
+        if (s.active[c]) {
+            const double pap = sum_part(part, nb, k, c);
+            s.iters[c] = it;
+            if (pap <= 0.0) {
+                s.active[c] = 0;
+                s.conv[c] = 0;
+            } else {
+                s.alpha[c] = s.rz[c] / pap;
+            }
+        }
+    }
+    count_active(s, k);
+}
+// cg.rs:94-103
+__global__ void cg_check_kernel(KState s, const double* part, int nb, int k) {
+    const int c = threadIdx.x;
+    if (c < k && s.active[c]) {
+        const double rn = sqrt(sum_part(part, nb, k, c));
+        s.rnorm[c] = rn;
+        if (rn / s.bnorm[c] <= s.tol[c]) { s.active[c] = 0; s.conv[c] = 1; }
+    }
+    count_active(s, k);
+}
+// cg.rs:105-125 (EPS^2 stagnation guard)
+__global__ void cg_beta_kernel(KState s, const double* part, int nb, int k) {
+    const int c = threadIdx.x;
+    if (c < k && s.active[c]) {
+        const double rzn = sum_part(part, nb, k, c);
+        const double eps = 2.220446049250313e-16;
+        const double thr = eps * eps * fmax(fabs(s.rz0[c]), 2.2250738585072014e-308);
+        if (fabs(rzn) < thr) {
+            s.active[c] = 0;
+            s.conv[c] = s.rnorm[c] / s.bnorm[c] <= s.tol[c];
+        } else {
+            s.beta[c] = rzn / s.rz[c];
+            s.rz[c] = rzn;
+        }
+    }
+    count_active(s, k);
+}
+__global__ void cg_final_kernel(KState s, int k, int maxiter) {
+    const int c = threadIdx.x;
+    if (c < k && s.active[c]) { s.active[c] = 0; s.conv[c] = 0; s.iters[c] = maxiter; }
+}
+
+template <typename TA, typename TB>
+__global__ void convert_kernel(const TA* __restrict__ a, TB* __restrict__ b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (TB)a[i];
+}
+// x64 += d (per RHS only where mask[c])
+template <typename TD>
+__global__ void masked_axpy_kernel(double* __restrict__ x, const TD* __restrict__ d, const int32_t* __restrict__ mask,
+                                   int64_t rows, int k) {
+    const int64_t n = rows * k;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (mask[i % k]) x[i] += (double)d[i];
+}
+__global__ void sub_kernel(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a[i] - b[i];
+}
+
+KState kstate(Workspace& w) {
+    return KState{w.st_bnorm.p, w.st_rz.p, w.st_rz0.p, w.st_alpha.p, w.st_beta.p, w.st_rnorm.p, w.st_tol.p,
+                  w.st_active.p, w.st_conv.p, w.st_iters.p, w.st_part.p, w.n_active.p};
+}
+
+void ensure_ws(SolverImpl& S, int k) {
+    Workspace& w = S.ws;
+    if (w.k >= k) return;
+    const size_t n = (size_t)S.d.n, m = (size_t)S.d.ndofs;
+    w.yi.alloc(n * k);
+    w.e.alloc(n * k);
+    w.b.alloc(m * k);
+    w.x.alloc(m * k);
+    w.r.alloc(m * k);
+    w.gx.alloc(m * k);
+    w.cx.alloc(m * k);
+    w.cr.alloc(m * k);
+    w.dz.alloc(m * k);
+    w.dp.alloc(m * k);
+    w.dap.alloc(m * k);
+    if (S.mixed()) {
+        w.frhs.alloc(m * k);
+        w.fr.alloc(m * k);
+        w.fx.alloc(m * k);
+        w.fz.alloc(m * k);
+        w.fp.alloc(m * k);
+        w.fap.alloc(m * k);
+        w.floc.alloc(std::max<size_t>(1, S.max_slots * k));
+        w.fcore_tmp.alloc(std::max<size_t>(1, S.max_core_total * k));
+        if (S.pc.kind == 2) w.frwork.alloc(m * k);
+    }
+    w.vloc.alloc(std::max<size_t>(1, S.max_slots * k));
+    w.core_tmp.alloc(std::max<size_t>(1, S.max_core_total * k));
+    if (S.pc.kind == 2) w.rwork.alloc(m * k);
+    w.msum.alloc(std::max<size_t>(1, 3 * (size_t)S.max_nsub * k));
+    w.part.alloc((size_t)S.n_sm * 8 * k + 64);
+    for (DArr<double>* a : {&w.st_bnorm, &w.st_rz, &w.st_rz0, &w.st_alpha, &w.st_beta, &w.st_rnorm, &w.st_tol}) a->alloc(32);
+    for (DArr<int32_t>* a : {&w.st_active, &w.st_conv, &w.st_iters, &w.st_part}) a->alloc(32);
+    w.n_active.alloc(1);
+    w.k = k;
+}
+
+// Preconditioned CG on all RHS marked in st_part (device), solution into x (zeroed here),
+// per-RHS relative tolerance st_tol (device).  Vectors of type T; inner products in FP64.
+template <typename T>
+void cg_device(SolverImpl& S, int k, const T* b, T* x, T* r, T* z, T* p, T* ap, int maxiter) {
+    Workspace& w = S.ws;
+    const int64_t m = S.d.ndofs;
+    const int G = group_width(k);
+    KState ks = kstate(w);
+    double* part = w.part.p;
+    int nb = 0;
+    WB_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * m * k, S.stream));
+    WB_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * m * k, cudaMemcpyDeviceToDevice, S.stream));
+    launch_dot<T, T>(S, b, b, m, k, part, nb);
+    cg_init_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k);
+    apply_precond<T>(S, r, z, k, part, nb);
+    cg_rz0_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k);
+    WB_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * m * k, cudaMemcpyDeviceToDevice, S.stream));
+    S.gpu_launches += 3;
+    const T* w_t = nullptr;
+    if (std::is_same<T, double>::value) w_t = (const T*)S.w64.p; else w_t = (const T*)S.w32.p;
+    cudaEvent_t ev;
+    WB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    auto enqueue_iter = [&](int it) {
+        launch_obs<T, OBS_GRAM>(S, k, w_t, p, nullptr, ap, nullptr);
+        launch_dot<T, T>(S, p, ap, m, k, part, nb);
+        cg_alpha_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k, it);
+        const int grid = S.nblk(m, G);
+        WB_DISPATCH_G(G, cg_xr_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(x, r, p, ap, w.st_alpha.p, m, k, part));
+        cg_check_kernel<<<1, 32, 0, S.stream>>>(ks, part, grid, k);
+        apply_precond<T>(S, r, z, k, part, nb);
+        cg_beta_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k);
+        WB_DISPATCH_G(G, cg_p_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(p, z, w.st_beta.p, w.st_active.p, m, k));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches += 5;
+        WB_CUDA(cudaMemcpyAsync(S.h_active, w.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaEventRecord(ev, S.stream));
+    };
+    // The host check of iteration `it` overlaps the device work of iteration it+1; an
+    // iteration enqueued after every RHS stopped changes nothing (alpha = 0, masked p).
+    WB_CUDA(cudaMemcpyAsync(S.h_active, w.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    if (*S.h_active > 0 && maxiter > 0) {
+        cudaEvent_t evb;
+        WB_CUDA(cudaEventCreateWithFlags(&evb, cudaEventDisableTiming));
+        enqueue_iter(1);  // records ev
+        int it = 1;
+        while (it < maxiter) {
+            std::swap(ev, evb);  // evb = event of iteration it
+            enqueue_iter(it + 1);  // records ev for iteration it+1
+            WB_CUDA(cudaEventSynchronize(evb));
+            ++it;
+            if (*S.h_active == 0) break;
+        }
+        WB_CUDA(cudaEventDestroy(evb));
+    }
+    WB_CUDA(cudaEventDestroy(ev));
+    cg_final_kernel<<<1, 32, 0, S.stream>>>(ks, k, maxiter);
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches++;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Solve drivers
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct BatchOut {
+    std::vector<int32_t> conv, iters;
+    std::vector<double> fres;
+};
+
+// Solve k <= 32 RHS with device inputs ycol (n x k RHS-major) into device outputs
+// x (n_dofs x k RHS-major) and dem (n x k RHS-major).  Solver::solve semantics
+// (solver.rs:209-238) batched over RHS, with the refinement residual b - G x.
+void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double* demcol, BatchOut& out) {
+    ensure_ws(S, k);
+    Workspace& w = S.ws;
+    const int64_t n = S.d.n, m = S.d.ndofs;
+    const uint32_t* perm = S.perm_identity ? nullptr : S.perm.p;
+    // y -> interleaved, primary-sorted
+    gather_interleave_kernel<double><<<(unsigned)((n + 31) / 32), 256, 0, S.stream>>>(ycol, n, k, perm, w.yi.p);
+    // b = D'W y (rmatvec_wdt, solver.rs:210-211)
+    launch_obs<double, OBS_RHS>(S, k, S.w64.p, nullptr, w.yi.p, w.b.p, nullptr);
+    int nb = 0;
+    launch_dot<double, double>(S, w.b.p, w.b.p, m, k, w.part.p, nb);
+    std::vector<double> hpart((size_t)nb * k);
+    WB_CUDA(cudaMemcpyAsync(hpart.data(), w.part.p, sizeof(double) * nb * k, cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    std::vector<double> rhs_norm(k), abs_tol(k);
+    for (int c = 0; c < k; ++c) {
+        double s = 0.0;
+        for (int b = 0; b < nb; ++b) s += hpart[(size_t)b * k + c];
+        rhs_norm[c] = std::max(std::sqrt(s), 1e-15);  // solver.rs:212
+        abs_tol[c] = S.params.tol * rhs_norm[c];
+    }
+    std::vector<int32_t> conv(k, 0), iters(k, 0), part_of(k, 1);
+    std::vector<double> tol(k, S.params.tol);
+    // One inner Krylov solve of G d = rhs on the RHS in `who` to relative tolerances tl;
+    // then x += d on those RHS.
+    auto run_inner = [&](const double* rhs, const std::vector<int32_t>& who, const std::vector<double>& tl,
+                         std::vector<int32_t>& cv, std::vector<int32_t>& it) {
+        WB_CUDA(cudaMemcpyAsync(w.st_part.p, who.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, S.stream));
+        WB_CUDA(cudaMemcpyAsync(w.st_tol.p, tl.data(), sizeof(double) * k, cudaMemcpyHostToDevice, S.stream));
+        WB_CUDA(cudaMemsetAsync(w.st_conv.p, 0, sizeof(int32_t) * 32, S.stream));
+        const int grid = S.nblk(m * k, 1);
+        if (!S.mixed()) {
+            cg_device<double>(S, k, rhs, w.cx.p, w.cr.p, w.dz.p, w.dp.p, w.dap.p, S.params.maxiter);
+            masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, k);
+        } else {
+            convert_kernel<double, float><<<grid, kBlock, 0, S.stream>>>(rhs, w.frhs.p, m * k);
+            cg_device<float>(S, k, w.frhs.p, w.fx.p, w.fr.p, w.fz.p, w.fp.p, w.fap.p, S.params.maxiter);
+            masked_axpy_kernel<float><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.fx.p, w.st_part.p, m, k);
+        }
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches += 2;
+        cv.assign(k, 0);
+        it.assign(k, 0);
+        WB_CUDA(cudaMemcpyAsync(cv.data(), w.st_conv.p, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaMemcpyAsync(it.data(), w.st_iters.p, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaStreamSynchronize(S.stream));
+    };
+    WB_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * m * k, S.stream));
+    std::vector<int32_t> cv, it;
+    // FP64: initial solve + max_refinements corrections (solver.rs:215-216, 296-333).
+    // Mixed: FP32 inner solves to >= 1e-5 relative inside an FP64 refinement loop of up to
+    // max_refinements + 4 corrections, stopping when ||b - G x|| <= tol ||b||.
+    const int n_corr = S.mixed() ? S.params.max_refinements + 4 : S.params.max_refinements;
+    if (!S.mixed()) {
+        run_inner(w.b.p, part_of, tol, cv, it);
+        conv = cv;
+        iters = it;
+    }
+    std::vector<int32_t> done(k, 0);
+    for (int ref = 0; ref <= n_corr; ++ref) {
+        if (!S.mixed() && ref == n_corr) break;
+        const bool first_mixed = S.mixed() && ref == 0;
+        const double* rhs = w.b.p;
+        if (!first_mixed) {  // r = b - G x in FP64
+            launch_obs<double, OBS_GRAM>(S, k, S.w64.p, w.x.p, nullptr, w.gx.p, nullptr);
+            const int grid = S.nblk(m * k, 1);
+            sub_kernel<<<grid, kBlock, 0, S.stream>>>(w.b.p, w.gx.p, w.r.p, m * k);
+            WB_CUDA(cudaGetLastError());
+            S.gpu_launches++;
+            rhs = w.r.p;
+        }
+        launch_dot<double, double>(S, rhs, rhs, m, k, w.part.p, nb);
+        WB_CUDA(cudaMemcpyAsync(hpart.data(), w.part.p, sizeof(double) * nb * k, cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaStreamSynchronize(S.stream));
+        std::vector<int32_t> who(k, 0);
+        std::vector<double> ctol(k, 1.0);
+        int nwho = 0;
+        for (int c = 0; c < k; ++c) {
+            if (done[c]) continue;
+            double s = 0.0;
+            for (int b = 0; b < nb; ++b) s += hpart[(size_t)b * k + c];
+            const double cn = std::sqrt(s);
+            if (cn <= abs_tol[c]) { done[c] = 1; continue; }
+            ctol[c] = std::min(abs_tol[c] / cn, 1.0);  // corr_tol (solver.rs:319-320)
+            if (S.mixed()) ctol[c] = std::max(ctol[c], 1e-5);
+            who[c] = 1;
+            ++nwho;
+        }
+        if (nwho == 0 || ref == n_corr) break;
+        run_inner(rhs, who, ctol, cv, it);
+        for (int c = 0; c < k; ++c)
+            if (who[c]) { iters[c] += it[c]; conv[c] = cv[c]; }
+    }
+    if (S.mixed()) {
+        // converged when the FP64 residual met the tolerance
+        for (int c = 0; c < k; ++c) conv[c] = done[c] ? 1 : 0;
+    }
+    // final demeaned e = y - D x and ||D'W e|| / ||b|| (solver.rs:222-227, 335-339)
+    launch_obs<double, OBS_RESID>(S, k, S.w64.p, w.x.p, w.yi.p, w.r.p, w.e.p);
+    launch_dot<double, double>(S, w.r.p, w.r.p, m, k, w.part.p, nb);
+    WB_CUDA(cudaMemcpyAsync(hpart.data(), w.part.p, sizeof(double) * nb * k, cudaMemcpyDeviceToHost, S.stream));
+    scatter_deinterleave_kernel<double><<<(unsigned)((n + 31) / 32), 256, 0, S.stream>>>(w.e.p, n, k, perm, demcol);
+    scatter_deinterleave_kernel<double><<<(unsigned)((m + 31) / 32), 256, 0, S.stream>>>(w.x.p, m, k, nullptr, xcol);
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches += 3;
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    out.conv = conv;
+    out.iters = iters;
+    out.fres.resize(k);
+    for (int c = 0; c < k; ++c) {
+        double s = 0.0;
+        for (int b = 0; b < nb; ++b) s += hpart[(size_t)b * k + c];
+        out.fres[c] = std::sqrt(s) / rhs_norm[c];
+    }
+}
+
+}  // namespace
+
+}  // namespace wb
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+using wb::SolverImpl;
+
+struct within_solver {
+    std::unique_ptr<SolverImpl> impl;
+};
+
+namespace {
+
+int guard(const std::function<int()>& f) {
+    try {
+        const int rc = f();
+        if (rc == WITHIN_OK) wb::g_last_error.clear();
+        return rc;
+    } catch (const wb::CudaError& e) {
+        return wb::fail(WITHIN_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return wb::fail(WITHIN_ERR_OVERFLOW, "out of host memory");
+    } catch (const std::exception& e) {
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, e.what());
+    }
+}
+
+int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t row_stride, int64_t col_stride,
+                 const double* weights, const within_params* params, const within_preconditioner* precond,
+                 std::unique_ptr<SolverImpl>& out) {
+    const double t0 = wb::now_s();
+    auto S = std::make_unique<SolverImpl>();
+    within_default_params(&S->params);
+    if (params) S->params = *params;
+    const within_params& p = S->params;
+    if (p.krylov != WITHIN_KRYLOV_CG && p.krylov != WITHIN_KRYLOV_GMRES)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "config must be CG or GMRES");
+    if (p.krylov == WITHIN_KRYLOV_GMRES)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "GMRES is not available on the device path yet");
+    if (precond && precond->kind == WITHIN_PRECOND_MULTIPLICATIVE && p.krylov == WITHIN_KRYLOV_CG)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT,
+                        "CG requires a symmetric preconditioner; use 'additive' or switch to GMRES");
+    if (p.precision != WITHIN_PRECISION_FP64 && p.precision != WITHIN_PRECISION_MIXED)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "precision must be FP64 or MIXED");
+    if (n_factors > (size_t)wb::kMaxQ) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "at most 16 factors are supported");
+    if (codes == nullptr && n_obs > 0) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "categories pointer is null");
+    wb::Status st = wb::build_design(codes, (int64_t)n_obs, (int)n_factors, row_stride, col_stride, weights, S->d);
+    if (!st.ok()) return wb::fail(st.code, st.msg);
+    S->pc.kind = precond ? precond->kind : 0;
+    if (precond) {
+        S->pc.ac_seed = precond->approx_chol_seed;
+        S->pc.ac_split = precond->approx_chol_split < 1 ? 1 : precond->approx_chol_split;
+        S->pc.approx_schur = precond->approx_schur_enabled != 0;
+        S->pc.schur_seed = precond->approx_schur_seed;
+        S->pc.schur_split = precond->approx_schur_split < 1 ? 1 : precond->approx_schur_split;
+        S->pc.dense_threshold = precond->dense_threshold;
+    }
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        return wb::fail(WITHIN_ERR_CUDA, "no CUDA device is available (the solve phase has no CPU path)");
+    if (S->pc.kind != 0) {
+        st = wb::build_subdomains(S->d, S->pc, S->subs);
+        if (!st.ok()) return wb::fail(st.code, st.msg);
+    }
+    int dev = 0;
+    WB_CUDA(cudaGetDevice(&dev));
+    WB_CUDA(cudaDeviceGetAttribute(&S->n_sm, cudaDevAttrMultiProcessorCount, dev));
+    WB_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    WB_CUDA(cudaMallocHost(&S->h_active, sizeof(int32_t)));
+    wb::upload_design(*S);
+    if (S->pc.kind != 0 && !S->subs.empty()) {
+        std::vector<std::vector<int32_t>> groups;
+        if (S->pc.kind == 1) {
+            groups.emplace_back(S->subs.size());
+            std::iota(groups[0].begin(), groups[0].end(), 0);
+        } else {
+            for (int32_t i = 0; i < (int32_t)S->subs.size(); ++i) {
+                if (groups.empty() || S->subs[groups.back()[0]].q != S->subs[i].q || S->subs[groups.back()[0]].r != S->subs[i].r)
+                    groups.emplace_back();
+                groups.back().push_back(i);
+            }
+        }
+        for (auto& g : groups) {
+            S->hstages.push_back(wb::build_stage(S->subs, g, S->d.ndofs, S->pc.kind == 1));
+            const wb::StageHost& h = S->hstages.back();
+            S->max_nsub = std::max(S->max_nsub, h.nsub);
+            S->max_slots = std::max(S->max_slots, h.nslots);
+            S->max_core_total = std::max(S->max_core_total, (int64_t)h.core_slot.size());
+            S->stages64.emplace_back();
+            wb::upload_stage(S->stages64.back(), h);
+            if (S->mixed()) {
+                S->stages32.emplace_back();
+                wb::upload_stage(S->stages32.back(), h);
+            }
+        }
+        if (S->pc.kind == 2) {
+            std::vector<int64_t> gp;
+            std::vector<uint32_t> gi;
+            std::vector<double> gv;
+            wb::build_explicit_gramian(S->d, gp, gi, gv);
+            S->g_ptr.upload(gp);
+            S->g_idx.upload(gi);
+            S->g_val64.upload(gv);
+            if (S->mixed()) S->g_val32.upload_cast(gv);
+        }
+        // host copies of the stages are only needed while uploading
+        std::vector<wb::StageHost>().swap(S->hstages);
+    }
+    WB_CUDA(cudaStreamSynchronize(S->stream));
+    S->setup_time = wb::now_s() - t0;
+    out = std::move(S);
+    return WITHIN_OK;
+}
+
+int solve_device(SolverImpl& S, const double* d_ys, size_t k, double* d_x, double* d_dem, within_solve_stats* stats) {
+    const int64_t n = S.d.n, m = S.d.ndofs;
+    for (size_t c0 = 0; c0 < k; c0 += 32) {
+        const int kc = (int)std::min<size_t>(32, k - c0);
+        const double t0 = wb::now_s();
+        wb::BatchOut bo;
+        wb::solve_chunk(S, d_ys + c0 * n, kc, d_x + c0 * m, d_dem + c0 * n, bo);
+        const double dt = wb::now_s() - t0;
+        if (stats)
+            for (int c = 0; c < kc; ++c) {
+                within_solve_stats& s = stats[c0 + c];
+                s.converged = bo.conv[c];
+                s.iterations = bo.iters[c];
+                s.final_residual = bo.fres[c];
+                s.time_solve = dt;
+                s.time_setup = 0.0;
+                s.time_total = dt;
+            }
+    }
+    return WITHIN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void within_default_params(within_params* p) {
+    p->krylov = WITHIN_KRYLOV_CG;
+    p->gmres_restart = 30;
+    p->operator_repr = WITHIN_OPERATOR_IMPLICIT;
+    p->tol = 1e-8;
+    p->maxiter = 1000;
+    p->max_refinements = 2;
+    p->precision = WITHIN_PRECISION_FP64;
+}
+
+void within_default_preconditioner(within_preconditioner* p) {
+    p->kind = WITHIN_PRECOND_ADDITIVE;
+    p->approx_chol_seed = 0;
+    p->approx_chol_split = 2;
+    p->approx_schur_enabled = 1;
+    p->approx_schur_seed = 0;
+    p->approx_schur_split = 1;
+    p->dense_threshold = 24;
+    p->reduction_strategy = 0;
+}
+
+int within_solver_new(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t row_stride, int64_t col_stride,
+                      const double* weights, const within_params* params, const within_preconditioner* precond,
+                      within_solver** out) {
+    if (!out) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "out pointer is null");
+    *out = nullptr;
+    return guard([&]() -> int {
+        std::unique_ptr<SolverImpl> S;
+        const int rc = build_solver(codes, n_obs, n_factors, row_stride, col_stride, weights, params,
+                                    (precond && precond->kind != WITHIN_PRECOND_OFF) ? precond : nullptr, S);
+        if (rc != WITHIN_OK) return rc;
+        *out = new within_solver{std::move(S)};
+        return WITHIN_OK;
+    });
+}
+
+void within_solver_free(within_solver* s) { delete s; }
+
+size_t within_solver_n_dofs(const within_solver* s) { return s ? (size_t)s->impl->d.ndofs : 0; }
+size_t within_solver_n_obs(const within_solver* s) { return s ? (size_t)s->impl->d.n : 0; }
+size_t within_solver_n_factors(const within_solver* s) { return s ? (size_t)s->impl->d.Q : 0; }
+
+int within_solver_solve_batch_device(within_solver* s, const double* d_ys, size_t k, double* d_x, double* d_dem,
+                                     within_solve_stats* stats, void* stream) {
+    if (!s) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "solver is null");
+    SolverImpl& S = *s->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    return guard([&]() -> int {
+        if (stream) {
+            cudaEvent_t ev;
+            WB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            WB_CUDA(cudaEventRecord(ev, (cudaStream_t)stream));
+            WB_CUDA(cudaStreamWaitEvent(S.stream, ev, 0));
+            WB_CUDA(cudaEventDestroy(ev));
+        }
+        const int rc = solve_device(S, d_ys, k, d_x, d_dem, stats);
+        if (stream) {
+            cudaEvent_t ev;
+            WB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            WB_CUDA(cudaEventRecord(ev, S.stream));
+            WB_CUDA(cudaStreamWaitEvent((cudaStream_t)stream, ev, 0));
+            WB_CUDA(cudaEventDestroy(ev));
+        }
+        return rc;
+    });
+}
+
+int within_solver_solve_batch(within_solver* s, const double* ys, size_t k, double* x, double* dem,
+                              within_solve_stats* stats) {
+    if (!s) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "solver is null");
+    SolverImpl& S = *s->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    return guard([&]() -> int {
+        const double t0 = wb::now_s();
+        if (k == 0) return WITHIN_OK;
+        if (!ys || !x || !dem) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "null buffer");
+        const size_t n = (size_t)S.d.n, m = (size_t)S.d.ndofs;
+        wb::DArr<double> dy, dx, dd;
+        dy.alloc(n * k);
+        dx.alloc(m * k);
+        dd.alloc(n * k);
+        WB_CUDA(cudaMemcpyAsync(dy.p, ys, sizeof(double) * n * k, cudaMemcpyHostToDevice, S.stream));
+        const int rc = solve_device(S, dy.p, k, dx.p, dd.p, stats);
+        if (rc != WITHIN_OK) return rc;
+        WB_CUDA(cudaMemcpyAsync(x, dx.p, sizeof(double) * m * k, cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaMemcpyAsync(dem, dd.p, sizeof(double) * n * k, cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaStreamSynchronize(S.stream));
+        if (stats) stats[0].time_total = wb::now_s() - t0;
+        return WITHIN_OK;
+    });
+}
+
+int within_solver_solve(within_solver* s, const double* y, double* x, double* dem, within_solve_stats* stats) {
+    return within_solver_solve_batch(s, y, 1, x, dem, stats);
+}
+
+int within_solve(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t row_stride, int64_t col_stride,
+                 const double* y, const double* weights, const within_params* params,
+                 const within_preconditioner* precond, double* x, double* dem, within_solve_stats* stats) {
+    return within_solve_batch(codes, n_obs, n_factors, row_stride, col_stride, y, 1, weights, params, precond, x, dem,
+                              stats);
+}
+
+int within_solve_batch(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t row_stride, int64_t col_stride,
+                       const double* ys, size_t k, const double* weights, const within_params* params,
+                       const within_preconditioner* precond, double* x, double* dem, within_solve_stats* stats) {
+    const double t0 = wb::now_s();
+    within_solver* s = nullptr;
+    int rc = within_solver_new(codes, n_obs, n_factors, row_stride, col_stride, weights, params, precond, &s);
+    if (rc != WITHIN_OK) return rc;
+    const double t_setup = wb::now_s() - t0;
+    rc = within_solver_solve_batch(s, ys, k, x, dem, stats);
+    within_solver_free(s);
+    if (rc == WITHIN_OK && stats)
+        for (size_t c = 0; c < k; ++c) {
+            stats[c].time_setup += t_setup;
+            stats[c].time_total = wb::now_s() - t0;
+        }
+    return rc;
+}
+
+// --- operator applies on host vectors (parity tests) ---
+
+static int apply_common(within_solver* s, const double* in, size_t k, double* out, int which) {
+    if (!s) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "solver is null");
+    SolverImpl& S = *s->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    return guard([&]() -> int {
+        if (k == 0) return WITHIN_OK;
+        if (k > 32) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "at most 32 vectors per call");
+        const int kk = (int)k;
+        wb::ensure_ws(S, kk);
+        const size_t n = (size_t)S.d.n, m = (size_t)S.d.ndofs;
+        const size_t nin = (which == 2 || which == 1 || which == 0) ? (which == 3 ? n : m) : n;
+        const size_t in_rows = (which == 3) ? n : m;
+        const size_t out_rows = (which == 2) ? n : m;
+        (void)nin;
+        wb::DArr<double> din, dout, iin, iout;
+        din.alloc(in_rows * k);
+        dout.alloc(out_rows * k);
+        iin.alloc(in_rows * k);
+        iout.alloc(out_rows * k);
+        WB_CUDA(cudaMemcpyAsync(din.p, in, sizeof(double) * in_rows * k, cudaMemcpyHostToDevice, S.stream));
+        const uint32_t* perm = S.perm_identity ? nullptr : S.perm.p;
+        // to interleaved (obs vectors primary-sorted)
+        wb::gather_interleave_kernel<double><<<(unsigned)((in_rows + 31) / 32), 256, 0, S.stream>>>(
+            din.p, (int64_t)in_rows, kk, which == 3 ? perm : nullptr, iin.p);
+        if (which == 0) {  // gramian
+            if (!S.mixed()) {
+                wb::launch_obs<double, wb::OBS_GRAM>(S, kk, S.w64.p, iin.p, nullptr, iout.p, nullptr);
+            } else {
+                wb::DArr<float> fi, fo;
+                fi.alloc(m * k);
+                fo.alloc(m * k);
+                wb::convert_kernel<double, float><<<S.nblk(m * k, 1), wb::kBlock, 0, S.stream>>>(iin.p, fi.p, m * k);
+                wb::launch_obs<float, wb::OBS_GRAM>(S, kk, S.w32.p, fi.p, nullptr, fo.p, nullptr);
+                wb::convert_kernel<float, double><<<S.nblk(m * k, 1), wb::kBlock, 0, S.stream>>>(fo.p, iout.p, m * k);
+                WB_CUDA(cudaStreamSynchronize(S.stream));
+            }
+        } else if (which == 1) {  // preconditioner
+            int nb = 0;
+            if (!S.mixed()) {
+                wb::apply_precond<double>(S, iin.p, iout.p, kk, nullptr, nb);
+            } else {
+                wb::DArr<float> fi, fo;
+                fi.alloc(m * k);
+                fo.alloc(m * k);
+                wb::convert_kernel<double, float><<<S.nblk(m * k, 1), wb::kBlock, 0, S.stream>>>(iin.p, fi.p, m * k);
+                wb::apply_precond<float>(S, fi.p, fo.p, kk, nullptr, nb);
+                wb::convert_kernel<float, double><<<S.nblk(m * k, 1), wb::kBlock, 0, S.stream>>>(fo.p, iout.p, m * k);
+                WB_CUDA(cudaStreamSynchronize(S.stream));
+            }
+        } else if (which == 2) {  // D x
+            wb::launch_obs<double, wb::OBS_DX>(S, kk, nullptr, iin.p, nullptr, nullptr, iout.p);
+        } else {  // D'W r
+            wb::launch_obs<double, wb::OBS_RHS>(S, kk, S.w64.p, nullptr, iin.p, iout.p, nullptr);
+        }
+        wb::scatter_deinterleave_kernel<double><<<(unsigned)((out_rows + 31) / 32), 256, 0, S.stream>>>(
+            iout.p, (int64_t)out_rows, kk, which == 2 ? perm : nullptr, dout.p);
+        WB_CUDA(cudaGetLastError());
+        WB_CUDA(cudaMemcpyAsync(out, dout.p, sizeof(double) * out_rows * k, cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaStreamSynchronize(S.stream));
+        return WITHIN_OK;
+    });
+}
+
+int within_solver_apply_gramian(within_solver* s, const double* x, size_t k, double* y) { return apply_common(s, x, k, y, 0); }
+int within_solver_apply_preconditioner(within_solver* s, const double* r, size_t k, double* z) { return apply_common(s, r, k, z, 1); }
+int within_solver_matvec_d(within_solver* s, const double* x, size_t k, double* y) { return apply_common(s, x, k, y, 2); }
+int within_solver_rmatvec_wdt(within_solver* s, const double* r, size_t k, double* x) { return apply_common(s, r, k, x, 3); }
+
+void within_solver_factor_meta(const within_solver* s, int64_t* n_levels, int64_t* offsets) {
+    const wb::Design& d = s->impl->d;
+    for (int q = 0; q < d.Q; ++q) { n_levels[q] = d.nlev[q]; offsets[q] = d.off[q]; }
+}
+int32_t within_solver_n_subdomains(const within_solver* s) { return (int32_t)s->impl->subs.size(); }
+void within_solver_subdomain_info(const within_solver* s, int32_t i, int64_t* info) {
+    const wb::Subdomain& sd = s->impl->subs[i];
+    info[0] = sd.q; info[1] = sd.r; info[2] = sd.n_local(); info[3] = sd.n_q(); info[4] = sd.n_r();
+    info[5] = sd.elim_q; info[6] = sd.kind; info[7] = sd.n_red;
+}
+void within_solver_subdomain_indices(const within_solver* s, int32_t i, uint32_t* gidx, double* pou) {
+    const wb::Subdomain& sd = s->impl->subs[i];
+    std::memcpy(gidx, sd.gidx.data(), sizeof(uint32_t) * sd.gidx.size());
+    for (size_t a = 0; a < sd.gidx.size(); ++a) pou[a] = sd.pou.empty() ? 1.0 : sd.pou[a];
+}
+void within_solver_ac_sizes(const within_solver* s, int32_t i, int64_t* sizes) {
+    const wb::Subdomain& sd = s->impl->subs[i];
+    for (int a = 0; a < 5; ++a) sizes[a] = 0;
+    if (sd.kind != 1) return;
+    sizes[0] = sd.ac.n; sizes[1] = sd.ac.nlev; sizes[2] = (int64_t)sd.ac.col_idx.size();
+    sizes[3] = sd.ac.ncol; sizes[4] = sd.ac.ncore;
+}
+void within_solver_ac_arrays(const within_solver* s, int32_t i, int32_t* level_ptr, int32_t* col_vertex,
+                             double* col_diag, int32_t* col_ptr, int32_t* col_idx, double* col_coef,
+                             int32_t* core_vertex, double* core_z) {
+    const wb::AcFactor& f = s->impl->subs[i].ac;
+    std::copy(f.level_ptr.begin(), f.level_ptr.end(), level_ptr);
+    std::copy(f.col_vertex.begin(), f.col_vertex.end(), col_vertex);
+    std::copy(f.col_diag.begin(), f.col_diag.end(), col_diag);
+    std::copy(f.col_ptr.begin(), f.col_ptr.end(), col_ptr);
+    std::copy(f.col_idx.begin(), f.col_idx.end(), col_idx);
+    std::copy(f.col_coef.begin(), f.col_coef.end(), col_coef);
+    std::copy(f.core_vertex.begin(), f.core_vertex.end(), core_vertex);
+    std::copy(f.core_z.begin(), f.core_z.end(), core_z);
+}
+
+const char* within_last_error(void) { return wb::g_last_error.c_str(); }
+
+int64_t within_solver_gpu_launches(const within_solver* s) { return s ? s->impl->gpu_launches : 0; }
+double within_solver_setup_time(const within_solver* s) { return s ? s->impl->setup_time : 0.0; }
+
+}  // extern "C"
