@@ -163,9 +163,16 @@ void within_solver_ac_arrays(const within_solver *solver, int32_t i, int32_t *le
                              int32_t *col_idx, double *col_coef, int32_t *core_vertex,
                              double *core_z);
 
-/* Number of kernels this solver has launched so far, and its setup wall time (s). */
+/* Number of kernels this solver has launched so far, and its setup wall time (s).
+ * Measurement hooks with no counterpart in the reference. */
 int64_t within_solver_gpu_launches(const within_solver *solver);
 double within_solver_setup_time(const within_solver *solver);
+/* Event timing of selected launches on the solver's stream (off by default; turning it
+ * on resets the totals).  which: 0 operator apply D'WD in FP64, 1 the same in FP32,
+ * 2 Schwarz apply in FP64, 3 the same in FP32. */
+void within_solver_set_profiling(within_solver *solver, int32_t on);
+void within_solver_kernel_time(const within_solver *solver, int32_t which, int64_t *launches,
+                               double *total_ms);
 
 /* Message of the last failed call on this host thread ("" when none). */
 const char *within_last_error(void);

@@ -132,8 +132,15 @@ def test_edge_cases():
     assert r.converged and r.iterations == 0 and not r.x.any()
     r = s.solve(np.full(3_000, 2.5))
     assert np.abs(r.demeaned).max() < 1e-8
-    r = wb.solve(cats, np.random.default_rng(0).standard_normal(3_000), wb.CG(maxiter=1, max_refinements=0))
-    assert not r.converged and np.all(np.isfinite(r.x))
+    # reference tests/test_edge_cases.py:161-180 (50 x 50 levels, tol 1e-15)
+    rng = np.random.default_rng(42)
+    hard = np.asfortranarray(np.column_stack([rng.integers(0, 50, 1000), rng.integers(0, 50, 1000)]).astype(np.uint32))
+    yh = rng.standard_normal(1000)
+    for it in (1, 2):
+        r = wb.solve(hard, yh, wb.CG(maxiter=it, tol=1e-15))
+        assert not r.converged and np.all(np.isfinite(r.x))
+    r = wb.solve(hard, yh, wb.CG(tol=1.0))
+    assert r.converged
     r = wb.solve(cats, np.random.default_rng(0).standard_normal(3_000), preconditioner=wb.Preconditioner.Off)
     assert r.converged
     # single observation / two observations (reference tests/test_edge_cases.py:244-262)

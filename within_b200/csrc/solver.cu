@@ -313,8 +313,51 @@ struct SolverImpl {
     int32_t* h_active = nullptr;  // pinned
     double setup_time = 0.0;
     int64_t gpu_launches = 0;
+    // Optional event timing of selected launches (0: FP64 operator, 1: FP32 operator,
+    // 2: Schwarz apply FP64, 3: Schwarz apply FP32).
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+    int64_t prof_count[4] = {0, 0, 0, 0};
+    double prof_ms[4] = {0, 0, 0, 0};
+    cudaEvent_t take_event() {
+        if (ev_pool.empty()) {
+            cudaEvent_t e;
+            WB_CUDA(cudaEventCreate(&e));
+            return e;
+        }
+        cudaEvent_t e = ev_pool.back();
+        ev_pool.pop_back();
+        return e;
+    }
+    void prof_begin(int which, cudaEvent_t& a) {
+        if (!profiling) return;
+        a = take_event();
+        WB_CUDA(cudaEventRecord(a, stream));
+        (void)which;
+    }
+    void prof_end(int which, cudaEvent_t a) {
+        if (!profiling) return;
+        cudaEvent_t b = take_event();
+        WB_CUDA(cudaEventRecord(b, stream));
+        ev_pending.push_back({which, {a, b}});
+    }
+    // after a stream synchronisation: fold finished intervals into the totals
+    void prof_harvest() {
+        for (auto& p : ev_pending) {
+            float ms = 0.f;
+            WB_CUDA(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+            prof_ms[p.first] += ms;
+            prof_count[p.first] += 1;
+            ev_pool.push_back(p.second.first);
+            ev_pool.push_back(p.second.second);
+        }
+        ev_pending.clear();
+    }
 
     ~SolverImpl() {
+        for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         if (h_active) cudaFreeHost(h_active);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -822,14 +865,21 @@ void cg_device(SolverImpl& S, int k, const T* b, T* x, T* r, T* z, T* p, T* ap, 
     if (std::is_same<T, double>::value) w_t = (const T*)S.w64.p; else w_t = (const T*)S.w32.p;
     cudaEvent_t ev;
     WB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    const int kind = std::is_same<T, double>::value ? 0 : 1;
     auto enqueue_iter = [&](int it) {
+        cudaEvent_t e0 = nullptr;
+        S.prof_begin(kind, e0);
         launch_obs<T, OBS_GRAM>(S, k, w_t, p, nullptr, ap, nullptr);
+        S.prof_end(kind, e0);
         launch_dot<T, T>(S, p, ap, m, k, part, nb);
         cg_alpha_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k, it);
         const int grid = S.nblk(m, G);
         WB_DISPATCH_G(G, cg_xr_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(x, r, p, ap, w.st_alpha.p, m, k, part));
         cg_check_kernel<<<1, 32, 0, S.stream>>>(ks, part, grid, k);
+        cudaEvent_t e1 = nullptr;
+        S.prof_begin(kind + 2, e1);
         apply_precond<T>(S, r, z, k, part, nb);
+        S.prof_end(kind + 2, e1);
         cg_beta_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k);
         WB_DISPATCH_G(G, cg_p_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(p, z, w.st_beta.p, w.st_active.p, m, k));
         WB_CUDA(cudaGetLastError());
@@ -941,7 +991,10 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
         const bool first_mixed = S.mixed() && ref == 0;
         const double* rhs = w.b.p;
         if (!first_mixed) {  // r = b - G x in FP64
+            cudaEvent_t e0 = nullptr;
+            S.prof_begin(0, e0);
             launch_obs<double, OBS_GRAM>(S, k, S.w64.p, w.x.p, nullptr, w.gx.p, nullptr);
+            S.prof_end(0, e0);
             const int grid = S.nblk(m * k, 1);
             sub_kernel<<<grid, kBlock, 0, S.stream>>>(w.b.p, w.gx.p, w.r.p, m * k);
             WB_CUDA(cudaGetLastError());
@@ -983,6 +1036,7 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
     WB_CUDA(cudaGetLastError());
     S.gpu_launches += 3;
     WB_CUDA(cudaStreamSynchronize(S.stream));
+    S.prof_harvest();
     out.conv = conv;
     out.iters = iters;
     out.fres.resize(k);
@@ -1366,6 +1420,20 @@ void within_solver_ac_arrays(const within_solver* s, int32_t i, int32_t* level_p
 const char* within_last_error(void) { return wb::g_last_error.c_str(); }
 
 int64_t within_solver_gpu_launches(const within_solver* s) { return s ? s->impl->gpu_launches : 0; }
+
+void within_solver_set_profiling(within_solver* s, int32_t on) {
+    if (!s) return;
+    std::lock_guard<std::mutex> lk(s->impl->mu);
+    s->impl->profiling = on != 0;
+    for (int a = 0; a < 4; ++a) { s->impl->prof_count[a] = 0; s->impl->prof_ms[a] = 0.0; }
+}
+void within_solver_kernel_time(const within_solver* s, int32_t which, int64_t* launches, double* total_ms) {
+    *launches = 0;
+    *total_ms = 0.0;
+    if (!s || which < 0 || which > 3) return;
+    *launches = s->impl->prof_count[which];
+    *total_ms = s->impl->prof_ms[which];
+}
 double within_solver_setup_time(const within_solver* s) { return s ? s->impl->setup_time : 0.0; }
 
 }  // extern "C"
