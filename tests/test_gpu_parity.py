@@ -168,3 +168,42 @@ def test_local_solver_variants(local):
     t = oracle.OracleSolver(cats, tol=1e-13).solve(y)
     assert r.converged
     assert rel(r.demeaned, t.demeaned) < 1e-7
+
+
+@pytest.mark.parametrize("pre", ["multiplicative", "additive"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gmres(pre, precision):
+    cats = synthetic.uniform_design(40_000, [400, 150, 12], seed=8)
+    w = np.random.default_rng(2).lognormal(0, 1, 40_000)
+    y = np.random.default_rng(3).standard_normal(40_000)
+    p = wb.MultiplicativeSchwarz() if pre == "multiplicative" else wb.AdditiveSchwarz()
+    r = wb.solve(cats, y, wb.GMRES(restart=30, precision=precision), weights=w, preconditioner=p)
+    o = oracle.OracleSolver(cats, w, krylov="gmres", preconditioner=pre).solve(y)
+    t = oracle.OracleSolver(cats, w, tol=1e-13).solve(y)
+    assert r.converged and o.converged and r.residual <= 1e-8
+    assert rel(r.demeaned, o.demeaned) < 1e-8
+    assert rel(r.demeaned, t.demeaned) < 1e-7
+    if precision == "fp64":
+        assert abs(r.iterations - o.iterations) <= 2
+
+
+def test_multiplicative_preconditioner_apply():
+    cats = synthetic.uniform_design(30_000, [300, 120, 10], seed=9)
+    g = wb.Solver(cats, wb.GMRES(), preconditioner=wb.MultiplicativeSchwarz())
+    o = oracle.OracleSolver(cats, krylov="gmres", preconditioner="multiplicative")
+    R = np.random.default_rng(1).standard_normal((g.n_dofs, 3))
+    Z = g.preconditioner().apply(R)
+    for c in range(3):
+        assert rel(Z[:, c], o.apply_precond(R[:, c])) < 1e-10
+
+
+def test_gmres_batch_and_edges():
+    cats = synthetic.uniform_design(20_000, [200, 100, 9], seed=10)
+    Y = np.random.default_rng(4).standard_normal((20_000, 5))
+    Y[:, 2] = 0.0
+    r = wb.solve_batch(cats, Y, wb.GMRES(restart=10))
+    assert all(r.converged) and r.iterations[2] == 0 and not r.x[:, 2].any()
+    one = wb.solve(cats, Y[:, 1], wb.GMRES(restart=10))
+    assert rel(one.demeaned, r.demeaned[:, 1]) < 1e-9
+    r1 = wb.solve(cats, Y[:, 0], wb.GMRES(restart=30, maxiter=1, tol=1e-15, max_refinements=0))
+    assert not r1.converged and r1.iterations == 1 and np.all(np.isfinite(r1.x))

@@ -49,13 +49,41 @@ struct ObsParams {
     int32_t smem_elems;
     const uint32_t* codes;  // Q x n, primary-sorted order
     int64_t off[kMaxQ];
-    int32_t smem_base[kMaxQ];  // >= 0: factor accumulated in shared memory at this offset
-    int32_t smem_len[kMaxQ];   // n_levels * k of a shared-memory factor
+    // Per non-primary factor, a block-local shared-memory region of smem_len[q] values at
+    // smem_base[q] (-1: none).  full[q]: the region holds every level (level*k + c);
+    // otherwise it holds the factor's hottest levels: hot_slot[q][level] >= 0 gives the
+    // slot, hot_level[q][slot] the level.  Other levels go to global atomics.
+    int32_t smem_base[kMaxQ];
+    int32_t smem_len[kMaxQ];
+    int32_t full[kMaxQ];
+    const int32_t* hot_slot[kMaxQ];
+    const uint32_t* hot_level[kMaxQ];
     const ObsChunk* chunks;
     int64_t nchunks;
 };
 
-// QT >= Q is the compile-time bound of the factor loops (2, 3, 4, 8 or 16).
+template <typename T>
+__device__ __forceinline__ void obs_flush(const ObsParams& P, T* sm, T* out, int q, uint32_t lvl, T a, int k, int c) {
+    if (a == T(0)) return;
+    if (P.smem_base[q] >= 0) {
+        if (P.full[q]) {
+            atomic_add(sm + P.smem_base[q] + (size_t)lvl * k + c, a);
+            return;
+        }
+        const int32_t h = __ldg(P.hot_slot[q] + lvl);
+        if (h >= 0) {
+            atomic_add(sm + P.smem_base[q] + (size_t)h * k + c, a);
+            return;
+        }
+    }
+    atomic_add(out + (size_t)(P.off[q] + lvl) * k + c, a);
+}
+
+// QT >= Q is the compile-time bound of the factor loops (4 or 16).
+// Each group walks a chunk of observations sorted by the primary factor: the primary
+// factor's sums close with a plain store when its level changes; every other factor
+// keeps a running sum while its level repeats (a worker's firm rarely changes) and
+// flushes it to shared memory (small factor or hot level) or a global atomic.
 template <typename T, int G, int MODE, int QT>
 __global__ void __launch_bounds__(kBlock) obs_pass_kernel(ObsParams P, const T* __restrict__ w,
                                                           const T* __restrict__ x, const T* __restrict__ yin,
@@ -82,6 +110,10 @@ __global__ void __launch_bounds__(kBlock) obs_pass_kernel(ObsParams P, const T* 
         const ObsChunk C = P.chunks[ch];
         uint32_t lvl = C.lvl_begin;
         T acc = T(0);
+        uint32_t run_l[QT];
+        T run_a[QT];
+#pragma unroll
+        for (int q = 0; q < QT; ++q) { run_l[q] = 0xffffffffu; run_a[q] = T(0); }
         for (uint32_t base = C.obs_begin; base < C.obs_end; base += G) {
             const uint32_t cnt = min((uint32_t)G, C.obs_end - base);
             // cooperative loads: lane j holds the codes and weight of observation base+j
@@ -125,20 +157,24 @@ __global__ void __launch_bounds__(kBlock) obs_pass_kernel(ObsParams P, const T* 
                         ++lvl;
                     }
                     acc += t;
-                    if (cval) {
 #pragma unroll
-                        for (int q = 0; q < QT; ++q) {
-                            if (q >= Q || q == pq) continue;
-                            if (P.smem_base[q] >= 0)
-                                atomic_add(sm + P.smem_base[q] + (size_t)lq[q] * k + c, t);
-                            else
-                                atomic_add(out + (size_t)(P.off[q] + lq[q]) * k + c, t);
+                    for (int q = 0; q < QT; ++q) {
+                        if (q >= Q || q == pq) continue;
+                        if (lq[q] == run_l[q]) {
+                            run_a[q] += t;
+                        } else {
+                            if (run_l[q] != 0xffffffffu && cval) obs_flush(P, sm, out, q, run_l[q], run_a[q], k, c);
+                            run_l[q] = lq[q];
+                            run_a[q] = t;
                         }
                     }
                 }
             }
         }
         if (kScatter && cval) {
+#pragma unroll
+            for (int q = 0; q < QT; ++q)
+                if (q < Q && q != pq && run_l[q] != 0xffffffffu) obs_flush(P, sm, out, q, run_l[q], run_a[q], k, c);
             if (C.split) {
                 atomic_add(out + (size_t)(P.off[pq] + C.lvl_begin) * k + c, acc);
             } else {
@@ -152,12 +188,15 @@ __global__ void __launch_bounds__(kBlock) obs_pass_kernel(ObsParams P, const T* 
     }
     if (kScatter && P.smem_elems > 0) {
         __syncthreads();
-        // the block's partial sums of each shared-memory factor, one atomic per entry
+        // the block's partial sums of each shared-memory region, one atomic per nonzero entry
         for (int q = 0; q < Q; ++q) {
             if (P.smem_base[q] < 0) continue;
             for (int idx = threadIdx.x; idx < P.smem_len[q]; idx += blockDim.x) {
                 const T v = sm[P.smem_base[q] + idx];
-                if (v != T(0)) atomic_add(out + (size_t)P.off[q] * k + idx, v);
+                if (v == T(0)) continue;
+                const int slot = idx / k, cc = idx % k;
+                const uint32_t lev = P.full[q] ? (uint32_t)slot : P.hot_level[q][slot];
+                atomic_add(out + (size_t)(P.off[q] + lev) * k + cc, v);
             }
         }
     }

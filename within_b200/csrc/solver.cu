@@ -297,6 +297,11 @@ struct SolverImpl {
     DArr<float> w32;
     DArr<ObsChunk> chunks;
     ObsParams obs{};
+    // hottest levels of every non-primary factor (by observation count), for the
+    // shared-memory accumulators of the observation pass
+    std::vector<DArr<int32_t>> hot_slot;
+    std::vector<DArr<uint32_t>> hot_level;
+    std::vector<int32_t> hot_count;
     bool has_split = false;
     // Schwarz stages
     std::vector<StageHost> hstages;
@@ -310,6 +315,7 @@ struct SolverImpl {
     DArr<double> g_val64;
     DArr<float> g_val32;
     Workspace ws;
+    std::shared_ptr<void> gmres;  // GmresBufs, created on first GMRES solve
     int32_t* h_active = nullptr;  // pinned
     double setup_time = 0.0;
     int64_t gpu_launches = 0;
@@ -435,24 +441,67 @@ void upload_design(SolverImpl& S) {
     for (int q = 0; q < d.Q; ++q) P.off[q] = d.off[q];
     P.chunks = S.chunks.p;
     P.nchunks = (int64_t)ch.size();
+    // hot levels: the kHot most frequent levels of each non-primary factor
+    constexpr int kHot = 256;
+    S.hot_slot.resize(d.Q);
+    S.hot_level.resize(d.Q);
+    S.hot_count.assign(d.Q, 0);
+    for (int q = 0; q < d.Q; ++q) {
+        if (q == S.primary) continue;
+        const int64_t L = d.nlev[q];
+        std::vector<int64_t> cnt((size_t)L, 0);
+        const uint32_t* c = d.codes.data() + (size_t)q * d.n;
+        for (int64_t i = 0; i < d.n; ++i) cnt[c[i]]++;
+        std::vector<uint32_t> order((size_t)L);
+        std::iota(order.begin(), order.end(), 0u);
+        const int64_t h = std::min<int64_t>(kHot, L);
+        std::partial_sort(order.begin(), order.begin() + h, order.end(),
+                          [&](uint32_t a, uint32_t b) { return cnt[a] != cnt[b] ? cnt[a] > cnt[b] : a < b; });
+        std::vector<int32_t> slot((size_t)L, -1);
+        std::vector<uint32_t> lev;
+        for (int64_t a = 0; a < h; ++a) {
+            if (cnt[order[a]] < 64) break;  // only levels hit often enough to contend
+            slot[order[a]] = (int32_t)lev.size();
+            lev.push_back(order[a]);
+        }
+        S.hot_count[q] = (int32_t)lev.size();
+        S.hot_slot[q].upload(slot);
+        S.hot_level[q].upload(lev);
+        P.hot_slot[q] = S.hot_slot[q].p;
+        P.hot_level[q] = S.hot_level[q].p;
+    }
 }
 
-// shared-memory factors for a given k: small non-primary factors within a budget
+// Shared-memory regions for a given k: a non-primary factor with few levels keeps all
+// of them; a larger one keeps its hot levels; within a 40 KB budget per block.
 void obs_params_for(SolverImpl& S, int k, size_t elem, ObsParams& P) {
     P = S.obs;
     P.k = k;
     int32_t used = 0;
-    const int32_t budget = (int32_t)(32768 / elem);
+    const int32_t budget = (int32_t)(40960 / elem);
     for (int q = 0; q < S.d.Q; ++q) {
         P.smem_base[q] = -1;
         P.smem_len[q] = 0;
+        P.full[q] = 0;
         if (q == S.primary) continue;
         const int64_t len = S.d.nlev[q] * k;
-        if (used + len <= budget) {
+        if (S.d.nlev[q] <= 256 && used + len <= budget) {
             P.smem_base[q] = used;
             P.smem_len[q] = (int32_t)len;
+            P.full[q] = 1;
             used += (int32_t)len;
         }
+    }
+    for (int q = 0; q < S.d.Q; ++q) {
+        if (q == S.primary || P.full[q] || S.hot_count[q] == 0) continue;
+        int32_t h = S.hot_count[q];
+        while (h > 0 && used + h * k > budget) h /= 2;
+        if (h == 0) continue;
+        // slots >= h of the hot table must fall back to global atomics: restrict the table
+        if (h < S.hot_count[q]) continue;
+        P.smem_base[q] = used;
+        P.smem_len[q] = h * k;
+        used += h * k;
     }
     P.smem_elems = used;
 }
@@ -911,6 +960,279 @@ void cg_device(SolverImpl& S, int k, const T* b, T* x, T* r, T* z, T* p, T* ap, 
     S.gpu_launches++;
 }
 
+// ---------------------------------------------------------------------------
+// Right-preconditioned GMRES(restart) on the device (gmres.rs:201-530), batched over
+// RHS: every RHS runs its own Arnoldi cycle; Hessenberg, Givens and the small solves
+// stay on the device in FP64, one thread per RHS.
+// ---------------------------------------------------------------------------
+
+struct GState {
+    int R;                 // restart
+    double *H, *g, *cs, *sn, *y, *scale, *hcur, *hmax, *abs_tol, *resid;
+    int32_t *cyc, *done, *conv, *iters, *jc, *brk, *n_active;
+};
+
+__device__ void g_count(GState s, int k) {
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        int na = 0;
+        for (int j = 0; j < k; ++j) na += s.cyc[j];
+        *s.n_active = na;
+    }
+}
+#define GH(s, c, i, j) (s).H[((size_t)(c) * ((s).R) + (j)) * ((s).R + 1) + (i)]
+
+// ||b||, abs_tol; zero RHS converge at iteration 0 (gmres.rs:357-369).  RHS outside
+// part_of do not take part.
+__global__ void gm_init_kernel(GState s, const double* part, int nb, int k, const double* tol,
+                               const int32_t* part_of) {
+    const int c = threadIdx.x;
+    if (c < k) {
+        const double bn = sqrt(sum_part(part, nb, k, c));
+        s.iters[c] = 0;
+        s.brk[c] = 0;
+        s.cyc[c] = 0;
+        s.abs_tol[c] = tol[c] * bn;
+        if (!part_of[c]) { s.done[c] = 1; s.conv[c] = 0; }
+        else if (bn < 2.220446049250313e-16) { s.done[c] = 1; s.conv[c] = 1; }
+        else { s.done[c] = 0; s.conv[c] = 0; }
+    }
+}
+// Start of a cycle: beta = ||b - A x|| (gmres.rs:375-393, 428-437).
+__global__ void gm_restart_kernel(GState s, const double* part, int nb, int k, int maxiter) {
+    const int c = threadIdx.x;
+    if (c < k) {
+        s.cyc[c] = 0;
+        s.jc[c] = 0;
+        if (!s.done[c]) {
+            const double beta = sqrt(sum_part(part, nb, k, c));
+            s.resid[c] = beta;
+            if (s.brk[c]) {  // lucky breakdown: true residual decides
+                s.done[c] = 1;
+                s.conv[c] = beta <= s.abs_tol[c];
+            } else if (beta <= s.abs_tol[c]) {
+                s.done[c] = 1;
+                s.conv[c] = 1;
+            } else if (s.iters[c] >= maxiter) {
+                s.done[c] = 1;
+                s.conv[c] = 0;
+            } else {
+                s.cyc[c] = 1;
+                for (int i = 0; i <= s.R; ++i) s.g[(size_t)c * (s.R + 1) + i] = 0.0;
+                for (int j = 0; j < s.R; ++j) {
+                    s.cs[(size_t)c * s.R + j] = 0.0;
+                    s.sn[(size_t)c * s.R + j] = 0.0;
+                    for (int i = 0; i <= s.R; ++i) GH(s, c, i, j) = 0.0;
+                }
+                s.g[(size_t)c * (s.R + 1)] = beta;
+                s.hmax[c] = 0.0;
+                s.scale[c] = 1.0 / beta;
+            }
+        }
+    }
+    g_count(s, k);
+}
+// MGS coefficient h_ij = w . v_i (gmres.rs:201-220).
+__global__ void gm_mgs_coef_kernel(GState s, const double* part, int nb, int k, int i, int j) {
+    const int c = threadIdx.x;
+    if (c < k) {
+        const double h = s.cyc[c] ? sum_part(part, nb, k, c) : 0.0;
+        s.hcur[c] = h;
+        if (s.cyc[c]) {
+            GH(s, c, i, j) = h;
+            s.hmax[c] = fmax(s.hmax[c], fabs(h));
+        }
+    }
+}
+template <typename T>
+__global__ void gm_axpy_kernel(T* __restrict__ w, const T* __restrict__ v, const double* __restrict__ h,
+                               int64_t rows, int k) {
+    const int64_t n = rows * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        w[e] -= (T)h[e % k] * v[e];
+}
+template <typename T>
+__global__ void gm_scale_kernel(const T* __restrict__ w, T* __restrict__ v, const double* __restrict__ scale,
+                                const int32_t* __restrict__ cyc, int64_t rows, int k) {
+    const int64_t n = rows * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % k);
+        v[e] = cyc[c] ? (T)((double)w[e] * scale[c]) : T(0);
+    }
+}
+// h_{j+1,j} = ||w||, Givens rotations, residual estimate, outcome (gmres.rs:256-313).
+__global__ void gm_givens_kernel(GState s, const double* part, int nb, int k, int j, int maxiter) {
+    const int c = threadIdx.x;
+    if (c < k && s.cyc[c]) {
+        const int R = s.R;
+        double* cs = s.cs + (size_t)c * R;
+        double* sn = s.sn + (size_t)c * R;
+        double* g = s.g + (size_t)c * (R + 1);
+        const double hn = sqrt(sum_part(part, nb, k, c));
+        GH(s, c, j + 1, j) = hn;
+        s.hmax[c] = fmax(s.hmax[c], hn);
+        for (int i = 0; i < j; ++i) {
+            const double a = GH(s, c, i, j), b = GH(s, c, i + 1, j);
+            const double t = cs[i] * a + sn[i] * b;
+            GH(s, c, i + 1, j) = -sn[i] * a + cs[i] * b;
+            GH(s, c, i, j) = t;
+        }
+        const double a = GH(s, c, j, j), b = GH(s, c, j + 1, j);
+        const double r = hypot(a, b);
+        double cc = 1.0, ss = 0.0;
+        if (r != 0.0) { cc = a / r; ss = b / r; }
+        cs[j] = cc;
+        sn[j] = ss;
+        GH(s, c, j, j) = cc * a + ss * b;
+        GH(s, c, j + 1, j) = 0.0;
+        const double t = cc * g[j] + ss * g[j + 1];
+        g[j + 1] = -ss * g[j] + cc * g[j + 1];
+        g[j] = t;
+        s.jc[c] = j + 1;
+        s.iters[c] += 1;
+        const double res = fabs(g[j + 1]);
+        s.resid[c] = res;
+        s.scale[c] = 0.0;
+        if (res <= s.abs_tol[c]) {
+            s.cyc[c] = 0; s.done[c] = 1; s.conv[c] = 1;
+        } else if (s.iters[c] >= maxiter) {
+            s.cyc[c] = 0; s.done[c] = 1; s.conv[c] = 0;
+        } else if (hn > 1e-14 * s.hmax[c]) {
+            s.scale[c] = 1.0 / hn;
+        } else {
+            s.cyc[c] = 0; s.brk[c] = 1;  // lucky breakdown
+        }
+    }
+    g_count(s, k);
+}
+// y = R^{-1} g over the cycle's jc steps (solve_upper_triangular, gmres.rs:499-519).
+__global__ void gm_trisolve_kernel(GState s, int k) {
+    const int c = threadIdx.x;
+    if (c >= k) return;
+    const int jn = s.jc[c], R = s.R;
+    double* y = s.y + (size_t)c * R;
+    const double* g = s.g + (size_t)c * (R + 1);
+    for (int i = 0; i < R; ++i) y[i] = 0.0;
+    for (int i = jn - 1; i >= 0; --i) {
+        double sum = g[i];
+        for (int jj = i + 1; jj < jn; ++jj) sum -= GH(s, c, i, jj) * y[jj];
+        const double d = GH(s, c, i, i);
+        y[i] = fabs(d) < 1e-14 * (1.0 + fabs(sum)) ? 0.0 : sum / d;
+    }
+}
+// x += sum_i y_i z_i (update_solution, gmres.rs:523-530).
+template <typename T>
+__global__ void gm_update_kernel(double* __restrict__ x, const T* __restrict__ Z, const double* __restrict__ y,
+                                 int R, int jmax, int64_t rows, int k) {
+    const int64_t n = rows * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % k);
+        double acc = 0.0;
+        for (int i = 0; i < jmax; ++i) acc += y[(size_t)c * R + i] * (double)Z[(size_t)i * n + e];
+        x[e] += acc;
+    }
+}
+__global__ void gm_final_kernel(GState s, int k) {
+    const int c = threadIdx.x;
+    if (c < k && !s.done[c]) { s.done[c] = 1; s.conv[c] = 0; }
+}
+#undef GH
+
+struct GmresBufs {
+    int R = 0, k = 0;
+    int64_t m = 0;
+    DArr<double> H, g, cs, sn, y, scale, hcur, hmax, abs_tol, resid;
+    DArr<int32_t> cyc, done, conv, iters, jc, brk, n_active;
+    DArr<double> r64, w64, V64, Z64;
+    DArr<float> w32, V32, Z32;
+};
+
+// GMRES(R) for A d = rhs (FP64 rhs and solution x; vectors of type T).  Per-RHS results
+// in the GState arrays (conv, iters).
+template <typename T>
+void gmres_device(SolverImpl& S, GmresBufs& B, int k, const double* rhs, double* x, int maxiter) {
+    const int64_t m = S.d.ndofs;
+    const int R = std::max(1, S.params.gmres_restart);
+    const size_t mk = (size_t)m * k;
+    if (B.R != R || B.k < k || B.m != m) {
+        B.R = R; B.k = k; B.m = m;
+        for (DArr<double>* a : {&B.g}) a->alloc((size_t)32 * (R + 1));
+        B.H.alloc((size_t)32 * R * (R + 1));
+        for (DArr<double>* a : {&B.cs, &B.sn, &B.y}) a->alloc((size_t)32 * R);
+        for (DArr<double>* a : {&B.scale, &B.hcur, &B.hmax, &B.abs_tol, &B.resid}) a->alloc(32);
+        for (DArr<int32_t>* a : {&B.cyc, &B.done, &B.conv, &B.iters, &B.jc, &B.brk, &B.n_active}) a->alloc(32);
+        B.r64.alloc(mk);
+        B.w64.alloc(mk);
+        if (std::is_same<T, double>::value) { B.V64.alloc(mk * (R + 1)); B.Z64.alloc(mk * R); }
+        else { B.w32.alloc(mk); B.V32.alloc(mk * (R + 1)); B.Z32.alloc(mk * R); }
+    }
+    GState s{R, B.H.p, B.g.p, B.cs.p, B.sn.p, B.y.p, B.scale.p, B.hcur.p, B.hmax.p, B.abs_tol.p, B.resid.p,
+             B.cyc.p, B.done.p, B.conv.p, B.iters.p, B.jc.p, B.brk.p, B.n_active.p};
+    T* V = std::is_same<T, double>::value ? (T*)B.V64.p : (T*)B.V32.p;
+    T* Z = std::is_same<T, double>::value ? (T*)B.Z64.p : (T*)B.Z32.p;
+    T* wv = std::is_same<T, double>::value ? (T*)B.w64.p : (T*)B.w32.p;
+    const T* w_t = std::is_same<T, double>::value ? (const T*)S.w64.p : (const T*)S.w32.p;
+    double* part = S.ws.part.p;
+    int nb = 0;
+    const int gridv = S.nblk(m * k, 1);
+    WB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * mk, S.stream));
+    launch_dot<double, double>(S, rhs, rhs, m, k, part, nb);
+    gm_init_kernel<<<1, 32, 0, S.stream>>>(s, part, nb, k, S.ws.st_tol.p, S.ws.st_part.p);
+    const int kind = std::is_same<T, double>::value ? 0 : 1;
+    for (int cycle = 0; cycle < maxiter + 2; ++cycle) {
+        // r = rhs - A x (FP64), beta, v_0 = r / beta
+        launch_obs<double, OBS_GRAM>(S, k, S.w64.p, x, nullptr, B.w64.p, nullptr);
+        sub_kernel<<<gridv, kBlock, 0, S.stream>>>(rhs, B.w64.p, B.r64.p, (int64_t)mk);
+        launch_dot<double, double>(S, B.r64.p, B.r64.p, m, k, part, nb);
+        gm_restart_kernel<<<1, 32, 0, S.stream>>>(s, part, nb, k, maxiter);
+        WB_CUDA(cudaMemcpyAsync(S.h_active, B.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaStreamSynchronize(S.stream));
+        S.gpu_launches += 4;
+        if (*S.h_active == 0) break;
+        if (std::is_same<T, double>::value) {
+            gm_scale_kernel<double><<<gridv, kBlock, 0, S.stream>>>(B.r64.p, (double*)V, B.scale.p, B.cyc.p, m, k);
+        } else {
+            convert_kernel<double, float><<<gridv, kBlock, 0, S.stream>>>(B.r64.p, B.w32.p, (int64_t)mk);
+            gm_scale_kernel<float><<<gridv, kBlock, 0, S.stream>>>(B.w32.p, (float*)V, B.scale.p, B.cyc.p, m, k);
+        }
+        int jmax = 0;
+        for (int j = 0; j < R; ++j) {
+            T* vj = V + (size_t)j * mk;
+            T* zj = Z + (size_t)j * mk;
+            int nbp = 0;
+            cudaEvent_t e1 = nullptr;
+            S.prof_begin(kind + 2, e1);
+            apply_precond<T>(S, vj, zj, k, nullptr, nbp);
+            S.prof_end(kind + 2, e1);
+            cudaEvent_t e0 = nullptr;
+            S.prof_begin(kind, e0);
+            launch_obs<T, OBS_GRAM>(S, k, w_t, zj, nullptr, wv, nullptr);
+            S.prof_end(kind, e0);
+            for (int i = 0; i <= j; ++i) {
+                const T* vi = V + (size_t)i * mk;
+                launch_dot<T, T>(S, wv, vi, m, k, part, nb);
+                gm_mgs_coef_kernel<<<1, 32, 0, S.stream>>>(s, part, nb, k, i, j);
+                gm_axpy_kernel<T><<<gridv, kBlock, 0, S.stream>>>(wv, vi, B.hcur.p, m, k);
+            }
+            launch_dot<T, T>(S, wv, wv, m, k, part, nb);
+            gm_givens_kernel<<<1, 32, 0, S.stream>>>(s, part, nb, k, j, maxiter);
+            gm_scale_kernel<T><<<gridv, kBlock, 0, S.stream>>>(wv, V + (size_t)(j + 1) * mk, B.scale.p, B.cyc.p, m, k);
+            WB_CUDA(cudaGetLastError());
+            S.gpu_launches += 2 * (j + 1) + 2;
+            jmax = j + 1;
+            WB_CUDA(cudaMemcpyAsync(S.h_active, B.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+            WB_CUDA(cudaStreamSynchronize(S.stream));
+            if (*S.h_active == 0) break;
+        }
+        gm_trisolve_kernel<<<1, 32, 0, S.stream>>>(s, k);
+        gm_update_kernel<T><<<gridv, kBlock, 0, S.stream>>>(x, Z, B.y.p, R, jmax, m, k);
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches += 2;
+    }
+    gm_final_kernel<<<1, 32, 0, S.stream>>>(s, k);
+    WB_CUDA(cudaGetLastError());
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -958,7 +1280,15 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
         WB_CUDA(cudaMemcpyAsync(w.st_tol.p, tl.data(), sizeof(double) * k, cudaMemcpyHostToDevice, S.stream));
         WB_CUDA(cudaMemsetAsync(w.st_conv.p, 0, sizeof(int32_t) * 32, S.stream));
         const int grid = S.nblk(m * k, 1);
-        if (!S.mixed()) {
+        if (S.params.krylov == WITHIN_KRYLOV_GMRES) {
+            if (!S.gmres) S.gmres = std::make_shared<GmresBufs>();
+            GmresBufs& B = *std::static_pointer_cast<GmresBufs>(S.gmres);
+            if (!S.mixed()) gmres_device<double>(S, B, k, rhs, w.cx.p, S.params.maxiter);
+            else gmres_device<float>(S, B, k, rhs, w.cx.p, S.params.maxiter);
+            masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, k);
+            WB_CUDA(cudaMemcpyAsync(w.st_conv.p, B.conv.p, sizeof(int32_t) * k, cudaMemcpyDeviceToDevice, S.stream));
+            WB_CUDA(cudaMemcpyAsync(w.st_iters.p, B.iters.p, sizeof(int32_t) * k, cudaMemcpyDeviceToDevice, S.stream));
+        } else if (!S.mixed()) {
             cg_device<double>(S, k, rhs, w.cx.p, w.cr.p, w.dz.p, w.dp.p, w.dap.p, S.params.maxiter);
             masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, k);
         } else {
@@ -1087,8 +1417,8 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
     const within_params& p = S->params;
     if (p.krylov != WITHIN_KRYLOV_CG && p.krylov != WITHIN_KRYLOV_GMRES)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "config must be CG or GMRES");
-    if (p.krylov == WITHIN_KRYLOV_GMRES)
-        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "GMRES is not available on the device path yet");
+    if (p.krylov == WITHIN_KRYLOV_GMRES && p.gmres_restart < 1)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "GMRES restart must be >= 1");
     if (precond && precond->kind == WITHIN_PRECOND_MULTIPLICATIVE && p.krylov == WITHIN_KRYLOV_CG)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT,
                         "CG requires a symmetric preconditioner; use 'additive' or switch to GMRES");
