@@ -87,15 +87,19 @@ struct CsrHost {
     int64_t nrows() const { return (int64_t)row_slot.size(); }
 };
 
-// One Schwarz stage: the local solves of a set of subdomains over their
-// concatenated slots (slots of subdomain s: q-block then r-block).
+// One Schwarz stage: the local solves of a set of subdomains over their concatenated
+// slots (slots of subdomain s: q-block then r-block), in the fused form of kernels.cuh.
 struct StageHost {
     int32_t nsub = 0;
     int64_t nslots = 0;
     std::vector<uint32_t> gidx, sub_of, keep_slots;
-    std::vector<double> spou, scale;
+    std::vector<double> spou, invd, rho;        // per slot, per slot (0 = kept), per keep entry
     std::vector<int32_t> sub_nloc, sub_nkeep;
-    CsrHost keep, elim;
+    std::vector<double> sub_I;                  // sum of invd over eliminated slots
+    CsrHost keep;                               // rows: keep list; cols: global dofs
+    std::vector<int64_t> bs_ptr{0};             // back substitution rows over all slots
+    std::vector<uint32_t> bs_col;               // keep slot
+    std::vector<double> bs_val;                 // C_ek
     // dense reduced solves
     std::vector<int64_t> dn_keep0, dn_loff;
     std::vector<int32_t> dn_n;
@@ -118,9 +122,13 @@ struct StageDev {
     int32_t nsub = 0;
     int64_t nslots = 0, nkeep = 0;
     DArr<uint32_t> gidx, sub_of, keep_slots;
-    DArr<T> spou, scale;
+    DArr<T> spou, invd, rho;
     DArr<int32_t> sub_nloc, sub_nkeep;
-    CsrDev<T> keep, elim, fwd, bwd;
+    DArr<double> sub_I;
+    CsrDev<T> keep, fwd, bwd;
+    DArr<int64_t> bs_ptr;
+    DArr<uint32_t> bs_col;
+    DArr<T> bs_val;
     std::vector<int64_t> fwd_lp, bwd_lp;  // host copies (launch ranges)
     int32_t ndense = 0;
     DArr<int64_t> dn_keep0, dn_loff;
@@ -136,6 +144,6 @@ struct StageDev {
     DArr<uint32_t> gslot;
 };
 
-constexpr int kCoreRowsPerBlock = 32;
+constexpr int kCoreRowsPerBlock = 8;
 
 }  // namespace wb

@@ -1,7 +1,10 @@
-// sm_100a kernels of the solve phase.  All vectors with k right-hand sides are
-// stored RHS-interleaved: element (row, c) at row*k + c, so one row of a
-// gather or scatter is k contiguous values (128 bytes for k = 16 in FP64).
-// A "group" of G = pow2ceil(k) <= 32 lanes works on one row; lane c owns RHS c.
+// sm_100a kernels of the solve phase.
+//
+// Vectors with k right-hand sides are RHS-interleaved with the RHS count padded to
+// kp, a multiple of 4: element (row, c) at row*kp + c.  A lane owns 4 consecutive RHS
+// (one 16-byte float4, or two double2), and a group of G = kp/4 lanes (1, 2, 4 or 8)
+// owns a row, so a row of a gather or scatter is one coalesced 16*G-byte (FP32) or
+// 32*G-byte (FP64) access.  Padded RHS are zero and stay inactive in the Krylov loops.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -13,21 +16,59 @@ constexpr int kMaxQ = 16;
 constexpr int kBlock = 256;
 
 // ---------------------------------------------------------------------------
-// small device helpers
+// 4-wide RHS vectors
 // ---------------------------------------------------------------------------
 
-template <int G>
-__device__ __forceinline__ unsigned group_mask() {
-    if constexpr (G == 32) {
-        return 0xffffffffu;
-    } else {
-        const unsigned lane = threadIdx.x & 31u;
-        return ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
-    }
-}
-
 template <typename T>
-__device__ __forceinline__ void atomic_add(T* p, T v) { atomicAdd(p, v); }
+struct V4 {
+    T a, b, c, d;
+    __device__ __forceinline__ V4() {}
+    __device__ __forceinline__ V4(T s) : a(s), b(s), c(s), d(s) {}
+    __device__ __forceinline__ V4(T a_, T b_, T c_, T d_) : a(a_), b(b_), c(c_), d(d_) {}
+    __device__ __forceinline__ V4& operator+=(const V4& o) { a += o.a; b += o.b; c += o.c; d += o.d; return *this; }
+    __device__ __forceinline__ V4& operator-=(const V4& o) { a -= o.a; b -= o.b; c -= o.c; d -= o.d; return *this; }
+    __device__ __forceinline__ V4& operator*=(T s) { a *= s; b *= s; c *= s; d *= s; return *this; }
+    __device__ __forceinline__ bool any() const { return a != T(0) || b != T(0) || c != T(0) || d != T(0); }
+};
+template <typename T>
+__device__ __forceinline__ V4<T> operator*(T s, const V4<T>& v) { return V4<T>(s * v.a, s * v.b, s * v.c, s * v.d); }
+template <typename T>
+__device__ __forceinline__ V4<T> operator+(V4<T> x, const V4<T>& y) { x += y; return x; }
+template <typename T>
+__device__ __forceinline__ V4<T> operator-(V4<T> x, const V4<T>& y) { x -= y; return x; }
+
+__device__ __forceinline__ V4<float> ld4(const float* p) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    return V4<float>(v.x, v.y, v.z, v.w);
+}
+__device__ __forceinline__ V4<double> ld4(const double* p) {
+    const double2 u = reinterpret_cast<const double2*>(p)[0], v = reinterpret_cast<const double2*>(p)[1];
+    return V4<double>(u.x, u.y, v.x, v.y);
+}
+__device__ __forceinline__ V4<float> ldg4(const float* p) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    return V4<float>(v.x, v.y, v.z, v.w);
+}
+__device__ __forceinline__ V4<double> ldg4(const double* p) {
+    const double2 u = __ldg(reinterpret_cast<const double2*>(p)), v = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return V4<double>(u.x, u.y, v.x, v.y);
+}
+__device__ __forceinline__ void st4(float* p, const V4<float>& v) {
+    *reinterpret_cast<float4*>(p) = make_float4(v.a, v.b, v.c, v.d);
+}
+__device__ __forceinline__ void st4(double* p, const V4<double>& v) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v.a, v.b);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v.c, v.d);
+}
+// global atomics, one per value
+template <typename T>
+__device__ __forceinline__ void atomic_add4(T* p, const V4<T>& v) {
+    atomicAdd(p, v.a); atomicAdd(p + 1, v.b); atomicAdd(p + 2, v.c); atomicAdd(p + 3, v.d);
+}
+template <typename T>
+__device__ __forceinline__ V4<double> to_d(const V4<T>& v) { return V4<double>(v.a, v.b, v.c, v.d); }
+template <typename T>
+__device__ __forceinline__ V4<T> from_d(const V4<double>& v) { return V4<T>((T)v.a, (T)v.b, (T)v.c, (T)v.d); }
 
 // ---------------------------------------------------------------------------
 // Observation pass: y = D'W(D x) and its relatives, one read of the codes.
@@ -35,9 +76,8 @@ __device__ __forceinline__ void atomic_add(T* p, T v) { atomicAdd(p, v); }
 
 enum ObsMode { OBS_GRAM = 0, OBS_RHS = 1, OBS_RESID = 2, OBS_DX = 3 };
 
-// Work unit of the observation pass: a run of observations (sorted by the primary
-// factor) covering primary levels [lvl_begin, lvl_end).  A split chunk holds a piece
-// of one long level and adds its partial sum atomically.
+// Work unit: observations [obs_begin, obs_end) (sorted by the primary factor) covering
+// primary levels [lvl_begin, lvl_end); a split chunk is a piece of one long level.
 struct ObsChunk {
     uint32_t obs_begin, obs_end, lvl_begin, lvl_end;
     uint32_t split;
@@ -45,14 +85,14 @@ struct ObsChunk {
 
 struct ObsParams {
     int64_t n;
-    int32_t Q, k, primary;
+    int32_t Q, kp, primary;
     int32_t smem_elems;
     const uint32_t* codes;  // Q x n, primary-sorted order
     int64_t off[kMaxQ];
     // Per non-primary factor, a block-local shared-memory region of smem_len[q] values at
-    // smem_base[q] (-1: none).  full[q]: the region holds every level (level*k + c);
-    // otherwise it holds the factor's hottest levels: hot_slot[q][level] >= 0 gives the
-    // slot, hot_level[q][slot] the level.  Other levels go to global atomics.
+    // smem_base[q] (-1: none).  full[q]: the region holds every level (level*kp + c);
+    // otherwise the factor's hottest levels: hot_slot[q][level] >= 0 is the slot and
+    // hot_level[q][slot] the level.  Other levels go to global atomics.
     int32_t smem_base[kMaxQ];
     int32_t smem_len[kMaxQ];
     int32_t full[kMaxQ];
@@ -63,124 +103,119 @@ struct ObsParams {
 };
 
 template <typename T>
-__device__ __forceinline__ void obs_flush(const ObsParams& P, T* sm, T* out, int q, uint32_t lvl, T a, int k, int c) {
-    if (a == T(0)) return;
+__device__ __forceinline__ void obs_flush(const ObsParams& P, T* sm, T* out, int q, uint32_t lvl,
+                                          const V4<T>& a, int c4) {
+    if (!a.any()) return;
     if (P.smem_base[q] >= 0) {
         if (P.full[q]) {
-            atomic_add(sm + P.smem_base[q] + (size_t)lvl * k + c, a);
+            atomic_add4(sm + P.smem_base[q] + (size_t)lvl * P.kp + c4, a);
             return;
         }
         const int32_t h = __ldg(P.hot_slot[q] + lvl);
         if (h >= 0) {
-            atomic_add(sm + P.smem_base[q] + (size_t)h * k + c, a);
+            atomic_add4(sm + P.smem_base[q] + (size_t)h * P.kp + c4, a);
             return;
         }
     }
-    atomic_add(out + (size_t)(P.off[q] + lvl) * k + c, a);
+    atomic_add4(out + (size_t)(P.off[q] + lvl) * P.kp + c4, a);
 }
 
-// QT >= Q is the compile-time bound of the factor loops (4 or 16).
-// Each group walks a chunk of observations sorted by the primary factor: the primary
-// factor's sums close with a plain store when its level changes; every other factor
-// keeps a running sum while its level repeats (a worker's firm rarely changes) and
-// flushes it to shared memory (small factor or hot level) or a global atomic.
-template <typename T, int G, int MODE, int QT>
+// QT >= Q bounds the factor loops; NB observations are loaded and gathered together.
+// Each group walks a chunk of primary-sorted observations: the primary factor's sums
+// close with a plain store when its level changes; every other factor keeps a running
+// sum while its level repeats (a worker's firm rarely changes) and flushes it to shared
+// memory (small factor or hot level) or a global atomic.
+template <typename T, int G, int MODE, int QT, int NB>
 __global__ void __launch_bounds__(kBlock) obs_pass_kernel(ObsParams P, const T* __restrict__ w,
                                                           const T* __restrict__ x, const T* __restrict__ yin,
                                                           T* __restrict__ out, T* __restrict__ eout) {
-    extern __shared__ unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
     constexpr bool kScatter = MODE != OBS_DX;
     if (kScatter) {
         for (int i = threadIdx.x; i < P.smem_elems; i += blockDim.x) sm[i] = T(0);
         __syncthreads();
     }
-    const int lane_g = threadIdx.x & (G - 1);
-    const int c = lane_g;
-    const bool cval = c < P.k;
-    const int k = P.k;
-    const unsigned mask = group_mask<G>();
-    const int64_t groups_per_block = blockDim.x / G;
-    const int64_t gid = (int64_t)blockIdx.x * groups_per_block + threadIdx.x / G;
-    const int64_t ngroups = (int64_t)gridDim.x * groups_per_block;
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const int kp = P.kp;
+    const int64_t gpb = blockDim.x / G;
+    const int64_t gid = (int64_t)blockIdx.x * gpb + threadIdx.x / G;
+    const int64_t ngroups = (int64_t)gridDim.x * gpb;
     const int Q = P.Q, pq = P.primary;
     const int64_t n = P.n;
 
     for (int64_t ch = gid; ch < P.nchunks; ch += ngroups) {
         const ObsChunk C = P.chunks[ch];
         uint32_t lvl = C.lvl_begin;
-        T acc = T(0);
+        V4<T> acc(T(0));
         uint32_t run_l[QT];
-        T run_a[QT];
+        V4<T> run_a[QT];
 #pragma unroll
-        for (int q = 0; q < QT; ++q) { run_l[q] = 0xffffffffu; run_a[q] = T(0); }
-        for (uint32_t base = C.obs_begin; base < C.obs_end; base += G) {
-            const uint32_t cnt = min((uint32_t)G, C.obs_end - base);
-            // cooperative loads: lane j holds the codes and weight of observation base+j
-            uint32_t my_codes[QT];
-            const uint32_t j = base + (lane_g < (int)cnt ? lane_g : 0);
+        for (int q = 0; q < QT; ++q) { run_l[q] = 0xffffffffu; run_a[q] = V4<T>(T(0)); }
+        for (uint32_t base = C.obs_begin; base < C.obs_end; base += NB) {
+            const uint32_t cnt = min((uint32_t)NB, C.obs_end - base);
+            uint32_t lq[NB][QT];
+            T wv[NB];
+            V4<T> s[NB];
+            // independent loads of NB observations: codes, weights, then all gathers
 #pragma unroll
-            for (int q = 0; q < QT; ++q)
-                my_codes[q] = q < Q ? __ldg(P.codes + (size_t)q * n + j) : 0u;
-            T my_w = (MODE == OBS_DX || w == nullptr) ? T(1) : __ldg(w + j);
-            for (uint32_t jj = 0; jj < cnt; ++jj) {
-                const uint32_t i = base + jj;
-                uint32_t lq[QT];
+            for (int b = 0; b < NB; ++b) {
+                const uint32_t i = base + (b < (int)cnt ? b : 0);
 #pragma unroll
-                for (int q = 0; q < QT; ++q) lq[q] = __shfl_sync(mask, my_codes[q], jj, G);
-                const T wi = __shfl_sync(mask, my_w, jj, G);
-                T t = T(0);
-                if (cval) {
-                    T s = T(0);
-                    if (MODE != OBS_RHS) {
+                for (int q = 0; q < QT; ++q) lq[b][q] = q < Q ? __ldg(P.codes + (size_t)q * n + i) : 0u;
+                wv[b] = (MODE == OBS_DX || w == nullptr) ? T(1) : __ldg(w + i);
+            }
 #pragma unroll
-                        for (int q = 0; q < QT; ++q)
-                            if (q < Q) s += __ldg(x + (size_t)(P.off[q] + lq[q]) * k + c);
-                    }
-                    if (MODE == OBS_GRAM) {
-                        t = wi * s;
-                    } else if (MODE == OBS_RHS) {
-                        t = wi * yin[(size_t)i * k + c];
-                    } else if (MODE == OBS_RESID) {
-                        const T e = yin[(size_t)i * k + c] - s;
-                        eout[(size_t)i * k + c] = e;
-                        t = wi * e;
-                    } else {
-                        eout[(size_t)i * k + c] = s;
-                    }
+            for (int b = 0; b < NB; ++b) {
+                s[b] = V4<T>(T(0));
+                if (MODE != OBS_RHS) {
+#pragma unroll
+                    for (int q = 0; q < QT; ++q)
+                        if (q < Q) s[b] += ldg4(x + (size_t)(P.off[q] + lq[b][q]) * kp + c4);
                 }
-                if (kScatter) {
-                    const uint32_t p = lq[pq];
-                    while (lvl < p) {  // primary level complete: plain store (zero for empty levels)
-                        if (cval) out[(size_t)(P.off[pq] + lvl) * k + c] = acc;
-                        acc = T(0);
-                        ++lvl;
-                    }
-                    acc += t;
+                if (MODE == OBS_RHS || MODE == OBS_RESID) {
+                    const uint32_t i = base + (b < (int)cnt ? b : 0);
+                    const V4<T> yv = ld4(yin + (size_t)i * kp + c4);
+                    s[b] = (MODE == OBS_RHS) ? yv : yv - s[b];
+                }
+            }
 #pragma unroll
-                    for (int q = 0; q < QT; ++q) {
-                        if (q >= Q || q == pq) continue;
-                        if (lq[q] == run_l[q]) {
-                            run_a[q] += t;
-                        } else {
-                            if (run_l[q] != 0xffffffffu && cval) obs_flush(P, sm, out, q, run_l[q], run_a[q], k, c);
-                            run_l[q] = lq[q];
-                            run_a[q] = t;
-                        }
+            for (int b = 0; b < NB; ++b) {
+                if (b >= (int)cnt) break;
+                const uint32_t i = base + b;
+                if (MODE == OBS_DX || MODE == OBS_RESID) st4(eout + (size_t)i * kp + c4, s[b]);
+                if (!kScatter) continue;
+                const V4<T> t = wv[b] * s[b];
+                const uint32_t p = lq[b][pq];
+                while (lvl < p) {  // primary level complete: plain store (zero for empty levels)
+                    st4(out + (size_t)(P.off[pq] + lvl) * kp + c4, acc);
+                    acc = V4<T>(T(0));
+                    ++lvl;
+                }
+                acc += t;
+#pragma unroll
+                for (int q = 0; q < QT; ++q) {
+                    if (q >= Q || q == pq) continue;
+                    if (lq[b][q] == run_l[q]) {
+                        run_a[q] += t;
+                    } else {
+                        if (run_l[q] != 0xffffffffu) obs_flush(P, sm, out, q, run_l[q], run_a[q], c4);
+                        run_l[q] = lq[b][q];
+                        run_a[q] = t;
                     }
                 }
             }
         }
-        if (kScatter && cval) {
+        if (kScatter) {
 #pragma unroll
             for (int q = 0; q < QT; ++q)
-                if (q < Q && q != pq && run_l[q] != 0xffffffffu) obs_flush(P, sm, out, q, run_l[q], run_a[q], k, c);
+                if (q < Q && q != pq && run_l[q] != 0xffffffffu) obs_flush(P, sm, out, q, run_l[q], run_a[q], c4);
             if (C.split) {
-                atomic_add(out + (size_t)(P.off[pq] + C.lvl_begin) * k + c, acc);
+                atomic_add4(out + (size_t)(P.off[pq] + C.lvl_begin) * kp + c4, acc);
             } else {
                 while (lvl < C.lvl_end) {
-                    out[(size_t)(P.off[pq] + lvl) * k + c] = acc;
-                    acc = T(0);
+                    st4(out + (size_t)(P.off[pq] + lvl) * kp + c4, acc);
+                    acc = V4<T>(T(0));
                     ++lvl;
                 }
             }
@@ -194,23 +229,23 @@ __global__ void __launch_bounds__(kBlock) obs_pass_kernel(ObsParams P, const T* 
             for (int idx = threadIdx.x; idx < P.smem_len[q]; idx += blockDim.x) {
                 const T v = sm[P.smem_base[q] + idx];
                 if (v == T(0)) continue;
-                const int slot = idx / k, cc = idx % k;
+                const int slot = idx / kp, cc = idx % kp;
                 const uint32_t lev = P.full[q] ? (uint32_t)slot : P.hot_level[q][slot];
-                atomic_add(out + (size_t)(P.off[q] + lev) * k + cc, v);
+                atomicAdd(out + (size_t)(P.off[q] + lev) * kp + cc, v);
             }
         }
     }
 }
 
-// Column-major (RHS-major) original order <-> interleaved primary-sorted order.
-// perm[i] = original index of sorted observation i (nullptr = identity).
+// Column-major (RHS-major) user order <-> interleaved primary-sorted order with kp
+// columns (padding columns are zero).  perm[i] = user index of sorted row i (or identity).
 template <typename T>
-__global__ void gather_interleave_kernel(const double* __restrict__ ycol, int64_t n, int k,
+__global__ void gather_interleave_kernel(const double* __restrict__ ycol, int64_t n, int k, int kp,
                                          const uint32_t* __restrict__ perm, T* __restrict__ yi) {
     __shared__ double tile[32][33];
     const int64_t i0 = (int64_t)blockIdx.x * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-    for (int c0 = 0; c0 < k; c0 += 32) {
+    for (int c0 = 0; c0 < kp; c0 += 32) {
         for (int cc = ty; cc < 32; cc += 8) {
             const int c = c0 + cc;
             const int64_t i = i0 + tx;
@@ -219,18 +254,18 @@ __global__ void gather_interleave_kernel(const double* __restrict__ ycol, int64_
             tile[cc][tx] = v;
         }
         __syncthreads();
-        const int cw = min(32, k - c0);
+        const int cw = min(32, kp - c0);
         for (int e = threadIdx.x; e < 32 * cw; e += blockDim.x) {
             const int r = e / cw, cc = e % cw;
             const int64_t i = i0 + r;
-            if (i < n) yi[(size_t)i * k + c0 + cc] = (T)tile[cc][r];
+            if (i < n) yi[(size_t)i * kp + c0 + cc] = (T)tile[cc][r];
         }
         __syncthreads();
     }
 }
 
 template <typename T>
-__global__ void scatter_deinterleave_kernel(const T* __restrict__ ei, int64_t n, int k,
+__global__ void scatter_deinterleave_kernel(const T* __restrict__ ei, int64_t n, int k, int kp,
                                             const uint32_t* __restrict__ perm, double* __restrict__ ecol) {
     __shared__ double tile[32][33];
     const int64_t i0 = (int64_t)blockIdx.x * 32;
@@ -240,7 +275,7 @@ __global__ void scatter_deinterleave_kernel(const T* __restrict__ ei, int64_t n,
         for (int e = threadIdx.x; e < 32 * cw; e += blockDim.x) {
             const int r = e / cw, cc = e % cw;
             const int64_t i = i0 + r;
-            tile[cc][r] = (i < n) ? (double)ei[(size_t)i * k + c0 + cc] : 0.0;
+            tile[cc][r] = (i < n) ? (double)ei[(size_t)i * kp + c0 + cc] : 0.0;
         }
         __syncthreads();
         for (int cc = ty; cc < 32; cc += 8) {
@@ -253,98 +288,122 @@ __global__ void scatter_deinterleave_kernel(const T* __restrict__ ei, int64_t n,
 }
 
 // ---------------------------------------------------------------------------
-// Row-wise vector kernels over (rows x k) interleaved vectors; dots in FP64.
+// Row-wise vector kernels over (rows x kp) vectors; dots accumulate in FP64.
 // ---------------------------------------------------------------------------
 
-// Each block reduces its share into part[blockIdx.x * k + c] (fixed order: deterministic).
+// Block partial sums: part[blockIdx.x * kp + c] (fixed order: deterministic).
 template <int G>
-__device__ __forceinline__ void block_reduce_store(double v, int k, double* part) {
-    __shared__ double red[kBlock];
-    red[threadIdx.x] = v;
+__device__ __forceinline__ void block_reduce_store4(const V4<double>& v, int kp, double* part) {
+    __shared__ double red[kBlock * 4];
+    const int t = threadIdx.x;
+    red[4 * t] = v.a; red[4 * t + 1] = v.b; red[4 * t + 2] = v.c; red[4 * t + 3] = v.d;
     __syncthreads();
+    // thread t owns RHS (t % G)*4 .. +3; fold groups onto the first group
     for (int s = blockDim.x / 2; s >= G; s >>= 1) {
-        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        if (t < s) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) red[4 * t + j] += red[4 * (t + s) + j];
+        }
         __syncthreads();
     }
-    if (threadIdx.x < G && threadIdx.x < k) part[(size_t)blockIdx.x * k + threadIdx.x] = red[threadIdx.x];
+    if (t < G) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) part[(size_t)blockIdx.x * kp + 4 * t + j] = red[4 * t + j];
+    }
 }
 
 template <typename TA, typename TB, int G>
 __global__ void __launch_bounds__(kBlock) dot_kernel(const TA* __restrict__ a, const TB* __restrict__ b,
-                                                     int64_t rows, int k, double* __restrict__ part) {
-    const int c = threadIdx.x & (G - 1);
-    double s = 0.0;
-    if (c < k) {
-        const int64_t rpb = blockDim.x / G;
-        for (int64_t r = (int64_t)blockIdx.x * rpb + threadIdx.x / G; r < rows; r += (int64_t)gridDim.x * rpb)
-            s += (double)a[(size_t)r * k + c] * (double)b[(size_t)r * k + c];
+                                                     int64_t rows, int kp, double* __restrict__ part) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    V4<double> s(0.0);
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t r = (int64_t)blockIdx.x * rpb + threadIdx.x / G; r < rows; r += (int64_t)gridDim.x * rpb) {
+        const V4<double> x = to_d(ld4(a + (size_t)r * kp + c4)), y = to_d(ld4(b + (size_t)r * kp + c4));
+        s.a += x.a * y.a; s.b += x.b * y.b; s.c += x.c * y.c; s.d += x.d * y.d;
     }
-    block_reduce_store<G>(s, k, part);
+    block_reduce_store4<G>(s, kp, part);
 }
 
-// CG step 4 (cg.rs:87-94): x += alpha p, r -= alpha ap, partial ||r||^2.
+// CG step (cg.rs:87-94): x += alpha p, r -= alpha ap, partial ||r||^2.
 template <typename T, int G>
 __global__ void __launch_bounds__(kBlock) cg_xr_kernel(T* __restrict__ x, T* __restrict__ r,
                                                        const T* __restrict__ p, const T* __restrict__ ap,
-                                                       const double* __restrict__ alpha, int64_t rows, int k,
+                                                       const double* __restrict__ alpha, int64_t rows, int kp,
                                                        double* __restrict__ part) {
-    const int c = threadIdx.x & (G - 1);
-    double s = 0.0;
-    if (c < k) {
-        const T al = (T)alpha[c];
-        const int64_t rpb = blockDim.x / G;
-        for (int64_t row = (int64_t)blockIdx.x * rpb + threadIdx.x / G; row < rows; row += (int64_t)gridDim.x * rpb) {
-            const size_t e = (size_t)row * k + c;
-            x[e] += al * p[e];
-            const T rv = r[e] - al * ap[e];
-            r[e] = rv;
-            s += (double)rv * (double)rv;
-        }
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const V4<T> al((T)alpha[c4], (T)alpha[c4 + 1], (T)alpha[c4 + 2], (T)alpha[c4 + 3]);
+    V4<double> s(0.0);
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t row = (int64_t)blockIdx.x * rpb + threadIdx.x / G; row < rows; row += (int64_t)gridDim.x * rpb) {
+        const size_t e = (size_t)row * kp + c4;
+        V4<T> xv = ld4(x + e), rv = ld4(r + e);
+        const V4<T> pv = ld4(p + e), av = ld4(ap + e);
+        xv.a += al.a * pv.a; xv.b += al.b * pv.b; xv.c += al.c * pv.c; xv.d += al.d * pv.d;
+        rv.a -= al.a * av.a; rv.b -= al.b * av.b; rv.c -= al.c * av.c; rv.d -= al.d * av.d;
+        st4(x + e, xv);
+        st4(r + e, rv);
+        s.a += (double)rv.a * rv.a; s.b += (double)rv.b * rv.b; s.c += (double)rv.c * rv.c; s.d += (double)rv.d * rv.d;
     }
-    block_reduce_store<G>(s, k, part);
+    block_reduce_store4<G>(s, kp, part);
 }
 
-// p = z + beta p (cg.rs:120-124); columns with active == 0 are left alone.
+// p = z + beta p (cg.rs:120-124); inactive RHS keep p.
 template <typename T, int G>
 __global__ void __launch_bounds__(kBlock) cg_p_kernel(T* __restrict__ p, const T* __restrict__ z,
                                                       const double* __restrict__ beta,
-                                                      const int32_t* __restrict__ active, int64_t rows, int k) {
-    const int c = threadIdx.x & (G - 1);
-    if (c >= k || !active[c]) return;
-    const T be = (T)beta[c];
+                                                      const int32_t* __restrict__ active, int64_t rows, int kp) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const bool o0 = active[c4], o1 = active[c4 + 1], o2 = active[c4 + 2], o3 = active[c4 + 3];
+    if (!(o0 || o1 || o2 || o3)) return;
+    const V4<T> be((T)beta[c4], (T)beta[c4 + 1], (T)beta[c4 + 2], (T)beta[c4 + 3]);
     const int64_t rpb = blockDim.x / G;
     for (int64_t row = (int64_t)blockIdx.x * rpb + threadIdx.x / G; row < rows; row += (int64_t)gridDim.x * rpb) {
-        const size_t e = (size_t)row * k + c;
-        p[e] = z[e] + be * p[e];
+        const size_t e = (size_t)row * kp + c4;
+        const V4<T> zv = ld4(z + e), pv = ld4(p + e);
+        V4<T> o;
+        o.a = o0 ? zv.a + be.a * pv.a : pv.a;
+        o.b = o1 ? zv.b + be.b * pv.b : pv.b;
+        o.c = o2 ? zv.c + be.c * pv.c : pv.c;
+        o.d = o3 ? zv.d + be.d * pv.d : pv.d;
+        st4(p + e, o);
     }
 }
 
 // ---------------------------------------------------------------------------
-// Schwarz local solves over the flattened slots of all subdomains of a stage.
+// Schwarz local solves over the flattened slots of a stage (block elimination,
+// local_solver.rs:360-449).  With u_l = spou_l r[gidx_l] (the restriction, r-block
+// sign folded into spou) and, per subdomain s of n_s slots:
+//   m0 = sum_l u_l / n_s                                   (first subtract_mean)
+//   red_k = u_k - m0 + sum_e C_ke invd_e (u_e - m0)        (keep rows, reduced rhs)
+//   red -= mean over keep;  sol_keep = Solve(red)          (dense or AC)
+//   sol_e = invd_e (u_e - m0) + invd_e sum_k C_ek sol_k     (back substitution)
+//   m2 = (sum_k sol_k (1 + rho_k) + SB - m0 I) / n_s        (final subtract_mean)
+//   z[gidx_l] += spou_l (sol_l - m2)
+// with rho_k = sum_e C_ke invd_e, SB = sum_e u_e invd_e and I = sum_e invd_e.  Only kept
+// slots are ever stored; eliminated slots are recomputed where they are needed.
 // ---------------------------------------------------------------------------
 
-// Work unit of a row-wise CSR pass: rows [row_begin, row_end) restricted to the
-// entries [nz_begin, nz_end); rows cut by the range are partial and add atomically.
+// Work unit of a row-wise CSR pass: rows [row_begin, row_end) restricted to entries
+// [nz_begin, nz_end); rows cut by the range are partial and add atomically.
 struct CsrChunk {
     uint32_t row_begin, row_end;
     int64_t nz_begin, nz_end;
 };
 
-enum CsrEpi { EPI_ACC = 0, EPI_ACC_SCALED = 1, EPI_PIVOT = 2 };
+enum CsrEpi { EPI_ACC = 0, EPI_PIVOT = 1 };
 
-// out[row_slot] (+)= [scale] * sum_e val[e] * v[col[e]]  per RHS.
-//   EPI_ACC:        v[row] += acc
-//   EPI_ACC_SCALED: v[row] += rscale[row] * acc     (back substitution, rscale = 1/D_elim)
-//   EPI_PIVOT:      v[row]  = v[row] * rscale[row] + acc   (backward AC sweep, rscale = 1/d)
+// dst[row_slot] (+)= sum_e val[e] * src[col[e]]   per RHS
+//   EPI_ACC:   dst[row] += acc (partial rows atomically)
+//   EPI_PIVOT: dst[row]  = dst[row] * rscale[row] + acc   (backward AC sweep; never split)
 template <typename T, int G, int EPI>
 __global__ void __launch_bounds__(kBlock) csr_rows_kernel(const CsrChunk* __restrict__ chunks, int64_t nchunks,
                                                           const uint32_t* __restrict__ row_slot,
                                                           const int64_t* __restrict__ ptr,
                                                           const uint32_t* __restrict__ col,
-                                                          const T* __restrict__ val,
-                                                          const T* __restrict__ rscale, T* __restrict__ v, int k) {
-    const int c = threadIdx.x & (G - 1);
-    const bool cval = c < k;
+                                                          const T* __restrict__ val, const T* __restrict__ rscale,
+                                                          const T* src, T* dst, int kp) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
     const int64_t gpb = blockDim.x / G;
     const int64_t ng = (int64_t)gridDim.x * gpb;
     for (int64_t ch = (int64_t)blockIdx.x * gpb + threadIdx.x / G; ch < nchunks; ch += ng) {
@@ -352,84 +411,283 @@ __global__ void __launch_bounds__(kBlock) csr_rows_kernel(const CsrChunk* __rest
         for (uint32_t row = C.row_begin; row < C.row_end; ++row) {
             const int64_t rb = ptr[row], re = ptr[row + 1];
             const int64_t e0 = max(rb, C.nz_begin), e1 = min(re, C.nz_end);
-            T acc = T(0);
-            if (cval)
-                for (int64_t e = e0; e < e1; ++e) acc += __ldg(val + e) * v[(size_t)__ldg(col + e) * k + c];
-            if (!cval) continue;
-            const uint32_t s = row_slot[row];
-            T* dst = v + (size_t)s * k + c;
-            const bool partial = (e0 != rb) || (e1 != re);
+            V4<T> acc(T(0));
+            int64_t e = e0;
+            for (; e + 4 <= e1; e += 4) {  // four independent gathers in flight
+                const uint32_t j0 = __ldg(col + e), j1 = __ldg(col + e + 1), j2 = __ldg(col + e + 2), j3 = __ldg(col + e + 3);
+                const T v0 = __ldg(val + e), v1 = __ldg(val + e + 1), v2 = __ldg(val + e + 2), v3 = __ldg(val + e + 3);
+                const V4<T> s0 = ld4(src + (size_t)j0 * kp + c4), s1 = ld4(src + (size_t)j1 * kp + c4);
+                const V4<T> s2 = ld4(src + (size_t)j2 * kp + c4), s3 = ld4(src + (size_t)j3 * kp + c4);
+                acc += v0 * s0; acc += v1 * s1; acc += v2 * s2; acc += v3 * s3;
+            }
+            for (; e < e1; ++e) acc += __ldg(val + e) * ld4(src + (size_t)__ldg(col + e) * kp + c4);
+            T* d = dst + (size_t)row_slot[row] * kp + c4;
             if (EPI == EPI_ACC) {
-                if (partial) atomic_add(dst, acc); else *dst += acc;
-            } else if (EPI == EPI_ACC_SCALED) {
-                const T sc = rscale[row];
-                if (partial) atomic_add(dst, sc * acc); else *dst += sc * acc;
+                if (e0 != rb || e1 != re) atomic_add4(d, acc);
+                else st4(d, ld4(d) + acc);
             } else {
-                *dst = *dst * rscale[row] + acc;  // rows of the backward sweep are never split
+                st4(d, rscale[row] * ld4(d) + acc);
             }
         }
     }
 }
 
-// Segmented sums over a list of slots (slot_list == nullptr: slots [0, nslots)) into
-// msum[sub_of[slot] * k + c]; one atomic per (run of equal subdomain, RHS).
-template <typename T, int G>
-__global__ void __launch_bounds__(kBlock) slot_sum_kernel(const uint32_t* __restrict__ slot_list, int64_t nslots,
-                                                          const uint32_t* __restrict__ sub_of,
-                                                          const T* __restrict__ v, int k, double* __restrict__ msum,
-                                                          int64_t chunk) {
-    const int c = threadIdx.x & (G - 1);
-    if (c >= k) return;
-    const int64_t gpb = blockDim.x / G;
-    const int64_t ng = (int64_t)gridDim.x * gpb;
-    for (int64_t g = (int64_t)blockIdx.x * gpb + threadIdx.x / G; g * chunk < nslots; g += ng) {
-        const int64_t a0 = g * chunk, a1 = min(nslots, a0 + chunk);
-        uint32_t cur = UINT32_MAX;
-        double acc = 0.0;
-        for (int64_t a = a0; a < a1; ++a) {
-            const uint32_t s = slot_list ? slot_list[a] : (uint32_t)a;
-            const uint32_t sb = sub_of[s];
-            if (sb != cur) {
-                if (cur != UINT32_MAX) atomicAdd(msum + (size_t)cur * k + c, acc);
-                cur = sb;
-                acc = 0.0;
-            }
-            acc += (double)v[(size_t)s * k + c];
+// Segmented per-subdomain sums over a contiguous range, block-reduced: the block's
+// first and last subdomain accumulate in shared memory (one global atomic per block),
+// other runs (small subdomains inside the block) go straight to global atomics.
+struct SegSum {
+    double* sm;  // [2 bins][2 quantities][kp]
+    uint32_t first, last;
+    int kp;
+    __device__ void flush(double* g0, double* g1, uint32_t sub, const V4<double>& a, const V4<double>& b, int c4) {
+        const int bin = sub == first ? 0 : (sub == last ? 1 : -1);
+        if (bin >= 0) {
+            double* s = sm + (size_t)bin * 2 * kp + c4;
+            atomic_add4(s, a);
+            if (g1) atomic_add4(s + kp, b);
+        } else {
+            atomic_add4(g0 + (size_t)sub * kp + c4, a);
+            if (g1) atomic_add4(g1 + (size_t)sub * kp + c4, b);
         }
-        if (cur != UINT32_MAX) atomicAdd(msum + (size_t)cur * k + c, acc);
     }
-}
+    __device__ void finish(double* g0, double* g1) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < 2 * kp; i += blockDim.x) {
+            const int bin = i / kp, c = i % kp;
+            if (bin == 1 && last == first) continue;
+            const uint32_t sub = bin == 0 ? first : last;
+            atomicAdd(g0 + (size_t)sub * kp + c, sm[bin * 2 * kp + c]);
+            if (g1) atomicAdd(g1 + (size_t)sub * kp + c, sm[bin * 2 * kp + kp + c]);
+        }
+    }
+};
 
-// Restrict: v[l] = spou[l] * r[gidx[l]] (sign of the r-block folded into spou),
-// followed by the subdomain sums of the first subtract_mean (local_solver.rs:360-367).
+// Pass 1 (all slots): S0[s] += u_l, SB[s] += u_l invd_l.  Block b owns slots [b*spb, +spb).
 template <typename T, int G>
-__global__ void __launch_bounds__(kBlock) restrict_kernel(int64_t nslots, const uint32_t* __restrict__ gidx,
-                                                          const T* __restrict__ spou, const T* __restrict__ r,
-                                                          T* __restrict__ v, int k) {
-    const int c = threadIdx.x & (G - 1);
-    if (c >= k) return;
-    const int64_t rpb = blockDim.x / G;
-    for (int64_t l = (int64_t)blockIdx.x * rpb + threadIdx.x / G; l < nslots; l += (int64_t)gridDim.x * rpb)
-        v[(size_t)l * k + c] = spou[l] * r[(size_t)gidx[l] * k + c];
-}
-
-// v[l] = (v[l] - msum[s]/n_s) * scale[l]   (scale = 1/D_elim on eliminated slots, 1 on kept).
-template <typename T, int G>
-__global__ void __launch_bounds__(kBlock) center_scale_kernel(const uint32_t* __restrict__ slot_list, int64_t nslots,
+__global__ void __launch_bounds__(kBlock) schwarz_sums_kernel(int64_t nslots, int spb,
+                                                              const uint32_t* __restrict__ gidx,
+                                                              const T* __restrict__ spou, const T* __restrict__ invd,
                                                               const uint32_t* __restrict__ sub_of,
-                                                              const int32_t* __restrict__ sub_n,
-                                                              const double* __restrict__ msum,
-                                                              const T* __restrict__ scale, T* __restrict__ v, int k) {
-    const int c = threadIdx.x & (G - 1);
-    if (c >= k) return;
+                                                              const T* __restrict__ r, int kp,
+                                                              double* __restrict__ S0, double* __restrict__ SB) {
+    __shared__ double sm[2 * 2 * 32];
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const int64_t b0 = (int64_t)blockIdx.x * spb, b1 = min(nslots, b0 + spb);
+    if (b0 >= nslots) return;  // uniform per block
+    for (int i = threadIdx.x; i < 4 * kp; i += blockDim.x) sm[i] = 0.0;
+    SegSum seg{sm, sub_of[b0], sub_of[b1 - 1], kp};
+    __syncthreads();
+    const int gpb = blockDim.x / G, g = threadIdx.x / G;
+    const int64_t per = (spb + gpb - 1) / gpb;
+    const int64_t a0 = b0 + g * per, a1 = min(b1, a0 + per);
+    uint32_t cur = 0xffffffffu;
+    V4<double> acc0(0.0), accb(0.0);
+    for (int64_t l = a0; l < a1; ++l) {
+        const uint32_t sb = sub_of[l];
+        if (sb != cur) {
+            if (cur != 0xffffffffu) seg.flush(S0, SB, cur, acc0, accb, c4);
+            cur = sb;
+            acc0 = V4<double>(0.0);
+            accb = V4<double>(0.0);
+        }
+        const V4<double> u = (double)spou[l] * to_d(ld4(r + (size_t)gidx[l] * kp + c4));
+        acc0 += u;
+        accb += (double)invd[l] * u;
+    }
+    if (cur != 0xffffffffu) seg.flush(S0, SB, cur, acc0, accb, c4);
+    seg.finish(S0, SB);
+}
+
+// Keep slots, in keep-list order: v[k] = u_k - m0 - m0 rho_k (the base of the reduced rhs).
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) keep_init_kernel(int64_t nkeep, const uint32_t* __restrict__ keep_slots,
+                                                           const uint32_t* __restrict__ gidx, const T* __restrict__ spou,
+                                                           const T* __restrict__ rho, const uint32_t* __restrict__ sub_of,
+                                                           const int32_t* __restrict__ sub_n,
+                                                           const double* __restrict__ S0, const T* __restrict__ r,
+                                                           T* __restrict__ v, int kp) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
     const int64_t rpb = blockDim.x / G;
-    for (int64_t a = (int64_t)blockIdx.x * rpb + threadIdx.x / G; a < nslots; a += (int64_t)gridDim.x * rpb) {
-        const uint32_t l = slot_list ? slot_list[a] : (uint32_t)a;
+    for (int64_t a = (int64_t)blockIdx.x * rpb + threadIdx.x / G; a < nkeep; a += (int64_t)gridDim.x * rpb) {
+        const uint32_t l = keep_slots[a];
         const uint32_t s = sub_of[l];
-        const double mean = msum[(size_t)s * k + c] / (double)sub_n[s];
-        T x = (T)((double)v[(size_t)l * k + c] - mean);
-        if (scale) x *= scale[l];
-        v[(size_t)l * k + c] = x;
+        const double inv_n = 1.0 / (double)sub_n[s];
+        const size_t o = (size_t)s * kp + c4;
+        const V4<double> m0 = inv_n * V4<double>(S0[o], S0[o + 1], S0[o + 2], S0[o + 3]);
+        const V4<double> u = (double)spou[l] * to_d(ld4(r + (size_t)gidx[l] * kp + c4));
+        st4(v + (size_t)l * kp + c4, from_d<T>(u - m0 - (double)rho[a] * m0));
+    }
+}
+
+// Keep-list segmented sums: M[s] += v[k] * (1 + rho_k if with_rho), block-reduced.
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) keep_sum_kernel(int64_t nkeep, int spb, const uint32_t* __restrict__ keep_slots,
+                                                          const T* __restrict__ rho, int with_rho,
+                                                          const uint32_t* __restrict__ sub_of,
+                                                          const T* __restrict__ v, int kp, double* __restrict__ M) {
+    __shared__ double sm[2 * 2 * 32];
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const int64_t b0 = (int64_t)blockIdx.x * spb, b1 = min(nkeep, b0 + spb);
+    if (b0 >= nkeep) return;  // uniform per block
+    for (int i = threadIdx.x; i < 4 * kp; i += blockDim.x) sm[i] = 0.0;
+    SegSum seg{sm, sub_of[keep_slots[b0]], sub_of[keep_slots[b1 - 1]], kp};
+    __syncthreads();
+    const int gpb = blockDim.x / G, g = threadIdx.x / G;
+    const int64_t per = (spb + gpb - 1) / gpb;
+    const int64_t a0 = b0 + g * per, a1 = min(b1, a0 + per);
+    uint32_t cur = 0xffffffffu;
+    V4<double> acc(0.0);
+    for (int64_t a = a0; a < a1; ++a) {
+        const uint32_t l = keep_slots[a];
+        const uint32_t sb = sub_of[l];
+        if (sb != cur) {
+            if (cur != 0xffffffffu) seg.flush(M, nullptr, cur, acc, acc, c4);
+            cur = sb;
+            acc = V4<double>(0.0);
+        }
+        const double f = with_rho ? 1.0 + (double)rho[a] : 1.0;
+        acc += f * to_d(ld4(v + (size_t)l * kp + c4));
+    }
+    if (cur != 0xffffffffu) seg.flush(M, nullptr, cur, acc, acc, c4);
+    seg.finish(M, nullptr);
+}
+
+// v[k] -= M1[s] / n_keep[s] over the keep list.
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) keep_center_kernel(int64_t nkeep, const uint32_t* __restrict__ keep_slots,
+                                                             const uint32_t* __restrict__ sub_of,
+                                                             const int32_t* __restrict__ sub_nkeep,
+                                                             const double* __restrict__ M1, T* __restrict__ v, int kp) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t a = (int64_t)blockIdx.x * rpb + threadIdx.x / G; a < nkeep; a += (int64_t)gridDim.x * rpb) {
+        const uint32_t l = keep_slots[a];
+        const uint32_t s = sub_of[l];
+        const double inv = 1.0 / (double)sub_nkeep[s];
+        const size_t o = (size_t)s * kp + c4;
+        const V4<double> m(M1[o] * inv, M1[o + 1] * inv, M1[o + 2] * inv, M1[o + 3] * inv);
+        T* p = v + (size_t)l * kp + c4;
+        st4(p, from_d<T>(to_d(ld4(p)) - m));
+    }
+}
+
+// Solution of slot l of a stage: kept slots read v; eliminated slots back-substitute
+// from the kept solution (sol_e = invd_e (u_e - m0) + invd_e sum_k C_ek v_k).
+template <typename T>
+__device__ __forceinline__ V4<double> slot_solution(uint32_t l, const V4<double>& u, const V4<double>& m0, T invd,
+                                                    const int64_t* __restrict__ bs_ptr,
+                                                    const uint32_t* __restrict__ bs_col,
+                                                    const T* __restrict__ bs_val, const T* __restrict__ v, int kp,
+                                                    int c4) {
+    if (invd == T(0)) return to_d(ld4(v + (size_t)l * kp + c4));
+    V4<T> acc(T(0));
+    const int64_t e0 = bs_ptr[l], e1 = bs_ptr[l + 1];
+    int64_t e = e0;
+    for (; e + 2 <= e1; e += 2) {
+        const uint32_t j0 = __ldg(bs_col + e), j1 = __ldg(bs_col + e + 1);
+        const T v0 = __ldg(bs_val + e), v1 = __ldg(bs_val + e + 1);
+        const V4<T> s0 = ld4(v + (size_t)j0 * kp + c4), s1 = ld4(v + (size_t)j1 * kp + c4);
+        acc += v0 * s0;
+        acc += v1 * s1;
+    }
+    if (e < e1) acc += __ldg(bs_val + e) * ld4(v + (size_t)__ldg(bs_col + e) * kp + c4);
+    const double id = (double)invd;
+    return id * (u - m0) + id * to_d(acc);
+}
+
+struct SubMeans {
+    const int32_t* sub_n;
+    const double *S0, *SB, *M2, *I;
+};
+__device__ __forceinline__ void sub_means(const SubMeans& M, uint32_t s, int kp, int c4, V4<double>& m0, V4<double>& m2) {
+    const double inv = 1.0 / (double)M.sub_n[s];
+    const double I = M.I[s];
+    const size_t o = (size_t)s * kp + c4;
+    m0 = V4<double>(M.S0[o], M.S0[o + 1], M.S0[o + 2], M.S0[o + 3]);
+    m0 *= inv;
+    const V4<double> sb(M.SB[o], M.SB[o + 1], M.SB[o + 2], M.SB[o + 3]);
+    const V4<double> k2(M.M2[o], M.M2[o + 1], M.M2[o + 2], M.M2[o + 3]);
+    m2 = inv * (k2 + sb - I * m0);
+}
+
+// Additive prolongation as a gather over global dofs (no atomics), with the back
+// substitution of eliminated slots folded in: z[j] = sum_{slots l of j} spou_l (sol_l - m2).
+// Dofs in no subdomain get z = 0.  Optionally the partial dot r.z for CG.
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) prolong_kernel(int64_t m, const int64_t* __restrict__ gptr,
+                                                         const uint32_t* __restrict__ gslot,
+                                                         const uint32_t* __restrict__ sub_of,
+                                                         const T* __restrict__ spou, const T* __restrict__ invd,
+                                                         const int64_t* __restrict__ bs_ptr,
+                                                         const uint32_t* __restrict__ bs_col,
+                                                         const T* __restrict__ bs_val, SubMeans M,
+                                                         const T* __restrict__ v, const T* __restrict__ r,
+                                                         T* __restrict__ z, int kp, double* __restrict__ part) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    V4<double> dotp(0.0);
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t j = (int64_t)blockIdx.x * rpb + threadIdx.x / G; j < m; j += (int64_t)gridDim.x * rpb) {
+        const V4<double> rj = to_d(ld4(r + (size_t)j * kp + c4));
+        V4<double> acc(0.0);
+        for (int64_t e = gptr[j]; e < gptr[j + 1]; ++e) {
+            const uint32_t l = gslot[e];
+            const uint32_t s = sub_of[l];
+            V4<double> m0, m2;
+            sub_means(M, s, kp, c4, m0, m2);
+            const double sp = (double)spou[l];
+            const V4<double> sol = slot_solution<T>(l, sp * rj, m0, invd[l], bs_ptr, bs_col, bs_val, v, kp, c4);
+            acc += sp * (sol - m2);
+        }
+        const V4<T> zt = from_d<T>(acc);
+        st4(z + (size_t)j * kp + c4, zt);
+        const V4<double> zd = to_d(zt);
+        dotp.a += rj.a * zd.a; dotp.b += rj.b * zd.b; dotp.c += rj.c * zd.c; dotp.d += rj.d * zd.d;
+    }
+    if (part) block_reduce_store4<G>(dotp, kp, part);
+}
+
+// Multiplicative stage, part 1: c_l = spou_l (sol_l - m2) into cbuf, z[gidx_l] += c_l
+// (dofs are unique within one factor-pair stage).
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) mult_sol_kernel(int64_t nslots, const uint32_t* __restrict__ gidx,
+                                                          const uint32_t* __restrict__ sub_of,
+                                                          const T* __restrict__ spou, const T* __restrict__ invd,
+                                                          const int64_t* __restrict__ bs_ptr,
+                                                          const uint32_t* __restrict__ bs_col,
+                                                          const T* __restrict__ bs_val, SubMeans M,
+                                                          const T* __restrict__ v, const T* __restrict__ rw,
+                                                          T* __restrict__ z, T* __restrict__ cbuf, int kp) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t l = (int64_t)blockIdx.x * rpb + threadIdx.x / G; l < nslots; l += (int64_t)gridDim.x * rpb) {
+        const uint32_t g = gidx[l];
+        const uint32_t s = sub_of[l];
+        V4<double> m0, m2;
+        sub_means(M, s, kp, c4, m0, m2);
+        const double sp = (double)spou[l];
+        const V4<double> u = sp * to_d(ld4(rw + (size_t)g * kp + c4));
+        const V4<double> sol = slot_solution<T>((uint32_t)l, u, m0, invd[l], bs_ptr, bs_col, bs_val, v, kp, c4);
+        const V4<T> cl = from_d<T>(sp * (sol - m2));
+        st4(cbuf + (size_t)l * kp + c4, cl);
+        T* zp = z + (size_t)g * kp + c4;
+        st4(zp, ld4(zp) + cl);
+    }
+}
+// Multiplicative stage, part 2: r_work -= G[:, gidx_l] c_l (residual_update.rs:36-53).
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) mult_resid_kernel(int64_t nslots, const uint32_t* __restrict__ gidx,
+                                                            const T* __restrict__ cbuf,
+                                                            const int64_t* __restrict__ gram_ptr,
+                                                            const uint32_t* __restrict__ gram_col,
+                                                            const T* __restrict__ gram_val, T* __restrict__ rw, int kp) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t l = (int64_t)blockIdx.x * rpb + threadIdx.x / G; l < nslots; l += (int64_t)gridDim.x * rpb) {
+        const V4<T> cl = ld4(cbuf + (size_t)l * kp + c4);
+        if (!cl.any()) continue;
+        const uint32_t g = gidx[l];
+        for (int64_t e = gram_ptr[g]; e < gram_ptr[g + 1]; ++e)
+            atomic_add4(rw + (size_t)gram_col[e] * kp + c4, (-__ldg(gram_val + e)) * cl);
     }
 }
 
@@ -439,22 +697,22 @@ __global__ void __launch_bounds__(kBlock) center_scale_kernel(const uint32_t* __
 template <typename T>
 __global__ void dense_solve_kernel(int32_t ndense, const int64_t* __restrict__ keep0,
                                    const int32_t* __restrict__ nkeep, const int64_t* __restrict__ loff,
-                                   const T* __restrict__ L, T* __restrict__ v, int k) {
+                                   const T* __restrict__ L, T* __restrict__ v, int kp) {
     const int warp = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
-    if (warp >= ndense * k) return;  // uniform per warp
-    const int d = warp / k, c = warp % k;
+    if (warp >= ndense * kp) return;  // uniform per warp
+    const int d = warp / kp, c = warp % kp;
     const int n = nkeep[d];
     const int64_t s0 = keep0[d];
     if (n == 0) return;
     if (n == 1) {
-        if (lane == 0) v[(size_t)s0 * k + c] = T(0);
+        if (lane == 0) v[(size_t)s0 * kp + c] = T(0);
         return;
     }
     const int m = n - 1;
     const T* Ld = L + loff[d];
     if (m <= 32) {
-        T xi = (lane < m) ? v[(size_t)(s0 + lane) * k + c] : T(0);
+        T xi = (lane < m) ? v[(size_t)(s0 + lane) * kp + c] : T(0);
         for (int j = 0; j < m; ++j) {  // forward L y = b
             T xj = __shfl_sync(0xffffffffu, xi, j);
             xj = xj / Ld[(size_t)j * m + j];
@@ -467,25 +725,25 @@ __global__ void dense_solve_kernel(int32_t ndense, const int64_t* __restrict__ k
             if (lane == j) xi = xj;
             if (lane < j) xi -= Ld[(size_t)j * m + lane] * xj;
         }
-        if (lane < m) v[(size_t)(s0 + lane) * k + c] = xi;
+        if (lane < m) v[(size_t)(s0 + lane) * kp + c] = xi;
     } else {
-        T* x = v + (size_t)s0 * k + c;  // element i at x[i*k]
+        T* x = v + (size_t)s0 * kp + c;  // element i at x[i*kp]
         for (int j = 0; j < m; ++j) {
-            const T xj = x[(size_t)j * k] / Ld[(size_t)j * m + j];
+            const T xj = x[(size_t)j * kp] / Ld[(size_t)j * m + j];
             __syncwarp();
-            if (lane == 0) x[(size_t)j * k] = xj;
-            for (int i = j + 1 + lane; i < m; i += 32) x[(size_t)i * k] -= Ld[(size_t)i * m + j] * xj;
+            if (lane == 0) x[(size_t)j * kp] = xj;
+            for (int i = j + 1 + lane; i < m; i += 32) x[(size_t)i * kp] -= Ld[(size_t)i * m + j] * xj;
             __syncwarp();
         }
         for (int j = m - 1; j >= 0; --j) {
-            const T xj = x[(size_t)j * k] / Ld[(size_t)j * m + j];
+            const T xj = x[(size_t)j * kp] / Ld[(size_t)j * m + j];
             __syncwarp();
-            if (lane == 0) x[(size_t)j * k] = xj;
-            for (int i = lane; i < j; i += 32) x[(size_t)i * k] -= Ld[(size_t)j * m + i] * xj;
+            if (lane == 0) x[(size_t)j * kp] = xj;
+            for (int i = lane; i < j; i += 32) x[(size_t)i * kp] -= Ld[(size_t)j * m + i] * xj;
             __syncwarp();
         }
     }
-    if (lane == 0) v[(size_t)(s0 + m) * k + c] = T(0);
+    if (lane == 0) v[(size_t)(s0 + m) * kp + c] = T(0);
 }
 
 // Dense core of an AC factor: v[core] = Z v[core] (anchored inverse), RHS [c0, c0+kc).
@@ -497,15 +755,15 @@ __global__ void core_gemv_kernel(const int32_t* __restrict__ core_of_block, cons
                                  const int32_t* __restrict__ core_n, const int64_t* __restrict__ core_slot_off,
                                  const uint32_t* __restrict__ core_slot, const int64_t* __restrict__ core_z_off,
                                  const T* __restrict__ Z, const T* __restrict__ v, T* __restrict__ tmp,
-                                 int k, int c0, int kc, int rows_per_block) {
-    extern __shared__ unsigned char smem_raw[];
+                                 int kp, int c0, int kc, int rows_per_block) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     T* yc = reinterpret_cast<T*>(smem_raw);
     const int g = core_of_block[blockIdx.x];
     const int r = core_n[g];
     const uint32_t* slots = core_slot + core_slot_off[g];
     for (int e = threadIdx.x; e < r * kc; e += blockDim.x) {
         const int c = e / r, a = e % r;
-        yc[e] = v[(size_t)slots[a] * k + c0 + c];
+        yc[e] = v[(size_t)slots[a] * kp + c0 + c];
     }
     __syncthreads();
     const T* Zg = Z + core_z_off[g];
@@ -528,79 +786,18 @@ __global__ void core_gemv_kernel(const int32_t* __restrict__ core_of_block, cons
             if (c >= kc) break;
             T a = acc[c];
             for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-            if (lane == 0) tmp[(size_t)(core_slot_off[g] + row) * k + c0 + c] = a;
+            if (lane == 0) tmp[(size_t)(core_slot_off[g] + row) * kp + c0 + c] = a;
         }
     }
 }
 
 template <typename T>
 __global__ void core_writeback_kernel(int64_t total, const uint32_t* __restrict__ core_slot,
-                                      const T* __restrict__ tmp, T* __restrict__ v, int k) {
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total * k; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t a = e / k;
-        const int c = (int)(e % k);
-        v[(size_t)core_slot[a] * k + c] = tmp[e];
-    }
-}
-
-// Additive prolongation as a gather over global dofs (no atomics):
-// z[j] = sum_{slots l of j} spou[l] * (v[l] - msum[s(l)]/n_s), optionally with the
-// partial dot r.z for CG.  Dofs in no subdomain get z = 0.
-template <typename T, int G>
-__global__ void __launch_bounds__(kBlock) prolong_gather_kernel(int64_t m, const int64_t* __restrict__ gptr,
-                                                                const uint32_t* __restrict__ gslot,
-                                                                const uint32_t* __restrict__ sub_of,
-                                                                const int32_t* __restrict__ sub_n,
-                                                                const T* __restrict__ spou,
-                                                                const double* __restrict__ msum,
-                                                                const T* __restrict__ v, T* __restrict__ z,
-                                                                const T* __restrict__ rdot, int k,
-                                                                double* __restrict__ part) {
-    const int c = threadIdx.x & (G - 1);
-    double s = 0.0;
-    if (c < k) {
-        const int64_t rpb = blockDim.x / G;
-        for (int64_t j = (int64_t)blockIdx.x * rpb + threadIdx.x / G; j < m; j += (int64_t)gridDim.x * rpb) {
-            double acc = 0.0;
-            for (int64_t e = gptr[j]; e < gptr[j + 1]; ++e) {
-                const uint32_t l = gslot[e];
-                const uint32_t sb = sub_of[l];
-                const double mean = msum[(size_t)sb * k + c] / (double)sub_n[sb];
-                acc += (double)spou[l] * ((double)v[(size_t)l * k + c] - mean);
-            }
-            const T zv = (T)acc;
-            z[(size_t)j * k + c] = zv;
-            if (rdot) s += (double)rdot[(size_t)j * k + c] * (double)zv;
-        }
-    }
-    if (part) block_reduce_store<G>(s, k, part);
-}
-
-// Multiplicative stage: z[gidx[l]] += c_l and r_work -= G[:, gidx[l]] * c_l with
-// c_l = spou[l] * (v[l] - mean) (multiplicative.rs:128-168, residual_update.rs:36-53).
-template <typename T, int G>
-__global__ void __launch_bounds__(kBlock) mult_update_kernel(int64_t nslots, const uint32_t* __restrict__ gidx,
-                                                             const uint32_t* __restrict__ sub_of,
-                                                             const int32_t* __restrict__ sub_n,
-                                                             const T* __restrict__ spou,
-                                                             const double* __restrict__ msum,
-                                                             const T* __restrict__ v, T* __restrict__ z,
-                                                             const int64_t* __restrict__ gram_ptr,
-                                                             const uint32_t* __restrict__ gram_col,
-                                                             const T* __restrict__ gram_val,
-                                                             T* __restrict__ rwork, int k) {
-    const int c = threadIdx.x & (G - 1);
-    if (c >= k) return;
-    const int64_t rpb = blockDim.x / G;
-    for (int64_t l = (int64_t)blockIdx.x * rpb + threadIdx.x / G; l < nslots; l += (int64_t)gridDim.x * rpb) {
-        const uint32_t sb = sub_of[l];
-        const double mean = msum[(size_t)sb * k + c] / (double)sub_n[sb];
-        const T cl = (T)((double)spou[l] * ((double)v[(size_t)l * k + c] - mean));
-        const uint32_t g = gidx[l];
-        z[(size_t)g * k + c] += cl;  // dofs are unique within one stage
-        if (cl == T(0)) continue;
-        for (int64_t e = gram_ptr[g]; e < gram_ptr[g + 1]; ++e)
-            atomic_add(rwork + (size_t)gram_col[e] * k + c, -cl * gram_val[e]);
+                                      const T* __restrict__ tmp, T* __restrict__ v, int kp) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total * kp; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = e / kp;
+        const int c = (int)(e % kp);
+        v[(size_t)core_slot[a] * kp + c] = tmp[e];
     }
 }
 

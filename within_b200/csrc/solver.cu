@@ -5,14 +5,15 @@
 
 #include <algorithm>
 #include <chrono>
-#include <functional>
-#include <type_traits>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/within_b200.h"
@@ -30,16 +31,7 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
-int pow2ceil(int k) {
-    int g = 1;
-    while (g < k) g <<= 1;
-    return g;
-}
-int group_width(int k) {  // 1, 4, 8, 16 or 32 lanes per row
-    int g = pow2ceil(k);
-    if (g == 2) g = 4;
-    return g;
-}
+int pad4(int k) { return (k + 3) & ~3; }
 
 double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -69,21 +61,13 @@ std::vector<CsrChunk> make_chunks(const std::vector<int64_t>& ptr, int64_t row_l
     return out;
 }
 
-void csr_add_row(CsrHost& c, uint32_t slot, double rscale) {
-    c.row_slot.push_back(slot);
-    c.rscale.push_back(rscale);
-}
-void csr_end_row(CsrHost& c) { c.ptr.push_back((int64_t)c.col.size()); }
-
-// Flatten the subdomains `ids` into one stage (see StageHost).
+// Flatten the subdomains `ids` into one stage (see StageHost and kernels.cuh).
 StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int32_t>& ids, int64_t ndofs,
                       bool with_gather) {
     StageHost st;
     st.nsub = (int32_t)ids.size();
-    struct AcRows {
-        std::vector<std::vector<std::pair<uint32_t, std::vector<std::pair<uint32_t, double>>>>> fwd;  // per level
-        std::vector<std::vector<std::tuple<uint32_t, double, std::vector<std::pair<uint32_t, double>>>>> bwd;
-    } ac;
+    std::vector<std::vector<std::pair<uint32_t, std::vector<std::pair<uint32_t, double>>>>> afwd;
+    std::vector<std::vector<std::tuple<uint32_t, double, std::vector<std::pair<uint32_t, double>>>>> abwd;
     int64_t o = 0;
     for (int32_t si = 0; si < st.nsub; ++si) {
         const Subdomain& sd = subs[ids[si]];
@@ -92,32 +76,46 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
         const int32_t n_keep = sd.elim_q ? nr : nq, n_elim = sd.elim_q ? nq : nr;
         st.sub_nloc.push_back(nl);
         st.sub_nkeep.push_back(n_keep);
+        double I = 0.0;
+        for (int32_t e = 0; e < n_elim; ++e) I += sd.inv_diag[e];
+        st.sub_I.push_back(I);
         for (int32_t a = 0; a < nl; ++a) {
             st.gidx.push_back(sd.gidx[a]);
             st.sub_of.push_back((uint32_t)si);
             const double pw = sd.pou.empty() ? 1.0 : sd.pou[a];
             st.spou.push_back(a < nq ? pw : -pw);  // r-block sign flip (local_solver.rs:83-87, 362, 447)
-            st.scale.push_back(1.0);
+            st.invd.push_back(0.0);
         }
-        for (int32_t e = 0; e < n_elim; ++e) st.scale[elim0 + e] = sd.inv_diag[e];
+        for (int32_t e = 0; e < n_elim; ++e) st.invd[elim0 + e] = sd.inv_diag[e];
         const Csr& k2e = sd.elim_q ? sd.ct.ct : sd.ct.c;
         const Csr& e2k = sd.elim_q ? sd.ct.c : sd.ct.ct;
-        for (int32_t i = 0; i < n_keep; ++i) {  // reduced rhs rows (local_solver.rs:374-381, 410-417)
+        // reduced rhs rows (local_solver.rs:374-381, 410-417), premultiplied by the restriction
+        for (int32_t i = 0; i < n_keep; ++i) {
             st.keep_slots.push_back((uint32_t)(keep0 + i));
-            csr_add_row(st.keep, (uint32_t)(keep0 + i), 1.0);
+            st.keep.row_slot.push_back((uint32_t)(keep0 + i));
+            st.keep.rscale.push_back(1.0);
+            double rho = 0.0;
             for (uint32_t e = k2e.ptr[i]; e < k2e.ptr[i + 1]; ++e) {
-                st.keep.col.push_back((uint32_t)(elim0 + k2e.idx[e]));
-                st.keep.val.push_back(k2e.val[e]);
+                const int64_t es = elim0 + k2e.idx[e];
+                const double ci = k2e.val[e] * sd.inv_diag[k2e.idx[e]];
+                rho += ci;
+                st.keep.col.push_back(st.gidx[es]);
+                st.keep.val.push_back(ci * st.spou[es]);
             }
-            csr_end_row(st.keep);
+            st.rho.push_back(rho);
+            st.keep.ptr.push_back((int64_t)st.keep.col.size());
         }
-        for (int32_t e = 0; e < n_elim; ++e) {  // back substitution rows (local_solver.rs:111-151)
-            csr_add_row(st.elim, (uint32_t)(elim0 + e), sd.inv_diag[e]);
-            for (uint32_t x = e2k.ptr[e]; x < e2k.ptr[e + 1]; ++x) {
-                st.elim.col.push_back((uint32_t)(keep0 + e2k.idx[x]));
-                st.elim.val.push_back(e2k.val[x]);
+        // back substitution rows over all slots of the subdomain (local_solver.rs:111-151)
+        for (int32_t a = 0; a < nl; ++a) {
+            const int64_t l = o + a;
+            if (l >= elim0 && l < elim0 + n_elim) {
+                const int32_t e = (int32_t)(l - elim0);
+                for (uint32_t x = e2k.ptr[e]; x < e2k.ptr[e + 1]; ++x) {
+                    st.bs_col.push_back((uint32_t)(keep0 + e2k.idx[x]));
+                    st.bs_val.push_back(e2k.val[x]);
+                }
             }
-            csr_end_row(st.elim);
+            st.bs_ptr.push_back((int64_t)st.bs_col.size());
         }
         if (sd.kind == 0) {
             st.dn_keep0.push_back(keep0);
@@ -126,10 +124,10 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
             st.dn_L.insert(st.dn_L.end(), sd.L.begin(), sd.L.end());
         } else {
             const AcFactor& f = sd.ac;
-            if ((int32_t)ac.fwd.size() < f.nlev) { ac.fwd.resize(f.nlev); ac.bwd.resize(f.nlev); }
-            for (int32_t l = 0; l < f.nlev; ++l) {
+            if ((int32_t)afwd.size() < f.nlev) { afwd.resize(f.nlev); abwd.resize(f.nlev); }
+            for (int32_t lv = 0; lv < f.nlev; ++lv) {
                 std::vector<std::tuple<uint32_t, uint32_t, double>> trip;  // (target, source, coef)
-                for (int32_t c = f.level_ptr[l]; c < f.level_ptr[l + 1]; ++c) {
+                for (int32_t c = f.level_ptr[lv]; c < f.level_ptr[lv + 1]; ++c) {
                     const uint32_t v = (uint32_t)(keep0 + f.col_vertex[c]);
                     std::vector<std::pair<uint32_t, double>> ent;
                     for (int32_t e = f.col_ptr[c]; e < f.col_ptr[c + 1]; ++e) {
@@ -137,8 +135,8 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
                         ent.push_back({u, f.col_coef[e]});
                         trip.emplace_back(u, v, f.col_coef[e]);
                     }
-                    const double d = f.col_diag[c];
-                    ac.bwd[l].emplace_back(v, d > 0.0 ? 1.0 / d : 0.0, std::move(ent));
+                    const double dd = f.col_diag[c];
+                    abwd[lv].emplace_back(v, dd > 0.0 ? 1.0 / dd : 0.0, std::move(ent));
                 }
                 std::stable_sort(trip.begin(), trip.end(), [](const auto& a, const auto& b) {
                     return std::get<0>(a) != std::get<0>(b) ? std::get<0>(a) < std::get<0>(b)
@@ -151,7 +149,7 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
                         ent.push_back({std::get<1>(trip[a]), std::get<2>(trip[a])});
                         ++a;
                     }
-                    ac.fwd[l].push_back({u, std::move(ent)});
+                    afwd[lv].push_back({u, std::move(ent)});
                 }
             }
             if (f.ncore > 0) {
@@ -173,28 +171,29 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
     // level-major AC rows: fwd (targets, may split) and bwd (columns, never split)
     st.fwd_lp.push_back(0);
     st.bwd_lp.push_back(0);
-    for (size_t l = 0; l < ac.fwd.size(); ++l) {
+    for (size_t lv = 0; lv < afwd.size(); ++lv) {
         const int64_t r0 = st.fwd.nrows();
-        for (auto& row : ac.fwd[l]) {
-            csr_add_row(st.fwd, row.first, 1.0);
+        for (auto& row : afwd[lv]) {
+            st.fwd.row_slot.push_back(row.first);
+            st.fwd.rscale.push_back(1.0);
             for (auto& e : row.second) { st.fwd.col.push_back(e.first); st.fwd.val.push_back(e.second); }
-            csr_end_row(st.fwd);
+            st.fwd.ptr.push_back((int64_t)st.fwd.col.size());
         }
-        auto fc = make_chunks(st.fwd.ptr, r0, st.fwd.nrows(), 256, 32, true);
+        auto fc = make_chunks(st.fwd.ptr, r0, st.fwd.nrows(), 64, 4, true);
         st.fwd.chunks.insert(st.fwd.chunks.end(), fc.begin(), fc.end());
         st.fwd_lp.push_back((int64_t)st.fwd.chunks.size());
         const int64_t b0 = st.bwd.nrows();
-        for (auto& row : ac.bwd[l]) {
-            csr_add_row(st.bwd, std::get<0>(row), std::get<1>(row));
+        for (auto& row : abwd[lv]) {
+            st.bwd.row_slot.push_back(std::get<0>(row));
+            st.bwd.rscale.push_back(std::get<1>(row));
             for (auto& e : std::get<2>(row)) { st.bwd.col.push_back(e.first); st.bwd.val.push_back(e.second); }
-            csr_end_row(st.bwd);
+            st.bwd.ptr.push_back((int64_t)st.bwd.col.size());
         }
-        auto bc = make_chunks(st.bwd.ptr, b0, st.bwd.nrows(), 256, 32, false);
+        auto bc = make_chunks(st.bwd.ptr, b0, st.bwd.nrows(), 64, 4, false);
         st.bwd.chunks.insert(st.bwd.chunks.end(), bc.begin(), bc.end());
         st.bwd_lp.push_back((int64_t)st.bwd.chunks.size());
     }
-    st.keep.chunks = make_chunks(st.keep.ptr, 0, st.keep.nrows(), 256, 32, true);
-    st.elim.chunks = make_chunks(st.elim.ptr, 0, st.elim.nrows(), 256, 32, true);
+    st.keep.chunks = make_chunks(st.keep.ptr, 0, st.keep.nrows(), 256, 8, true);
     if (with_gather) {
         st.gptr.assign((size_t)ndofs + 1, 0);
         for (uint32_t g : st.gidx) st.gptr[g + 1]++;
@@ -227,13 +226,17 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
     d.sub_of.upload(h.sub_of);
     d.keep_slots.upload(h.keep_slots);
     d.spou.upload_cast(h.spou);
-    d.scale.upload_cast(h.scale);
+    d.invd.upload_cast(h.invd);
+    d.rho.upload_cast(h.rho);
     d.sub_nloc.upload(h.sub_nloc);
     d.sub_nkeep.upload(h.sub_nkeep);
+    d.sub_I.upload(h.sub_I);
     upload_csr(d.keep, h.keep);
-    upload_csr(d.elim, h.elim);
     upload_csr(d.fwd, h.fwd);
     upload_csr(d.bwd, h.bwd);
+    d.bs_ptr.upload(h.bs_ptr);
+    d.bs_col.upload(h.bs_col);
+    d.bs_val.upload_cast(h.bs_val);
     d.fwd_lp = h.fwd_lp;
     d.bwd_lp = h.bwd_lp;
     d.ndense = (int32_t)h.dn_n.size();
@@ -262,19 +265,20 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
 // ---------------------------------------------------------------------------
 
 struct Workspace {
-    int k = 0;
-    DArr<double> yi, e;          // n x k interleaved (primary-sorted)
-    DArr<double> b, x, r, gx;    // m x k FP64: rhs, solution, refinement residual, G x
-    DArr<double> cx, cr, dz, dp, dap;           // FP64 inner CG vectors
-    DArr<float> frhs, fx, fr, fz, fp, fap;      // FP32 inner CG vectors (mixed precision)
-    DArr<double> vloc;           // slots x k (FP64 local vectors)
-    DArr<float> floc;            // slots x k (FP32)
+    int kp = 0;
+    DArr<double> yi, e;                      // n x kp interleaved (primary-sorted)
+    DArr<double> b, x, r, gx;                // m x kp FP64: rhs, solution, refinement residual, G x
+    DArr<double> cx, cr, dz, dp, dap;        // FP64 inner CG vectors
+    DArr<float> frhs, fx, fr, fz, fp, fap;   // FP32 inner CG vectors (mixed precision)
+    DArr<double> vloc, cbuf;                 // slots x kp (FP64)
+    DArr<float> floc, fcbuf;                 // slots x kp (FP32)
     DArr<double> core_tmp;
     DArr<float> fcore_tmp;
-    DArr<double> rwork;          // multiplicative residual
+    DArr<double> rwork;                      // multiplicative residual
     DArr<float> frwork;
-    DArr<double> msum;           // 3 x nsub x k
-    DArr<double> part;           // partial sums
+    DArr<double> msum;                       // 4 x nsub x kp: S0, SB, M1, M2
+    DArr<double> part;                       // block partial sums
+    DArr<double> red;                        // reduced partial sums (kp)
     // per-RHS Krylov state
     DArr<double> st_bnorm, st_rz, st_rz0, st_alpha, st_beta, st_rnorm, st_tol;
     DArr<int32_t> st_active, st_conv, st_iters, st_part;
@@ -297,14 +301,12 @@ struct SolverImpl {
     DArr<float> w32;
     DArr<ObsChunk> chunks;
     ObsParams obs{};
-    // hottest levels of every non-primary factor (by observation count), for the
-    // shared-memory accumulators of the observation pass
+    bool has_split = false;
+    // hottest levels of every non-primary factor, for the observation pass
     std::vector<DArr<int32_t>> hot_slot;
     std::vector<DArr<uint32_t>> hot_level;
     std::vector<int32_t> hot_count;
-    bool has_split = false;
     // Schwarz stages
-    std::vector<StageHost> hstages;
     std::vector<StageDev<double>> stages64;
     std::vector<StageDev<float>> stages32;
     int32_t max_nsub = 0;
@@ -326,6 +328,19 @@ struct SolverImpl {
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
     int64_t prof_count[4] = {0, 0, 0, 0};
     double prof_ms[4] = {0, 0, 0, 0};
+
+    ~SolverImpl() {
+        for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+        if (h_active) cudaFreeHost(h_active);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    bool mixed() const { return params.precision == WITHIN_PRECISION_MIXED; }
+    // blocks for a grid-stride pass over `rows` rows with G lanes per row
+    int nblk(int64_t rows, int G, int cap_per_sm = 8) const {
+        const int64_t need = (rows * G + kBlock - 1) / kBlock;
+        return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)n_sm * cap_per_sm));
+    }
     cudaEvent_t take_event() {
         if (ev_pool.empty()) {
             cudaEvent_t e;
@@ -336,11 +351,10 @@ struct SolverImpl {
         ev_pool.pop_back();
         return e;
     }
-    void prof_begin(int which, cudaEvent_t& a) {
+    void prof_begin(cudaEvent_t& a) {
         if (!profiling) return;
         a = take_event();
         WB_CUDA(cudaEventRecord(a, stream));
-        (void)which;
     }
     void prof_end(int which, cudaEvent_t a) {
         if (!profiling) return;
@@ -360,25 +374,32 @@ struct SolverImpl {
         }
         ev_pending.clear();
     }
-
-    ~SolverImpl() {
-        for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
-        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
-        if (h_active) cudaFreeHost(h_active);
-        if (stream) cudaStreamDestroy(stream);
-    }
-    bool mixed() const { return params.precision == WITHIN_PRECISION_MIXED; }
-    int nblk(int64_t rows, int G) const {
-        const int64_t need = (rows * G + kBlock - 1) / kBlock;
-        return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)n_sm * 8));
-    }
 };
 
 namespace {
 
+#define WB_DISPATCH_G(G, ...)                                      \
+    switch (G) {                                                   \
+        case 1: { constexpr int GV = 1; __VA_ARGS__; } break;      \
+        case 2: { constexpr int GV = 2; __VA_ARGS__; } break;      \
+        case 4: { constexpr int GV = 4; __VA_ARGS__; } break;      \
+        default: { constexpr int GV = 8; __VA_ARGS__; } break;     \
+    }
+
+// Lanes per row for kp RHS (kp a multiple of 4, <= 32): kp/4 rounded up to 1, 2, 4 or 8.
+// For kp in {12, 20, 24, 28} the extra lanes would own columns past kp, so those widths
+// are padded: kp is rounded to 16 or 32 by pad_kp below.
+int group_for(int kp) { return kp / 4; }
+int pad_kp(int k) {
+    const int kp = pad4(k);
+    if (kp <= 8) return kp;
+    if (kp <= 16) return 16;
+    return 32;
+}
+
 // Observation chunks over primary-sorted observations (level-aligned; long levels split).
 std::vector<ObsChunk> make_obs_chunks(const std::vector<int64_t>& lvl_ptr, int64_t nlev, bool& has_split) {
-    constexpr int64_t kObsPerChunk = 256;
+    constexpr int64_t kObsPerChunk = 128;
     std::vector<ObsChunk> out;
     has_split = false;
     int64_t l = 0;
@@ -393,7 +414,8 @@ std::vector<ObsChunk> make_obs_chunks(const std::vector<int64_t>& lvl_ptr, int64
             continue;
         }
         int64_t l1 = l + 1;
-        while (l1 < nlev && lvl_ptr[l1 + 1] - lvl_ptr[l] <= kObsPerChunk && lvl_ptr[l1 + 1] - lvl_ptr[l1] <= 2 * kObsPerChunk)
+        while (l1 < nlev && lvl_ptr[l1 + 1] - lvl_ptr[l] <= kObsPerChunk &&
+               lvl_ptr[l1 + 1] - lvl_ptr[l1] <= 2 * kObsPerChunk)
             ++l1;
         out.push_back(ObsChunk{(uint32_t)lvl_ptr[l], (uint32_t)lvl_ptr[l1], (uint32_t)l, (uint32_t)l1, 0u});
         l = l1;
@@ -441,7 +463,7 @@ void upload_design(SolverImpl& S) {
     for (int q = 0; q < d.Q; ++q) P.off[q] = d.off[q];
     P.chunks = S.chunks.p;
     P.nchunks = (int64_t)ch.size();
-    // hot levels: the kHot most frequent levels of each non-primary factor
+    // hot levels: the 256 most frequent levels (hit >= 64 times) of each non-primary factor
     constexpr int kHot = 256;
     S.hot_slot.resize(d.Q);
     S.hot_level.resize(d.Q);
@@ -460,7 +482,7 @@ void upload_design(SolverImpl& S) {
         std::vector<int32_t> slot((size_t)L, -1);
         std::vector<uint32_t> lev;
         for (int64_t a = 0; a < h; ++a) {
-            if (cnt[order[a]] < 64) break;  // only levels hit often enough to contend
+            if (cnt[order[a]] < 64) break;
             slot[order[a]] = (int32_t)lev.size();
             lev.push_back(order[a]);
         }
@@ -472,11 +494,11 @@ void upload_design(SolverImpl& S) {
     }
 }
 
-// Shared-memory regions for a given k: a non-primary factor with few levels keeps all
-// of them; a larger one keeps its hot levels; within a 40 KB budget per block.
-void obs_params_for(SolverImpl& S, int k, size_t elem, ObsParams& P) {
+// Shared-memory regions for kp RHS: a non-primary factor with <= 256 levels keeps all
+// of them, a larger one its hot levels, within a 40 KB budget per block.
+void obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
     P = S.obs;
-    P.k = k;
+    P.kp = kp;
     int32_t used = 0;
     const int32_t budget = (int32_t)(40960 / elem);
     for (int q = 0; q < S.d.Q; ++q) {
@@ -484,7 +506,7 @@ void obs_params_for(SolverImpl& S, int k, size_t elem, ObsParams& P) {
         P.smem_len[q] = 0;
         P.full[q] = 0;
         if (q == S.primary) continue;
-        const int64_t len = S.d.nlev[q] * k;
+        const int64_t len = S.d.nlev[q] * kp;
         if (S.d.nlev[q] <= 256 && used + len <= budget) {
             P.smem_base[q] = used;
             P.smem_len[q] = (int32_t)len;
@@ -494,166 +516,169 @@ void obs_params_for(SolverImpl& S, int k, size_t elem, ObsParams& P) {
     }
     for (int q = 0; q < S.d.Q; ++q) {
         if (q == S.primary || P.full[q] || S.hot_count[q] == 0) continue;
-        int32_t h = S.hot_count[q];
-        while (h > 0 && used + h * k > budget) h /= 2;
-        if (h == 0) continue;
-        // slots >= h of the hot table must fall back to global atomics: restrict the table
-        if (h < S.hot_count[q]) continue;
+        const int32_t len = S.hot_count[q] * kp;
+        if (used + len > budget) continue;  // the whole hot table or none of it
         P.smem_base[q] = used;
-        P.smem_len[q] = h * k;
-        used += h * k;
+        P.smem_len[q] = len;
+        used += len;
     }
     P.smem_elems = used;
 }
 
 template <typename T, int MODE>
-void launch_obs(SolverImpl& S, int k, const T* w, const T* x, const T* yin, T* out, T* eout) {
+void launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* out, T* eout) {
     ObsParams P;
-    obs_params_for(S, k, sizeof(T), P);
-    const int G = group_width(k);
+    obs_params_for(S, kp, sizeof(T), P);
+    const int G = group_for(kp);
     if (MODE != OBS_DX && out) {
-        // zero the outputs accumulated atomically (every non-primary factor, split levels)
+        // zero the outputs that are accumulated (every non-primary factor, split levels)
         const size_t m = (size_t)S.d.ndofs;
         if (S.has_split) {
-            WB_CUDA(cudaMemsetAsync(out, 0, m * k * sizeof(T), S.stream));
+            WB_CUDA(cudaMemsetAsync(out, 0, m * kp * sizeof(T), S.stream));
         } else {
-            const size_t a = (size_t)S.d.off[S.primary] * k, b = (size_t)(S.d.off[S.primary] + S.d.nlev[S.primary]) * k;
+            const size_t a = (size_t)S.d.off[S.primary] * kp, b = (size_t)(S.d.off[S.primary] + S.d.nlev[S.primary]) * kp;
             if (a > 0) WB_CUDA(cudaMemsetAsync(out, 0, a * sizeof(T), S.stream));
-            if (m * k > b) WB_CUDA(cudaMemsetAsync(out + b, 0, (m * k - b) * sizeof(T), S.stream));
+            if (m * kp > b) WB_CUDA(cudaMemsetAsync(out + b, 0, (m * kp - b) * sizeof(T), S.stream));
         }
     }
     const size_t smem = (size_t)P.smem_elems * sizeof(T);
-    const int64_t groups = (int64_t)P.nchunks;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((groups * G + kBlock - 1) / kBlock, (int64_t)S.n_sm * 8));
+    const int grid = S.nblk(P.nchunks, G, 4);
     auto go = [&](auto kern) {
         if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, kBlock, smem, S.stream>>>(P, w, x, yin, out, eout);
         WB_CUDA(cudaGetLastError());
         S.gpu_launches++;
     };
-#define WB_OBS_Q(GV)                                                            \
-    if (S.d.Q <= 4) go(obs_pass_kernel<T, GV, MODE, 4>);                      \
-    else go(obs_pass_kernel<T, GV, MODE, kMaxQ>);
+    constexpr int NB = std::is_same<T, float>::value ? 4 : 2;
+#define WB_OBS_Q(GV)                                                 \
+    if (S.d.Q <= 4) go(obs_pass_kernel<T, GV, MODE, 4, NB>);         \
+    else go(obs_pass_kernel<T, GV, MODE, kMaxQ, 1>);
     switch (G) {
         case 1: WB_OBS_Q(1) break;
+        case 2: WB_OBS_Q(2) break;
         case 4: WB_OBS_Q(4) break;
-        case 8: WB_OBS_Q(8) break;
-        case 16: WB_OBS_Q(16) break;
-        default: WB_OBS_Q(32) break;
+        default: WB_OBS_Q(8) break;
     }
 #undef WB_OBS_Q
 }
 
-#define WB_DISPATCH_G(G, ...)                         \
-    switch (G) {                                      \
-        case 1: { constexpr int GV = 1; __VA_ARGS__; } break;   \
-        case 4: { constexpr int GV = 4; __VA_ARGS__; } break;   \
-        case 8: { constexpr int GV = 8; __VA_ARGS__; } break;   \
-        case 16: { constexpr int GV = 16; __VA_ARGS__; } break; \
-        default: { constexpr int GV = 32; __VA_ARGS__; } break; \
-    }
-
+// Dot partials over rows (at most 2 blocks per SM: few partials to reduce).
 template <typename TA, typename TB>
-void launch_dot(SolverImpl& S, const TA* a, const TB* b, int64_t rows, int k, double* part, int& nb) {
-    const int G = group_width(k);
-    nb = S.nblk(rows, G);
-    WB_DISPATCH_G(G, dot_kernel<TA, TB, GV><<<nb, kBlock, 0, S.stream>>>(a, b, rows, k, part));
+void launch_dot(SolverImpl& S, const TA* a, const TB* b, int64_t rows, int kp, double* part, int& nb) {
+    const int G = group_for(kp);
+    nb = S.nblk(rows, G, 2);
+    WB_DISPATCH_G(G, dot_kernel<TA, TB, GV><<<nb, kBlock, 0, S.stream>>>(a, b, rows, kp, part));
     WB_CUDA(cudaGetLastError());
     S.gpu_launches++;
 }
 
-template <typename T>
-Workspace& ws_for(SolverImpl& S, int k);
+// red[c] = sum_b part[b*kp + c] (fixed order per c; deterministic).
+__global__ void reduce_parts_kernel(const double* __restrict__ part, int nb, int kp, double* __restrict__ red) {
+    __shared__ double sm[kBlock];
+    const int t = threadIdx.x;
+    const int J = blockDim.x / kp;
+    double s = 0.0;
+    if (t < J * kp) {
+        const int c = t % kp, j = t / kp;
+        for (int b = j; b < nb; b += J) s += part[(size_t)b * kp + c];
+    }
+    sm[t] = s;
+    __syncthreads();
+    if (t < kp) {
+        double a = 0.0;
+        for (int j = 0; j < J; ++j) a += sm[j * kp + t];
+        red[t] = a;
+    }
+}
 
-template <typename T>
-T* loc_buf(SolverImpl& S);
-template <>
-double* loc_buf<double>(SolverImpl& S) { return S.ws.vloc.p; }
-template <>
-float* loc_buf<float>(SolverImpl& S) { return S.ws.floc.p; }
-template <typename T>
-T* core_buf(SolverImpl& S);
-template <>
-double* core_buf<double>(SolverImpl& S) { return S.ws.core_tmp.p; }
-template <>
-float* core_buf<float>(SolverImpl& S) { return S.ws.fcore_tmp.p; }
-template <typename T>
-std::vector<StageDev<T>>& stages(SolverImpl& S);
-template <>
-std::vector<StageDev<double>>& stages<double>(SolverImpl& S) { return S.stages64; }
-template <>
-std::vector<StageDev<float>>& stages<float>(SolverImpl& S) { return S.stages32; }
-template <typename T>
-const T* gram_val(SolverImpl& S);
-template <>
-const double* gram_val<double>(SolverImpl& S) { return S.g_val64.p; }
-template <>
-const float* gram_val<float>(SolverImpl& S) { return S.g_val32.p; }
+void launch_reduce(SolverImpl& S, const double* part, int nb, int kp, double* red) {
+    reduce_parts_kernel<<<1, kBlock, 0, S.stream>>>(part, nb, kp, red);
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches++;
+}
+
+template <typename T> T* loc_buf(SolverImpl& S);
+template <> double* loc_buf<double>(SolverImpl& S) { return S.ws.vloc.p; }
+template <> float* loc_buf<float>(SolverImpl& S) { return S.ws.floc.p; }
+template <typename T> T* cbuf(SolverImpl& S);
+template <> double* cbuf<double>(SolverImpl& S) { return S.ws.cbuf.p; }
+template <> float* cbuf<float>(SolverImpl& S) { return S.ws.fcbuf.p; }
+template <typename T> T* core_buf(SolverImpl& S);
+template <> double* core_buf<double>(SolverImpl& S) { return S.ws.core_tmp.p; }
+template <> float* core_buf<float>(SolverImpl& S) { return S.ws.fcore_tmp.p; }
+template <typename T> std::vector<StageDev<T>>& stages(SolverImpl& S);
+template <> std::vector<StageDev<double>>& stages<double>(SolverImpl& S) { return S.stages64; }
+template <> std::vector<StageDev<float>>& stages<float>(SolverImpl& S) { return S.stages32; }
+template <typename T> const T* gram_val(SolverImpl& S);
+template <> const double* gram_val<double>(SolverImpl& S) { return S.g_val64.p; }
+template <> const float* gram_val<float>(SolverImpl& S) { return S.g_val32.p; }
+template <typename T> T* rwork_buf(SolverImpl& S);
+template <> double* rwork_buf<double>(SolverImpl& S) { return S.ws.rwork.p; }
+template <> float* rwork_buf<float>(SolverImpl& S) { return S.ws.frwork.p; }
 
 template <typename T, int EPI>
-void launch_csr(SolverImpl& S, CsrDev<T>& c, int64_t ch0, int64_t ch1, T* v, int k) {
+void launch_csr(SolverImpl& S, CsrDev<T>& c, int64_t ch0, int64_t ch1, const T* src, T* dst, int kp) {
     const int64_t nch = ch1 - ch0;
     if (nch <= 0) return;
-    const int G = group_width(k);
+    const int G = group_for(kp);
     const int grid = S.nblk(nch, G);
     WB_DISPATCH_G(G, csr_rows_kernel<T, GV, EPI><<<grid, kBlock, 0, S.stream>>>(
-                         c.chunks.p + ch0, nch, c.row_slot.p, c.ptr.p, c.col.p, c.val.p, c.rscale.p, v, k));
+                         c.chunks.p + ch0, nch, c.row_slot.p, c.ptr.p, c.col.p, c.val.p, c.rscale.p, src, dst, kp));
     WB_CUDA(cudaGetLastError());
     S.gpu_launches++;
 }
 
-// Local solves of one stage on the slots vector v (restricted input already in v):
-// everything between the restriction and the prolongation.
+// The local solves of one stage from the restriction input r up to the kept solution
+// in v and the subdomain sums in msum (see kernels.cuh for the algebra).
 template <typename T>
-void stage_local_solve(SolverImpl& S, StageDev<T>& st, T* v, int k, double* msum) {
-    const int G = group_width(k);
-    const int64_t L = st.nslots;
-    double* m0 = msum;
-    double* m1 = msum + (size_t)S.max_nsub * k;
-    double* m2 = msum + (size_t)2 * S.max_nsub * k;
-    WB_CUDA(cudaMemsetAsync(msum, 0, sizeof(double) * 3 * (size_t)S.max_nsub * k, S.stream));
-    const int64_t kSumChunk = 64;
-    auto slot_sum = [&](const uint32_t* list, int64_t cnt, double* out) {
-        const int64_t groups = (cnt + kSumChunk - 1) / kSumChunk;
-        const int grid = S.nblk(groups, G);
-        WB_DISPATCH_G(G, slot_sum_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(list, cnt, st.sub_of.p, v, k, out, kSumChunk));
-        WB_CUDA(cudaGetLastError());
-        S.gpu_launches++;
-    };
-    auto center = [&](const uint32_t* list, int64_t cnt, const int32_t* sub_n, const double* ms, const T* scale) {
-        const int grid = S.nblk(cnt, G);
-        WB_DISPATCH_G(G, center_scale_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(list, cnt, st.sub_of.p, sub_n, ms, scale, v, k));
-        WB_CUDA(cudaGetLastError());
-        S.gpu_launches++;
-    };
-    // subtract_mean over the subdomain, then scale eliminated slots by 1/D_elim (:366-370)
-    slot_sum(nullptr, L, m0);
-    center(nullptr, L, st.sub_nloc.p, m0, st.scale.p);
-    // reduced right-hand side: keep += C^T (scaled elim) (:374-381), then subtract_mean (:385)
-    launch_csr<T, EPI_ACC>(S, st.keep, 0, st.keep.nchunks, v, k);
-    slot_sum(st.keep_slots.p, st.nkeep, m1);
-    center(st.keep_slots.p, st.nkeep, st.sub_nkeep.p, m1, nullptr);
+SubMeans stage_local_solve(SolverImpl& S, StageDev<T>& st, const T* r, T* v, int kp) {
+    const int G = group_for(kp);
+    double* msum = S.ws.msum.p;
+    const size_t ms = (size_t)S.max_nsub * kp;
+    double *S0 = msum, *SB = msum + ms, *M1 = msum + 2 * ms, *M2 = msum + 3 * ms;
+    WB_CUDA(cudaMemsetAsync(msum, 0, sizeof(double) * 4 * ms, S.stream));
+    constexpr int kSpb = 1024;  // slots per block of the segmented sums
+    {
+        const int grid = (int)std::max<int64_t>(1, (st.nslots + kSpb - 1) / kSpb);
+        WB_DISPATCH_G(G, schwarz_sums_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(
+                             st.nslots, kSpb, st.gidx.p, st.spou.p, st.invd.p, st.sub_of.p, r, kp, S0, SB));
+    }
+    if (st.nkeep > 0) {
+        const int grid = S.nblk(st.nkeep, G);
+        WB_DISPATCH_G(G, keep_init_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(
+                             st.nkeep, st.keep_slots.p, st.gidx.p, st.spou.p, st.rho.p, st.sub_of.p, st.sub_nloc.p, S0, r,
+                             v, kp));
+        launch_csr<T, EPI_ACC>(S, st.keep, 0, st.keep.nchunks, r, v, kp);
+        const int gs = (int)std::max<int64_t>(1, (st.nkeep + kSpb - 1) / kSpb);
+        WB_DISPATCH_G(G, keep_sum_kernel<T, GV><<<gs, kBlock, 0, S.stream>>>(st.nkeep, kSpb, st.keep_slots.p, st.rho.p, 0,
+                                                                              st.sub_of.p, v, kp, M1));
+        WB_DISPATCH_G(G, keep_center_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(st.nkeep, st.keep_slots.p, st.sub_of.p,
+                                                                                 st.sub_nkeep.p, M1, v, kp));
+    }
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches += 4;
     // reduced solves: dense anchored Cholesky and approximate Cholesky sweeps
     if (st.ndense > 0) {
-        const int64_t warps = (int64_t)st.ndense * k;
+        const int64_t warps = (int64_t)st.ndense * kp;
         const int grid = (int)((warps * 32 + kBlock - 1) / kBlock);
-        dense_solve_kernel<T><<<grid, kBlock, 0, S.stream>>>(st.ndense, st.dn_keep0.p, st.dn_n.p, st.dn_loff.p, st.dn_L.p, v, k);
+        dense_solve_kernel<T><<<grid, kBlock, 0, S.stream>>>(st.ndense, st.dn_keep0.p, st.dn_n.p, st.dn_loff.p, st.dn_L.p,
+                                                             v, kp);
         WB_CUDA(cudaGetLastError());
         S.gpu_launches++;
     }
     const int nlev = (int)st.fwd_lp.size() - 1;
-    for (int l = 0; l < nlev; ++l) launch_csr<T, EPI_ACC>(S, st.fwd, st.fwd_lp[l], st.fwd_lp[l + 1], v, k);
+    for (int l = 0; l < nlev; ++l) launch_csr<T, EPI_ACC>(S, st.fwd, st.fwd_lp[l], st.fwd_lp[l + 1], v, v, kp);
     if (st.ncore_blocks > 0) {
         T* tmp = core_buf<T>(S);
-        const int kc_max = std::max(1, std::min(k, (int)(200 * 1024 / ((size_t)st.core_rmax * sizeof(T)))));
-        for (int c0 = 0; c0 < k; c0 += kc_max) {
-            const int kc = std::min(kc_max, k - c0);
+        const int kc_max = std::max(1, std::min(kp, (int)(200 * 1024 / ((size_t)st.core_rmax * sizeof(T)))));
+        for (int c0 = 0; c0 < kp; c0 += kc_max) {
+            const int kc = std::min(kc_max, kp - c0);
             const size_t smem = (size_t)st.core_rmax * kc * sizeof(T);
             auto go = [&](auto kern) {
                 if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 kern<<<st.ncore_blocks, kBlock, smem, S.stream>>>(st.core_of_block.p, st.row0_of_block.p, st.core_n.p,
                                                                  st.core_slot_off.p, st.core_slot.p, st.core_z_off.p,
-                                                                 st.core_z.p, v, tmp, k, c0, kc, kCoreRowsPerBlock);
+                                                                 st.core_z.p, v, tmp, kp, c0, kc, kCoreRowsPerBlock);
                 WB_CUDA(cudaGetLastError());
                 S.gpu_launches++;
             };
@@ -662,79 +687,71 @@ void stage_local_solve(SolverImpl& S, StageDev<T>& st, T* v, int k, double* msum
             else if (kc <= 16) go(core_gemv_kernel<T, 16>);
             else go(core_gemv_kernel<T, 32>);
         }
-        const int grid = S.nblk(st.core_total * k, 1);
-        core_writeback_kernel<T><<<grid, kBlock, 0, S.stream>>>(st.core_total, st.core_slot.p, tmp, v, k);
+        const int grid = S.nblk(st.core_total * kp, 1);
+        core_writeback_kernel<T><<<grid, kBlock, 0, S.stream>>>(st.core_total, st.core_slot.p, tmp, v, kp);
         WB_CUDA(cudaGetLastError());
         S.gpu_launches++;
     }
-    for (int l = nlev - 1; l >= 0; --l) launch_csr<T, EPI_PIVOT>(S, st.bwd, st.bwd_lp[l], st.bwd_lp[l + 1], v, k);
-    // back substitution of the eliminated block (:425-436), then subtract_mean (:446)
-    launch_csr<T, EPI_ACC_SCALED>(S, st.elim, 0, st.elim.nchunks, v, k);
-    slot_sum(nullptr, L, m2);
+    for (int l = nlev - 1; l >= 0; --l) launch_csr<T, EPI_PIVOT>(S, st.bwd, st.bwd_lp[l], st.bwd_lp[l + 1], v, v, kp);
+    // sum over the kept solution with the back-substitution weights -> final means
+    if (st.nkeep > 0) {
+        const int gs = (int)std::max<int64_t>(1, (st.nkeep + kSpb - 1) / kSpb);
+        WB_DISPATCH_G(G, keep_sum_kernel<T, GV><<<gs, kBlock, 0, S.stream>>>(st.nkeep, kSpb, st.keep_slots.p, st.rho.p, 1,
+                                                                              st.sub_of.p, v, kp, M2));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+    }
+    return SubMeans{st.sub_nloc.p, S0, SB, M2, st.sub_I.p};
 }
 
-// z = M^{-1} r.  For additive Schwarz also returns partial sums of r.z in part (if non-null).
+// z = M^{-1} r.  With part non-null also the block partials of r.z (nb_part blocks).
 template <typename T>
-void apply_precond(SolverImpl& S, const T* r, T* z, int k, double* part, int& nb_part) {
+void apply_precond(SolverImpl& S, const T* r, T* z, int kp, double* part, int& nb_part) {
     const int64_t m = S.d.ndofs;
-    const int G = group_width(k);
+    const int G = group_for(kp);
     auto& sts = stages<T>(S);
     T* v = loc_buf<T>(S);
-    double* msum = S.ws.msum.p;
     nb_part = 0;
     if (S.pc.kind == 0 || sts.empty()) {
-        if (S.pc.kind == 0) {
-            WB_CUDA(cudaMemcpyAsync(z, r, sizeof(T) * m * k, cudaMemcpyDeviceToDevice, S.stream));
-        } else {
-            WB_CUDA(cudaMemsetAsync(z, 0, sizeof(T) * m * k, S.stream));
-        }
-        if (part) launch_dot<T, T>(S, r, z, m, k, part, nb_part);
+        if (S.pc.kind == 0) WB_CUDA(cudaMemcpyAsync(z, r, sizeof(T) * m * kp, cudaMemcpyDeviceToDevice, S.stream));
+        else WB_CUDA(cudaMemsetAsync(z, 0, sizeof(T) * m * kp, S.stream));
+        if (part) launch_dot<T, T>(S, r, z, m, kp, part, nb_part);
         return;
     }
     if (S.pc.kind == 1) {
         StageDev<T>& st = sts[0];
-        const int grid = S.nblk(st.nslots, G);
-        WB_DISPATCH_G(G, restrict_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(st.nslots, st.gidx.p, st.spou.p, r, v, k));
-        WB_CUDA(cudaGetLastError());
-        S.gpu_launches++;
-        stage_local_solve<T>(S, st, v, k, msum);
-        nb_part = S.nblk(m, G);
-        double* m2 = msum + (size_t)2 * S.max_nsub * k;
-        WB_DISPATCH_G(G, prolong_gather_kernel<T, GV><<<nb_part, kBlock, 0, S.stream>>>(
-                             m, st.gptr.p, st.gslot.p, st.sub_of.p, st.sub_nloc.p, st.spou.p, m2, v, z, part ? r : nullptr, k, part));
+        const SubMeans M = stage_local_solve<T>(S, st, r, v, kp);
+        nb_part = S.nblk(m, G, part ? 2 : 8);
+        WB_DISPATCH_G(G, prolong_kernel<T, GV><<<nb_part, kBlock, 0, S.stream>>>(
+                             m, st.gptr.p, st.gslot.p, st.sub_of.p, st.spou.p, st.invd.p, st.bs_ptr.p, st.bs_col.p,
+                             st.bs_val.p, M, v, r, z, kp, part));
         WB_CUDA(cudaGetLastError());
         S.gpu_launches++;
         if (!part) nb_part = 0;
         return;
     }
     // multiplicative: sequential stages (one per factor pair), residual updated after each
-    T* rw = std::is_same<T, double>::value ? (T*)S.ws.rwork.p : (T*)S.ws.frwork.p;
-    WB_CUDA(cudaMemcpyAsync(rw, r, sizeof(T) * m * k, cudaMemcpyDeviceToDevice, S.stream));
-    WB_CUDA(cudaMemsetAsync(z, 0, sizeof(T) * m * k, S.stream));
+    T* rw = rwork_buf<T>(S);
+    T* cb = cbuf<T>(S);
+    WB_CUDA(cudaMemcpyAsync(rw, r, sizeof(T) * m * kp, cudaMemcpyDeviceToDevice, S.stream));
+    WB_CUDA(cudaMemsetAsync(z, 0, sizeof(T) * m * kp, S.stream));
     for (auto& st : sts) {
+        const SubMeans M = stage_local_solve<T>(S, st, rw, v, kp);
         const int grid = S.nblk(st.nslots, G);
-        WB_DISPATCH_G(G, restrict_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(st.nslots, st.gidx.p, st.spou.p, rw, v, k));
-        WB_CUDA(cudaGetLastError());
-        stage_local_solve<T>(S, st, v, k, msum);
-        double* m2 = msum + (size_t)2 * S.max_nsub * k;
-        WB_DISPATCH_G(G, mult_update_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(
-                             st.nslots, st.gidx.p, st.sub_of.p, st.sub_nloc.p, st.spou.p, m2, v, z, S.g_ptr.p,
-                             S.g_idx.p, gram_val<T>(S), rw, k));
+        WB_DISPATCH_G(G, mult_sol_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(
+                             st.nslots, st.gidx.p, st.sub_of.p, st.spou.p, st.invd.p, st.bs_ptr.p, st.bs_col.p,
+                             st.bs_val.p, M, v, rw, z, cb, kp));
+        WB_DISPATCH_G(G, mult_resid_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(st.nslots, st.gidx.p, cb, S.g_ptr.p,
+                                                                                S.g_idx.p, gram_val<T>(S), rw, kp));
         WB_CUDA(cudaGetLastError());
         S.gpu_launches += 2;
     }
-    if (part) launch_dot<T, T>(S, r, z, m, k, part, nb_part);
+    if (part) launch_dot<T, T>(S, r, z, m, kp, part, nb_part);
 }
 
 // ---------------------------------------------------------------------------
-// Krylov state kernels (one thread per RHS)
+// Krylov state kernels (one thread per RHS; inputs reduced by reduce_parts_kernel)
 // ---------------------------------------------------------------------------
-
-__device__ double sum_part(const double* part, int nb, int k, int c) {
-    double s = 0.0;
-    for (int b = 0; b < nb; ++b) s += part[(size_t)b * k + c];
-    return s;
-}
 
 struct KState {
     double *bnorm, *rz, *rz0, *alpha, *beta, *rnorm, *tol;
@@ -742,21 +759,20 @@ struct KState {
     int32_t* n_active;
 };
 
-// The state kernels run as one warp (k <= 32 lanes); lanes >= k only join the count.
-__device__ void count_active(KState s, int k) {
+__device__ void count_active(KState s, int kp) {
     __syncwarp();
     if (threadIdx.x == 0) {
         int na = 0;
-        for (int j = 0; j < k; ++j) na += s.active[j];
+        for (int j = 0; j < kp; ++j) na += s.active[j];
         *s.n_active = na;
     }
 }
 
-// cg.rs:52-74: ||b||; zero RHS converge at iteration 0.
-__global__ void cg_init_kernel(KState s, const double* part_bb, int nb, int k) {
+// cg.rs:52-74: ||b||; zero RHS converge at iteration 0.  Columns outside part_of idle.
+__global__ void cg_init_kernel(KState s, const double* red, int kp) {
     const int c = threadIdx.x;
-    if (c < k) {
-        const double bn = sqrt(sum_part(part_bb, nb, k, c));
+    if (c < kp) {
+        const double bn = sqrt(red[c]);
         s.bnorm[c] = bn;
         s.iters[c] = 0;
         s.alpha[c] = 0.0;
@@ -773,22 +789,21 @@ __global__ void cg_init_kernel(KState s, const double* part_bb, int nb, int k) {
         }
     }
 }
-__global__ void cg_rz0_kernel(KState s, const double* part, int nb, int k) {
+__global__ void cg_rz0_kernel(KState s, const double* red, int kp) {
     const int c = threadIdx.x;
-    if (c < k) {
-        const double rz = sum_part(part, nb, k, c);
-        s.rz[c] = rz;
-        s.rz0[c] = rz;
+    if (c < kp) {
+        s.rz[c] = red[c];
+        s.rz0[c] = red[c];
     }
-    count_active(s, k);
+    count_active(s, kp);
 }
 // cg.rs:76-86
-__global__ void cg_alpha_kernel(KState s, const double* part, int nb, int k, int it) {
+__global__ void cg_alpha_kernel(KState s, const double* red, int kp, int it) {
     const int c = threadIdx.x;
-    if (c < k) {
+    if (c < kp) {
         s.alpha[c] = 0.0;
         if (s.active[c]) {
-            const double pap = sum_part(part, nb, k, c);
+            const double pap = red[c];
             s.iters[c] = it;
             if (pap <= 0.0) {
                 s.active[c] = 0;
@@ -798,23 +813,23 @@ __global__ void cg_alpha_kernel(KState s, const double* part, int nb, int k, int
             }
         }
     }
-    count_active(s, k);
+    count_active(s, kp);
 }
 // cg.rs:94-103
-__global__ void cg_check_kernel(KState s, const double* part, int nb, int k) {
+__global__ void cg_check_kernel(KState s, const double* red, int kp) {
     const int c = threadIdx.x;
-    if (c < k && s.active[c]) {
-        const double rn = sqrt(sum_part(part, nb, k, c));
+    if (c < kp && s.active[c]) {
+        const double rn = sqrt(red[c]);
         s.rnorm[c] = rn;
         if (rn / s.bnorm[c] <= s.tol[c]) { s.active[c] = 0; s.conv[c] = 1; }
     }
-    count_active(s, k);
+    count_active(s, kp);
 }
 // cg.rs:105-125 (EPS^2 stagnation guard)
-__global__ void cg_beta_kernel(KState s, const double* part, int nb, int k) {
+__global__ void cg_beta_kernel(KState s, const double* red, int kp) {
     const int c = threadIdx.x;
-    if (c < k && s.active[c]) {
-        const double rzn = sum_part(part, nb, k, c);
+    if (c < kp && s.active[c]) {
+        const double rzn = red[c];
         const double eps = 2.220446049250313e-16;
         const double thr = eps * eps * fmax(fabs(s.rz0[c]), 2.2250738585072014e-308);
         if (fabs(rzn) < thr) {
@@ -825,11 +840,11 @@ __global__ void cg_beta_kernel(KState s, const double* part, int nb, int k) {
             s.rz[c] = rzn;
         }
     }
-    count_active(s, k);
+    count_active(s, kp);
 }
-__global__ void cg_final_kernel(KState s, int k, int maxiter) {
+__global__ void cg_final_kernel(KState s, int kp, int maxiter) {
     const int c = threadIdx.x;
-    if (c < k && s.active[c]) { s.active[c] = 0; s.conv[c] = 0; s.iters[c] = maxiter; }
+    if (c < kp && s.active[c]) { s.active[c] = 0; s.conv[c] = 0; s.iters[c] = maxiter; }
 }
 
 template <typename TA, typename TB>
@@ -837,13 +852,13 @@ __global__ void convert_kernel(const TA* __restrict__ a, TB* __restrict__ b, int
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         b[i] = (TB)a[i];
 }
-// x64 += d (per RHS only where mask[c])
+// x64 += d on the RHS with mask[c]
 template <typename TD>
 __global__ void masked_axpy_kernel(double* __restrict__ x, const TD* __restrict__ d, const int32_t* __restrict__ mask,
-                                   int64_t rows, int k) {
-    const int64_t n = rows * k;
+                                   int64_t rows, int kp) {
+    const int64_t n = rows * kp;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        if (mask[i % k]) x[i] += (double)d[i];
+        if (mask[i % kp]) x[i] += (double)d[i];
 }
 __global__ void sub_kernel(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -855,82 +870,76 @@ KState kstate(Workspace& w) {
                   w.st_active.p, w.st_conv.p, w.st_iters.p, w.st_part.p, w.n_active.p};
 }
 
-void ensure_ws(SolverImpl& S, int k) {
+void ensure_ws(SolverImpl& S, int kp) {
     Workspace& w = S.ws;
-    if (w.k >= k) return;
+    if (w.kp >= kp) return;
     const size_t n = (size_t)S.d.n, m = (size_t)S.d.ndofs;
-    w.yi.alloc(n * k);
-    w.e.alloc(n * k);
-    w.b.alloc(m * k);
-    w.x.alloc(m * k);
-    w.r.alloc(m * k);
-    w.gx.alloc(m * k);
-    w.cx.alloc(m * k);
-    w.cr.alloc(m * k);
-    w.dz.alloc(m * k);
-    w.dp.alloc(m * k);
-    w.dap.alloc(m * k);
+    w.yi.alloc(n * kp);
+    w.e.alloc(n * kp);
+    for (DArr<double>* a : {&w.b, &w.x, &w.r, &w.gx, &w.cx, &w.cr, &w.dz, &w.dp, &w.dap}) a->alloc(m * kp);
     if (S.mixed()) {
-        w.frhs.alloc(m * k);
-        w.fr.alloc(m * k);
-        w.fx.alloc(m * k);
-        w.fz.alloc(m * k);
-        w.fp.alloc(m * k);
-        w.fap.alloc(m * k);
-        w.floc.alloc(std::max<size_t>(1, S.max_slots * k));
-        w.fcore_tmp.alloc(std::max<size_t>(1, S.max_core_total * k));
-        if (S.pc.kind == 2) w.frwork.alloc(m * k);
+        for (DArr<float>* a : {&w.frhs, &w.fx, &w.fr, &w.fz, &w.fp, &w.fap}) a->alloc(m * kp);
+        w.floc.alloc(std::max<size_t>(1, S.max_slots * kp));
+        w.fcore_tmp.alloc(std::max<size_t>(1, S.max_core_total * kp));
+        if (S.pc.kind == 2) { w.frwork.alloc(m * kp); w.fcbuf.alloc(std::max<size_t>(1, S.max_slots * kp)); }
     }
-    w.vloc.alloc(std::max<size_t>(1, S.max_slots * k));
-    w.core_tmp.alloc(std::max<size_t>(1, S.max_core_total * k));
-    if (S.pc.kind == 2) w.rwork.alloc(m * k);
-    w.msum.alloc(std::max<size_t>(1, 3 * (size_t)S.max_nsub * k));
-    w.part.alloc((size_t)S.n_sm * 8 * k + 64);
+    w.vloc.alloc(std::max<size_t>(1, S.max_slots * kp));
+    w.core_tmp.alloc(std::max<size_t>(1, S.max_core_total * kp));
+    if (S.pc.kind == 2) { w.rwork.alloc(m * kp); w.cbuf.alloc(std::max<size_t>(1, S.max_slots * kp)); }
+    w.msum.alloc(std::max<size_t>(1, 4 * (size_t)std::max(S.max_nsub, 1) * kp));
+    w.part.alloc((size_t)S.n_sm * 8 * kp + 64);
+    w.red.alloc(32);
     for (DArr<double>* a : {&w.st_bnorm, &w.st_rz, &w.st_rz0, &w.st_alpha, &w.st_beta, &w.st_rnorm, &w.st_tol}) a->alloc(32);
     for (DArr<int32_t>* a : {&w.st_active, &w.st_conv, &w.st_iters, &w.st_part}) a->alloc(32);
     w.n_active.alloc(1);
-    w.k = k;
+    w.kp = kp;
 }
 
-// Preconditioned CG on all RHS marked in st_part (device), solution into x (zeroed here),
+// Preconditioned CG on the RHS marked in st_part (device), solution into x (zeroed here),
 // per-RHS relative tolerance st_tol (device).  Vectors of type T; inner products in FP64.
 template <typename T>
-void cg_device(SolverImpl& S, int k, const T* b, T* x, T* r, T* z, T* p, T* ap, int maxiter) {
+void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap, int maxiter) {
     Workspace& w = S.ws;
     const int64_t m = S.d.ndofs;
-    const int G = group_width(k);
+    const int G = group_for(kp);
     KState ks = kstate(w);
     double* part = w.part.p;
+    double* red = w.red.p;
     int nb = 0;
-    WB_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * m * k, S.stream));
-    WB_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * m * k, cudaMemcpyDeviceToDevice, S.stream));
-    launch_dot<T, T>(S, b, b, m, k, part, nb);
-    cg_init_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k);
-    apply_precond<T>(S, r, z, k, part, nb);
-    cg_rz0_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k);
-    WB_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * m * k, cudaMemcpyDeviceToDevice, S.stream));
-    S.gpu_launches += 3;
-    const T* w_t = nullptr;
-    if (std::is_same<T, double>::value) w_t = (const T*)S.w64.p; else w_t = (const T*)S.w32.p;
+    WB_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * m * kp, S.stream));
+    WB_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * m * kp, cudaMemcpyDeviceToDevice, S.stream));
+    launch_dot<T, T>(S, b, b, m, kp, part, nb);
+    launch_reduce(S, part, nb, kp, red);
+    cg_init_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
+    apply_precond<T>(S, r, z, kp, part, nb);
+    launch_reduce(S, part, nb, kp, red);
+    cg_rz0_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
+    WB_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * m * kp, cudaMemcpyDeviceToDevice, S.stream));
+    S.gpu_launches += 2;
+    const T* w_t = std::is_same<T, double>::value ? (const T*)S.w64.p : (const T*)S.w32.p;
+    const int kind = std::is_same<T, double>::value ? 0 : 1;
     cudaEvent_t ev;
     WB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    const int kind = std::is_same<T, double>::value ? 0 : 1;
     auto enqueue_iter = [&](int it) {
         cudaEvent_t e0 = nullptr;
-        S.prof_begin(kind, e0);
-        launch_obs<T, OBS_GRAM>(S, k, w_t, p, nullptr, ap, nullptr);
+        S.prof_begin(e0);
+        launch_obs<T, OBS_GRAM>(S, kp, w_t, p, nullptr, ap, nullptr);
         S.prof_end(kind, e0);
-        launch_dot<T, T>(S, p, ap, m, k, part, nb);
-        cg_alpha_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k, it);
-        const int grid = S.nblk(m, G);
-        WB_DISPATCH_G(G, cg_xr_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(x, r, p, ap, w.st_alpha.p, m, k, part));
-        cg_check_kernel<<<1, 32, 0, S.stream>>>(ks, part, grid, k);
+        launch_dot<T, T>(S, p, ap, m, kp, part, nb);
+        launch_reduce(S, part, nb, kp, red);
+        cg_alpha_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp, it);
+        const int grid = S.nblk(m, G, 2);
+        WB_DISPATCH_G(G, cg_xr_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(x, r, p, ap, w.st_alpha.p, m, kp, part));
+        launch_reduce(S, part, grid, kp, red);
+        cg_check_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
         cudaEvent_t e1 = nullptr;
-        S.prof_begin(kind + 2, e1);
-        apply_precond<T>(S, r, z, k, part, nb);
+        S.prof_begin(e1);
+        apply_precond<T>(S, r, z, kp, part, nb);
         S.prof_end(kind + 2, e1);
-        cg_beta_kernel<<<1, 32, 0, S.stream>>>(ks, part, nb, k);
-        WB_DISPATCH_G(G, cg_p_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(p, z, w.st_beta.p, w.st_active.p, m, k));
+        launch_reduce(S, part, nb, kp, red);
+        cg_beta_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
+        const int gridp = S.nblk(m, G);
+        WB_DISPATCH_G(G, cg_p_kernel<T, GV><<<gridp, kBlock, 0, S.stream>>>(p, z, w.st_beta.p, w.st_active.p, m, kp));
         WB_CUDA(cudaGetLastError());
         S.gpu_launches += 5;
         WB_CUDA(cudaMemcpyAsync(S.h_active, w.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
@@ -943,11 +952,11 @@ void cg_device(SolverImpl& S, int k, const T* b, T* x, T* r, T* z, T* p, T* ap, 
     if (*S.h_active > 0 && maxiter > 0) {
         cudaEvent_t evb;
         WB_CUDA(cudaEventCreateWithFlags(&evb, cudaEventDisableTiming));
-        enqueue_iter(1);  // records ev
+        enqueue_iter(1);
         int it = 1;
         while (it < maxiter) {
-            std::swap(ev, evb);  // evb = event of iteration it
-            enqueue_iter(it + 1);  // records ev for iteration it+1
+            std::swap(ev, evb);     // evb = event of iteration it
+            enqueue_iter(it + 1);   // records ev for iteration it+1
             WB_CUDA(cudaEventSynchronize(evb));
             ++it;
             if (*S.h_active == 0) break;
@@ -955,7 +964,7 @@ void cg_device(SolverImpl& S, int k, const T* b, T* x, T* r, T* z, T* p, T* ap, 
         WB_CUDA(cudaEventDestroy(evb));
     }
     WB_CUDA(cudaEventDestroy(ev));
-    cg_final_kernel<<<1, 32, 0, S.stream>>>(ks, k, maxiter);
+    cg_final_kernel<<<1, 32, 0, S.stream>>>(ks, kp, maxiter);
     WB_CUDA(cudaGetLastError());
     S.gpu_launches++;
 }
@@ -967,16 +976,16 @@ void cg_device(SolverImpl& S, int k, const T* b, T* x, T* r, T* z, T* p, T* ap, 
 // ---------------------------------------------------------------------------
 
 struct GState {
-    int R;                 // restart
+    int R;  // restart
     double *H, *g, *cs, *sn, *y, *scale, *hcur, *hmax, *abs_tol, *resid;
     int32_t *cyc, *done, *conv, *iters, *jc, *brk, *n_active;
 };
 
-__device__ void g_count(GState s, int k) {
+__device__ void g_count(GState s, int kp) {
     __syncwarp();
     if (threadIdx.x == 0) {
         int na = 0;
-        for (int j = 0; j < k; ++j) na += s.cyc[j];
+        for (int j = 0; j < kp; ++j) na += s.cyc[j];
         *s.n_active = na;
     }
 }
@@ -984,11 +993,10 @@ __device__ void g_count(GState s, int k) {
 
 // ||b||, abs_tol; zero RHS converge at iteration 0 (gmres.rs:357-369).  RHS outside
 // part_of do not take part.
-__global__ void gm_init_kernel(GState s, const double* part, int nb, int k, const double* tol,
-                               const int32_t* part_of) {
+__global__ void gm_init_kernel(GState s, const double* red, int kp, const double* tol, const int32_t* part_of) {
     const int c = threadIdx.x;
-    if (c < k) {
-        const double bn = sqrt(sum_part(part, nb, k, c));
+    if (c < kp) {
+        const double bn = sqrt(red[c]);
         s.iters[c] = 0;
         s.brk[c] = 0;
         s.cyc[c] = 0;
@@ -999,15 +1007,15 @@ __global__ void gm_init_kernel(GState s, const double* part, int nb, int k, cons
     }
 }
 // Start of a cycle: beta = ||b - A x|| (gmres.rs:375-393, 428-437).
-__global__ void gm_restart_kernel(GState s, const double* part, int nb, int k, int maxiter) {
+__global__ void gm_restart_kernel(GState s, const double* red, int kp, int maxiter) {
     const int c = threadIdx.x;
-    if (c < k) {
+    if (c < kp) {
         s.cyc[c] = 0;
         s.jc[c] = 0;
         if (!s.done[c]) {
-            const double beta = sqrt(sum_part(part, nb, k, c));
+            const double beta = sqrt(red[c]);
             s.resid[c] = beta;
-            if (s.brk[c]) {  // lucky breakdown: true residual decides
+            if (s.brk[c]) {  // lucky breakdown: the true residual decides
                 s.done[c] = 1;
                 s.conv[c] = beta <= s.abs_tol[c];
             } else if (beta <= s.abs_tol[c]) {
@@ -1030,13 +1038,13 @@ __global__ void gm_restart_kernel(GState s, const double* part, int nb, int k, i
             }
         }
     }
-    g_count(s, k);
+    g_count(s, kp);
 }
 // MGS coefficient h_ij = w . v_i (gmres.rs:201-220).
-__global__ void gm_mgs_coef_kernel(GState s, const double* part, int nb, int k, int i, int j) {
+__global__ void gm_mgs_coef_kernel(GState s, const double* red, int kp, int i, int j) {
     const int c = threadIdx.x;
-    if (c < k) {
-        const double h = s.cyc[c] ? sum_part(part, nb, k, c) : 0.0;
+    if (c < kp) {
+        const double h = s.cyc[c] ? red[c] : 0.0;
         s.hcur[c] = h;
         if (s.cyc[c]) {
             GH(s, c, i, j) = h;
@@ -1046,29 +1054,29 @@ __global__ void gm_mgs_coef_kernel(GState s, const double* part, int nb, int k, 
 }
 template <typename T>
 __global__ void gm_axpy_kernel(T* __restrict__ w, const T* __restrict__ v, const double* __restrict__ h,
-                               int64_t rows, int k) {
-    const int64_t n = rows * k;
+                               int64_t rows, int kp) {
+    const int64_t n = rows * kp;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
-        w[e] -= (T)h[e % k] * v[e];
+        w[e] -= (T)h[e % kp] * v[e];
 }
 template <typename T>
 __global__ void gm_scale_kernel(const T* __restrict__ w, T* __restrict__ v, const double* __restrict__ scale,
-                                const int32_t* __restrict__ cyc, int64_t rows, int k) {
-    const int64_t n = rows * k;
+                                const int32_t* __restrict__ cyc, int64_t rows, int kp) {
+    const int64_t n = rows * kp;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % k);
+        const int c = (int)(e % kp);
         v[e] = cyc[c] ? (T)((double)w[e] * scale[c]) : T(0);
     }
 }
 // h_{j+1,j} = ||w||, Givens rotations, residual estimate, outcome (gmres.rs:256-313).
-__global__ void gm_givens_kernel(GState s, const double* part, int nb, int k, int j, int maxiter) {
+__global__ void gm_givens_kernel(GState s, const double* red, int kp, int j, int maxiter) {
     const int c = threadIdx.x;
-    if (c < k && s.cyc[c]) {
+    if (c < kp && s.cyc[c]) {
         const int R = s.R;
         double* cs = s.cs + (size_t)c * R;
         double* sn = s.sn + (size_t)c * R;
         double* g = s.g + (size_t)c * (R + 1);
-        const double hn = sqrt(sum_part(part, nb, k, c));
+        const double hn = sqrt(red[c]);
         GH(s, c, j + 1, j) = hn;
         s.hmax[c] = fmax(s.hmax[c], hn);
         for (int i = 0; i < j; ++i) {
@@ -1103,12 +1111,12 @@ __global__ void gm_givens_kernel(GState s, const double* part, int nb, int k, in
             s.cyc[c] = 0; s.brk[c] = 1;  // lucky breakdown
         }
     }
-    g_count(s, k);
+    g_count(s, kp);
 }
 // y = R^{-1} g over the cycle's jc steps (solve_upper_triangular, gmres.rs:499-519).
-__global__ void gm_trisolve_kernel(GState s, int k) {
+__global__ void gm_trisolve_kernel(GState s, int kp) {
     const int c = threadIdx.x;
-    if (c >= k) return;
+    if (c >= kp) return;
     const int jn = s.jc[c], R = s.R;
     double* y = s.y + (size_t)c * R;
     const double* g = s.g + (size_t)c * (R + 1);
@@ -1123,23 +1131,23 @@ __global__ void gm_trisolve_kernel(GState s, int k) {
 // x += sum_i y_i z_i (update_solution, gmres.rs:523-530).
 template <typename T>
 __global__ void gm_update_kernel(double* __restrict__ x, const T* __restrict__ Z, const double* __restrict__ y,
-                                 int R, int jmax, int64_t rows, int k) {
-    const int64_t n = rows * k;
+                                 int R, int jmax, int64_t rows, int kp) {
+    const int64_t n = rows * kp;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % k);
+        const int c = (int)(e % kp);
         double acc = 0.0;
         for (int i = 0; i < jmax; ++i) acc += y[(size_t)c * R + i] * (double)Z[(size_t)i * n + e];
         x[e] += acc;
     }
 }
-__global__ void gm_final_kernel(GState s, int k) {
+__global__ void gm_final_kernel(GState s, int kp) {
     const int c = threadIdx.x;
-    if (c < k && !s.done[c]) { s.done[c] = 1; s.conv[c] = 0; }
+    if (c < kp && !s.done[c]) { s.done[c] = 1; s.conv[c] = 0; }
 }
 #undef GH
 
 struct GmresBufs {
-    int R = 0, k = 0;
+    int R = 0, kp = 0;
     int64_t m = 0;
     DArr<double> H, g, cs, sn, y, scale, hcur, hmax, abs_tol, resid;
     DArr<int32_t> cyc, done, conv, iters, jc, brk, n_active;
@@ -1147,16 +1155,15 @@ struct GmresBufs {
     DArr<float> w32, V32, Z32;
 };
 
-// GMRES(R) for A d = rhs (FP64 rhs and solution x; vectors of type T).  Per-RHS results
-// in the GState arrays (conv, iters).
+// GMRES(R) for A d = rhs (FP64 rhs and solution x; Arnoldi vectors of type T).
 template <typename T>
-void gmres_device(SolverImpl& S, GmresBufs& B, int k, const double* rhs, double* x, int maxiter) {
+void gmres_device(SolverImpl& S, GmresBufs& B, int kp, const double* rhs, double* x, int maxiter) {
     const int64_t m = S.d.ndofs;
     const int R = std::max(1, S.params.gmres_restart);
-    const size_t mk = (size_t)m * k;
-    if (B.R != R || B.k < k || B.m != m) {
-        B.R = R; B.k = k; B.m = m;
-        for (DArr<double>* a : {&B.g}) a->alloc((size_t)32 * (R + 1));
+    const size_t mk = (size_t)m * kp;
+    if (B.R != R || B.kp < kp || B.m != m) {
+        B.R = R; B.kp = kp; B.m = m;
+        B.g.alloc((size_t)32 * (R + 1));
         B.H.alloc((size_t)32 * R * (R + 1));
         for (DArr<double>* a : {&B.cs, &B.sn, &B.y}) a->alloc((size_t)32 * R);
         for (DArr<double>* a : {&B.scale, &B.hcur, &B.hmax, &B.abs_tol, &B.resid}) a->alloc(32);
@@ -1173,27 +1180,30 @@ void gmres_device(SolverImpl& S, GmresBufs& B, int k, const double* rhs, double*
     T* wv = std::is_same<T, double>::value ? (T*)B.w64.p : (T*)B.w32.p;
     const T* w_t = std::is_same<T, double>::value ? (const T*)S.w64.p : (const T*)S.w32.p;
     double* part = S.ws.part.p;
+    double* red = S.ws.red.p;
     int nb = 0;
-    const int gridv = S.nblk(m * k, 1);
+    const int gridv = S.nblk(m * kp, 1);
     WB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * mk, S.stream));
-    launch_dot<double, double>(S, rhs, rhs, m, k, part, nb);
-    gm_init_kernel<<<1, 32, 0, S.stream>>>(s, part, nb, k, S.ws.st_tol.p, S.ws.st_part.p);
+    launch_dot<double, double>(S, rhs, rhs, m, kp, part, nb);
+    launch_reduce(S, part, nb, kp, red);
+    gm_init_kernel<<<1, 32, 0, S.stream>>>(s, red, kp, S.ws.st_tol.p, S.ws.st_part.p);
     const int kind = std::is_same<T, double>::value ? 0 : 1;
     for (int cycle = 0; cycle < maxiter + 2; ++cycle) {
         // r = rhs - A x (FP64), beta, v_0 = r / beta
-        launch_obs<double, OBS_GRAM>(S, k, S.w64.p, x, nullptr, B.w64.p, nullptr);
+        launch_obs<double, OBS_GRAM>(S, kp, S.w64.p, x, nullptr, B.w64.p, nullptr);
         sub_kernel<<<gridv, kBlock, 0, S.stream>>>(rhs, B.w64.p, B.r64.p, (int64_t)mk);
-        launch_dot<double, double>(S, B.r64.p, B.r64.p, m, k, part, nb);
-        gm_restart_kernel<<<1, 32, 0, S.stream>>>(s, part, nb, k, maxiter);
+        launch_dot<double, double>(S, B.r64.p, B.r64.p, m, kp, part, nb);
+        launch_reduce(S, part, nb, kp, red);
+        gm_restart_kernel<<<1, 32, 0, S.stream>>>(s, red, kp, maxiter);
         WB_CUDA(cudaMemcpyAsync(S.h_active, B.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
         WB_CUDA(cudaStreamSynchronize(S.stream));
-        S.gpu_launches += 4;
+        S.gpu_launches += 2;
         if (*S.h_active == 0) break;
         if (std::is_same<T, double>::value) {
-            gm_scale_kernel<double><<<gridv, kBlock, 0, S.stream>>>(B.r64.p, (double*)V, B.scale.p, B.cyc.p, m, k);
+            gm_scale_kernel<double><<<gridv, kBlock, 0, S.stream>>>(B.r64.p, (double*)V, B.scale.p, B.cyc.p, m, kp);
         } else {
             convert_kernel<double, float><<<gridv, kBlock, 0, S.stream>>>(B.r64.p, B.w32.p, (int64_t)mk);
-            gm_scale_kernel<float><<<gridv, kBlock, 0, S.stream>>>(B.w32.p, (float*)V, B.scale.p, B.cyc.p, m, k);
+            gm_scale_kernel<float><<<gridv, kBlock, 0, S.stream>>>(B.w32.p, (float*)V, B.scale.p, B.cyc.p, m, kp);
         }
         int jmax = 0;
         for (int j = 0; j < R; ++j) {
@@ -1201,22 +1211,24 @@ void gmres_device(SolverImpl& S, GmresBufs& B, int k, const double* rhs, double*
             T* zj = Z + (size_t)j * mk;
             int nbp = 0;
             cudaEvent_t e1 = nullptr;
-            S.prof_begin(kind + 2, e1);
-            apply_precond<T>(S, vj, zj, k, nullptr, nbp);
+            S.prof_begin(e1);
+            apply_precond<T>(S, vj, zj, kp, nullptr, nbp);
             S.prof_end(kind + 2, e1);
             cudaEvent_t e0 = nullptr;
-            S.prof_begin(kind, e0);
-            launch_obs<T, OBS_GRAM>(S, k, w_t, zj, nullptr, wv, nullptr);
+            S.prof_begin(e0);
+            launch_obs<T, OBS_GRAM>(S, kp, w_t, zj, nullptr, wv, nullptr);
             S.prof_end(kind, e0);
             for (int i = 0; i <= j; ++i) {
                 const T* vi = V + (size_t)i * mk;
-                launch_dot<T, T>(S, wv, vi, m, k, part, nb);
-                gm_mgs_coef_kernel<<<1, 32, 0, S.stream>>>(s, part, nb, k, i, j);
-                gm_axpy_kernel<T><<<gridv, kBlock, 0, S.stream>>>(wv, vi, B.hcur.p, m, k);
+                launch_dot<T, T>(S, wv, vi, m, kp, part, nb);
+                launch_reduce(S, part, nb, kp, red);
+                gm_mgs_coef_kernel<<<1, 32, 0, S.stream>>>(s, red, kp, i, j);
+                gm_axpy_kernel<T><<<gridv, kBlock, 0, S.stream>>>(wv, vi, B.hcur.p, m, kp);
             }
-            launch_dot<T, T>(S, wv, wv, m, k, part, nb);
-            gm_givens_kernel<<<1, 32, 0, S.stream>>>(s, part, nb, k, j, maxiter);
-            gm_scale_kernel<T><<<gridv, kBlock, 0, S.stream>>>(wv, V + (size_t)(j + 1) * mk, B.scale.p, B.cyc.p, m, k);
+            launch_dot<T, T>(S, wv, wv, m, kp, part, nb);
+            launch_reduce(S, part, nb, kp, red);
+            gm_givens_kernel<<<1, 32, 0, S.stream>>>(s, red, kp, j, maxiter);
+            gm_scale_kernel<T><<<gridv, kBlock, 0, S.stream>>>(wv, V + (size_t)(j + 1) * mk, B.scale.p, B.cyc.p, m, kp);
             WB_CUDA(cudaGetLastError());
             S.gpu_launches += 2 * (j + 1) + 2;
             jmax = j + 1;
@@ -1224,12 +1236,12 @@ void gmres_device(SolverImpl& S, GmresBufs& B, int k, const double* rhs, double*
             WB_CUDA(cudaStreamSynchronize(S.stream));
             if (*S.h_active == 0) break;
         }
-        gm_trisolve_kernel<<<1, 32, 0, S.stream>>>(s, k);
-        gm_update_kernel<T><<<gridv, kBlock, 0, S.stream>>>(x, Z, B.y.p, R, jmax, m, k);
+        gm_trisolve_kernel<<<1, 32, 0, S.stream>>>(s, kp);
+        gm_update_kernel<T><<<gridv, kBlock, 0, S.stream>>>(x, Z, B.y.p, R, jmax, m, kp);
         WB_CUDA(cudaGetLastError());
         S.gpu_launches += 2;
     }
-    gm_final_kernel<<<1, 32, 0, S.stream>>>(s, k);
+    gm_final_kernel<<<1, 32, 0, S.stream>>>(s, kp);
     WB_CUDA(cudaGetLastError());
 }
 
@@ -1246,65 +1258,72 @@ struct BatchOut {
     std::vector<double> fres;
 };
 
+std::vector<double> host_reduce(SolverImpl& S, int nb, int kp) {
+    std::vector<double> hpart((size_t)nb * kp), out(kp, 0.0);
+    WB_CUDA(cudaMemcpyAsync(hpart.data(), S.ws.part.p, sizeof(double) * nb * kp, cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    for (int c = 0; c < kp; ++c)
+        for (int b = 0; b < nb; ++b) out[c] += hpart[(size_t)b * kp + c];
+    return out;
+}
+
 // Solve k <= 32 RHS with device inputs ycol (n x k RHS-major) into device outputs
 // x (n_dofs x k RHS-major) and dem (n x k RHS-major).  Solver::solve semantics
 // (solver.rs:209-238) batched over RHS, with the refinement residual b - G x.
 void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double* demcol, BatchOut& out) {
-    ensure_ws(S, k);
+    const int kp = pad_kp(k);
+    ensure_ws(S, kp);
     Workspace& w = S.ws;
     const int64_t n = S.d.n, m = S.d.ndofs;
     const uint32_t* perm = S.perm_identity ? nullptr : S.perm.p;
-    // y -> interleaved, primary-sorted
-    gather_interleave_kernel<double><<<(unsigned)((n + 31) / 32), 256, 0, S.stream>>>(ycol, n, k, perm, w.yi.p);
+    // y -> interleaved, primary-sorted, padded to kp columns
+    gather_interleave_kernel<double><<<(unsigned)((n + 31) / 32), 256, 0, S.stream>>>(ycol, n, k, kp, perm, w.yi.p);
     // b = D'W y (rmatvec_wdt, solver.rs:210-211)
-    launch_obs<double, OBS_RHS>(S, k, S.w64.p, nullptr, w.yi.p, w.b.p, nullptr);
+    launch_obs<double, OBS_RHS>(S, kp, S.w64.p, nullptr, w.yi.p, w.b.p, nullptr);
     int nb = 0;
-    launch_dot<double, double>(S, w.b.p, w.b.p, m, k, w.part.p, nb);
-    std::vector<double> hpart((size_t)nb * k);
-    WB_CUDA(cudaMemcpyAsync(hpart.data(), w.part.p, sizeof(double) * nb * k, cudaMemcpyDeviceToHost, S.stream));
-    WB_CUDA(cudaStreamSynchronize(S.stream));
-    std::vector<double> rhs_norm(k), abs_tol(k);
-    for (int c = 0; c < k; ++c) {
-        double s = 0.0;
-        for (int b = 0; b < nb; ++b) s += hpart[(size_t)b * k + c];
-        rhs_norm[c] = std::max(std::sqrt(s), 1e-15);  // solver.rs:212
+    launch_dot<double, double>(S, w.b.p, w.b.p, m, kp, w.part.p, nb);
+    std::vector<double> bb = host_reduce(S, nb, kp);
+    std::vector<double> rhs_norm(kp), abs_tol(kp);
+    for (int c = 0; c < kp; ++c) {
+        rhs_norm[c] = std::max(std::sqrt(bb[c]), 1e-15);  // solver.rs:212
         abs_tol[c] = S.params.tol * rhs_norm[c];
     }
-    std::vector<int32_t> conv(k, 0), iters(k, 0), part_of(k, 1);
-    std::vector<double> tol(k, S.params.tol);
-    // One inner Krylov solve of G d = rhs on the RHS in `who` to relative tolerances tl;
+    std::vector<int32_t> conv(kp, 0), iters(kp, 0), part_of(kp, 0);
+    for (int c = 0; c < k; ++c) part_of[c] = 1;
+    std::vector<double> tol(kp, S.params.tol);
+    // One inner Krylov solve of G d = rhs on the RHS in `who` to relative tolerances tl,
     // then x += d on those RHS.
     auto run_inner = [&](const double* rhs, const std::vector<int32_t>& who, const std::vector<double>& tl,
                          std::vector<int32_t>& cv, std::vector<int32_t>& it) {
-        WB_CUDA(cudaMemcpyAsync(w.st_part.p, who.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, S.stream));
-        WB_CUDA(cudaMemcpyAsync(w.st_tol.p, tl.data(), sizeof(double) * k, cudaMemcpyHostToDevice, S.stream));
+        WB_CUDA(cudaMemcpyAsync(w.st_part.p, who.data(), sizeof(int32_t) * kp, cudaMemcpyHostToDevice, S.stream));
+        WB_CUDA(cudaMemcpyAsync(w.st_tol.p, tl.data(), sizeof(double) * kp, cudaMemcpyHostToDevice, S.stream));
         WB_CUDA(cudaMemsetAsync(w.st_conv.p, 0, sizeof(int32_t) * 32, S.stream));
-        const int grid = S.nblk(m * k, 1);
+        const int grid = S.nblk(m * kp, 1);
         if (S.params.krylov == WITHIN_KRYLOV_GMRES) {
             if (!S.gmres) S.gmres = std::make_shared<GmresBufs>();
             GmresBufs& B = *std::static_pointer_cast<GmresBufs>(S.gmres);
-            if (!S.mixed()) gmres_device<double>(S, B, k, rhs, w.cx.p, S.params.maxiter);
-            else gmres_device<float>(S, B, k, rhs, w.cx.p, S.params.maxiter);
-            masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, k);
-            WB_CUDA(cudaMemcpyAsync(w.st_conv.p, B.conv.p, sizeof(int32_t) * k, cudaMemcpyDeviceToDevice, S.stream));
-            WB_CUDA(cudaMemcpyAsync(w.st_iters.p, B.iters.p, sizeof(int32_t) * k, cudaMemcpyDeviceToDevice, S.stream));
+            if (!S.mixed()) gmres_device<double>(S, B, kp, rhs, w.cx.p, S.params.maxiter);
+            else gmres_device<float>(S, B, kp, rhs, w.cx.p, S.params.maxiter);
+            masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, kp);
+            WB_CUDA(cudaMemcpyAsync(w.st_conv.p, B.conv.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToDevice, S.stream));
+            WB_CUDA(cudaMemcpyAsync(w.st_iters.p, B.iters.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToDevice, S.stream));
         } else if (!S.mixed()) {
-            cg_device<double>(S, k, rhs, w.cx.p, w.cr.p, w.dz.p, w.dp.p, w.dap.p, S.params.maxiter);
-            masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, k);
+            cg_device<double>(S, kp, rhs, w.cx.p, w.cr.p, w.dz.p, w.dp.p, w.dap.p, S.params.maxiter);
+            masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, kp);
         } else {
-            convert_kernel<double, float><<<grid, kBlock, 0, S.stream>>>(rhs, w.frhs.p, m * k);
-            cg_device<float>(S, k, w.frhs.p, w.fx.p, w.fr.p, w.fz.p, w.fp.p, w.fap.p, S.params.maxiter);
-            masked_axpy_kernel<float><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.fx.p, w.st_part.p, m, k);
+            convert_kernel<double, float><<<grid, kBlock, 0, S.stream>>>(rhs, w.frhs.p, m * kp);
+            cg_device<float>(S, kp, w.frhs.p, w.fx.p, w.fr.p, w.fz.p, w.fp.p, w.fap.p, S.params.maxiter);
+            masked_axpy_kernel<float><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.fx.p, w.st_part.p, m, kp);
         }
         WB_CUDA(cudaGetLastError());
         S.gpu_launches += 2;
-        cv.assign(k, 0);
-        it.assign(k, 0);
-        WB_CUDA(cudaMemcpyAsync(cv.data(), w.st_conv.p, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, S.stream));
-        WB_CUDA(cudaMemcpyAsync(it.data(), w.st_iters.p, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, S.stream));
+        cv.assign(kp, 0);
+        it.assign(kp, 0);
+        WB_CUDA(cudaMemcpyAsync(cv.data(), w.st_conv.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaMemcpyAsync(it.data(), w.st_iters.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
         WB_CUDA(cudaStreamSynchronize(S.stream));
     };
-    WB_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * m * k, S.stream));
+    WB_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * m * kp, S.stream));
     std::vector<int32_t> cv, it;
     // FP64: initial solve + max_refinements corrections (solver.rs:215-216, 296-333).
     // Mixed: FP32 inner solves to >= 1e-5 relative inside an FP64 refinement loop of up to
@@ -1315,33 +1334,31 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
         conv = cv;
         iters = it;
     }
-    std::vector<int32_t> done(k, 0);
+    std::vector<int32_t> done(kp, 0);
+    for (int c = k; c < kp; ++c) done[c] = 1;
     for (int ref = 0; ref <= n_corr; ++ref) {
         if (!S.mixed() && ref == n_corr) break;
         const bool first_mixed = S.mixed() && ref == 0;
         const double* rhs = w.b.p;
         if (!first_mixed) {  // r = b - G x in FP64
             cudaEvent_t e0 = nullptr;
-            S.prof_begin(0, e0);
-            launch_obs<double, OBS_GRAM>(S, k, S.w64.p, w.x.p, nullptr, w.gx.p, nullptr);
+            S.prof_begin(e0);
+            launch_obs<double, OBS_GRAM>(S, kp, S.w64.p, w.x.p, nullptr, w.gx.p, nullptr);
             S.prof_end(0, e0);
-            const int grid = S.nblk(m * k, 1);
-            sub_kernel<<<grid, kBlock, 0, S.stream>>>(w.b.p, w.gx.p, w.r.p, m * k);
+            const int grid = S.nblk(m * kp, 1);
+            sub_kernel<<<grid, kBlock, 0, S.stream>>>(w.b.p, w.gx.p, w.r.p, m * kp);
             WB_CUDA(cudaGetLastError());
             S.gpu_launches++;
             rhs = w.r.p;
         }
-        launch_dot<double, double>(S, rhs, rhs, m, k, w.part.p, nb);
-        WB_CUDA(cudaMemcpyAsync(hpart.data(), w.part.p, sizeof(double) * nb * k, cudaMemcpyDeviceToHost, S.stream));
-        WB_CUDA(cudaStreamSynchronize(S.stream));
-        std::vector<int32_t> who(k, 0);
-        std::vector<double> ctol(k, 1.0);
+        launch_dot<double, double>(S, rhs, rhs, m, kp, w.part.p, nb);
+        std::vector<double> rr = host_reduce(S, nb, kp);
+        std::vector<int32_t> who(kp, 0);
+        std::vector<double> ctol(kp, 1.0);
         int nwho = 0;
         for (int c = 0; c < k; ++c) {
             if (done[c]) continue;
-            double s = 0.0;
-            for (int b = 0; b < nb; ++b) s += hpart[(size_t)b * k + c];
-            const double cn = std::sqrt(s);
+            const double cn = std::sqrt(rr[c]);
             if (cn <= abs_tol[c]) { done[c] = 1; continue; }
             ctol[c] = std::min(abs_tol[c] / cn, 1.0);  // corr_tol (solver.rs:319-320)
             if (S.mixed()) ctol[c] = std::max(ctol[c], 1e-5);
@@ -1358,23 +1375,18 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
         for (int c = 0; c < k; ++c) conv[c] = done[c] ? 1 : 0;
     }
     // final demeaned e = y - D x and ||D'W e|| / ||b|| (solver.rs:222-227, 335-339)
-    launch_obs<double, OBS_RESID>(S, k, S.w64.p, w.x.p, w.yi.p, w.r.p, w.e.p);
-    launch_dot<double, double>(S, w.r.p, w.r.p, m, k, w.part.p, nb);
-    WB_CUDA(cudaMemcpyAsync(hpart.data(), w.part.p, sizeof(double) * nb * k, cudaMemcpyDeviceToHost, S.stream));
-    scatter_deinterleave_kernel<double><<<(unsigned)((n + 31) / 32), 256, 0, S.stream>>>(w.e.p, n, k, perm, demcol);
-    scatter_deinterleave_kernel<double><<<(unsigned)((m + 31) / 32), 256, 0, S.stream>>>(w.x.p, m, k, nullptr, xcol);
+    launch_obs<double, OBS_RESID>(S, kp, S.w64.p, w.x.p, w.yi.p, w.r.p, w.e.p);
+    launch_dot<double, double>(S, w.r.p, w.r.p, m, kp, w.part.p, nb);
+    scatter_deinterleave_kernel<double><<<(unsigned)((n + 31) / 32), 256, 0, S.stream>>>(w.e.p, n, k, kp, perm, demcol);
+    scatter_deinterleave_kernel<double><<<(unsigned)((m + 31) / 32), 256, 0, S.stream>>>(w.x.p, m, k, kp, nullptr, xcol);
     WB_CUDA(cudaGetLastError());
     S.gpu_launches += 3;
-    WB_CUDA(cudaStreamSynchronize(S.stream));
+    std::vector<double> ee = host_reduce(S, nb, kp);
     S.prof_harvest();
-    out.conv = conv;
-    out.iters = iters;
+    out.conv.assign(conv.begin(), conv.begin() + k);
+    out.iters.assign(iters.begin(), iters.begin() + k);
     out.fres.resize(k);
-    for (int c = 0; c < k; ++c) {
-        double s = 0.0;
-        for (int b = 0; b < nb; ++b) s += hpart[(size_t)b * k + c];
-        out.fres[c] = std::sqrt(s) / rhs_norm[c];
-    }
+    for (int c = 0; c < k; ++c) out.fres[c] = std::sqrt(ee[c]) / rhs_norm[c];
 }
 
 }  // namespace
@@ -1457,14 +1469,14 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
             std::iota(groups[0].begin(), groups[0].end(), 0);
         } else {
             for (int32_t i = 0; i < (int32_t)S->subs.size(); ++i) {
-                if (groups.empty() || S->subs[groups.back()[0]].q != S->subs[i].q || S->subs[groups.back()[0]].r != S->subs[i].r)
+                if (groups.empty() || S->subs[groups.back()[0]].q != S->subs[i].q ||
+                    S->subs[groups.back()[0]].r != S->subs[i].r)
                     groups.emplace_back();
                 groups.back().push_back(i);
             }
         }
         for (auto& g : groups) {
-            S->hstages.push_back(wb::build_stage(S->subs, g, S->d.ndofs, S->pc.kind == 1));
-            const wb::StageHost& h = S->hstages.back();
+            const wb::StageHost h = wb::build_stage(S->subs, g, S->d.ndofs, S->pc.kind == 1);
             S->max_nsub = std::max(S->max_nsub, h.nsub);
             S->max_slots = std::max(S->max_slots, h.nslots);
             S->max_core_total = std::max(S->max_core_total, (int64_t)h.core_slot.size());
@@ -1485,8 +1497,6 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
             S->g_val64.upload(gv);
             if (S->mixed()) S->g_val32.upload_cast(gv);
         }
-        // host copies of the stages are only needed while uploading
-        std::vector<wb::StageHost>().swap(S->hstages);
     }
     WB_CUDA(cudaStreamSynchronize(S->stream));
     S->setup_time = wb::now_s() - t0;
@@ -1650,55 +1660,49 @@ static int apply_common(within_solver* s, const double* in, size_t k, double* ou
     return guard([&]() -> int {
         if (k == 0) return WITHIN_OK;
         if (k > 32) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "at most 32 vectors per call");
-        const int kk = (int)k;
-        wb::ensure_ws(S, kk);
+        const int kk = (int)k, kp = wb::pad_kp(kk);
+        wb::ensure_ws(S, kp);
         const size_t n = (size_t)S.d.n, m = (size_t)S.d.ndofs;
-        const size_t nin = (which == 2 || which == 1 || which == 0) ? (which == 3 ? n : m) : n;
         const size_t in_rows = (which == 3) ? n : m;
         const size_t out_rows = (which == 2) ? n : m;
-        (void)nin;
         wb::DArr<double> din, dout, iin, iout;
         din.alloc(in_rows * k);
         dout.alloc(out_rows * k);
-        iin.alloc(in_rows * k);
-        iout.alloc(out_rows * k);
+        iin.alloc(in_rows * kp);
+        iout.alloc(out_rows * kp);
         WB_CUDA(cudaMemcpyAsync(din.p, in, sizeof(double) * in_rows * k, cudaMemcpyHostToDevice, S.stream));
         const uint32_t* perm = S.perm_identity ? nullptr : S.perm.p;
-        // to interleaved (obs vectors primary-sorted)
         wb::gather_interleave_kernel<double><<<(unsigned)((in_rows + 31) / 32), 256, 0, S.stream>>>(
-            din.p, (int64_t)in_rows, kk, which == 3 ? perm : nullptr, iin.p);
-        if (which == 0) {  // gramian
+            din.p, (int64_t)in_rows, kk, kp, which == 3 ? perm : nullptr, iin.p);
+        if (which == 0 || which == 1) {
             if (!S.mixed()) {
-                wb::launch_obs<double, wb::OBS_GRAM>(S, kk, S.w64.p, iin.p, nullptr, iout.p, nullptr);
+                if (which == 0) {
+                    wb::launch_obs<double, wb::OBS_GRAM>(S, kp, S.w64.p, iin.p, nullptr, iout.p, nullptr);
+                } else {
+                    int nb = 0;
+                    wb::apply_precond<double>(S, iin.p, iout.p, kp, nullptr, nb);
+                }
             } else {
                 wb::DArr<float> fi, fo;
-                fi.alloc(m * k);
-                fo.alloc(m * k);
-                wb::convert_kernel<double, float><<<S.nblk(m * k, 1), wb::kBlock, 0, S.stream>>>(iin.p, fi.p, m * k);
-                wb::launch_obs<float, wb::OBS_GRAM>(S, kk, S.w32.p, fi.p, nullptr, fo.p, nullptr);
-                wb::convert_kernel<float, double><<<S.nblk(m * k, 1), wb::kBlock, 0, S.stream>>>(fo.p, iout.p, m * k);
-                WB_CUDA(cudaStreamSynchronize(S.stream));
-            }
-        } else if (which == 1) {  // preconditioner
-            int nb = 0;
-            if (!S.mixed()) {
-                wb::apply_precond<double>(S, iin.p, iout.p, kk, nullptr, nb);
-            } else {
-                wb::DArr<float> fi, fo;
-                fi.alloc(m * k);
-                fo.alloc(m * k);
-                wb::convert_kernel<double, float><<<S.nblk(m * k, 1), wb::kBlock, 0, S.stream>>>(iin.p, fi.p, m * k);
-                wb::apply_precond<float>(S, fi.p, fo.p, kk, nullptr, nb);
-                wb::convert_kernel<float, double><<<S.nblk(m * k, 1), wb::kBlock, 0, S.stream>>>(fo.p, iout.p, m * k);
+                fi.alloc(m * kp);
+                fo.alloc(m * kp);
+                wb::convert_kernel<double, float><<<S.nblk(m * kp, 1), wb::kBlock, 0, S.stream>>>(iin.p, fi.p, m * kp);
+                if (which == 0) {
+                    wb::launch_obs<float, wb::OBS_GRAM>(S, kp, S.w32.p, fi.p, nullptr, fo.p, nullptr);
+                } else {
+                    int nb = 0;
+                    wb::apply_precond<float>(S, fi.p, fo.p, kp, nullptr, nb);
+                }
+                wb::convert_kernel<float, double><<<S.nblk(m * kp, 1), wb::kBlock, 0, S.stream>>>(fo.p, iout.p, m * kp);
                 WB_CUDA(cudaStreamSynchronize(S.stream));
             }
         } else if (which == 2) {  // D x
-            wb::launch_obs<double, wb::OBS_DX>(S, kk, nullptr, iin.p, nullptr, nullptr, iout.p);
+            wb::launch_obs<double, wb::OBS_DX>(S, kp, nullptr, iin.p, nullptr, nullptr, iout.p);
         } else {  // D'W r
-            wb::launch_obs<double, wb::OBS_RHS>(S, kk, S.w64.p, nullptr, iin.p, iout.p, nullptr);
+            wb::launch_obs<double, wb::OBS_RHS>(S, kp, S.w64.p, nullptr, iin.p, iout.p, nullptr);
         }
         wb::scatter_deinterleave_kernel<double><<<(unsigned)((out_rows + 31) / 32), 256, 0, S.stream>>>(
-            iout.p, (int64_t)out_rows, kk, which == 2 ? perm : nullptr, dout.p);
+            iout.p, (int64_t)out_rows, kk, kp, which == 2 ? perm : nullptr, dout.p);
         WB_CUDA(cudaGetLastError());
         WB_CUDA(cudaMemcpyAsync(out, dout.p, sizeof(double) * out_rows * k, cudaMemcpyDeviceToHost, S.stream));
         WB_CUDA(cudaStreamSynchronize(S.stream));
@@ -1750,6 +1754,7 @@ void within_solver_ac_arrays(const within_solver* s, int32_t i, int32_t* level_p
 const char* within_last_error(void) { return wb::g_last_error.c_str(); }
 
 int64_t within_solver_gpu_launches(const within_solver* s) { return s ? s->impl->gpu_launches : 0; }
+double within_solver_setup_time(const within_solver* s) { return s ? s->impl->setup_time : 0.0; }
 
 void within_solver_set_profiling(within_solver* s, int32_t on) {
     if (!s) return;
@@ -1764,6 +1769,5 @@ void within_solver_kernel_time(const within_solver* s, int32_t which, int64_t* l
     *launches = s->impl->prof_count[which];
     *total_ms = s->impl->prof_ms[which];
 }
-double within_solver_setup_time(const within_solver* s) { return s ? s->impl->setup_time : 0.0; }
 
 }  // extern "C"
