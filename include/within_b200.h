@@ -174,6 +174,22 @@ void within_solver_set_profiling(within_solver *solver, int32_t on);
 void within_solver_kernel_time(const within_solver *solver, int32_t which, int64_t *launches,
                                double *total_ms);
 
+/* G x = D'W(D x) like within_solver_apply_gramian, but on device buffers and without
+ * allocating: d_x and d_y are n_dofs*k RHS-major device arrays, k <= 32, and the work
+ * is queued on `cuda_stream` (NULL = the solver's stream) without waiting for it.
+ * This entry point has no counterpart in the reference.  It exists for callers that
+ * cannot allocate device memory while they run -- code under a fixed memory budget or
+ * a custom allocator, or loops that cannot take an allocation's synchronisation.  Its
+ * working space is a static 16 MiB device array (resident on every GPU that loads the
+ * library until exit), so 2 x n_dofs x k (k rounded up to 4, 8, 16 or 32) must not
+ * exceed 2^21 doubles; larger sizes are rejected with WITHIN_ERR_INVALID_ARGUMENT.
+ * The first call on a device looks the array's address up (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Every call shares the one array:
+ * calls whose work overlaps on the GPU (different streams, or several solvers) race.
+ * Arithmetic is FP64 whatever the solver's precision. */
+int within_solver_apply_gramian_noalloc(within_solver *solver, const double *d_x, size_t k,
+                                        double *d_y, void *cuda_stream);
+
 /* Message of the last failed call on this host thread ("" when none). */
 const char *within_last_error(void);
 

@@ -54,7 +54,7 @@ EXPORTED = [
     "within_solver_rmatvec_wdt", "within_solver_factor_meta", "within_solver_n_subdomains",
     "within_solver_subdomain_info", "within_solver_subdomain_indices", "within_solver_ac_sizes",
     "within_solver_ac_arrays", "within_solver_gpu_launches", "within_solver_setup_time", "within_last_error",
-    "within_solver_set_profiling", "within_solver_kernel_time",
+    "within_solver_set_profiling", "within_solver_kernel_time", "within_solver_apply_gramian_noalloc",
 ]
 
 _lib = None
@@ -104,6 +104,8 @@ def load():
     L.within_solver_setup_time.argtypes = [vp]
     L.within_solver_setup_time.restype = C.c_double
     L.within_last_error.restype = C.c_char_p
+    L.within_solver_apply_gramian_noalloc.argtypes = [vp, vp, C.c_size_t, vp, vp]
+    L.within_solver_apply_gramian_noalloc.restype = C.c_int
     L.within_solver_set_profiling.argtypes = [vp, C.c_int32]
     L.within_solver_kernel_time.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     _lib = L

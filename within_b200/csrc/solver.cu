@@ -1771,3 +1771,80 @@ void within_solver_kernel_time(const within_solver* s, int32_t which, int64_t* l
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Gramian apply that allocates nothing
+// ---------------------------------------------------------------------------
+//
+// Some callers cannot allocate device memory while they run: host code under a fixed
+// device-memory budget or a custom allocator that forbids outside allocations, and
+// loops where an allocation's synchronisation is not acceptable.  within_solver_apply_gramian_noalloc serves them:
+// its working space -- the RHS-interleaved copies of x and of y = G x -- lives in the
+// static device array below instead of cudaMalloc'd buffers.  The array is 16 MiB and
+// stays resident on every GPU that loads this library until the process exits.
+
+namespace {
+constexpr size_t kNoAllocScratchDoubles = (size_t)1 << 21;  // 16 MiB of FP64
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once per
+// device (host code may not use the symbol itself as a device pointer).
+int noalloc_scratch(double** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return wb::fail(WITHIN_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return wb::fail(WITHIN_ERR_CUDA, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return wb::fail(WITHIN_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return WITHIN_OK;
+}
+}  // namespace
+
+extern "C" int within_solver_apply_gramian_noalloc(within_solver* s, const double* d_x, size_t k, double* d_y,
+                                                   void* stream) {
+    if (!s) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "solver is null");
+    if (!d_x || !d_y) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "null buffer");
+    if (k == 0) return WITHIN_OK;
+    if (k > 32) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "at most 32 vectors per call");
+    SolverImpl& S = *s->impl;
+    const int kk = (int)k, kp = wb::pad_kp(kk);
+    const size_t m = (size_t)S.d.ndofs;
+    const size_t need = 2 * m * (size_t)kp;
+    if (need > kNoAllocScratchDoubles)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT,
+                        "n_dofs x k is too large for the no-allocation path: it needs " + std::to_string(need) +
+                            " doubles of scratch (2 x n_dofs x k rounded up to 4, 8, 16 or 32), the limit is " +
+                            std::to_string(kNoAllocScratchDoubles));
+    std::lock_guard<std::mutex> lk(S.mu);
+    double* scratch = nullptr;
+    const int rc = noalloc_scratch(&scratch);
+    if (rc != WITHIN_OK) return rc;
+    double* xi = scratch;               // x, RHS-interleaved (m x kp)
+    double* yi = scratch + m * kp;      // G x, RHS-interleaved (m x kp)
+    cudaStream_t saved = S.stream;
+    S.stream = stream ? (cudaStream_t)stream : saved;
+    int status = WITHIN_OK;
+    try {  // no std::function wrapper here: nothing on this path allocates
+        wb::gather_interleave_kernel<double><<<(unsigned)((m + 31) / 32), 256, 0, S.stream>>>(d_x, (int64_t)m, kk, kp,
+                                                                                             nullptr, xi);
+        wb::launch_obs<double, wb::OBS_GRAM>(S, kp, S.w64.p, xi, nullptr, yi, nullptr);
+        wb::scatter_deinterleave_kernel<double><<<(unsigned)((m + 31) / 32), 256, 0, S.stream>>>(yi, (int64_t)m, kk, kp,
+                                                                                                nullptr, d_y);
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches += 2;
+    } catch (const wb::CudaError& e) {
+        status = wb::fail(WITHIN_ERR_CUDA, e.what());
+    }
+    S.stream = saved;
+    return status;
+}
