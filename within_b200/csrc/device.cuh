@@ -112,9 +112,15 @@ struct StageHost {
     std::vector<int64_t> core_slot_off, core_z_off;
     std::vector<uint32_t> core_slot;
     std::vector<double> core_z;
-    // additive prolongation gather: dof j <- slots gslot[gptr[j]..gptr[j+1])
+    // additive prolongation gather: dof j <- slots gslot[gptr[j]..gptr[j+1]), with the
+    // per-slot data and back-substitution rows stored in the same (gather) order, so the
+    // prolongation reads them without going through the slot index
     std::vector<int64_t> gptr;
-    std::vector<uint32_t> gslot;
+    std::vector<uint32_t> gslot, gsub;
+    std::vector<double> gspou, ginvd;
+    std::vector<int64_t> gbs_ptr;
+    std::vector<uint32_t> gbs_col;
+    std::vector<double> gbs_val;
 };
 
 template <typename T>
@@ -141,7 +147,11 @@ struct StageDev {
     DArr<uint32_t> core_slot;
     DArr<T> core_z;
     DArr<int64_t> gptr;
-    DArr<uint32_t> gslot;
+    DArr<uint32_t> gslot, gsub;
+    DArr<T> gspou, ginvd;
+    DArr<int64_t> gbs_ptr;
+    DArr<uint32_t> gbs_col;
+    DArr<T> gbs_val;
 };
 
 constexpr int kCoreRowsPerBlock = 8;

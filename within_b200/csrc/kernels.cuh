@@ -60,10 +60,28 @@ __device__ __forceinline__ void st4(double* p, const V4<double>& v) {
     reinterpret_cast<double2*>(p)[0] = make_double2(v.a, v.b);
     reinterpret_cast<double2*>(p)[1] = make_double2(v.c, v.d);
 }
-// global atomics, one per value
-template <typename T>
-__device__ __forceinline__ void atomic_add4(T* p, const V4<T>& v) {
+// global reductions (result unused): one 16-byte vector reduction for FP32, one per
+// value for FP64; p is 16-byte aligned
+__device__ __forceinline__ void atomic_add4(float* p, const V4<float>& v) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(p), "f"(v.a), "f"(v.b), "f"(v.c), "f"(v.d)
+                 : "memory");
+}
+__device__ __forceinline__ void atomic_add4(double* p, const V4<double>& v) {
     atomicAdd(p, v.a); atomicAdd(p + 1, v.b); atomicAdd(p + 2, v.c); atomicAdd(p + 3, v.d);
+}
+// shared-memory reductions without a returned value (red.shared: no retry loop, no
+// scoreboard wait on the result)
+__device__ __forceinline__ void red_shared(float* p, float v) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void red_shared(double* p, double v) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void red_shared4(T* p, const V4<T>& v) {
+    red_shared(p, v.a); red_shared(p + 1, v.b); red_shared(p + 2, v.c); red_shared(p + 3, v.d);
 }
 template <typename T>
 __device__ __forceinline__ V4<double> to_d(const V4<T>& v) { return V4<double>(v.a, v.b, v.c, v.d); }
@@ -83,155 +101,224 @@ struct ObsChunk {
     uint32_t split;
 };
 
+// Where a non-primary factor's weighted sums go.
+enum ObsSink : int32_t {
+    SINK_GLOBAL = 0,   // run sums flushed by global atomics
+    SINK_BLOCK = 1,    // run sums flushed into a block-shared table of every level
+    SINK_HOT = 2,      // run sums of the factor's hottest levels into a block-shared table, others global
+    SINK_PRIVATE = 3,  // every observation updates a table of every level owned by its lane group
+};
+
+// A packed factor's device codes carry, above the level's kObsLevelBits bits, its hot
+// slot + 1 (0: not hot), so the observation pass needs no lookup to find a hot level.
+constexpr int kObsLevelBits = 24;
+constexpr uint32_t kObsLevelMask = (1u << kObsLevelBits) - 1u;
+constexpr int kObsMaxHot = 255;
+
+// Factor slots are in device order: slot 0 is the primary factor, the one the
+// observations are sorted by.
 struct ObsParams {
-    int64_t n;
-    int32_t Q, kp, primary;
-    int32_t smem_elems;
-    const uint32_t* codes;  // Q x n, primary-sorted order
-    int64_t off[kMaxQ];
-    // Per non-primary factor, a block-local shared-memory region of smem_len[q] values at
-    // smem_base[q] (-1: none).  full[q]: the region holds every level (level*kp + c);
-    // otherwise the factor's hottest levels: hot_slot[q][level] >= 0 is the slot and
-    // hot_level[q][slot] the level.  Other levels go to global atomics.
+    int64_t n, ns;          // observations; stride of one factor's codes (n rounded up to 4)
+    int32_t Q, kp;
+    int32_t smem_elems;     // dynamic shared memory, elements
+    int32_t priv_stride;    // elements between consecutive lane groups' private tables
+    const uint32_t* codes;  // Q x ns, primary-sorted
+    int64_t off[kMaxQ];     // first dof of each slot's level block
+    int32_t sink[kMaxQ];
+    int32_t packed[kMaxQ];  // codes carry a hot slot (see kObsLevelBits)
+    // SINK_PRIVATE: offset of the factor's table inside a group's private area;
+    // SINK_BLOCK / SINK_HOT: offset of the block-shared table (after all private areas).
     int32_t smem_base[kMaxQ];
-    int32_t smem_len[kMaxQ];
-    int32_t full[kMaxQ];
-    const int32_t* hot_slot[kMaxQ];
-    const uint32_t* hot_level[kMaxQ];
+    int32_t smem_len[kMaxQ];           // levels x kp (SINK_HOT: hot levels x kp)
+    const uint32_t* hot_level[kMaxQ];  // hot slot -> level
     const ObsChunk* chunks;
     int64_t nchunks;
 };
 
+// Add a run sum of factor slot q (device code c) into its sink.
 template <typename T>
-__device__ __forceinline__ void obs_flush(const ObsParams& P, T* sm, T* out, int q, uint32_t lvl,
-                                          const V4<T>& a, int c4) {
-    if (!a.any()) return;
-    if (P.smem_base[q] >= 0) {
-        if (P.full[q]) {
-            atomic_add4(sm + P.smem_base[q] + (size_t)lvl * P.kp + c4, a);
-            return;
-        }
-        const int32_t h = __ldg(P.hot_slot[q] + lvl);
-        if (h >= 0) {
-            atomic_add4(sm + P.smem_base[q] + (size_t)h * P.kp + c4, a);
-            return;
-        }
-    }
-    atomic_add4(out + (size_t)(P.off[q] + lvl) * P.kp + c4, a);
+__device__ __forceinline__ void obs_flush(const ObsParams& P, T* sm, T* out, int q, uint32_t c, const V4<T>& a,
+                                          int c4) {
+    const int32_t sink = P.sink[q];
+    const uint32_t lvl = P.packed[q] ? (c & kObsLevelMask) : c, hot = P.packed[q] ? (c >> kObsLevelBits) : 0u;
+    if (sink == SINK_BLOCK) red_shared4(sm + P.smem_base[q] + (size_t)lvl * P.kp + c4, a);
+    else if (sink == SINK_HOT && hot) red_shared4(sm + P.smem_base[q] + (size_t)(hot - 1) * P.kp + c4, a);
+    else atomic_add4(out + (size_t)(P.off[q] + lvl) * P.kp + c4, a);
 }
 
-// QT >= Q bounds the factor loops; NB observations are loaded and gathered together.
-// Each group walks a chunk of primary-sorted observations: the primary factor's sums
-// close with a plain store when its level changes; every other factor keeps a running
-// sum while its level repeats (a worker's firm rarely changes) and flushes it to shared
-// memory (small factor or hot level) or a global atomic.
+template <typename T>
+__device__ __forceinline__ void load_w4(const T* __restrict__ w, uint32_t i, T (&wv)[4]);
+template <>
+__device__ __forceinline__ void load_w4<float>(const float* __restrict__ w, uint32_t i, float (&wv)[4]) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(w + i));
+    wv[0] = v.x; wv[1] = v.y; wv[2] = v.z; wv[3] = v.w;
+}
+template <>
+__device__ __forceinline__ void load_w4<double>(const double* __restrict__ w, uint32_t i, double (&wv)[4]) {
+    const double2 u = __ldg(reinterpret_cast<const double2*>(w + i)), v = __ldg(reinterpret_cast<const double2*>(w + i) + 1);
+    wv[0] = u.x; wv[1] = u.y; wv[2] = v.x; wv[3] = v.y;
+}
+
+// One pass over the observations computing, with one read of the codes,
+//   GRAM:  out = D'W D x          RHS:  out = D'W yin
+//   RESID: eout = yin - D x, out = D'W eout          DX: eout = D x
+// QT == Q (QT = kMaxQ: any Q up to 16).  NB = 4: observations are taken in aligned
+// batches of 4 (one 16-byte load of 4 codes per factor, and of 4 weights), the chunk's
+// head and tail masked; NB = 1: one observation at a time.
+// Each lane group (G lanes, 4 RHS each) walks whole chunks: the primary factor's sums
+// close with a plain store when its level changes; a gathered coefficient row is reused
+// while its factor's level repeats; a non-primary factor keeps a running sum while its
+// level repeats and flushes it to its sink, except SINK_PRIVATE factors (few levels,
+// changing every observation) whose group-private table is updated without atomics.
+// The groups of a warp walk different chunks, so the per-observation steps are written
+// as short predicated updates rather than branches around long paths.  The block adds
+// its shared tables into `out` at the end.
 template <typename T, int G, int MODE, int QT, int NB>
-__global__ void __launch_bounds__(kBlock) obs_pass_kernel(ObsParams P, const T* __restrict__ w,
-                                                          const T* __restrict__ x, const T* __restrict__ yin,
-                                                          T* __restrict__ out, T* __restrict__ eout) {
+__global__ void __launch_bounds__(kBlock, 2) obs_pass_kernel(ObsParams P, const T* __restrict__ w,
+                                                             const T* __restrict__ x, const T* __restrict__ yin,
+                                                             T* __restrict__ out, T* __restrict__ eout) {
+    static_assert(NB == 1 || NB == 4, "batch of 1 or 4 observations");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
     constexpr bool kScatter = MODE != OBS_DX;
+    constexpr bool kGather = MODE != OBS_RHS;
+    constexpr uint32_t kNone = 0xffffffffu;
     if (kScatter) {
         for (int i = threadIdx.x; i < P.smem_elems; i += blockDim.x) sm[i] = T(0);
         __syncthreads();
     }
     const int c4 = (threadIdx.x & (G - 1)) * 4;
     const int kp = P.kp;
+    const int gl = threadIdx.x / G;
     const int64_t gpb = blockDim.x / G;
-    const int64_t gid = (int64_t)blockIdx.x * gpb + threadIdx.x / G;
     const int64_t ngroups = (int64_t)gridDim.x * gpb;
-    const int Q = P.Q, pq = P.primary;
-    const int64_t n = P.n;
+    const int Q = (QT == kMaxQ) ? P.Q : QT;
+    const int64_t ns = P.ns;
+    T* const priv = sm + (size_t)gl * P.priv_stride + c4;
+    T* const out0 = out + (size_t)P.off[0] * kp + c4;  // primary block, this lane's RHS
 
-    for (int64_t ch = gid; ch < P.nchunks; ch += ngroups) {
+    for (int64_t ch = (int64_t)blockIdx.x * gpb + gl; ch < P.nchunks; ch += ngroups) {
         const ObsChunk C = P.chunks[ch];
         uint32_t lvl = C.lvl_begin;
         V4<T> acc(T(0));
-        uint32_t run_l[QT];
-        V4<T> run_a[QT];
+        uint32_t run_l[QT], cl[QT];
+        V4<T> run_a[QT], cv[QT];
 #pragma unroll
-        for (int q = 0; q < QT; ++q) { run_l[q] = 0xffffffffu; run_a[q] = V4<T>(T(0)); }
-        for (uint32_t base = C.obs_begin; base < C.obs_end; base += NB) {
-            const uint32_t cnt = min((uint32_t)NB, C.obs_end - base);
+        for (int q = 0; q < QT; ++q) {
+            run_l[q] = kNone;
+            cl[q] = kNone;
+            run_a[q] = V4<T>(T(0));
+            cv[q] = V4<T>(T(0));
+        }
+        const uint32_t first = (NB == 4) ? (C.obs_begin & ~3u) : C.obs_begin;
+        for (uint32_t base = first; base < C.obs_end; base += NB) {
             uint32_t lq[NB][QT];
             T wv[NB];
-            V4<T> s[NB];
-            // independent loads of NB observations: codes, weights, then all gathers
+            if constexpr (NB == 4) {
 #pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const uint32_t i = base + (b < (int)cnt ? b : 0);
-#pragma unroll
-                for (int q = 0; q < QT; ++q) lq[b][q] = q < Q ? __ldg(P.codes + (size_t)q * n + i) : 0u;
-                wv[b] = (MODE == OBS_DX || w == nullptr) ? T(1) : __ldg(w + i);
-            }
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                s[b] = V4<T>(T(0));
-                if (MODE != OBS_RHS) {
-#pragma unroll
-                    for (int q = 0; q < QT; ++q)
-                        if (q < Q) s[b] += ldg4(x + (size_t)(P.off[q] + lq[b][q]) * kp + c4);
+                for (int q = 0; q < QT; ++q) {
+                    if (q < Q) {
+                        const uint4 c = __ldg(reinterpret_cast<const uint4*>(P.codes + (size_t)q * ns + base));
+                        lq[0][q] = c.x; lq[1][q] = c.y; lq[2][q] = c.z; lq[3][q] = c.w;
+                    }
                 }
-                if (MODE == OBS_RHS || MODE == OBS_RESID) {
-                    const uint32_t i = base + (b < (int)cnt ? b : 0);
+                if (MODE != OBS_DX && w != nullptr) load_w4(w, base, wv);
+                else { wv[0] = wv[1] = wv[2] = wv[3] = T(1); }
+            } else {
+#pragma unroll
+                for (int q = 0; q < QT; ++q)
+                    if (q < Q) lq[0][q] = __ldg(P.codes + (size_t)q * ns + base);
+                wv[0] = (MODE != OBS_DX && w != nullptr) ? __ldg(w + base) : T(1);
+            }
+            V4<T> s[NB];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const uint32_t i = base + b;
+                const bool act = (NB == 1) || (i >= C.obs_begin && i < C.obs_end);
+                s[b] = V4<T>(T(0));
+                if (kGather && act) {
+#pragma unroll
+                    for (int q = 0; q < QT; ++q) {
+                        if (q >= Q) continue;
+                        const uint32_t c = lq[b][q];
+                        const T* xr = x + (size_t)(P.off[q] + (P.packed[q] ? (c & kObsLevelMask) : c)) * kp + c4;
+                        if (QT == kMaxQ || (q > 0 && P.sink[q] == SINK_PRIVATE)) {
+                            s[b] += ldg4(xr);  // no reuse: registers, or a level that changes every time
+                            continue;
+                        }
+                        if (c != cl[q]) cv[q] = ldg4(xr);
+                        cl[q] = c;
+                        s[b] += cv[q];
+                    }
+                }
+                if ((MODE == OBS_RHS || MODE == OBS_RESID) && act) {
                     const V4<T> yv = ld4(yin + (size_t)i * kp + c4);
                     s[b] = (MODE == OBS_RHS) ? yv : yv - s[b];
                 }
             }
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
-                if (b >= (int)cnt) break;
                 const uint32_t i = base + b;
+                const bool act = (NB == 1) || (i >= C.obs_begin && i < C.obs_end);
+                if (!act) continue;
                 if (MODE == OBS_DX || MODE == OBS_RESID) st4(eout + (size_t)i * kp + c4, s[b]);
                 if (!kScatter) continue;
                 const V4<T> t = wv[b] * s[b];
-                const uint32_t p = lq[b][pq];
-                while (lvl < p) {  // primary level complete: plain store (zero for empty levels)
-                    st4(out + (size_t)(P.off[pq] + lvl) * kp + c4, acc);
+                const uint32_t p = lq[b][0];
+                if (p != lvl) {  // primary level complete: plain store
+                    st4(out0 + (size_t)lvl * kp, acc);
+                    for (uint32_t l = lvl + 1; l < p; ++l) st4(out0 + (size_t)l * kp, V4<T>(T(0)));  // empty levels
                     acc = V4<T>(T(0));
-                    ++lvl;
+                    lvl = p;
                 }
                 acc += t;
 #pragma unroll
-                for (int q = 0; q < QT; ++q) {
-                    if (q >= Q || q == pq) continue;
-                    if (lq[b][q] == run_l[q]) {
-                        run_a[q] += t;
-                    } else {
-                        if (run_l[q] != 0xffffffffu) obs_flush(P, sm, out, q, run_l[q], run_a[q], c4);
-                        run_l[q] = lq[b][q];
-                        run_a[q] = t;
+                for (int q = 1; q < QT; ++q) {
+                    if (q >= Q) continue;
+                    const uint32_t c = lq[b][q];
+                    if (P.sink[q] == SINK_PRIVATE) {
+                        T* pt = priv + P.smem_base[q] + (size_t)c * kp;
+                        st4(pt, ld4(pt) + t);
+                        continue;
                     }
+                    const bool brk = c != run_l[q];
+                    if (brk && run_l[q] != kNone) obs_flush(P, sm, out, q, run_l[q], run_a[q], c4);
+                    run_a[q] = brk ? t : run_a[q] + t;
+                    run_l[q] = c;
                 }
             }
         }
         if (kScatter) {
 #pragma unroll
-            for (int q = 0; q < QT; ++q)
-                if (q < Q && q != pq && run_l[q] != 0xffffffffu) obs_flush(P, sm, out, q, run_l[q], run_a[q], c4);
+            for (int q = 1; q < QT; ++q)
+                if (q < Q && run_l[q] != kNone) obs_flush(P, sm, out, q, run_l[q], run_a[q], c4);
             if (C.split) {
-                atomic_add4(out + (size_t)(P.off[pq] + C.lvl_begin) * kp + c4, acc);
+                atomic_add4(out0 + (size_t)C.lvl_begin * kp, acc);
             } else {
-                while (lvl < C.lvl_end) {
-                    st4(out + (size_t)(P.off[pq] + lvl) * kp + c4, acc);
+                for (; lvl < C.lvl_end; ++lvl) {
+                    st4(out0 + (size_t)lvl * kp, acc);
                     acc = V4<T>(T(0));
-                    ++lvl;
                 }
             }
         }
     }
     if (kScatter && P.smem_elems > 0) {
         __syncthreads();
-        // the block's partial sums of each shared-memory region, one atomic per nonzero entry
-        for (int q = 0; q < Q; ++q) {
-            if (P.smem_base[q] < 0) continue;
-            for (int idx = threadIdx.x; idx < P.smem_len[q]; idx += blockDim.x) {
-                const T v = sm[P.smem_base[q] + idx];
-                if (v == T(0)) continue;
-                const int slot = idx / kp, cc = idx % kp;
-                const uint32_t lev = P.full[q] ? (uint32_t)slot : P.hot_level[q][slot];
-                atomicAdd(out + (size_t)(P.off[q] + lev) * kp + cc, v);
+        // the block's shared tables into `out`: one atomic per nonzero entry
+        for (int q = 1; q < Q; ++q) {
+            const int32_t sink = P.sink[q];
+            if (sink == SINK_GLOBAL) continue;
+            for (int e = threadIdx.x; e < P.smem_len[q]; e += blockDim.x) {
+                T v = T(0);
+                uint32_t lev;
+                if (sink == SINK_PRIVATE) {
+                    for (int g = 0; g < (int)gpb; ++g) v += sm[(size_t)g * P.priv_stride + P.smem_base[q] + e];
+                    lev = (uint32_t)(e / kp);
+                } else {
+                    v = sm[P.smem_base[q] + e];
+                    lev = (sink == SINK_BLOCK) ? (uint32_t)(e / kp) : P.hot_level[q][e / kp];
+                }
+                if (v != T(0)) atomicAdd(out + (size_t)(P.off[q] + lev) * kp + e % kp, v);
             }
         }
     }
@@ -396,6 +483,11 @@ enum CsrEpi { EPI_ACC = 0, EPI_PIVOT = 1 };
 // dst[row_slot] (+)= sum_e val[e] * src[col[e]]   per RHS
 //   EPI_ACC:   dst[row] += acc (partial rows atomically)
 //   EPI_PIVOT: dst[row]  = dst[row] * rscale[row] + acc   (backward AC sweep; never split)
+// One warp per chunk (a row, or a piece of a long row): its 32/G lane groups take the
+// row's entries in turn, so a row costs one round of gathers instead of a chain of
+// them (the sweeps of one AC level are latency-bound), then combine with shuffles.
+// src and dst may be the same vector: a row's own slot is never among its columns'
+// slots in one launch (an AC level is an independent set).
 template <typename T, int G, int EPI>
 __global__ void __launch_bounds__(kBlock) csr_rows_kernel(const CsrChunk* __restrict__ chunks, int64_t nchunks,
                                                           const uint32_t* __restrict__ row_slot,
@@ -403,30 +495,45 @@ __global__ void __launch_bounds__(kBlock) csr_rows_kernel(const CsrChunk* __rest
                                                           const uint32_t* __restrict__ col,
                                                           const T* __restrict__ val, const T* __restrict__ rscale,
                                                           const T* src, T* dst, int kp) {
-    const int c4 = (threadIdx.x & (G - 1)) * 4;
-    const int64_t gpb = blockDim.x / G;
-    const int64_t ng = (int64_t)gridDim.x * gpb;
-    for (int64_t ch = (int64_t)blockIdx.x * gpb + threadIdx.x / G; ch < nchunks; ch += ng) {
+    constexpr int NG = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / G;
+    const int c4 = (lane & (G - 1)) * 4;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t ch = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < nchunks; ch += nw) {
         const CsrChunk C = chunks[ch];
         for (uint32_t row = C.row_begin; row < C.row_end; ++row) {
             const int64_t rb = ptr[row], re = ptr[row + 1];
             const int64_t e0 = max(rb, C.nz_begin), e1 = min(re, C.nz_end);
             V4<T> acc(T(0));
-            int64_t e = e0;
-            for (; e + 4 <= e1; e += 4) {  // four independent gathers in flight
-                const uint32_t j0 = __ldg(col + e), j1 = __ldg(col + e + 1), j2 = __ldg(col + e + 2), j3 = __ldg(col + e + 3);
-                const T v0 = __ldg(val + e), v1 = __ldg(val + e + 1), v2 = __ldg(val + e + 2), v3 = __ldg(val + e + 3);
+            int64_t e = e0 + grp;
+            for (; e + 3 * NG < e1; e += 4 * NG) {  // four independent gathers in flight
+                const uint32_t j0 = __ldg(col + e), j1 = __ldg(col + e + NG);
+                const uint32_t j2 = __ldg(col + e + 2 * NG), j3 = __ldg(col + e + 3 * NG);
+                const T v0 = __ldg(val + e), v1 = __ldg(val + e + NG), v2 = __ldg(val + e + 2 * NG), v3 = __ldg(val + e + 3 * NG);
                 const V4<T> s0 = ld4(src + (size_t)j0 * kp + c4), s1 = ld4(src + (size_t)j1 * kp + c4);
                 const V4<T> s2 = ld4(src + (size_t)j2 * kp + c4), s3 = ld4(src + (size_t)j3 * kp + c4);
-                acc += v0 * s0; acc += v1 * s1; acc += v2 * s2; acc += v3 * s3;
+                acc += v0 * s0;
+                acc += v1 * s1;
+                acc += v2 * s2;
+                acc += v3 * s3;
             }
-            for (; e < e1; ++e) acc += __ldg(val + e) * ld4(src + (size_t)__ldg(col + e) * kp + c4);
-            T* d = dst + (size_t)row_slot[row] * kp + c4;
-            if (EPI == EPI_ACC) {
-                if (e0 != rb || e1 != re) atomic_add4(d, acc);
-                else st4(d, ld4(d) + acc);
-            } else {
-                st4(d, rscale[row] * ld4(d) + acc);
+            for (; e < e1; e += NG) acc += __ldg(val + e) * ld4(src + (size_t)__ldg(col + e) * kp + c4);
+#pragma unroll
+            for (int off = G; off < 32; off <<= 1) {
+                acc.a += __shfl_xor_sync(0xffffffffu, acc.a, off);
+                acc.b += __shfl_xor_sync(0xffffffffu, acc.b, off);
+                acc.c += __shfl_xor_sync(0xffffffffu, acc.c, off);
+                acc.d += __shfl_xor_sync(0xffffffffu, acc.d, off);
+            }
+            if (grp == 0) {
+                T* d = dst + (size_t)row_slot[row] * kp + c4;
+                if (EPI == EPI_ACC) {
+                    if (e0 != rb || e1 != re) atomic_add4(d, acc);
+                    else st4(d, ld4(d) + acc);
+                } else {
+                    st4(d, rscale[row] * ld4(d) + acc);
+                }
             }
         }
     }
@@ -610,17 +717,31 @@ __device__ __forceinline__ void sub_means(const SubMeans& M, uint32_t s, int kp,
     m2 = inv * (k2 + sb - I * m0);
 }
 
+// Per-subdomain means once per apply: mm[s][0] = m0 = S0/n, mm[s][1] = m2.
+__global__ void sub_means_kernel(int32_t nsub, int kp, SubMeans M, double* __restrict__ mm) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)nsub * kp) return;
+    const int64_t s = i / kp, c = i % kp;
+    const double inv = 1.0 / (double)M.sub_n[s];
+    const double m0 = M.S0[i] * inv;
+    mm[(s * 2) * kp + c] = m0;
+    mm[(s * 2 + 1) * kp + c] = inv * (M.M2[i] + M.SB[i] - M.I[s] * m0);
+}
+
 // Additive prolongation as a gather over global dofs (no atomics), with the back
-// substitution of eliminated slots folded in: z[j] = sum_{slots l of j} spou_l (sol_l - m2).
-// Dofs in no subdomain get z = 0.  Optionally the partial dot r.z for CG.
+// substitution of eliminated slots folded in: z[j] = sum_{slots l of j} spou_l (sol_l - m2),
+// sol_e = invd_e (spou_e r_j - m0) + invd_e sum_k C_ek v_k on eliminated slots, v_l on
+// kept ones.  The slot data and back-substitution rows are read in gather order, so a
+// dof's loads depend only on gptr[j].  Dofs in no subdomain get z = 0.  Optionally the
+// partial dot r.z for CG.
 template <typename T, int G>
 __global__ void __launch_bounds__(kBlock) prolong_kernel(int64_t m, const int64_t* __restrict__ gptr,
                                                          const uint32_t* __restrict__ gslot,
-                                                         const uint32_t* __restrict__ sub_of,
-                                                         const T* __restrict__ spou, const T* __restrict__ invd,
-                                                         const int64_t* __restrict__ bs_ptr,
-                                                         const uint32_t* __restrict__ bs_col,
-                                                         const T* __restrict__ bs_val, SubMeans M,
+                                                         const uint32_t* __restrict__ gsub,
+                                                         const T* __restrict__ gspou, const T* __restrict__ ginvd,
+                                                         const int64_t* __restrict__ gbs_ptr,
+                                                         const uint32_t* __restrict__ gbs_col,
+                                                         const T* __restrict__ gbs_val, const double* __restrict__ mm,
                                                          const T* __restrict__ v, const T* __restrict__ r,
                                                          T* __restrict__ z, int kp, double* __restrict__ part) {
     const int c4 = (threadIdx.x & (G - 1)) * 4;
@@ -629,13 +750,30 @@ __global__ void __launch_bounds__(kBlock) prolong_kernel(int64_t m, const int64_
     for (int64_t j = (int64_t)blockIdx.x * rpb + threadIdx.x / G; j < m; j += (int64_t)gridDim.x * rpb) {
         const V4<double> rj = to_d(ld4(r + (size_t)j * kp + c4));
         V4<double> acc(0.0);
-        for (int64_t e = gptr[j]; e < gptr[j + 1]; ++e) {
-            const uint32_t l = gslot[e];
-            const uint32_t s = sub_of[l];
-            V4<double> m0, m2;
-            sub_means(M, s, kp, c4, m0, m2);
-            const double sp = (double)spou[l];
-            const V4<double> sol = slot_solution<T>(l, sp * rj, m0, invd[l], bs_ptr, bs_col, bs_val, v, kp, c4);
+        const int64_t e0 = gptr[j], e1 = gptr[j + 1];
+        for (int64_t e = e0; e < e1; ++e) {
+            const uint32_t s = gsub[e];
+            const double sp = (double)gspou[e];
+            const T id = ginvd[e];
+            const V4<double> m0 = ld4(mm + (size_t)(2 * s) * kp + c4), m2 = ld4(mm + (size_t)(2 * s + 1) * kp + c4);
+            V4<double> sol;
+            if (id == T(0)) {
+                sol = to_d(ld4(v + (size_t)gslot[e] * kp + c4));
+            } else {
+                V4<T> bs(T(0));
+                const int64_t t0 = gbs_ptr[e], t1 = gbs_ptr[e + 1];
+                int64_t t = t0;
+                for (; t + 2 <= t1; t += 2) {
+                    const uint32_t j0 = __ldg(gbs_col + t), j1 = __ldg(gbs_col + t + 1);
+                    const T v0 = __ldg(gbs_val + t), v1 = __ldg(gbs_val + t + 1);
+                    const V4<T> s0 = ld4(v + (size_t)j0 * kp + c4), s1 = ld4(v + (size_t)j1 * kp + c4);
+                    bs += v0 * s0;
+                    bs += v1 * s1;
+                }
+                if (t < t1) bs += __ldg(gbs_val + t) * ld4(v + (size_t)__ldg(gbs_col + t) * kp + c4);
+                const double idd = (double)id;
+                sol = idd * (sp * rj - m0) + idd * to_d(bs);
+            }
             acc += sp * (sol - m2);
         }
         const V4<T> zt = from_d<T>(acc);
@@ -761,9 +899,9 @@ __global__ void core_gemv_kernel(const int32_t* __restrict__ core_of_block, cons
     const int g = core_of_block[blockIdx.x];
     const int r = core_n[g];
     const uint32_t* slots = core_slot + core_slot_off[g];
-    for (int e = threadIdx.x; e < r * kc; e += blockDim.x) {
-        const int c = e / r, a = e % r;
-        yc[e] = v[(size_t)slots[a] * kp + c0 + c];
+    for (int e = threadIdx.x; e < r * kc; e += blockDim.x) {  // a slot's kc values are contiguous in v
+        const int a = e / kc, c = e % kc;
+        yc[c * r + a] = v[(size_t)slots[a] * kp + c0 + c];
     }
     __syncthreads();
     const T* Zg = Z + core_z_off[g];

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -179,7 +180,7 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
             for (auto& e : row.second) { st.fwd.col.push_back(e.first); st.fwd.val.push_back(e.second); }
             st.fwd.ptr.push_back((int64_t)st.fwd.col.size());
         }
-        auto fc = make_chunks(st.fwd.ptr, r0, st.fwd.nrows(), 64, 4, true);
+        auto fc = make_chunks(st.fwd.ptr, r0, st.fwd.nrows(), 64, 1, true);  // long rows in pieces (atomics)
         st.fwd.chunks.insert(st.fwd.chunks.end(), fc.begin(), fc.end());
         st.fwd_lp.push_back((int64_t)st.fwd.chunks.size());
         const int64_t b0 = st.bwd.nrows();
@@ -189,11 +190,12 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
             for (auto& e : std::get<2>(row)) { st.bwd.col.push_back(e.first); st.bwd.val.push_back(e.second); }
             st.bwd.ptr.push_back((int64_t)st.bwd.col.size());
         }
-        auto bc = make_chunks(st.bwd.ptr, b0, st.bwd.nrows(), 64, 4, false);
+        auto bc = make_chunks(st.bwd.ptr, b0, st.bwd.nrows(), 256, 1, false);
         st.bwd.chunks.insert(st.bwd.chunks.end(), bc.begin(), bc.end());
         st.bwd_lp.push_back((int64_t)st.bwd.chunks.size());
     }
-    st.keep.chunks = make_chunks(st.keep.ptr, 0, st.keep.nrows(), 256, 8, true);
+    // one warp per chunk (csr_rows_kernel): single rows, long rows in pieces of 256
+    st.keep.chunks = make_chunks(st.keep.ptr, 0, st.keep.nrows(), 256, 1, true);
     if (with_gather) {
         st.gptr.assign((size_t)ndofs + 1, 0);
         for (uint32_t g : st.gidx) st.gptr[g + 1]++;
@@ -201,6 +203,24 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
         st.gslot.resize(st.gidx.size());
         std::vector<int64_t> cur(st.gptr.begin(), st.gptr.end() - 1);
         for (size_t l = 0; l < st.gidx.size(); ++l) st.gslot[cur[st.gidx[l]]++] = (uint32_t)l;
+        const size_t ng = st.gslot.size();
+        st.gsub.resize(ng);
+        st.gspou.resize(ng);
+        st.ginvd.resize(ng);
+        st.gbs_ptr.assign(1, 0);
+        st.gbs_col.reserve(st.bs_col.size());
+        st.gbs_val.reserve(st.bs_val.size());
+        for (size_t e = 0; e < ng; ++e) {
+            const uint32_t l = st.gslot[e];
+            st.gsub[e] = st.sub_of[l];
+            st.gspou[e] = st.spou[l];
+            st.ginvd[e] = st.invd[l];
+            for (int64_t t = st.bs_ptr[l]; t < st.bs_ptr[l + 1]; ++t) {
+                st.gbs_col.push_back(st.bs_col[t]);
+                st.gbs_val.push_back(st.bs_val[t]);
+            }
+            st.gbs_ptr.push_back((int64_t)st.gbs_col.size());
+        }
     }
     return st;
 }
@@ -234,9 +254,11 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
     upload_csr(d.keep, h.keep);
     upload_csr(d.fwd, h.fwd);
     upload_csr(d.bwd, h.bwd);
-    d.bs_ptr.upload(h.bs_ptr);
-    d.bs_col.upload(h.bs_col);
-    d.bs_val.upload_cast(h.bs_val);
+    if (h.gptr.empty()) {  // slot-order back substitution (multiplicative stages)
+        d.bs_ptr.upload(h.bs_ptr);
+        d.bs_col.upload(h.bs_col);
+        d.bs_val.upload_cast(h.bs_val);
+    }
     d.fwd_lp = h.fwd_lp;
     d.bwd_lp = h.bwd_lp;
     d.ndense = (int32_t)h.dn_n.size();
@@ -256,6 +278,12 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
     d.core_z.upload_cast(h.core_z);
     d.gptr.upload(h.gptr);
     d.gslot.upload(h.gslot);
+    d.gsub.upload(h.gsub);
+    d.gspou.upload_cast(h.gspou);
+    d.ginvd.upload_cast(h.ginvd);
+    d.gbs_ptr.upload(h.gbs_ptr);
+    d.gbs_col.upload(h.gbs_col);
+    d.gbs_val.upload_cast(h.gbs_val);
 }
 
 }  // namespace
@@ -266,6 +294,7 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
 
 struct Workspace {
     int kp = 0;
+    int64_t gen = 0;                         // bumped whenever the buffers move
     DArr<double> yi, e;                      // n x kp interleaved (primary-sorted)
     DArr<double> b, x, r, gx;                // m x kp FP64: rhs, solution, refinement residual, G x
     DArr<double> cx, cr, dz, dp, dap;        // FP64 inner CG vectors
@@ -276,7 +305,7 @@ struct Workspace {
     DArr<float> fcore_tmp;
     DArr<double> rwork;                      // multiplicative residual
     DArr<float> frwork;
-    DArr<double> msum;                       // 4 x nsub x kp: S0, SB, M1, M2
+    DArr<double> msum;                       // 6 x nsub x kp: S0, SB, M1, M2, means (m0, m2)
     DArr<double> part;                       // block partial sums
     DArr<double> red;                        // reduced partial sums (kp)
     // per-RHS Krylov state
@@ -303,9 +332,9 @@ struct SolverImpl {
     ObsParams obs{};
     bool has_split = false;
     // hottest levels of every non-primary factor, for the observation pass
-    std::vector<DArr<int32_t>> hot_slot;
     std::vector<DArr<uint32_t>> hot_level;
     std::vector<int32_t> hot_count;
+    std::vector<int> dev_factor;  // device factor slot -> design factor (slot 0 = primary)
     // Schwarz stages
     std::vector<StageDev<double>> stages64;
     std::vector<StageDev<float>> stages32;
@@ -328,10 +357,15 @@ struct SolverImpl {
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
     int64_t prof_count[4] = {0, 0, 0, 0};
     double prof_ms[4] = {0, 0, 0, 0};
+    // One CG iteration captured as a CUDA graph, reused while its buffers stay the same.
+    cudaGraphExec_t cg_exec = nullptr;
+    std::array<uintptr_t, 9> cg_key{};
+    int64_t cg_launches = 0;  // kernels in one captured iteration
 
     ~SolverImpl() {
         for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
         for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+        if (cg_exec) cudaGraphExecDestroy(cg_exec);
         if (h_active) cudaFreeHost(h_active);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -442,87 +476,140 @@ void upload_design(SolverImpl& S) {
     S.perm_identity = true;
     for (int64_t i = 0; i < d.n; ++i)
         if (perm[i] != (uint32_t)i) { S.perm_identity = false; break; }
-    std::vector<uint32_t> codes((size_t)d.n * d.Q);
+    // device factor order: the primary factor first, the others in their order
+    S.dev_factor.clear();
+    S.dev_factor.push_back(S.primary);
     for (int q = 0; q < d.Q; ++q)
-        for (int64_t i = 0; i < d.n; ++i) codes[(size_t)q * d.n + i] = d.codes[(size_t)q * d.n + perm[i]];
-    S.codes.upload(codes);
+        if (q != S.primary) S.dev_factor.push_back(q);
+    // hot levels: the 255 most frequent levels (hit >= 64 times) of each non-primary
+    // factor with more than 256 levels and fewer than 2^24; their codes on the device
+    // carry the hot slot + 1 in bits 24-31 (kObsLevelBits) next to the level
+    S.hot_level.clear();
+    S.hot_level.resize(d.Q);
+    S.hot_count.assign(d.Q, 0);
+    std::vector<std::vector<uint32_t>> hot_tag((size_t)d.Q);  // level -> tag (slot + 1) << 24, or 0
+    ObsParams& P = S.obs;
+    for (int sl = 1; sl < d.Q; ++sl) {
+        P.packed[sl] = 0;
+        P.hot_level[sl] = nullptr;
+        const int q = S.dev_factor[sl];
+        const int64_t L = d.nlev[q];
+        if (L <= 256 || L >= ((int64_t)1 << kObsLevelBits)) continue;
+        std::vector<int64_t> cnt((size_t)L, 0);
+        const uint32_t* c = d.codes.data() + (size_t)q * d.n;
+        for (int64_t i = 0; i < d.n; ++i) cnt[c[i]]++;
+        std::vector<uint32_t> order((size_t)L);
+        std::iota(order.begin(), order.end(), 0u);
+        const int64_t h = std::min<int64_t>(kObsMaxHot, L);
+        std::partial_sort(order.begin(), order.begin() + h, order.end(),
+                          [&](uint32_t a, uint32_t b) { return cnt[a] != cnt[b] ? cnt[a] > cnt[b] : a < b; });
+        std::vector<uint32_t> lev;
+        hot_tag[sl].assign((size_t)L, 0u);
+        for (int64_t a = 0; a < h; ++a) {
+            if (cnt[order[a]] < 64) break;
+            hot_tag[sl][order[a]] = (uint32_t)(lev.size() + 1) << kObsLevelBits;
+            lev.push_back(order[a]);
+        }
+        P.packed[sl] = 1;
+        S.hot_count[sl] = (int32_t)lev.size();
+        S.hot_level[sl].upload(lev);
+        P.hot_level[sl] = S.hot_level[sl].p;
+    }
+    // codes and weights padded to a multiple of 4 observations (16-byte batch loads)
+    const int64_t ns = (d.n + 3) / 4 * 4;
+    {
+        std::vector<uint32_t> codes((size_t)ns * d.Q, 0u);
+        for (int s = 0; s < d.Q; ++s) {
+            const uint32_t* src = d.codes.data() + (size_t)S.dev_factor[s] * d.n;
+            uint32_t* dst = codes.data() + (size_t)s * ns;
+            if (P.packed[s]) {
+                const std::vector<uint32_t>& tag = hot_tag[s];
+                for (int64_t i = 0; i < d.n; ++i) dst[i] = src[perm[i]] | tag[src[perm[i]]];
+            } else {
+                for (int64_t i = 0; i < d.n; ++i) dst[i] = src[perm[i]];
+            }
+        }
+        S.codes.upload(codes);
+    }
     if (!S.perm_identity) S.perm.upload(perm);
     if (!d.w.empty()) {
-        std::vector<double> w((size_t)d.n);
+        std::vector<double> w((size_t)ns, 0.0);
         for (int64_t i = 0; i < d.n; ++i) w[i] = d.w[perm[i]];
         S.w64.upload(w);
         if (S.mixed()) S.w32.upload_cast(w);
     }
     auto ch = make_obs_chunks(lvl_ptr, np, S.has_split);
     S.chunks.upload(ch);
-    ObsParams& P = S.obs;
     P.n = d.n;
+    P.ns = ns;
     P.Q = d.Q;
-    P.primary = S.primary;
+    P.packed[0] = 0;
     P.codes = S.codes.p;
-    for (int q = 0; q < d.Q; ++q) P.off[q] = d.off[q];
+    for (int s = 0; s < d.Q; ++s) P.off[s] = d.off[S.dev_factor[s]];
     P.chunks = S.chunks.p;
     P.nchunks = (int64_t)ch.size();
-    // hot levels: the 256 most frequent levels (hit >= 64 times) of each non-primary factor
-    constexpr int kHot = 256;
-    S.hot_slot.resize(d.Q);
-    S.hot_level.resize(d.Q);
-    S.hot_count.assign(d.Q, 0);
-    for (int q = 0; q < d.Q; ++q) {
-        if (q == S.primary) continue;
-        const int64_t L = d.nlev[q];
-        std::vector<int64_t> cnt((size_t)L, 0);
-        const uint32_t* c = d.codes.data() + (size_t)q * d.n;
-        for (int64_t i = 0; i < d.n; ++i) cnt[c[i]]++;
-        std::vector<uint32_t> order((size_t)L);
-        std::iota(order.begin(), order.end(), 0u);
-        const int64_t h = std::min<int64_t>(kHot, L);
-        std::partial_sort(order.begin(), order.begin() + h, order.end(),
-                          [&](uint32_t a, uint32_t b) { return cnt[a] != cnt[b] ? cnt[a] > cnt[b] : a < b; });
-        std::vector<int32_t> slot((size_t)L, -1);
-        std::vector<uint32_t> lev;
-        for (int64_t a = 0; a < h; ++a) {
-            if (cnt[order[a]] < 64) break;
-            slot[order[a]] = (int32_t)lev.size();
-            lev.push_back(order[a]);
-        }
-        S.hot_count[q] = (int32_t)lev.size();
-        S.hot_slot[q].upload(slot);
-        S.hot_level[q].upload(lev);
-        P.hot_slot[q] = S.hot_slot[q].p;
-        P.hot_level[q] = S.hot_level[q].p;
-    }
 }
 
-// Shared-memory regions for kp RHS: a non-primary factor with <= 256 levels keeps all
-// of them, a larger one its hot levels, within a 40 KB budget per block.
+// Shared-memory plan of the observation pass for kp interleaved RHS of `elem` bytes:
+// the smallest non-primary factors get a table private to every lane group while those
+// fit (kObsPrivBytes per block); then factors of <= 256 levels get a block-shared table
+// and the others their hottest levels, within kObsSmemBytes per block (two blocks/SM).
+constexpr int64_t kObsPrivBytes = 96 * 1024, kObsSmemBytes = 110 * 1024;
+
 void obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
     P = S.obs;
     P.kp = kp;
-    int32_t used = 0;
-    const int32_t budget = (int32_t)(40960 / elem);
-    for (int q = 0; q < S.d.Q; ++q) {
-        P.smem_base[q] = -1;
-        P.smem_len[q] = 0;
-        P.full[q] = 0;
-        if (q == S.primary) continue;
-        const int64_t len = S.d.nlev[q] * kp;
-        if (S.d.nlev[q] <= 256 && used + len <= budget) {
-            P.smem_base[q] = used;
-            P.smem_len[q] = (int32_t)len;
-            P.full[q] = 1;
-            used += (int32_t)len;
+    const int G = group_for(kp);
+    const int64_t gpb = kBlock / G;
+    for (int sl = 0; sl < kMaxQ; ++sl) {
+        P.sink[sl] = SINK_GLOBAL;
+        P.smem_base[sl] = -1;
+        P.smem_len[sl] = 0;
+    }
+    // private tables; a group's area stride is padded so that the 16-byte accesses of
+    // neighbouring groups at the same level fall in different banks
+    const int64_t target = elem == 4 ? (16 * G) % 128 : 16;
+    auto padded = [&](int64_t r) {
+        int64_t st = r;
+        while ((st * (int64_t)elem) % 128 != target) ++st;
+        return st;
+    };
+    std::vector<int> order;
+    for (int sl = 1; sl < S.d.Q; ++sl) order.push_back(sl);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return S.d.nlev[S.dev_factor[a]] < S.d.nlev[S.dev_factor[b]]; });
+    int64_t raw = 0;
+    for (int sl : order) {
+        const int64_t len = S.d.nlev[S.dev_factor[sl]] * kp;
+        if (gpb * padded(raw + len) * (int64_t)elem > kObsPrivBytes) break;
+        P.sink[sl] = SINK_PRIVATE;
+        P.smem_base[sl] = (int32_t)raw;
+        P.smem_len[sl] = (int32_t)len;
+        raw += len;
+    }
+    P.priv_stride = raw > 0 ? (int32_t)padded(raw) : 0;
+    int64_t used = gpb * P.priv_stride;
+    const int64_t budget = kObsSmemBytes / (int64_t)elem;
+    for (int sl : order) {
+        if (P.sink[sl] == SINK_PRIVATE) continue;
+        const int64_t nl = S.d.nlev[S.dev_factor[sl]];
+        if (nl <= 256 && used + nl * kp <= budget) {
+            P.sink[sl] = SINK_BLOCK;
+            P.smem_base[sl] = (int32_t)used;
+            P.smem_len[sl] = (int32_t)(nl * kp);
+            used += nl * kp;
         }
     }
-    for (int q = 0; q < S.d.Q; ++q) {
-        if (q == S.primary || P.full[q] || S.hot_count[q] == 0) continue;
-        const int32_t len = S.hot_count[q] * kp;
+    for (int sl : order) {
+        if (P.sink[sl] != SINK_GLOBAL || S.hot_count[sl] == 0) continue;
+        const int64_t len = (int64_t)S.hot_count[sl] * kp;
         if (used + len > budget) continue;  // the whole hot table or none of it
-        P.smem_base[q] = used;
-        P.smem_len[q] = len;
+        P.sink[sl] = SINK_HOT;
+        P.smem_base[sl] = (int32_t)used;
+        P.smem_len[sl] = (int32_t)len;
         used += len;
     }
-    P.smem_elems = used;
+    P.smem_elems = (int32_t)used;
 }
 
 template <typename T, int MODE>
@@ -542,17 +629,22 @@ void launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* 
         }
     }
     const size_t smem = (size_t)P.smem_elems * sizeof(T);
-    const int grid = S.nblk(P.nchunks, G, 4);
+    const int grid = S.nblk(P.nchunks, G, 2);
     auto go = [&](auto kern) {
         if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, kBlock, smem, S.stream>>>(P, w, x, yin, out, eout);
         WB_CUDA(cudaGetLastError());
         S.gpu_launches++;
     };
-    constexpr int NB = std::is_same<T, float>::value ? 4 : 2;
-#define WB_OBS_Q(GV)                                                 \
-    if (S.d.Q <= 4) go(obs_pass_kernel<T, GV, MODE, 4, NB>);         \
-    else go(obs_pass_kernel<T, GV, MODE, kMaxQ, 1>);
+    constexpr int NB = 4;
+#define WB_OBS_Q(GV)                                                     \
+    switch (S.d.Q) {                                                     \
+        case 1: go(obs_pass_kernel<T, GV, MODE, 1, NB>); break;          \
+        case 2: go(obs_pass_kernel<T, GV, MODE, 2, NB>); break;          \
+        case 3: go(obs_pass_kernel<T, GV, MODE, 3, NB>); break;          \
+        case 4: go(obs_pass_kernel<T, GV, MODE, 4, NB>); break;          \
+        default: go(obs_pass_kernel<T, GV, MODE, kMaxQ, 1>); break;      \
+    }
     switch (G) {
         case 1: WB_OBS_Q(1) break;
         case 2: WB_OBS_Q(2) break;
@@ -621,7 +713,7 @@ void launch_csr(SolverImpl& S, CsrDev<T>& c, int64_t ch0, int64_t ch1, const T* 
     const int64_t nch = ch1 - ch0;
     if (nch <= 0) return;
     const int G = group_for(kp);
-    const int grid = S.nblk(nch, G);
+    const int grid = S.nblk(nch, 32);  // one warp per chunk
     WB_DISPATCH_G(G, csr_rows_kernel<T, GV, EPI><<<grid, kBlock, 0, S.stream>>>(
                          c.chunks.p + ch0, nch, c.row_slot.p, c.ptr.p, c.col.p, c.val.p, c.rscale.p, src, dst, kp));
     WB_CUDA(cudaGetLastError());
@@ -721,12 +813,15 @@ void apply_precond(SolverImpl& S, const T* r, T* z, int kp, double* part, int& n
     if (S.pc.kind == 1) {
         StageDev<T>& st = sts[0];
         const SubMeans M = stage_local_solve<T>(S, st, r, v, kp);
+        double* mm = S.ws.msum.p + (size_t)4 * S.max_nsub * kp;  // [nsub][2][kp]
+        const int64_t nm = (int64_t)st.nsub * kp;
+        sub_means_kernel<<<(unsigned)((nm + kBlock - 1) / kBlock), kBlock, 0, S.stream>>>(st.nsub, kp, M, mm);
         nb_part = S.nblk(m, G, part ? 2 : 8);
         WB_DISPATCH_G(G, prolong_kernel<T, GV><<<nb_part, kBlock, 0, S.stream>>>(
-                             m, st.gptr.p, st.gslot.p, st.sub_of.p, st.spou.p, st.invd.p, st.bs_ptr.p, st.bs_col.p,
-                             st.bs_val.p, M, v, r, z, kp, part));
+                             m, st.gptr.p, st.gslot.p, st.gsub.p, st.gspou.p, st.ginvd.p, st.gbs_ptr.p, st.gbs_col.p,
+                             st.gbs_val.p, mm, v, r, z, kp, part));
         WB_CUDA(cudaGetLastError());
-        S.gpu_launches++;
+        S.gpu_launches += 2;
         if (!part) nb_part = 0;
         return;
     }
@@ -798,13 +893,15 @@ __global__ void cg_rz0_kernel(KState s, const double* red, int kp) {
     count_active(s, kp);
 }
 // cg.rs:76-86
-__global__ void cg_alpha_kernel(KState s, const double* red, int kp, int it) {
+// An RHS is active from the first iteration until it stops, so counting its alpha steps
+// gives the iteration number without passing it in (the iteration is graph-captured).
+__global__ void cg_alpha_kernel(KState s, const double* red, int kp) {
     const int c = threadIdx.x;
     if (c < kp) {
         s.alpha[c] = 0.0;
         if (s.active[c]) {
             const double pap = red[c];
-            s.iters[c] = it;
+            s.iters[c] += 1;
             if (pap <= 0.0) {
                 s.active[c] = 0;
                 s.conv[c] = 0;
@@ -886,13 +983,14 @@ void ensure_ws(SolverImpl& S, int kp) {
     w.vloc.alloc(std::max<size_t>(1, S.max_slots * kp));
     w.core_tmp.alloc(std::max<size_t>(1, S.max_core_total * kp));
     if (S.pc.kind == 2) { w.rwork.alloc(m * kp); w.cbuf.alloc(std::max<size_t>(1, S.max_slots * kp)); }
-    w.msum.alloc(std::max<size_t>(1, 4 * (size_t)std::max(S.max_nsub, 1) * kp));
+    w.msum.alloc(std::max<size_t>(1, 6 * (size_t)std::max(S.max_nsub, 1) * kp));  // S0, SB, M1, M2, means
     w.part.alloc((size_t)S.n_sm * 8 * kp + 64);
     w.red.alloc(32);
     for (DArr<double>* a : {&w.st_bnorm, &w.st_rz, &w.st_rz0, &w.st_alpha, &w.st_beta, &w.st_rnorm, &w.st_tol}) a->alloc(32);
     for (DArr<int32_t>* a : {&w.st_active, &w.st_conv, &w.st_iters, &w.st_part}) a->alloc(32);
     w.n_active.alloc(1);
     w.kp = kp;
+    ++w.gen;
 }
 
 // Preconditioned CG on the RHS marked in st_part (device), solution into x (zeroed here),
@@ -918,16 +1016,15 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
     S.gpu_launches += 2;
     const T* w_t = std::is_same<T, double>::value ? (const T*)S.w64.p : (const T*)S.w32.p;
     const int kind = std::is_same<T, double>::value ? 0 : 1;
-    cudaEvent_t ev;
-    WB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    auto enqueue_iter = [&](int it) {
+    // one iteration: q = G p, alpha, x/r update, convergence check, z = M r, beta, p update
+    auto body = [&]() {
         cudaEvent_t e0 = nullptr;
         S.prof_begin(e0);
         launch_obs<T, OBS_GRAM>(S, kp, w_t, p, nullptr, ap, nullptr);
         S.prof_end(kind, e0);
         launch_dot<T, T>(S, p, ap, m, kp, part, nb);
         launch_reduce(S, part, nb, kp, red);
-        cg_alpha_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp, it);
+        cg_alpha_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
         const int grid = S.nblk(m, G, 2);
         WB_DISPATCH_G(G, cg_xr_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(x, r, p, ap, w.st_alpha.p, m, kp, part));
         launch_reduce(S, part, grid, kp, red);
@@ -942,6 +1039,46 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
         WB_DISPATCH_G(G, cg_p_kernel<T, GV><<<gridp, kBlock, 0, S.stream>>>(p, z, w.st_beta.p, w.st_active.p, m, kp));
         WB_CUDA(cudaGetLastError());
         S.gpu_launches += 5;
+    };
+    // Without event timing, the iteration is captured once as a CUDA graph and replayed
+    // (one launch per iteration); the capture is kept while its buffers stay the same.
+    const bool graph = !S.profiling;
+    if (graph) {
+        const std::array<uintptr_t, 9> key{(uintptr_t)b, (uintptr_t)x, (uintptr_t)r, (uintptr_t)z, (uintptr_t)p,
+                                           (uintptr_t)ap, (uintptr_t)kp, (uintptr_t)w.gen, sizeof(T)};
+        if (!S.cg_exec || key != S.cg_key) {
+            if (S.cg_exec) {
+                WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
+                S.cg_exec = nullptr;
+            }
+            const int64_t l0 = S.gpu_launches;
+            cudaGraph_t g = nullptr;
+            WB_CUDA(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeRelaxed));
+            try {
+                body();
+            } catch (...) {
+                cudaStreamEndCapture(S.stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            WB_CUDA(cudaStreamEndCapture(S.stream, &g));
+            const cudaError_t ie = cudaGraphInstantiate(&S.cg_exec, g, 0);
+            cudaGraphDestroy(g);
+            WB_CUDA(ie);
+            S.cg_key = key;
+            S.cg_launches = S.gpu_launches - l0;
+            S.gpu_launches = l0;
+        }
+    }
+    cudaEvent_t ev;
+    WB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    auto enqueue_iter = [&]() {
+        if (graph) {
+            WB_CUDA(cudaGraphLaunch(S.cg_exec, S.stream));
+            S.gpu_launches += S.cg_launches;
+        } else {
+            body();
+        }
         WB_CUDA(cudaMemcpyAsync(S.h_active, w.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
         WB_CUDA(cudaEventRecord(ev, S.stream));
     };
@@ -952,11 +1089,11 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
     if (*S.h_active > 0 && maxiter > 0) {
         cudaEvent_t evb;
         WB_CUDA(cudaEventCreateWithFlags(&evb, cudaEventDisableTiming));
-        enqueue_iter(1);
+        enqueue_iter();
         int it = 1;
         while (it < maxiter) {
             std::swap(ev, evb);     // evb = event of iteration it
-            enqueue_iter(it + 1);   // records ev for iteration it+1
+            enqueue_iter();         // records ev for iteration it+1
             WB_CUDA(cudaEventSynchronize(evb));
             ++it;
             if (*S.h_active == 0) break;
