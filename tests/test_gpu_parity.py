@@ -17,6 +17,13 @@ DESIGNS = {
     "akm": lambda: synthetic.config2(scale=0.05)[0::2],
     "akm_w": lambda: (lambda c, Y, w: (c, np.random.default_rng(3).lognormal(0, 1, c.shape[0])))(*synthetic.config2(scale=0.03)),
     "shuffled": lambda: (np.asfortranarray(synthetic.config2(scale=0.02)[0][np.random.default_rng(9).permutation(40_000)]), None),
+    # four factors, weighted; five factors (the generic factor-count kernels)
+    "uniform4w": lambda: (synthetic.uniform_design(50_000, [600, 250, 40, 6], seed=11),
+                          np.random.default_rng(6).lognormal(0, 1, 50_000)),
+    "uniform5": lambda: (synthetic.uniform_design(30_000, [350, 120, 30, 8, 4], seed=12), None),
+    # primary factor with most of its levels unobserved (empty levels inside chunks)
+    "sparse_primary": lambda: (np.asfortranarray(np.column_stack([
+        np.random.default_rng(13).integers(0, 5000, 3000), np.random.default_rng(14).integers(0, 50, 3000)]).astype(np.uint32)), None),
 }
 
 
@@ -48,7 +55,7 @@ def test_setup_is_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", list(DESIGNS))
-@pytest.mark.parametrize("k", [1, 5, 16])
+@pytest.mark.parametrize("k", [1, 5, 16, 32])
 def test_operator_applies(name, k):
     cats, w = DESIGNS[name]()
     g = wb.Solver(cats, weights=w)

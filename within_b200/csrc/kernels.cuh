@@ -135,139 +135,131 @@ struct ObsParams {
     int64_t nchunks;
 };
 
-// Add a run sum of factor slot q (device code c) into its sink.
+template <typename T> struct W4;
+template <> struct W4<float> { using type = float4; };
+template <> struct W4<double> { struct type { double2 lo, hi; }; };
 template <typename T>
-__device__ __forceinline__ void obs_flush(const ObsParams& P, T* sm, T* out, int q, uint32_t c, const V4<T>& a,
-                                          int c4) {
-    const int32_t sink = P.sink[q];
-    const uint32_t lvl = P.packed[q] ? (c & kObsLevelMask) : c, hot = P.packed[q] ? (c >> kObsLevelBits) : 0u;
-    if (sink == SINK_BLOCK) red_shared4(sm + P.smem_base[q] + (size_t)lvl * P.kp + c4, a);
-    else if (sink == SINK_HOT && hot) red_shared4(sm + P.smem_base[q] + (size_t)(hot - 1) * P.kp + c4, a);
-    else atomic_add4(out + (size_t)(P.off[q] + lvl) * P.kp + c4, a);
-}
-
-template <typename T>
-__device__ __forceinline__ void load_w4(const T* __restrict__ w, uint32_t i, T (&wv)[4]);
+__device__ __forceinline__ typename W4<T>::type load_w4v(const T* __restrict__ w, uint32_t i);
 template <>
-__device__ __forceinline__ void load_w4<float>(const float* __restrict__ w, uint32_t i, float (&wv)[4]) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(w + i));
-    wv[0] = v.x; wv[1] = v.y; wv[2] = v.z; wv[3] = v.w;
+__device__ __forceinline__ float4 load_w4v<float>(const float* __restrict__ w, uint32_t i) {
+    return __ldg(reinterpret_cast<const float4*>(w + i));
 }
 template <>
-__device__ __forceinline__ void load_w4<double>(const double* __restrict__ w, uint32_t i, double (&wv)[4]) {
-    const double2 u = __ldg(reinterpret_cast<const double2*>(w + i)), v = __ldg(reinterpret_cast<const double2*>(w + i) + 1);
-    wv[0] = u.x; wv[1] = u.y; wv[2] = v.x; wv[3] = v.y;
+__device__ __forceinline__ W4<double>::type load_w4v<double>(const double* __restrict__ w, uint32_t i) {
+    return W4<double>::type{__ldg(reinterpret_cast<const double2*>(w + i)), __ldg(reinterpret_cast<const double2*>(w + i) + 1)};
 }
+__device__ __forceinline__ float wcomp(const float4& v, int b) { return b == 0 ? v.x : b == 1 ? v.y : b == 2 ? v.z : v.w; }
+__device__ __forceinline__ double wcomp(const W4<double>::type& v, int b) {
+    return b == 0 ? v.lo.x : b == 1 ? v.lo.y : b == 2 ? v.hi.x : v.hi.y;
+}
+__device__ __forceinline__ uint32_t ucomp(const uint4& v, int b) { return b == 0 ? v.x : b == 1 ? v.y : b == 2 ? v.z : v.w; }
 
 // One pass over the observations computing, with one read of the codes,
 //   GRAM:  out = D'W D x          RHS:  out = D'W yin
 //   RESID: eout = yin - D x, out = D'W eout          DX: eout = D x
-// QT == Q (QT = kMaxQ: any Q up to 16).  NB = 4: observations are taken in aligned
-// batches of 4 (one 16-byte load of 4 codes per factor, and of 4 weights), the chunk's
-// head and tail masked; NB = 1: one observation at a time.
-// Each lane group (G lanes, 4 RHS each) walks whole chunks: the primary factor's sums
-// close with a plain store when its level changes; a gathered coefficient row is reused
-// while its factor's level repeats; a non-primary factor keeps a running sum while its
-// level repeats and flushes it to its sink, except SINK_PRIVATE factors (few levels,
-// changing every observation) whose group-private table is updated without atomics.
-// The groups of a warp walk different chunks, so the per-observation steps are written
-// as short predicated updates rather than branches around long paths.  The block adds
+// QT == Q, and the last NP factor slots are SINK_PRIVATE (both compile-time); QT = kMaxQ
+// is the generic kernel (any Q up to 16, sinks read at run time, no reuse of gathered
+// rows).  kp = 4 G.
+// Each lane group (G lanes, 4 RHS each) walks whole chunks of primary-sorted
+// observations: the primary factor's sums close with a plain store when its level
+// changes; a gathered coefficient row is reused while its factor's level repeats; a
+// non-primary factor keeps a running sum while its level repeats and flushes it to its
+// sink, except SINK_PRIVATE factors (few levels, changing every observation), whose
+// group-private table is updated without atomics.  Observations go in aligned batches
+// of 4 (one 16-byte load of 4 codes per factor, and of 4 weights) with, registers
+// permitting, the next batch's loads in flight; a chunk's unaligned head and tail (and
+// every observation of the generic kernel) go one at a time.  Addresses come from
+// per-factor base pointers with the row stride a compile-time constant.  The block adds
 // its shared tables into `out` at the end.
-template <typename T, int G, int MODE, int QT, int NB>
+template <typename T, int G, int MODE, int QT, int NP>
 __global__ void __launch_bounds__(kBlock, 2) obs_pass_kernel(ObsParams P, const T* __restrict__ w,
                                                              const T* __restrict__ x, const T* __restrict__ yin,
                                                              T* __restrict__ out, T* __restrict__ eout) {
-    static_assert(NB == 1 || NB == 4, "batch of 1 or 4 observations");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* sm = reinterpret_cast<T*>(smem_raw);
+    constexpr int KP = 4 * G;
     constexpr bool kScatter = MODE != OBS_DX;
     constexpr bool kGather = MODE != OBS_RHS;
+    constexpr bool kGeneric = QT == kMaxQ;
+    constexpr bool kBatch = !kGeneric;                                    // 4-observation batches
+    constexpr bool kPrefetch = kBatch && (sizeof(T) == 4 || QT <= 2);    // registers permitting
+    constexpr int NS = kGeneric ? 1 : QT;                                 // per-slot register arrays
     constexpr uint32_t kNone = 0xffffffffu;
+    static_assert(kGeneric || NP < QT, "the primary slot is never private");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
     if (kScatter) {
         for (int i = threadIdx.x; i < P.smem_elems; i += blockDim.x) sm[i] = T(0);
         __syncthreads();
     }
     const int c4 = (threadIdx.x & (G - 1)) * 4;
-    const int kp = P.kp;
     const int gl = threadIdx.x / G;
     const int64_t gpb = blockDim.x / G;
     const int64_t ngroups = (int64_t)gridDim.x * gpb;
-    const int Q = (QT == kMaxQ) ? P.Q : QT;
+    const int Q = kGeneric ? P.Q : QT;
     const int64_t ns = P.ns;
+    const bool weighted = MODE != OBS_DX && w != nullptr;
     T* const priv = sm + (size_t)gl * P.priv_stride + c4;
-    T* const out0 = out + (size_t)P.off[0] * kp + c4;  // primary block, this lane's RHS
+    T* const out0 = out + (size_t)P.off[0] * KP + c4;  // primary block, this lane's RHS
+    // slot q is private: compile-time for the exact kernels
+    auto is_priv = [&](int q) -> bool {
+        if constexpr (kGeneric) return q > 0 && P.sink[q] == SINK_PRIVATE;
+        else return q >= QT - NP;
+    };
+    auto lev = [&](int q, uint32_t c) { return P.packed[q] ? (c & kObsLevelMask) : c; };
+    auto xrow = [&](int q, uint32_t c) -> const T* {
+        return x + ((size_t)P.off[q] + (q == 0 || is_priv(q) ? c : lev(q, c))) * KP + c4;
+    };
+    // run sum of non-private slot q at device code c into its sink
+    auto flush = [&](int q, uint32_t c, const V4<T>& a) {
+        const int32_t sink = P.sink[q];
+        const uint32_t lv = lev(q, c), hot = P.packed[q] ? (c >> kObsLevelBits) : 0u;
+        if (sink == SINK_BLOCK) red_shared4(sm + P.smem_base[q] + c4 + (size_t)lv * KP, a);
+        else if (sink == SINK_HOT && hot) red_shared4(sm + P.smem_base[q] + c4 + (size_t)(hot - 1) * KP, a);
+        else atomic_add4(out + ((size_t)P.off[q] + lv) * KP + c4, a);
+    };
 
     for (int64_t ch = (int64_t)blockIdx.x * gpb + gl; ch < P.nchunks; ch += ngroups) {
         const ObsChunk C = P.chunks[ch];
         uint32_t lvl = C.lvl_begin;
         V4<T> acc(T(0));
-        uint32_t run_l[QT], cl[QT];
-        V4<T> run_a[QT], cv[QT];
+        uint32_t run_l[QT], cl[NS];
+        V4<T> run_a[QT], cv[NS];
 #pragma unroll
         for (int q = 0; q < QT; ++q) {
             run_l[q] = kNone;
-            cl[q] = kNone;
             run_a[q] = V4<T>(T(0));
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            cl[q] = kNone;
             cv[q] = V4<T>(T(0));
         }
-        const uint32_t first = (NB == 4) ? (C.obs_begin & ~3u) : C.obs_begin;
-        for (uint32_t base = first; base < C.obs_end; base += NB) {
-            uint32_t lq[NB][QT];
-            T wv[NB];
-            if constexpr (NB == 4) {
+        // one observation: codes c[0..Q), weight wi
+        auto body = [&](uint32_t i, const uint32_t (&c)[QT], T wi) {
+            V4<T> s(T(0));
+            if constexpr (kGather) {
 #pragma unroll
                 for (int q = 0; q < QT; ++q) {
-                    if (q < Q) {
-                        const uint4 c = __ldg(reinterpret_cast<const uint4*>(P.codes + (size_t)q * ns + base));
-                        lq[0][q] = c.x; lq[1][q] = c.y; lq[2][q] = c.z; lq[3][q] = c.w;
+                    if (q >= Q) continue;
+                    if (kGeneric || is_priv(q)) {
+                        s += ldg4(xrow(q, c[q]));  // generic kernel, or a level that changes every time
+                    } else {
+                        if (c[q] != cl[q]) cv[q] = ldg4(xrow(q, c[q]));
+                        cl[q] = c[q];
+                        s += cv[q];
                     }
                 }
-                if (MODE != OBS_DX && w != nullptr) load_w4(w, base, wv);
-                else { wv[0] = wv[1] = wv[2] = wv[3] = T(1); }
-            } else {
-#pragma unroll
-                for (int q = 0; q < QT; ++q)
-                    if (q < Q) lq[0][q] = __ldg(P.codes + (size_t)q * ns + base);
-                wv[0] = (MODE != OBS_DX && w != nullptr) ? __ldg(w + base) : T(1);
             }
-            V4<T> s[NB];
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const uint32_t i = base + b;
-                const bool act = (NB == 1) || (i >= C.obs_begin && i < C.obs_end);
-                s[b] = V4<T>(T(0));
-                if (kGather && act) {
-#pragma unroll
-                    for (int q = 0; q < QT; ++q) {
-                        if (q >= Q) continue;
-                        const uint32_t c = lq[b][q];
-                        const T* xr = x + (size_t)(P.off[q] + (P.packed[q] ? (c & kObsLevelMask) : c)) * kp + c4;
-                        if (QT == kMaxQ || (q > 0 && P.sink[q] == SINK_PRIVATE)) {
-                            s[b] += ldg4(xr);  // no reuse: registers, or a level that changes every time
-                            continue;
-                        }
-                        if (c != cl[q]) cv[q] = ldg4(xr);
-                        cl[q] = c;
-                        s[b] += cv[q];
-                    }
-                }
-                if ((MODE == OBS_RHS || MODE == OBS_RESID) && act) {
-                    const V4<T> yv = ld4(yin + (size_t)i * kp + c4);
-                    s[b] = (MODE == OBS_RHS) ? yv : yv - s[b];
-                }
+            if constexpr (MODE == OBS_RHS || MODE == OBS_RESID) {
+                const V4<T> yv = ld4(yin + (size_t)i * KP + c4);
+                s = (MODE == OBS_RHS) ? yv : yv - s;
             }
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const uint32_t i = base + b;
-                const bool act = (NB == 1) || (i >= C.obs_begin && i < C.obs_end);
-                if (!act) continue;
-                if (MODE == OBS_DX || MODE == OBS_RESID) st4(eout + (size_t)i * kp + c4, s[b]);
-                if (!kScatter) continue;
-                const V4<T> t = wv[b] * s[b];
-                const uint32_t p = lq[b][0];
+            if constexpr (MODE == OBS_DX || MODE == OBS_RESID) st4(eout + (size_t)i * KP + c4, s);
+            if constexpr (kScatter) {
+                const V4<T> t = wi * s;
+                const uint32_t p = c[0];
                 if (p != lvl) {  // primary level complete: plain store
-                    st4(out0 + (size_t)lvl * kp, acc);
-                    for (uint32_t l = lvl + 1; l < p; ++l) st4(out0 + (size_t)l * kp, V4<T>(T(0)));  // empty levels
+                    st4(out0 + (size_t)lvl * KP, acc);
+                    for (uint32_t l = lvl + 1; l < p; ++l) st4(out0 + (size_t)l * KP, V4<T>(T(0)));  // empty levels
                     acc = V4<T>(T(0));
                     lvl = p;
                 }
@@ -275,28 +267,74 @@ __global__ void __launch_bounds__(kBlock, 2) obs_pass_kernel(ObsParams P, const 
 #pragma unroll
                 for (int q = 1; q < QT; ++q) {
                     if (q >= Q) continue;
-                    const uint32_t c = lq[b][q];
-                    if (P.sink[q] == SINK_PRIVATE) {
-                        T* pt = priv + P.smem_base[q] + (size_t)c * kp;
+                    if (is_priv(q)) {
+                        T* pt = priv + P.smem_base[q] + (size_t)c[q] * KP;
                         st4(pt, ld4(pt) + t);
-                        continue;
+                    } else if (c[q] != run_l[q]) {
+                        if (run_l[q] != kNone) flush(q, run_l[q], run_a[q]);
+                        run_l[q] = c[q];
+                        run_a[q] = t;
+                    } else {
+                        run_a[q] += t;
                     }
-                    const bool brk = c != run_l[q];
-                    if (brk && run_l[q] != kNone) obs_flush(P, sm, out, q, run_l[q], run_a[q], c4);
-                    run_a[q] = brk ? t : run_a[q] + t;
-                    run_l[q] = c;
+                }
+            }
+        };
+        auto single = [&](uint32_t i) {
+            uint32_t c[QT];
+#pragma unroll
+            for (int q = 0; q < QT; ++q) c[q] = q < Q ? __ldg(P.codes + (size_t)q * ns + i) : 0u;
+            body(i, c, weighted ? __ldg(w + i) : T(1));
+        };
+        uint32_t i = C.obs_begin;
+        if constexpr (kBatch) {
+            for (; i < C.obs_end && (i & 3u); ++i) single(i);
+            if (i + 4 <= C.obs_end) {
+                uint4 cb[QT];
+                typename W4<T>::type wb{};
+#pragma unroll
+                for (int q = 0; q < QT; ++q) cb[q] = __ldg(reinterpret_cast<const uint4*>(P.codes + (size_t)q * ns + i));
+                if (weighted) wb = load_w4v(w, i);
+                for (; i + 4 <= C.obs_end; i += 4) {
+                    uint4 nb[kPrefetch ? QT : 1];
+                    typename W4<T>::type nw = wb;
+                    const bool more = i + 8 <= C.obs_end;
+                    if constexpr (kPrefetch) {  // next batch in flight while this one is processed
+#pragma unroll
+                        for (int q = 0; q < QT; ++q)
+                            nb[q] = more ? __ldg(reinterpret_cast<const uint4*>(P.codes + (size_t)q * ns + i + 4)) : cb[q];
+                        if (weighted && more) nw = load_w4v(w, i + 4);
+                    }
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        uint32_t c[QT];
+#pragma unroll
+                        for (int q = 0; q < QT; ++q) c[q] = ucomp(cb[q], b);
+                        body(i + b, c, weighted ? (T)wcomp(wb, b) : T(1));
+                    }
+                    if constexpr (kPrefetch) {
+#pragma unroll
+                        for (int q = 0; q < QT; ++q) cb[q] = nb[q];
+                        wb = nw;
+                    } else if (more) {
+#pragma unroll
+                        for (int q = 0; q < QT; ++q)
+                            cb[q] = __ldg(reinterpret_cast<const uint4*>(P.codes + (size_t)q * ns + i + 4));
+                        if (weighted) wb = load_w4v(w, i + 4);
+                    }
                 }
             }
         }
-        if (kScatter) {
+        for (; i < C.obs_end; ++i) single(i);
+        if constexpr (kScatter) {
 #pragma unroll
             for (int q = 1; q < QT; ++q)
-                if (q < Q && run_l[q] != kNone) obs_flush(P, sm, out, q, run_l[q], run_a[q], c4);
+                if (q < Q && !is_priv(q) && run_l[q] != kNone) flush(q, run_l[q], run_a[q]);
             if (C.split) {
-                atomic_add4(out0 + (size_t)C.lvl_begin * kp, acc);
+                atomic_add4(out0 + (size_t)C.lvl_begin * KP, acc);
             } else {
                 for (; lvl < C.lvl_end; ++lvl) {
-                    st4(out0 + (size_t)lvl * kp, acc);
+                    st4(out0 + (size_t)lvl * KP, acc);
                     acc = V4<T>(T(0));
                 }
             }
@@ -310,15 +348,15 @@ __global__ void __launch_bounds__(kBlock, 2) obs_pass_kernel(ObsParams P, const 
             if (sink == SINK_GLOBAL) continue;
             for (int e = threadIdx.x; e < P.smem_len[q]; e += blockDim.x) {
                 T v = T(0);
-                uint32_t lev;
+                uint32_t lv;
                 if (sink == SINK_PRIVATE) {
                     for (int g = 0; g < (int)gpb; ++g) v += sm[(size_t)g * P.priv_stride + P.smem_base[q] + e];
-                    lev = (uint32_t)(e / kp);
+                    lv = (uint32_t)(e / KP);
                 } else {
                     v = sm[P.smem_base[q] + e];
-                    lev = (sink == SINK_BLOCK) ? (uint32_t)(e / kp) : P.hot_level[q][e / kp];
+                    lv = (sink == SINK_BLOCK) ? (uint32_t)(e / KP) : P.hot_level[q][e / KP];
                 }
-                if (v != T(0)) atomicAdd(out + (size_t)(P.off[q] + lev) * kp + e % kp, v);
+                if (v != T(0)) atomicAdd(out + (size_t)(P.off[q] + lv) * KP + e % KP, v);
             }
         }
     }

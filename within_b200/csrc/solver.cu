@@ -346,6 +346,7 @@ struct SolverImpl {
     DArr<double> g_val64;
     DArr<float> g_val32;
     Workspace ws;
+    DArr<double> host_y, host_x, host_dem;  // device side of the host-buffer entry points
     std::shared_ptr<void> gmres;  // GmresBufs, created on first GMRES solve
     int32_t* h_active = nullptr;  // pinned
     double setup_time = 0.0;
@@ -476,11 +477,14 @@ void upload_design(SolverImpl& S) {
     S.perm_identity = true;
     for (int64_t i = 0; i < d.n; ++i)
         if (perm[i] != (uint32_t)i) { S.perm_identity = false; break; }
-    // device factor order: the primary factor first, the others in their order
+    // device factor order: the primary factor first, then the others by level count,
+    // largest first (the observation pass's private-table factors are a suffix)
     S.dev_factor.clear();
     S.dev_factor.push_back(S.primary);
     for (int q = 0; q < d.Q; ++q)
         if (q != S.primary) S.dev_factor.push_back(q);
+    std::stable_sort(S.dev_factor.begin() + 1, S.dev_factor.end(),
+                     [&](int a, int b) { return d.nlev[a] > d.nlev[b]; });
     // hot levels: the 255 most frequent levels (hit >= 64 times) of each non-primary
     // factor with more than 256 levels and fewer than 2^24; their codes on the device
     // carry the hot slot + 1 in bits 24-31 (kObsLevelBits) next to the level
@@ -556,41 +560,41 @@ void upload_design(SolverImpl& S) {
 // and the others their hottest levels, within kObsSmemBytes per block (two blocks/SM).
 constexpr int64_t kObsPrivBytes = 96 * 1024, kObsSmemBytes = 110 * 1024;
 
-void obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
+int obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
     P = S.obs;
     P.kp = kp;
     const int G = group_for(kp);
     const int64_t gpb = kBlock / G;
+    const int Q = S.d.Q;
     for (int sl = 0; sl < kMaxQ; ++sl) {
         P.sink[sl] = SINK_GLOBAL;
         P.smem_base[sl] = -1;
         P.smem_len[sl] = 0;
     }
-    // private tables; a group's area stride is padded so that the 16-byte accesses of
-    // neighbouring groups at the same level fall in different banks
+    // private tables for a suffix of the slots (the smallest factors); a group's area
+    // stride is padded so that the 16-byte accesses of neighbouring groups at the same
+    // level fall in different banks
     const int64_t target = elem == 4 ? (16 * G) % 128 : 16;
     auto padded = [&](int64_t r) {
         int64_t st = r;
         while ((st * (int64_t)elem) % 128 != target) ++st;
         return st;
     };
-    std::vector<int> order;
-    for (int sl = 1; sl < S.d.Q; ++sl) order.push_back(sl);
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return S.d.nlev[S.dev_factor[a]] < S.d.nlev[S.dev_factor[b]]; });
     int64_t raw = 0;
-    for (int sl : order) {
+    int np = 0;
+    for (int sl = Q - 1; sl >= 1; --sl) {
         const int64_t len = S.d.nlev[S.dev_factor[sl]] * kp;
         if (gpb * padded(raw + len) * (int64_t)elem > kObsPrivBytes) break;
         P.sink[sl] = SINK_PRIVATE;
         P.smem_base[sl] = (int32_t)raw;
         P.smem_len[sl] = (int32_t)len;
         raw += len;
+        ++np;
     }
     P.priv_stride = raw > 0 ? (int32_t)padded(raw) : 0;
     int64_t used = gpb * P.priv_stride;
     const int64_t budget = kObsSmemBytes / (int64_t)elem;
-    for (int sl : order) {
+    for (int sl = Q - 1; sl >= 1; --sl) {  // smallest first
         if (P.sink[sl] == SINK_PRIVATE) continue;
         const int64_t nl = S.d.nlev[S.dev_factor[sl]];
         if (nl <= 256 && used + nl * kp <= budget) {
@@ -600,7 +604,7 @@ void obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
             used += nl * kp;
         }
     }
-    for (int sl : order) {
+    for (int sl = 1; sl < Q; ++sl) {
         if (P.sink[sl] != SINK_GLOBAL || S.hot_count[sl] == 0) continue;
         const int64_t len = (int64_t)S.hot_count[sl] * kp;
         if (used + len > budget) continue;  // the whole hot table or none of it
@@ -610,12 +614,13 @@ void obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
         used += len;
     }
     P.smem_elems = (int32_t)used;
+    return np;
 }
 
 template <typename T, int MODE>
 void launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* out, T* eout) {
     ObsParams P;
-    obs_params_for(S, kp, sizeof(T), P);
+    const int np = obs_params_for(S, kp, sizeof(T), P);
     const int G = group_for(kp);
     if (MODE != OBS_DX && out) {
         // zero the outputs that are accumulated (every non-primary factor, split levels)
@@ -636,15 +641,20 @@ void launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* 
         WB_CUDA(cudaGetLastError());
         S.gpu_launches++;
     };
-    constexpr int NB = 4;
-#define WB_OBS_Q(GV)                                                     \
-    switch (S.d.Q) {                                                     \
-        case 1: go(obs_pass_kernel<T, GV, MODE, 1, NB>); break;          \
-        case 2: go(obs_pass_kernel<T, GV, MODE, 2, NB>); break;          \
-        case 3: go(obs_pass_kernel<T, GV, MODE, 3, NB>); break;          \
-        case 4: go(obs_pass_kernel<T, GV, MODE, 4, NB>); break;          \
-        default: go(obs_pass_kernel<T, GV, MODE, kMaxQ, 1>); break;      \
+#define WB_OBS_Q(GV)                                                                        \
+    switch (S.d.Q * 8 + std::min(np, 2)) {                                                  \
+        case 1 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 1, 0>); break;                      \
+        case 2 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 2, 0>); break;                      \
+        case 2 * 8 + 1: go(obs_pass_kernel<T, GV, MODE, 2, 1>); break;                      \
+        case 3 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 3, 0>); break;                      \
+        case 3 * 8 + 1: go(obs_pass_kernel<T, GV, MODE, 3, 1>); break;                      \
+        case 3 * 8 + 2: go(obs_pass_kernel<T, GV, MODE, 3, 2>); break;                      \
+        case 4 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 4, 0>); break;                      \
+        case 4 * 8 + 1: go(obs_pass_kernel<T, GV, MODE, 4, 1>); break;                      \
+        default: go(obs_pass_kernel<T, GV, MODE, kMaxQ, 0>); break;                         \
     }
+    // exact kernels for Q <= 4 with the private slots as the trailing NP (Q = 4: NP <= 1);
+    // anything else runs the generic kernel, which reads every slot's sink
     switch (G) {
         case 1: WB_OBS_Q(1) break;
         case 2: WB_OBS_Q(2) break;
@@ -1744,7 +1754,10 @@ int within_solver_solve_batch(within_solver* s, const double* ys, size_t k, doub
         if (k == 0) return WITHIN_OK;
         if (!ys || !x || !dem) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "null buffer");
         const size_t n = (size_t)S.d.n, m = (size_t)S.d.ndofs;
-        wb::DArr<double> dy, dx, dd;
+        // device copies of the host buffers, kept by the solver (grow-only)
+        wb::DArr<double>& dy = S.host_y;
+        wb::DArr<double>& dx = S.host_x;
+        wb::DArr<double>& dd = S.host_dem;
         dy.alloc(n * k);
         dx.alloc(m * k);
         dd.alloc(n * k);
