@@ -12,8 +12,12 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwithin_b200.so")
-SOURCES = ["solver.cu", "setup.cpp"]
-DEPS = SOURCES + ["kernels.cuh", "device.cuh", "setup.hpp", os.path.join("..", "..", "include", "within_b200.h")]
+# translation units, compiled in parallel (the observation-pass instantiations are split
+# out because ptxas spends most of the build on them)
+SOURCES = ["solver.cu", "obs_f64.cu", "obs_f32.cu", "setup.cpp"]
+DEPS = SOURCES + ["kernels.cuh", "device.cuh", "obs_launch.cuh", "setup.hpp",
+                  os.path.join("..", "..", "include", "within_b200.h")]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
 def nvcc() -> str:
@@ -33,10 +37,22 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc(), "-std=c++17", "-O3", "-lineinfo",
-           "-gencode", "arch=compute_100a,code=sm_100a",
-           "-Xcompiler", "-fPIC,-O3", "-shared", "-o", LIB]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    procs = []
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc(), "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-O3", "-c",
+               os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((src, subprocess.Popen(cmd)))
+        objs.append(obj)
+    failed = [src for src, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(failed))
+    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

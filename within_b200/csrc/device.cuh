@@ -136,6 +136,7 @@ struct StageDev {
     DArr<uint32_t> bs_col;
     DArr<T> bs_val;
     std::vector<int64_t> fwd_lp, bwd_lp;  // host copies (launch ranges)
+    DArr<int64_t> fwd_lp_d, bwd_lp_d;     // device copies (fused sweeps)
     int32_t ndense = 0;
     DArr<int64_t> dn_keep0, dn_loff;
     DArr<int32_t> dn_n;
@@ -154,6 +155,6 @@ struct StageDev {
     DArr<T> gbs_val;
 };
 
-constexpr int kCoreRowsPerBlock = 8;
+constexpr int kCoreRowsPerBlock = 2;  // output rows per block of core_gemv_kernel (4 warps each)
 
 }  // namespace wb

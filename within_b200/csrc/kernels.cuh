@@ -130,6 +130,7 @@ struct ObsParams {
     // SINK_BLOCK / SINK_HOT: offset of the block-shared table (after all private areas).
     int32_t smem_base[kMaxQ];
     int32_t smem_len[kMaxQ];           // levels x kp (SINK_HOT: hot levels x kp)
+    int32_t hot_cap[kMaxQ];            // SINK_HOT: hot slots held in the table (the rest go global)
     const uint32_t* hot_level[kMaxQ];  // hot slot -> level
     const ObsChunk* chunks;
     int64_t nchunks;
@@ -166,13 +167,18 @@ __device__ __forceinline__ uint32_t ucomp(const uint4& v, int b) { return b == 0
 // non-primary factor keeps a running sum while its level repeats and flushes it to its
 // sink, except SINK_PRIVATE factors (few levels, changing every observation), whose
 // group-private table is updated without atomics.  Observations go in aligned batches
-// of 4 (one 16-byte load of 4 codes per factor, and of 4 weights) with, registers
-// permitting, the next batch's loads in flight; a chunk's unaligned head and tail (and
+// of 4 (one 16-byte load of 4 codes per factor, and of 4 weights) with the next
+// batch's loads in flight; a chunk's unaligned head and tail (and
 // every observation of the generic kernel) go one at a time.  Addresses come from
 // per-factor base pointers with the row stride a compile-time constant.  The block adds
 // its shared tables into `out` at the end.
+// Threads per block of the observation pass: 256, or 128 for FP64, whose group-private
+// tables are twice as large (the tables of a block are its lane groups' copies).
+template <typename T>
+constexpr int obs_block() { return sizeof(T) == 8 ? 128 : 256; }
+
 template <typename T, int G, int MODE, int QT, int NP>
-__global__ void __launch_bounds__(kBlock, 2) obs_pass_kernel(ObsParams P, const T* __restrict__ w,
+__global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P, const T* __restrict__ w,
                                                              const T* __restrict__ x, const T* __restrict__ yin,
                                                              T* __restrict__ out, T* __restrict__ eout) {
     constexpr int KP = 4 * G;
@@ -180,7 +186,7 @@ __global__ void __launch_bounds__(kBlock, 2) obs_pass_kernel(ObsParams P, const 
     constexpr bool kGather = MODE != OBS_RHS;
     constexpr bool kGeneric = QT == kMaxQ;
     constexpr bool kBatch = !kGeneric;                                    // 4-observation batches
-    constexpr bool kPrefetch = kBatch && (sizeof(T) == 4 || QT <= 2);    // registers permitting
+    constexpr bool kPrefetch = kBatch;  // next batch's codes and weights in flight
     constexpr int NS = kGeneric ? 1 : QT;                                 // per-slot register arrays
     constexpr uint32_t kNone = 0xffffffffu;
     static_assert(kGeneric || NP < QT, "the primary slot is never private");
@@ -213,7 +219,8 @@ __global__ void __launch_bounds__(kBlock, 2) obs_pass_kernel(ObsParams P, const 
         const int32_t sink = P.sink[q];
         const uint32_t lv = lev(q, c), hot = P.packed[q] ? (c >> kObsLevelBits) : 0u;
         if (sink == SINK_BLOCK) red_shared4(sm + P.smem_base[q] + c4 + (size_t)lv * KP, a);
-        else if (sink == SINK_HOT && hot) red_shared4(sm + P.smem_base[q] + c4 + (size_t)(hot - 1) * KP, a);
+        else if (sink == SINK_HOT && hot && (int32_t)hot <= P.hot_cap[q])
+            red_shared4(sm + P.smem_base[q] + c4 + (size_t)(hot - 1) * KP, a);
         else atomic_add4(out + ((size_t)P.off[q] + lv) * KP + c4, a);
     };
 
@@ -577,6 +584,110 @@ __global__ void __launch_bounds__(kBlock) csr_rows_kernel(const CsrChunk* __rest
     }
 }
 
+// L2-coherent loads and stores, for data that other blocks of the same launch write
+// (an L1 line read before a grid barrier may be stale after it).
+__device__ __forceinline__ V4<float> ldcg4(const float* p) {
+    const float4 v = __ldcg(reinterpret_cast<const float4*>(p));
+    return V4<float>(v.x, v.y, v.z, v.w);
+}
+__device__ __forceinline__ V4<double> ldcg4(const double* p) {
+    const double2 u = __ldcg(reinterpret_cast<const double2*>(p)), v = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    return V4<double>(u.x, u.y, v.x, v.y);
+}
+__device__ __forceinline__ void stcg4(float* p, const V4<float>& v) {
+    __stcg(reinterpret_cast<float4*>(p), make_float4(v.a, v.b, v.c, v.d));
+}
+__device__ __forceinline__ void stcg4(double* p, const V4<double>& v) {
+    __stcg(reinterpret_cast<double2*>(p), make_double2(v.a, v.b));
+    __stcg(reinterpret_cast<double2*>(p) + 1, make_double2(v.c, v.d));
+}
+
+// Barrier over all blocks of a cooperative launch (every block is resident): each block
+// adds one to *count and waits until it reaches `target`.  The wait is bounded; if it
+// runs out, *err is set and the block goes on (the results are then invalid and the
+// host reports the error).
+constexpr unsigned kBarrierSpins = 1u << 22;
+__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned target, int* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(count, 1u);
+        for (unsigned spins = 0;; ++spins) {
+            unsigned c;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(count) : "memory");
+            if (c >= target) break;
+            if (spins >= kBarrierSpins) {
+                atomicExch(err, 1);
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// Every level of one AC sweep direction in one cooperative launch: level l's chunks are
+// [lp[l], lp[l+1]); levels run in order (backward: from the last), separated by grid
+// barriers; within a level the work is that of csr_rows_kernel (one warp per chunk) on
+// the vector v, read and written through L2.
+template <typename T, int G, int EPI>
+__global__ void __launch_bounds__(kBlock) csr_levels_kernel(const CsrChunk* __restrict__ chunks,
+                                                            const int64_t* __restrict__ lp, int nlev, int backward,
+                                                            const uint32_t* __restrict__ row_slot,
+                                                            const int64_t* __restrict__ ptr,
+                                                            const uint32_t* __restrict__ col,
+                                                            const T* __restrict__ val, const T* __restrict__ rscale,
+                                                            T* v, int kp, unsigned* bar, int* err) {
+    constexpr int NG = 32 / G;
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / G;
+    const int c4 = (lane & (G - 1)) * 4;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    for (int li = 0; li < nlev; ++li) {
+        const int l = backward ? nlev - 1 - li : li;
+        for (int64_t ch = lp[l] + wid; ch < lp[l + 1]; ch += nw) {
+            const CsrChunk C = chunks[ch];
+            for (uint32_t row = C.row_begin; row < C.row_end; ++row) {
+                const int64_t rb = ptr[row], re = ptr[row + 1];
+                const int64_t e0 = max(rb, C.nz_begin), e1 = min(re, C.nz_end);
+                V4<T> acc(T(0));
+                int64_t e = e0 + grp;
+                for (; e + 3 * NG < e1; e += 4 * NG) {
+                    const uint32_t j0 = __ldg(col + e), j1 = __ldg(col + e + NG);
+                    const uint32_t j2 = __ldg(col + e + 2 * NG), j3 = __ldg(col + e + 3 * NG);
+                    const T v0 = __ldg(val + e), v1 = __ldg(val + e + NG), v2 = __ldg(val + e + 2 * NG), v3 = __ldg(val + e + 3 * NG);
+                    const V4<T> s0 = ldcg4(v + (size_t)j0 * kp + c4), s1 = ldcg4(v + (size_t)j1 * kp + c4);
+                    const V4<T> s2 = ldcg4(v + (size_t)j2 * kp + c4), s3 = ldcg4(v + (size_t)j3 * kp + c4);
+                    acc += v0 * s0;
+                    acc += v1 * s1;
+                    acc += v2 * s2;
+                    acc += v3 * s3;
+                }
+                for (; e < e1; e += NG) acc += __ldg(val + e) * ldcg4(v + (size_t)__ldg(col + e) * kp + c4);
+#pragma unroll
+                for (int off = G; off < 32; off <<= 1) {
+                    acc.a += __shfl_xor_sync(0xffffffffu, acc.a, off);
+                    acc.b += __shfl_xor_sync(0xffffffffu, acc.b, off);
+                    acc.c += __shfl_xor_sync(0xffffffffu, acc.c, off);
+                    acc.d += __shfl_xor_sync(0xffffffffu, acc.d, off);
+                }
+                if (grp == 0) {
+                    T* d = v + (size_t)row_slot[row] * kp + c4;
+                    if (EPI == EPI_ACC) {
+                        if (e0 != rb || e1 != re) atomic_add4(d, acc);
+                        else stcg4(d, ldcg4(d) + acc);
+                    } else {
+                        stcg4(d, rscale[row] * ldcg4(d) + acc);
+                    }
+                }
+            }
+        }
+        if (li + 1 < nlev) grid_barrier(bar, (unsigned)(li + 1) * gridDim.x, err);
+    }
+}
+
 // Segmented per-subdomain sums over a contiguous range, block-reduced: the block's
 // first and last subdomain accumulate in shared memory (one global atomic per block),
 // other runs (small subdomains inside the block) go straight to global atomics.
@@ -595,11 +706,12 @@ struct SegSum {
             if (g1) atomic_add4(g1 + (size_t)sub * kp + c4, b);
         }
     }
-    __device__ void finish(double* g0, double* g1) {
+    __device__ void finish(double* g0, double* g1, bool skip_first = false) {
         __syncthreads();
         for (int i = threadIdx.x; i < 2 * kp; i += blockDim.x) {
             const int bin = i / kp, c = i % kp;
             if (bin == 1 && last == first) continue;
+            if (bin == 0 && skip_first) continue;
             const uint32_t sub = bin == 0 ? first : last;
             atomicAdd(g0 + (size_t)sub * kp + c, sm[bin * 2 * kp + c]);
             if (g1) atomicAdd(g1 + (size_t)sub * kp + c, sm[bin * 2 * kp + kp + c]);
@@ -607,7 +719,24 @@ struct SegSum {
     }
 };
 
-// Pass 1 (all slots): S0[s] += u_l, SB[s] += u_l invd_l.  Block b owns slots [b*spb, +spb).
+// Sum of a V4 over the lane groups of a warp (lanes with equal lane % G).
+template <int G>
+__device__ __forceinline__ V4<double> warp_sum_groups(V4<double> v) {
+#pragma unroll
+    for (int off = G; off < 32; off <<= 1) {
+        v.a += __shfl_xor_sync(0xffffffffu, v.a, off);
+        v.b += __shfl_xor_sync(0xffffffffu, v.b, off);
+        v.c += __shfl_xor_sync(0xffffffffu, v.c, off);
+        v.d += __shfl_xor_sync(0xffffffffu, v.d, off);
+    }
+    return v;
+}
+
+// Pass 1 (all slots): S0[s] += u_l, SB[s] += u_l invd_l.  Block b owns slots
+// [b*spb, +spb), a lane group spb/(groups) consecutive slots, four loads at a time.
+// Subdomains are long runs of slots, so nearly everything belongs to the block's first
+// subdomain: that part is summed in registers, then over the block with shuffles (one
+// set of global atomics per block); other runs go through SegSum.
 template <typename T, int G>
 __global__ void __launch_bounds__(kBlock) schwarz_sums_kernel(int64_t nslots, int spb,
                                                               const uint32_t* __restrict__ gidx,
@@ -616,7 +745,9 @@ __global__ void __launch_bounds__(kBlock) schwarz_sums_kernel(int64_t nslots, in
                                                               const T* __restrict__ r, int kp,
                                                               double* __restrict__ S0, double* __restrict__ SB) {
     __shared__ double sm[2 * 2 * 32];
+    __shared__ double wsum[2][kBlock / 32][32];
     const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t b0 = (int64_t)blockIdx.x * spb, b1 = min(nslots, b0 + spb);
     if (b0 >= nslots) return;  // uniform per block
     for (int i = threadIdx.x; i < 4 * kp; i += blockDim.x) sm[i] = 0.0;
@@ -626,21 +757,61 @@ __global__ void __launch_bounds__(kBlock) schwarz_sums_kernel(int64_t nslots, in
     const int64_t per = (spb + gpb - 1) / gpb;
     const int64_t a0 = b0 + g * per, a1 = min(b1, a0 + per);
     uint32_t cur = 0xffffffffu;
-    V4<double> acc0(0.0), accb(0.0);
-    for (int64_t l = a0; l < a1; ++l) {
-        const uint32_t sb = sub_of[l];
-        if (sb != cur) {
-            if (cur != 0xffffffffu) seg.flush(S0, SB, cur, acc0, accb, c4);
-            cur = sb;
-            acc0 = V4<double>(0.0);
-            accb = V4<double>(0.0);
+    V4<double> acc0(0.0), accb(0.0), f0(0.0), fb(0.0);
+    auto close = [&]() {
+        if (cur == seg.first) {
+            f0 += acc0;
+            fb += accb;
+        } else if (cur != 0xffffffffu) {
+            seg.flush(S0, SB, cur, acc0, accb, c4);
         }
-        const V4<double> u = (double)spou[l] * to_d(ld4(r + (size_t)gidx[l] * kp + c4));
-        acc0 += u;
-        accb += (double)invd[l] * u;
+    };
+    for (int64_t l = a0; l < a1; l += 4) {
+        const int nb = (int)min((int64_t)4, a1 - l);
+        uint32_t sbv[4], gv[4];
+        T spv[4], iv[4];
+        V4<T> rv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (j < nb) {
+                sbv[j] = sub_of[l + j];
+                gv[j] = gidx[l + j];
+                spv[j] = spou[l + j];
+                iv[j] = invd[l + j];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (j < nb) rv[j] = ld4(r + (size_t)gv[j] * kp + c4);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (j >= nb) break;
+            if (sbv[j] != cur) {
+                close();
+                cur = sbv[j];
+                acc0 = V4<double>(0.0);
+                accb = V4<double>(0.0);
+            }
+            const V4<double> u = (double)spv[j] * to_d(rv[j]);
+            acc0 += u;
+            accb += (double)iv[j] * u;
+        }
     }
-    if (cur != 0xffffffffu) seg.flush(S0, SB, cur, acc0, accb, c4);
-    seg.finish(S0, SB);
+    close();
+    f0 = warp_sum_groups<G>(f0);
+    fb = warp_sum_groups<G>(fb);
+    if (lane < G) {
+        wsum[0][warp][c4] = f0.a; wsum[0][warp][c4 + 1] = f0.b; wsum[0][warp][c4 + 2] = f0.c; wsum[0][warp][c4 + 3] = f0.d;
+        wsum[1][warp][c4] = fb.a; wsum[1][warp][c4 + 1] = fb.b; wsum[1][warp][c4 + 2] = fb.c; wsum[1][warp][c4 + 3] = fb.d;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * kp; i += blockDim.x) {
+        const int q = i / kp, c = i % kp;
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += wsum[q][w][c];
+        atomicAdd((q ? SB : S0) + (size_t)seg.first * kp + c, s);
+    }
+    seg.finish(S0, SB, /*skip_first=*/true);
 }
 
 // Keep slots, in keep-list order: v[k] = u_k - m0 - m0 rho_k (the base of the reduced rhs).
@@ -756,7 +927,7 @@ __device__ __forceinline__ void sub_means(const SubMeans& M, uint32_t s, int kp,
 }
 
 // Per-subdomain means once per apply: mm[s][0] = m0 = S0/n, mm[s][1] = m2.
-__global__ void sub_means_kernel(int32_t nsub, int kp, SubMeans M, double* __restrict__ mm) {
+static __global__ void sub_means_kernel(int32_t nsub, int kp, SubMeans M, double* __restrict__ mm) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)nsub * kp) return;
     const int64_t s = i / kp, c = i % kp;
@@ -798,17 +969,23 @@ __global__ void __launch_bounds__(kBlock) prolong_kernel(int64_t m, const int64_
             if (id == T(0)) {
                 sol = to_d(ld4(v + (size_t)gslot[e] * kp + c4));
             } else {
-                V4<T> bs(T(0));
+                V4<T> bs(T(0)), bs2(T(0));
                 const int64_t t0 = gbs_ptr[e], t1 = gbs_ptr[e + 1];
                 int64_t t = t0;
-                for (; t + 2 <= t1; t += 2) {
+                for (; t + 4 <= t1; t += 4) {  // four independent gathers in flight
                     const uint32_t j0 = __ldg(gbs_col + t), j1 = __ldg(gbs_col + t + 1);
+                    const uint32_t j2 = __ldg(gbs_col + t + 2), j3 = __ldg(gbs_col + t + 3);
                     const T v0 = __ldg(gbs_val + t), v1 = __ldg(gbs_val + t + 1);
+                    const T v2 = __ldg(gbs_val + t + 2), v3 = __ldg(gbs_val + t + 3);
                     const V4<T> s0 = ld4(v + (size_t)j0 * kp + c4), s1 = ld4(v + (size_t)j1 * kp + c4);
+                    const V4<T> s2 = ld4(v + (size_t)j2 * kp + c4), s3 = ld4(v + (size_t)j3 * kp + c4);
                     bs += v0 * s0;
-                    bs += v1 * s1;
+                    bs2 += v1 * s1;
+                    bs += v2 * s2;
+                    bs2 += v3 * s3;
                 }
-                if (t < t1) bs += __ldg(gbs_val + t) * ld4(v + (size_t)__ldg(gbs_col + t) * kp + c4);
+                for (; t < t1; ++t) bs += __ldg(gbs_val + t) * ld4(v + (size_t)__ldg(gbs_col + t) * kp + c4);
+                bs += bs2;
                 const double idd = (double)id;
                 sol = idd * (sp * rj - m0) + idd * to_d(bs);
             }
@@ -922,58 +1099,76 @@ __global__ void dense_solve_kernel(int32_t ndense, const int64_t* __restrict__ k
     if (lane == 0) v[(size_t)(s0 + m) * kp + c] = T(0);
 }
 
-// Dense core of an AC factor: v[core] = Z v[core] (anchored inverse), RHS [c0, c0+kc).
-// Block b of core g computes rows [row0, row0 + rows_per_block); the core input is
-// staged in shared memory (c-major, conflict-free) before any output is produced, and
-// outputs go to `tmp` because other blocks of the same core still read the input.
-template <typename T, int KC>
-__global__ void core_gemv_kernel(const int32_t* __restrict__ core_of_block, const int32_t* __restrict__ row0_of_block,
-                                 const int32_t* __restrict__ core_n, const int64_t* __restrict__ core_slot_off,
-                                 const uint32_t* __restrict__ core_slot, const int64_t* __restrict__ core_z_off,
-                                 const T* __restrict__ Z, const T* __restrict__ v, T* __restrict__ tmp,
-                                 int kp, int c0, int kc, int rows_per_block) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* yc = reinterpret_cast<T*>(smem_raw);
-    const int g = core_of_block[blockIdx.x];
-    const int r = core_n[g];
-    const uint32_t* slots = core_slot + core_slot_off[g];
-    for (int e = threadIdx.x; e < r * kc; e += blockDim.x) {  // a slot's kc values are contiguous in v
-        const int a = e / kc, c = e % kc;
-        yc[c * r + a] = v[(size_t)slots[a] * kp + c0 + c];
-    }
-    __syncthreads();
-    const T* Zg = Z + core_z_off[g];
-    const int row0 = row0_of_block[blockIdx.x];
-    const int row1 = min(r, row0 + rows_per_block);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int row = row0 + warp; row < row1; row += nw) {
-        const T* zr = Zg + (size_t)row * r;
-        T acc[KC];
-#pragma unroll
-        for (int c = 0; c < KC; ++c) acc[c] = T(0);
-        for (int b = lane; b < r; b += 32) {
-            const T zv = __ldg(zr + b);
-#pragma unroll
-            for (int c = 0; c < KC; ++c)
-                if (c < kc) acc[c] += zv * yc[c * r + b];
-        }
-#pragma unroll
-        for (int c = 0; c < KC; ++c) {
-            if (c >= kc) break;
-            T a = acc[c];
-            for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-            if (lane == 0) tmp[(size_t)(core_slot_off[g] + row) * kp + c0 + c] = a;
-        }
-    }
+// Dense core of an AC factor: v[core] = Z v[core] (anchored inverse).  First the core
+// rows of v are copied to a contiguous buffer (core_stage_kernel), then each block
+// computes kCoreRowsPerBlock output rows with four warps per row: a warp takes a
+// quarter of the row's columns, its lane groups (4 RHS per lane) take the columns in
+// turn with four loads in flight, and the partial sums combine with shuffles and
+// shared memory before the row is written back into v.
+template <typename T>
+__global__ void core_stage_kernel(int64_t total, const uint32_t* __restrict__ core_slot, const T* __restrict__ v,
+                                  T* __restrict__ cin, int kp) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total * kp; e += (int64_t)gridDim.x * blockDim.x)
+        cin[e] = v[(size_t)core_slot[e / kp] * kp + e % kp];
 }
 
-template <typename T>
-__global__ void core_writeback_kernel(int64_t total, const uint32_t* __restrict__ core_slot,
-                                      const T* __restrict__ tmp, T* __restrict__ v, int kp) {
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total * kp; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t a = e / kp;
-        const int c = (int)(e % kp);
-        v[(size_t)core_slot[a] * kp + c] = tmp[e];
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) core_gemv_kernel(const int32_t* __restrict__ core_of_block,
+                                                           const int32_t* __restrict__ row0_of_block,
+                                                           const int32_t* __restrict__ core_n,
+                                                           const int64_t* __restrict__ core_slot_off,
+                                                           const uint32_t* __restrict__ core_slot,
+                                                           const int64_t* __restrict__ core_z_off,
+                                                           const T* __restrict__ Z, const T* __restrict__ cin,
+                                                           T* __restrict__ v, int kp) {
+    constexpr int NG = 32 / G;
+    constexpr int kParts = 4;  // warps per row
+    __shared__ T part[kBlock / 32][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / G, c4 = (lane & (G - 1)) * 4;
+    const int g = core_of_block[blockIdx.x];
+    const int r = core_n[g];
+    const int64_t off = core_slot_off[g];
+    const int row = row0_of_block[blockIdx.x] + warp / kParts;
+    V4<T> acc(T(0)), acc2(T(0));
+    if (row < r) {
+        const T* zr = Z + core_z_off[g] + (size_t)row * r;
+        const T* x = cin + (size_t)off * kp + c4;
+        const int q = warp % kParts;
+        const int b0 = (int)((int64_t)r * q / kParts), b1 = (int)((int64_t)r * (q + 1) / kParts);
+        int b = b0 + grp;
+        for (; b + 3 * NG < b1; b += 4 * NG) {
+            const T z0 = __ldg(zr + b), z1 = __ldg(zr + b + NG), z2 = __ldg(zr + b + 2 * NG), z3 = __ldg(zr + b + 3 * NG);
+            const V4<T> s0 = ldg4(x + (size_t)b * kp), s1 = ldg4(x + (size_t)(b + NG) * kp);
+            const V4<T> s2 = ldg4(x + (size_t)(b + 2 * NG) * kp), s3 = ldg4(x + (size_t)(b + 3 * NG) * kp);
+            acc += z0 * s0;
+            acc2 += z1 * s1;
+            acc += z2 * s2;
+            acc2 += z3 * s3;
+        }
+        for (; b < b1; b += NG) acc += __ldg(zr + b) * ldg4(x + (size_t)b * kp);
+    }
+    acc += acc2;
+#pragma unroll
+    for (int o = G; o < 32; o <<= 1) {
+        acc.a += __shfl_xor_sync(0xffffffffu, acc.a, o);
+        acc.b += __shfl_xor_sync(0xffffffffu, acc.b, o);
+        acc.c += __shfl_xor_sync(0xffffffffu, acc.c, o);
+        acc.d += __shfl_xor_sync(0xffffffffu, acc.d, o);
+    }
+    if (lane < G) {
+        part[warp][c4] = acc.a; part[warp][c4 + 1] = acc.b; part[warp][c4 + 2] = acc.c; part[warp][c4 + 3] = acc.d;
+    }
+    __syncthreads();
+    const int rows_here = kBlock / 32 / kParts;
+    for (int t = threadIdx.x; t < rows_here * kp; t += blockDim.x) {
+        const int rr = t / kp, c = t % kp;
+        const int orow = row0_of_block[blockIdx.x] + rr;
+        if (orow >= r) continue;
+        T s = T(0);
+#pragma unroll
+        for (int w = 0; w < kParts; ++w) s += part[rr * kParts + w][c];
+        v[(size_t)core_slot[off + orow] * kp + c] = s;
     }
 }
 

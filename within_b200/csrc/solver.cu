@@ -19,6 +19,7 @@
 
 #include "../../include/within_b200.h"
 #include "device.cuh"
+#include "obs_launch.cuh"
 #include "kernels.cuh"
 #include "setup.hpp"
 
@@ -261,6 +262,8 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
     }
     d.fwd_lp = h.fwd_lp;
     d.bwd_lp = h.bwd_lp;
+    d.fwd_lp_d.upload(h.fwd_lp);
+    d.bwd_lp_d.upload(h.bwd_lp);
     d.ndense = (int32_t)h.dn_n.size();
     d.dn_keep0.upload(h.dn_keep0);
     d.dn_loff.upload(h.dn_loff);
@@ -312,6 +315,8 @@ struct Workspace {
     DArr<double> st_bnorm, st_rz, st_rz0, st_alpha, st_beta, st_rnorm, st_tol;
     DArr<int32_t> st_active, st_conv, st_iters, st_part;
     DArr<int32_t> n_active;
+    DArr<unsigned> sweep_bar;                // grid-barrier counters of the fused AC sweeps
+    DArr<int32_t> sweep_err;                 // set when a barrier wait ran out
 };
 
 struct SolverImpl {
@@ -324,6 +329,7 @@ struct SolverImpl {
     bool perm_identity = true;
     cudaStream_t stream = nullptr;
     int n_sm = 148;
+    bool coop = false;  // cooperative launches available (fused AC sweeps)
     // device design
     DArr<uint32_t> codes, perm;
     DArr<double> w64;
@@ -564,7 +570,7 @@ int obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
     P = S.obs;
     P.kp = kp;
     const int G = group_for(kp);
-    const int64_t gpb = kBlock / G;
+    const int64_t gpb = (elem == 8 ? obs_block<double>() : obs_block<float>()) / G;
     const int Q = S.d.Q;
     for (int sl = 0; sl < kMaxQ; ++sl) {
         P.sink[sl] = SINK_GLOBAL;
@@ -604,14 +610,16 @@ int obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
             used += nl * kp;
         }
     }
-    for (int sl = 1; sl < Q; ++sl) {
+    for (int sl = 1; sl < Q; ++sl) {  // hot levels, the hottest first, as many as fit
+        P.hot_cap[sl] = 0;
         if (P.sink[sl] != SINK_GLOBAL || S.hot_count[sl] == 0) continue;
-        const int64_t len = (int64_t)S.hot_count[sl] * kp;
-        if (used + len > budget) continue;  // the whole hot table or none of it
+        const int64_t cap = std::min<int64_t>(S.hot_count[sl], (budget - used) / kp);
+        if (cap < 16) continue;
         P.sink[sl] = SINK_HOT;
+        P.hot_cap[sl] = (int32_t)cap;
         P.smem_base[sl] = (int32_t)used;
-        P.smem_len[sl] = (int32_t)len;
-        used += len;
+        P.smem_len[sl] = (int32_t)(cap * kp);
+        used += cap * kp;
     }
     P.smem_elems = (int32_t)used;
     return np;
@@ -634,34 +642,11 @@ void launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* 
         }
     }
     const size_t smem = (size_t)P.smem_elems * sizeof(T);
-    const int grid = S.nblk(P.nchunks, G, 2);
-    auto go = [&](auto kern) {
-        if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<grid, kBlock, smem, S.stream>>>(P, w, x, yin, out, eout);
-        WB_CUDA(cudaGetLastError());
-        S.gpu_launches++;
-    };
-#define WB_OBS_Q(GV)                                                                        \
-    switch (S.d.Q * 8 + std::min(np, 2)) {                                                  \
-        case 1 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 1, 0>); break;                      \
-        case 2 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 2, 0>); break;                      \
-        case 2 * 8 + 1: go(obs_pass_kernel<T, GV, MODE, 2, 1>); break;                      \
-        case 3 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 3, 0>); break;                      \
-        case 3 * 8 + 1: go(obs_pass_kernel<T, GV, MODE, 3, 1>); break;                      \
-        case 3 * 8 + 2: go(obs_pass_kernel<T, GV, MODE, 3, 2>); break;                      \
-        case 4 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 4, 0>); break;                      \
-        case 4 * 8 + 1: go(obs_pass_kernel<T, GV, MODE, 4, 1>); break;                      \
-        default: go(obs_pass_kernel<T, GV, MODE, kMaxQ, 0>); break;                         \
-    }
-    // exact kernels for Q <= 4 with the private slots as the trailing NP (Q = 4: NP <= 1);
-    // anything else runs the generic kernel, which reads every slot's sink
-    switch (G) {
-        case 1: WB_OBS_Q(1) break;
-        case 2: WB_OBS_Q(2) break;
-        case 4: WB_OBS_Q(4) break;
-        default: WB_OBS_Q(8) break;
-    }
-#undef WB_OBS_Q
+    const int bt = obs_block<T>();  // two resident blocks per SM (registers and shared memory)
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P.nchunks * G + bt - 1) / bt, (int64_t)S.n_sm * 2));
+    const cudaError_t err = obs_dispatch<T, MODE>(P, np, G, grid, smem, S.stream, w, x, yin, out, eout);
+    WB_CUDA(err);
+    S.gpu_launches++;
 }
 
 // Dot partials over rows (at most 2 blocks per SM: few partials to reduce).
@@ -730,6 +715,54 @@ void launch_csr(SolverImpl& S, CsrDev<T>& c, int64_t ch0, int64_t ch1, const T* 
     S.gpu_launches++;
 }
 
+// All levels of one AC sweep direction of a stage as one cooperative launch (grid
+// barriers between levels), when the device supports it; otherwise one launch per level.
+template <typename T, int EPI>
+void launch_sweep(SolverImpl& S, CsrDev<T>& c, const std::vector<int64_t>& lp, const int64_t* lp_d, bool backward,
+                  T* v, int kp, int which) {
+    const int nlev = (int)lp.size() - 1;
+    if (nlev <= 0) return;
+    if (!S.coop || nlev == 1) {
+        if (!backward)
+            for (int l = 0; l < nlev; ++l) launch_csr<T, EPI>(S, c, lp[l], lp[l + 1], v, v, kp);
+        else
+            for (int l = nlev - 1; l >= 0; --l) launch_csr<T, EPI>(S, c, lp[l], lp[l + 1], v, v, kp);
+        return;
+    }
+    const int G = group_for(kp);
+    unsigned* bar = S.ws.sweep_bar.p + which;
+    int* err = S.ws.sweep_err.p;
+    WB_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned), S.stream));
+    auto go = [&](auto kern) {
+        static int per_sm = 0;  // resident blocks per SM of this instantiation
+        if (per_sm == 0) WB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0));
+        const int grid = std::max(1, per_sm) * S.n_sm;
+        const CsrChunk* ch = c.chunks.p;
+        const uint32_t* rs = c.row_slot.p;
+        const int64_t* pt = c.ptr.p;
+        const uint32_t* cl = c.col.p;
+        const T* vl = c.val.p;
+        const T* sc = c.rscale.p;
+        int nl = nlev, bw = backward ? 1 : 0, k = kp;
+        void* args[] = {(void*)&ch, (void*)&lp_d, (void*)&nl, (void*)&bw, (void*)&rs, (void*)&pt, (void*)&cl,
+                        (void*)&vl, (void*)&sc, (void*)&v, (void*)&k, (void*)&bar, (void*)&err};
+        WB_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kBlock), args, 0, S.stream));
+        S.gpu_launches++;
+    };
+    WB_DISPATCH_G(G, go(csr_levels_kernel<T, GV, EPI>));
+}
+
+// The host learns of a grid-barrier timeout here (after the work that set it is done).
+void check_sweeps(SolverImpl& S) {
+    if (!S.coop || !S.ws.sweep_err.p) return;
+    int32_t e = 0;
+    WB_CUDA(cudaMemcpy(&e, S.ws.sweep_err.p, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (e) {
+        WB_CUDA(cudaMemset(S.ws.sweep_err.p, 0, sizeof(int32_t)));
+        throw CudaError("an AC sweep grid barrier wait exceeded its limit; the result is invalid");
+    }
+}
+
 // The local solves of one stage from the restriction input r up to the kept solution
 // in v and the subdomain sums in msum (see kernels.cuh for the algebra).
 template <typename T>
@@ -739,11 +772,12 @@ SubMeans stage_local_solve(SolverImpl& S, StageDev<T>& st, const T* r, T* v, int
     const size_t ms = (size_t)S.max_nsub * kp;
     double *S0 = msum, *SB = msum + ms, *M1 = msum + 2 * ms, *M2 = msum + 3 * ms;
     WB_CUDA(cudaMemsetAsync(msum, 0, sizeof(double) * 4 * ms, S.stream));
-    constexpr int kSpb = 1024;  // slots per block of the segmented sums
+    constexpr int kSpb = 256;  // keep-list entries per block of the segmented sums (4 per lane group)
     {
-        const int grid = (int)std::max<int64_t>(1, (st.nslots + kSpb - 1) / kSpb);
+        constexpr int kSlotsPerBlock = 1024;  // 16 slots per lane group
+        const int grid = (int)std::max<int64_t>(1, (st.nslots + kSlotsPerBlock - 1) / kSlotsPerBlock);
         WB_DISPATCH_G(G, schwarz_sums_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(
-                             st.nslots, kSpb, st.gidx.p, st.spou.p, st.invd.p, st.sub_of.p, r, kp, S0, SB));
+                             st.nslots, kSlotsPerBlock, st.gidx.p, st.spou.p, st.invd.p, st.sub_of.p, r, kp, S0, SB));
     }
     if (st.nkeep > 0) {
         const int grid = S.nblk(st.nkeep, G);
@@ -768,33 +802,18 @@ SubMeans stage_local_solve(SolverImpl& S, StageDev<T>& st, const T* r, T* v, int
         WB_CUDA(cudaGetLastError());
         S.gpu_launches++;
     }
-    const int nlev = (int)st.fwd_lp.size() - 1;
-    for (int l = 0; l < nlev; ++l) launch_csr<T, EPI_ACC>(S, st.fwd, st.fwd_lp[l], st.fwd_lp[l + 1], v, v, kp);
+    launch_sweep<T, EPI_ACC>(S, st.fwd, st.fwd_lp, st.fwd_lp_d.p, false, v, kp, 0);
     if (st.ncore_blocks > 0) {
-        T* tmp = core_buf<T>(S);
-        const int kc_max = std::max(1, std::min(kp, (int)(200 * 1024 / ((size_t)st.core_rmax * sizeof(T)))));
-        for (int c0 = 0; c0 < kp; c0 += kc_max) {
-            const int kc = std::min(kc_max, kp - c0);
-            const size_t smem = (size_t)st.core_rmax * kc * sizeof(T);
-            auto go = [&](auto kern) {
-                if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                kern<<<st.ncore_blocks, kBlock, smem, S.stream>>>(st.core_of_block.p, st.row0_of_block.p, st.core_n.p,
-                                                                 st.core_slot_off.p, st.core_slot.p, st.core_z_off.p,
-                                                                 st.core_z.p, v, tmp, kp, c0, kc, kCoreRowsPerBlock);
-                WB_CUDA(cudaGetLastError());
-                S.gpu_launches++;
-            };
-            if (kc <= 4) go(core_gemv_kernel<T, 4>);
-            else if (kc <= 8) go(core_gemv_kernel<T, 8>);
-            else if (kc <= 16) go(core_gemv_kernel<T, 16>);
-            else go(core_gemv_kernel<T, 32>);
-        }
-        const int grid = S.nblk(st.core_total * kp, 1);
-        core_writeback_kernel<T><<<grid, kBlock, 0, S.stream>>>(st.core_total, st.core_slot.p, tmp, v, kp);
+        T* cin = core_buf<T>(S);  // the cores' input rows, contiguous
+        core_stage_kernel<T><<<S.nblk(st.core_total * kp, 1), kBlock, 0, S.stream>>>(st.core_total, st.core_slot.p, v,
+                                                                                     cin, kp);
+        WB_DISPATCH_G(G, core_gemv_kernel<T, GV><<<st.ncore_blocks, kBlock, 0, S.stream>>>(
+                             st.core_of_block.p, st.row0_of_block.p, st.core_n.p, st.core_slot_off.p, st.core_slot.p,
+                             st.core_z_off.p, st.core_z.p, cin, v, kp));
         WB_CUDA(cudaGetLastError());
-        S.gpu_launches++;
+        S.gpu_launches += 2;
     }
-    for (int l = nlev - 1; l >= 0; --l) launch_csr<T, EPI_PIVOT>(S, st.bwd, st.bwd_lp[l], st.bwd_lp[l + 1], v, v, kp);
+    launch_sweep<T, EPI_PIVOT>(S, st.bwd, st.bwd_lp, st.bwd_lp_d.p, true, v, kp, 1);
     // sum over the kept solution with the back-substitution weights -> final means
     if (st.nkeep > 0) {
         const int gs = (int)std::max<int64_t>(1, (st.nkeep + kSpb - 1) / kSpb);
@@ -826,7 +845,7 @@ void apply_precond(SolverImpl& S, const T* r, T* z, int kp, double* part, int& n
         double* mm = S.ws.msum.p + (size_t)4 * S.max_nsub * kp;  // [nsub][2][kp]
         const int64_t nm = (int64_t)st.nsub * kp;
         sub_means_kernel<<<(unsigned)((nm + kBlock - 1) / kBlock), kBlock, 0, S.stream>>>(st.nsub, kp, M, mm);
-        nb_part = S.nblk(m, G, part ? 2 : 8);
+        nb_part = S.nblk(m, G, 4);  // latency-bound gathers: as many resident blocks as registers allow
         WB_DISPATCH_G(G, prolong_kernel<T, GV><<<nb_part, kBlock, 0, S.stream>>>(
                              m, st.gptr.p, st.gslot.p, st.gsub.p, st.gspou.p, st.ginvd.p, st.gbs_ptr.p, st.gbs_col.p,
                              st.gbs_val.p, mm, v, r, z, kp, part));
@@ -999,6 +1018,11 @@ void ensure_ws(SolverImpl& S, int kp) {
     for (DArr<double>* a : {&w.st_bnorm, &w.st_rz, &w.st_rz0, &w.st_alpha, &w.st_beta, &w.st_rnorm, &w.st_tol}) a->alloc(32);
     for (DArr<int32_t>* a : {&w.st_active, &w.st_conv, &w.st_iters, &w.st_part}) a->alloc(32);
     w.n_active.alloc(1);
+    if (!w.sweep_err.p) {
+        w.sweep_bar.alloc(2);
+        w.sweep_err.alloc(1);
+        WB_CUDA(cudaMemset(w.sweep_err.p, 0, sizeof(int32_t)));
+    }
     w.kp = kp;
     ++w.gen;
 }
@@ -1062,19 +1086,35 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
                 S.cg_exec = nullptr;
             }
             const int64_t l0 = S.gpu_launches;
-            cudaGraph_t g = nullptr;
-            WB_CUDA(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeRelaxed));
-            try {
-                body();
-            } catch (...) {
-                cudaStreamEndCapture(S.stream, &g);
+            // a capture that fails with the fused (cooperative) sweeps is retried without them
+            for (int attempt = 0;; ++attempt) {
+                S.gpu_launches = l0;
+                cudaGraph_t g = nullptr;
+                WB_CUDA(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeRelaxed));
+                try {
+                    body();
+                } catch (const CudaError&) {
+                    cudaStreamEndCapture(S.stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                    cudaGetLastError();
+                    if (attempt == 0 && S.coop) {
+                        S.coop = false;
+                        continue;
+                    }
+                    throw;
+                }
+                cudaError_t ie = cudaStreamEndCapture(S.stream, &g);
+                if (ie == cudaSuccess) ie = cudaGraphInstantiate(&S.cg_exec, g, 0);
                 if (g) cudaGraphDestroy(g);
-                throw;
+                if (ie != cudaSuccess && attempt == 0 && S.coop) {
+                    cudaGetLastError();
+                    S.cg_exec = nullptr;
+                    S.coop = false;
+                    continue;
+                }
+                WB_CUDA(ie);
+                break;
             }
-            WB_CUDA(cudaStreamEndCapture(S.stream, &g));
-            const cudaError_t ie = cudaGraphInstantiate(&S.cg_exec, g, 0);
-            cudaGraphDestroy(g);
-            WB_CUDA(ie);
             S.cg_key = key;
             S.cg_launches = S.gpu_launches - l0;
             S.gpu_launches = l0;
@@ -1606,6 +1646,9 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
     int dev = 0;
     WB_CUDA(cudaGetDevice(&dev));
     WB_CUDA(cudaDeviceGetAttribute(&S->n_sm, cudaDevAttrMultiProcessorCount, dev));
+    int coop = 0;
+    WB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    S->coop = coop != 0;
     WB_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
     WB_CUDA(cudaMallocHost(&S->h_active, sizeof(int32_t)));
     wb::upload_design(*S);
@@ -1670,6 +1713,7 @@ int solve_device(SolverImpl& S, const double* d_ys, size_t k, double* d_x, doubl
                 s.time_total = dt;
             }
     }
+    wb::check_sweeps(S);
     return WITHIN_OK;
 }
 
@@ -1856,6 +1900,7 @@ static int apply_common(within_solver* s, const double* in, size_t k, double* ou
         WB_CUDA(cudaGetLastError());
         WB_CUDA(cudaMemcpyAsync(out, dout.p, sizeof(double) * out_rows * k, cudaMemcpyDeviceToHost, S.stream));
         WB_CUDA(cudaStreamSynchronize(S.stream));
+        if (which == 1) wb::check_sweeps(S);
         return WITHIN_OK;
     });
 }
