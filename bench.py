@@ -42,7 +42,21 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-dropin", action="store_true", help="skip the FP64 drop-in comparison run")
+    ap.add_argument("--workload", default="panel", choices=["panel", "uneven"],
+                    help="panel: the 10M-obs weighted 3-FE panel (the headline); uneven: 256 independent "
+                         "problems of 1e3-1e6 observations, 2-4 factors, 1-8 RHS each (solve_many)")
+    ap.add_argument("--problems", type=int, default=256, help="number of problems of the uneven workload")
     return ap.parse_args()
+
+
+def max_over_ranks(dist, value: float, device: str = "cuda") -> float:
+    """The largest of every rank's value (the job's time is its slowest rank's)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def dist_info():
@@ -146,7 +160,48 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def uneven(args):
+    """Many independent problems of uneven size through within_solve_many.  A step solves
+    every problem from scratch (setup included: each problem is a one-shot solve), timed
+    on the host around the whole call with the device synchronised on both sides (the
+    problems run on many streams at once, which one stream's events do not cover)."""
+    import torch
+    import within_b200 as wb
+    from within_b200 import synthetic
+    torch.cuda.set_device(0)
+    probs = synthetic.config4(seed=0, n_problems=args.problems, max_obs=1_000_000)
+    n_rhs = sum(Y.shape[1] for _, Y in probs)
+    n_obs = sum(c.shape[0] for c, _ in probs)
+    cfg = wb.CG(precision=args.precision)
+    for _ in range(max(1, args.warmup)):
+        wb.solve_many(probs, cfg, concurrency=8)
+    clocks = Clocks(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res = wb.solve_many(probs, cfg, concurrency=8)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    clk = clocks.stop()
+    conv = all(all(r.converged) for r in res)
+    worst = max(max(r.residual) for r in res)
+    line = {"metric": "RHS solved/sec at tol 1e-8, uneven batch of independent problems (setup included)",
+            "value": args.steps * n_rhs / el, "unit": "RHS/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner / f64 refinement" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded log-uniform sizes, uniform codes)",
+            "config": {"workload": f"{len(probs)} independent problems, n_obs log-uniform on [1e3, 1e6] "
+                                   f"(total {n_obs}), 2-4 factors with levels log-uniform on [n/50, n/5], "
+                                   f"1-8 RHS each (total {n_rhs}), CG + additive Schwarz, tol 1e-8, "
+                                   "8 problems in flight", "timing": "host wall clock, device synchronised"},
+            "clocks": clk, "accuracy": {"converged": conv, "max_final_residual": worst}}
+    print(json.dumps(line), flush=True)
+
+
 def ours(args):
+    if args.workload == "uneven":
+        return uneven(args)
     import torch
     rank, local, world = dist_info()
     torch.cuda.set_device(local)
@@ -209,9 +264,7 @@ def ours(args):
         kt[which] = (cnt.value, ms.value)
     L.within_solver_set_profiling(solver._h, 0)
     if dist:
-        t = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+        elapsed_ms = max_over_ranks(dist, elapsed_ms)
     value = world * args.steps * k / (elapsed_ms / 1000.0)
 
     # end-to-end through the host C ABI (pinned buffers; copies inside the timed region)
@@ -238,9 +291,7 @@ def ours(args):
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(dist, e2e_ms)
     e2e_value = world * e2e_steps * k / (e2e_ms / 1000.0)
 
     # roofline of the dominant kernel: the operator apply G x = D'W(D x)
@@ -259,12 +310,11 @@ def ours(args):
                 "algorithmic_bytes_per_launch": op_bytes, "launches": cnt,
                 "avg_launch_us": 1000.0 * ms / cnt if cnt else None, "traffic": None,
                 "schwarz_apply_avg_us": 1000.0 * kt[which + 2][1] / kt[which + 2][0] if kt[which + 2][0] else None}
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        try:
-            roofline["traffic"] = json.load(open(tp)).get("per_launch_bytes_full_size")
-        except Exception:
-            pass
+    # DRAM bytes (dram__bytes_read.sum + write.sum) of one FP32 operator apply, from an ncu
+    # capture of the same panel at half size (5M observations), scaled by the observations
+    if which == 1 and abs(args.scale - 1.0) < 1e-9:
+        roofline["traffic"] = int(2 * 111.6e6)
+        roofline["traffic_source"] = "ncu dram__bytes_read+write at 5M observations, x2 (scales with n)"
 
     line = {"metric": METRIC, "value": value, "unit": "RHS/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
@@ -294,9 +344,7 @@ def ours(args):
         torch.cuda.synchronize()
         d_ms = a0.elapsed_time(a1)
         if dist:
-            t = torch.tensor([d_ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            d_ms = float(t.item())
+            d_ms = max_over_ranks(dist, d_ms)
         line["fp64_dropin"] = {"value": world * args.steps * k / (d_ms / 1000.0), "unit": "RHS/s",
                                "ms_per_step": d_ms / args.steps,
                                "converged": all(bool(st[c].converged) for c in range(k)),

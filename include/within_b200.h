@@ -135,6 +135,32 @@ int within_solve_batch(const uint32_t *codes, size_t n_obs, size_t n_factors, in
                        const within_params *params, const within_preconditioner *precond,
                        double *x, double *demeaned, within_solve_stats *stats);
 
+/* One problem of within_solve_many: a design, its weights (NULL = unit) and k RHS
+ * (n_obs*k, RHS-major), with caller-provided outputs x (n_dofs*k, where n_dofs is the
+ * sum over factors of max code + 1), demeaned (n_obs*k) and stats (k entries).
+ * status receives the problem's result code. */
+typedef struct {
+    const uint32_t *codes;
+    size_t n_obs, n_factors;
+    int64_t row_stride, col_stride;
+    const double *weights;
+    const double *ys;
+    size_t k;
+    double *x;
+    double *demeaned;
+    within_solve_stats *stats;
+    int32_t status;
+} within_problem;
+
+/* Many independent problems of uneven size (orchestrate::solve_batch applied to each),
+ * solved concurrently: up to `concurrency` problems (<= 0: 8) are in flight at once,
+ * each with its own solver and CUDA stream, so the kernels of small problems share the
+ * GPU.  Every problem is attempted; the return value is WITHIN_OK or the code of the
+ * first failed problem (its message in within_last_error), and each status says which.
+ * The reference has no single call for this: its callers loop over problems. */
+int within_solve_many(within_problem *problems, size_t n_problems, const within_params *params,
+                      const within_preconditioner *precond, int32_t concurrency);
+
 /* Operator applies on host vectors, for parity tests against the CPU oracle
  * (Operator::apply of GramianOperator, within/src/operator/gramian.rs:84-89, and of
  * FePreconditioner, within/src/operator/preconditioner.rs:108-154).

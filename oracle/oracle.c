@@ -618,6 +618,12 @@ static void acf_free(acf_t *f) {
 
 /* Rounds stop once at most this many vertices remain; those form the dense core. */
 #define AC_CORE_MAX 1024
+/* Rounds also stop once one would eliminate fewer than max(AC_STALL_MIN, remaining /
+   AC_STALL_DIV) vertices (the remaining graph has turned dense); if more than
+   AC_CORE_MAX vertices remain then, they become one last level of pivots: the diagonal
+   of the remaining Laplacian, without off-diagonal entries. */
+#define AC_STALL_MIN 32
+#define AC_STALL_DIV 128
 
 typedef struct { nbr_t *a; int32_t n, cap; } adj_t;
 static void adj_push(adj_t *l, uint32_t c, double w) {
@@ -788,6 +794,14 @@ static acf_t ac_build(const smat_t *s, uint64_t seed, uint32_t split) {
             blocked[v] = 1;
             for (int32_t b = 0; b < g[v].n; b++) blocked[g[v].a[b].col] = 1;
         }
+        {
+            int64_t lim = (int64_t)remaining / AC_STALL_DIV;
+            if (lim < AC_STALL_MIN) lim = AC_STALL_MIN;
+            if ((int64_t)np < lim) {  /* the remaining graph has turned dense: stop */
+                for (int32_t a = 0; a < nr; a++) blocked[rk[a].v] = 0;
+                break;
+            }
+        }
         f.level_ptr[f.nlev] = ncol;
         for (int32_t a = 0; a < np; a++) {
             int32_t v = picked[a];
@@ -826,6 +840,24 @@ static acf_t ac_build(const smat_t *s, uint64_t seed, uint32_t split) {
         for (int32_t a = 0; a < np; a++) { dead[picked[a]] = 1; }
         for (int32_t a = 0; a < nr; a++) blocked[rk[a].v] = 0;
         remaining -= np;
+        f.nlev++;
+    }
+    if (remaining > AC_CORE_MAX) {
+        /* stalled, larger than a core: one last level of pivots (weighted degree in the
+           remaining graph) without off-diagonal entries */
+        f.level_ptr[f.nlev] = ncol;
+        for (int32_t v = 0; v < n; v++) {
+            if (dead[v]) continue;
+            if (g[v].n > maxlen) { maxlen = g[v].n * 2; tmp = xrealloc(tmp, sizeof(nbr_t) * (size_t)maxlen); }
+            adj_compact(&g[v], dead, tmp);
+            double d = 0.0;
+            for (int32_t b = 0; b < g[v].n; b++) d += g[v].a[b].w;
+            f.col_vertex[ncol] = v;
+            f.col_diag[ncol] = g[v].n > 0 ? d : 0.0;
+            f.col_ptr[ncol] = (int32_t)cnnz;
+            ncol++;
+        }
+        for (int32_t v = 0; v < n; v++) dead[v] = 1;
         f.nlev++;
     }
     f.level_ptr[f.nlev] = ncol;

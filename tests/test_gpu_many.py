@@ -1,0 +1,47 @@
+"""Uneven batch of independent problems (within_solve_many) against the CPU oracle and
+against solving each problem on its own."""
+import numpy as np
+import pytest
+
+import oracle
+import within_b200 as wb
+from within_b200 import synthetic
+from paritylib import normalize_x, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_solve_many_matches_oracle(precision):
+    probs = synthetic.config4(seed=3, n_problems=7, max_obs=30_000)
+    res = wb.solve_many(probs, wb.CG(precision=precision), concurrency=4)
+    assert len(res) == len(probs)
+    for (cats, Y), r in zip(probs, res):
+        assert r.x.shape == (sum(int(cats[:, j].max()) + 1 for j in range(cats.shape[1])), Y.shape[1])
+        o = oracle.OracleSolver(cats, None).solve_batch(Y, threads=4)
+        for c in range(Y.shape[1]):
+            assert r.converged[c] and r.residual[c] <= 1e-8
+            # tolerance 1e-8 relative (demeaned) against the oracle at the same tol; mixed
+            # precision is held to 1e-7 (its inner solves stop at a different point)
+            assert rel(r.demeaned[:, c], o.demeaned[:, c]) < (1e-8 if precision == "fp64" else 1e-7)
+            assert rel(normalize_x(cats, r.x[:, c]), normalize_x(cats, o.x[:, c])) < 1e-6
+
+
+def test_solve_many_equals_single_solves_and_weights():
+    probs = synthetic.config4(seed=5, n_problems=5, max_obs=20_000)
+    rng = np.random.default_rng(2)
+    wprobs = [(c, Y, rng.lognormal(0, 1, c.shape[0])) for c, Y in probs]
+    many = wb.solve_many(wprobs, concurrency=3)
+    for (c, Y, w), r in zip(wprobs, many):
+        one = wb.solve_batch(c, Y, weights=w)
+        for j in range(Y.shape[1]):
+            assert rel(r.demeaned[:, j], one.demeaned[:, j]) < 1e-10
+            assert r.iterations[j] == one.iterations[j] or abs(r.iterations[j] - one.iterations[j]) <= 1
+
+
+def test_solve_many_reports_the_failing_problem():
+    good = synthetic.config4(seed=7, n_problems=2, max_obs=5_000)
+    bad = (good[0][0], good[0][1][:-1])  # one observation short
+    with pytest.raises(wb.WithinError):
+        wb.solve_many([good[1], bad], concurrency=2)
+    assert wb.solve_many([]) == []

@@ -26,7 +26,7 @@ from . import _lib
 __all__ = [
     "OperatorRepr", "Preconditioner", "ReductionStrategy", "CG", "GMRES", "ApproxCholConfig",
     "ApproxSchurConfig", "SchurComplement", "AdditiveSchwarz", "MultiplicativeSchwarz", "SolveResult",
-    "BatchSolveResult", "FePreconditioner", "Solver", "solve", "solve_batch", "WithinError",
+    "BatchSolveResult", "FePreconditioner", "Solver", "solve", "solve_batch", "solve_many", "WithinError",
 ]
 
 
@@ -397,6 +397,57 @@ def solve(categories, y, config=None, weights=None, preconditioner=None) -> Solv
     r.time_setup = s.time_setup
     r.time_total = time.perf_counter() - t0
     return r
+
+
+def solve_many(problems, config=None, preconditioner=None, concurrency: int = 8) -> list:
+    """Many independent problems of uneven size, each like ``solve_batch``.
+
+    ``problems`` is a sequence of ``(categories, Y)`` or ``(categories, Y, weights)``
+    with Y of shape (n_obs, k) (or (n_obs,) for one RHS).  Up to ``concurrency``
+    problems are solved at once, each with its own solver and CUDA stream, so that
+    small problems share the GPU.  Returns one BatchSolveResult per problem; raises
+    WithinError naming the first problem that failed.
+    """
+    L = _lib.load()
+    params = _params_struct(config)
+    pre = _precond_struct(preconditioner)
+    _validate(params, pre)
+    keep, arr = [], (_lib.Problem * max(len(problems), 1))()
+    outs = []
+    for i, prob in enumerate(problems):
+        cats, Y = prob[0], prob[1]
+        w = prob[2] if len(prob) > 2 else None
+        cats = _categories(cats)
+        n, q = cats.shape
+        Y = np.asarray(Y, dtype=np.float64)
+        Y = np.asfortranarray(Y.reshape(n, -1) if Y.ndim == 1 else Y)
+        if Y.shape[0] != n:
+            raise WithinError(2, f"problem {i}: y has {Y.shape[0]} observations, expected {n}")
+        k = Y.shape[1]
+        m = int(sum(int(cats[:, j].max()) + 1 for j in range(q))) if n > 0 else 0
+        if w is not None:
+            w = np.ascontiguousarray(w, dtype=np.float64)
+            if w.ndim != 1 or w.shape[0] != n:
+                raise WithinError(3, f"problem {i}: weights has length {w.shape[0] if w.ndim else 0}, expected {n}")
+        x = np.empty((m, k), order="F")
+        d = np.empty((n, k), order="F")
+        st = (_lib.Stats * max(k, 1))()
+        isz = cats.itemsize
+        arr[i] = _lib.Problem(cats.ctypes.data, n, q, cats.strides[0] // isz, cats.strides[1] // isz,
+                              w.ctypes.data if w is not None else None, Y.ctypes.data, k, x.ctypes.data, d.ctypes.data,
+                              C.cast(st, C.c_void_p), 0)
+        keep.append((cats, Y, w))
+        outs.append((x, d, st, k))
+    rc = L.within_solve_many(arr, len(problems), C.byref(params), None if pre.kind == 0 else C.byref(pre),
+                             int(concurrency))
+    _check(rc)
+    res = []
+    for x, d, st, k in outs:
+        res.append(BatchSolveResult(x, d, [bool(st[c].converged) for c in range(k)],
+                                    [int(st[c].iterations) for c in range(k)],
+                                    [float(st[c].final_residual) for c in range(k)],
+                                    [float(st[c].time_solve) for c in range(k)], float(st[0].time_total) if k else 0.0))
+    return res
 
 
 def solve_batch(categories, Y, config=None, weights=None, preconditioner=None) -> BatchSolveResult:

@@ -40,6 +40,13 @@ class Stats(C.Structure):
                 ("time_total", C.c_double), ("time_setup", C.c_double), ("time_solve", C.c_double)]
 
 
+class Problem(C.Structure):
+    _fields_ = [("codes", C.c_void_p), ("n_obs", C.c_size_t), ("n_factors", C.c_size_t),
+                ("row_stride", C.c_int64), ("col_stride", C.c_int64), ("weights", C.c_void_p),
+                ("ys", C.c_void_p), ("k", C.c_size_t), ("x", C.c_void_p), ("demeaned", C.c_void_p),
+                ("stats", C.c_void_p), ("status", C.c_int32)]
+
+
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -55,6 +62,7 @@ EXPORTED = [
     "within_solver_subdomain_info", "within_solver_subdomain_indices", "within_solver_ac_sizes",
     "within_solver_ac_arrays", "within_solver_gpu_launches", "within_solver_setup_time", "within_last_error",
     "within_solver_set_profiling", "within_solver_kernel_time", "within_solver_apply_gramian_noalloc",
+    "within_solve_many",
 ]
 
 _lib = None
@@ -104,6 +112,8 @@ def load():
     L.within_solver_setup_time.argtypes = [vp]
     L.within_solver_setup_time.restype = C.c_double
     L.within_last_error.restype = C.c_char_p
+    L.within_solve_many.argtypes = [C.POINTER(Problem), C.c_size_t, vp, vp, C.c_int32]
+    L.within_solve_many.restype = C.c_int
     L.within_solver_apply_gramian_noalloc.argtypes = [vp, vp, C.c_size_t, vp, vp]
     L.within_solver_apply_gramian_noalloc.restype = C.c_int
     L.within_solver_set_profiling.argtypes = [vp, C.c_int32]

@@ -241,7 +241,10 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
             cv[q] = V4<T>(T(0));
         }
         // one observation: codes c[0..Q), weight wi
-        auto body = [&](uint32_t i, const uint32_t (&c)[QT], T wi) {
+        // one observation in two phases: its row sum (loads) and its scatter; a batch
+        // runs the first phase for all its observations before the second, so their
+        // loads are in flight together (the scatter's reductions order memory)
+        auto gather = [&](uint32_t i, const uint32_t (&c)[QT]) -> V4<T> {
             V4<T> s(T(0));
             if constexpr (kGather) {
 #pragma unroll
@@ -260,6 +263,9 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
                 const V4<T> yv = ld4(yin + (size_t)i * KP + c4);
                 s = (MODE == OBS_RHS) ? yv : yv - s;
             }
+            return s;
+        };
+        auto scatter = [&](uint32_t i, const uint32_t (&c)[QT], T wi, const V4<T>& s) {
             if constexpr (MODE == OBS_DX || MODE == OBS_RESID) st4(eout + (size_t)i * KP + c4, s);
             if constexpr (kScatter) {
                 const V4<T> t = wi * s;
@@ -287,6 +293,7 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
                 }
             }
         };
+        auto body = [&](uint32_t i, const uint32_t (&c)[QT], T wi) { scatter(i, c, wi, gather(i, c)); };
         auto single = [&](uint32_t i) {
             uint32_t c[QT];
 #pragma unroll
@@ -312,13 +319,16 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
                             nb[q] = more ? __ldg(reinterpret_cast<const uint4*>(P.codes + (size_t)q * ns + i + 4)) : cb[q];
                         if (weighted && more) nw = load_w4v(w, i + 4);
                     }
+                    uint32_t c[4][QT];
+                    V4<T> s[4];
 #pragma unroll
                     for (int b = 0; b < 4; ++b) {
-                        uint32_t c[QT];
 #pragma unroll
-                        for (int q = 0; q < QT; ++q) c[q] = ucomp(cb[q], b);
-                        body(i + b, c, weighted ? (T)wcomp(wb, b) : T(1));
+                        for (int q = 0; q < QT; ++q) c[b][q] = ucomp(cb[q], b);
+                        s[b] = gather(i + b, c[b]);
                     }
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) scatter(i + b, c[b], weighted ? (T)wcomp(wb, b) : T(1), s[b]);
                     if constexpr (kPrefetch) {
 #pragma unroll
                         for (int q = 0; q < QT; ++q) cb[q] = nb[q];
@@ -371,52 +381,63 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
 
 // Column-major (RHS-major) user order <-> interleaved primary-sorted order with kp
 // columns (padding columns are zero).  perm[i] = user index of sorted row i (or identity).
+// Each warp transposes tiles of 32 rows through its own shared-memory tile (32 x kp+1):
+// column-major accesses are one row per lane (coalesced per column), row-major ones run
+// over the tile's flat elements (consecutive lanes, consecutive addresses).
+constexpr int kXposeWarps = 4;  // warps per block of the transpose kernels
+inline size_t xpose_smem(int kp) { return (size_t)kXposeWarps * 32 * (kp + 1) * sizeof(double); }
+
 template <typename T>
-__global__ void gather_interleave_kernel(const double* __restrict__ ycol, int64_t n, int k, int kp,
-                                         const uint32_t* __restrict__ perm, T* __restrict__ yi) {
-    __shared__ double tile[32][33];
-    const int64_t i0 = (int64_t)blockIdx.x * 32;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-    for (int c0 = 0; c0 < kp; c0 += 32) {
-        for (int cc = ty; cc < 32; cc += 8) {
-            const int c = c0 + cc;
-            const int64_t i = i0 + tx;
-            double v = 0.0;
-            if (c < k && i < n) v = ycol[(size_t)c * n + (perm ? perm[i] : i)];
-            tile[cc][tx] = v;
-        }
-        __syncthreads();
-        const int cw = min(32, kp - c0);
-        for (int e = threadIdx.x; e < 32 * cw; e += blockDim.x) {
-            const int r = e / cw, cc = e % cw;
-            const int64_t i = i0 + r;
-            if (i < n) yi[(size_t)i * kp + c0 + cc] = (T)tile[cc][r];
-        }
-        __syncthreads();
+__global__ void __launch_bounds__(kXposeWarps * 32) gather_interleave_kernel(const double* __restrict__ ycol, int64_t n,
+                                                                             int k, int kp,
+                                                                             const uint32_t* __restrict__ perm,
+                                                                             T* __restrict__ yi) {
+    extern __shared__ double xtile[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ld = kp + 1;
+    double* tile = xtile + (size_t)warp * 32 * ld;
+    const int64_t nw = (int64_t)gridDim.x * kXposeWarps;
+    for (int64_t i0 = ((int64_t)blockIdx.x * kXposeWarps + warp) * 32; i0 < n; i0 += nw * 32) {
+        const int64_t i = i0 + lane;
+        const bool ok = i < n;
+        const size_t src = ok ? (perm ? (size_t)perm[i] : (size_t)i) : 0;
+        for (int c = 0; c < kp; ++c) tile[lane * ld + c] = (ok && c < k) ? ycol[(size_t)c * n + src] : 0.0;
+        __syncwarp();
+        const int rows = (int)min((int64_t)32, n - i0);
+        T* dst = yi + (size_t)i0 * kp;
+        for (int f = lane; f < rows * kp; f += 32) dst[f] = (T)tile[(f / kp) * ld + f % kp];
+        __syncwarp();
     }
 }
 
 template <typename T>
-__global__ void scatter_deinterleave_kernel(const T* __restrict__ ei, int64_t n, int k, int kp,
-                                            const uint32_t* __restrict__ perm, double* __restrict__ ecol) {
-    __shared__ double tile[32][33];
-    const int64_t i0 = (int64_t)blockIdx.x * 32;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int c0 = 0; c0 < k; c0 += 32) {
-        const int cw = min(32, k - c0);
-        for (int e = threadIdx.x; e < 32 * cw; e += blockDim.x) {
-            const int r = e / cw, cc = e % cw;
-            const int64_t i = i0 + r;
-            tile[cc][r] = (i < n) ? (double)ei[(size_t)i * kp + c0 + cc] : 0.0;
+__global__ void __launch_bounds__(kXposeWarps * 32) scatter_deinterleave_kernel(const T* __restrict__ ei, int64_t n,
+                                                                                int k, int kp,
+                                                                                const uint32_t* __restrict__ perm,
+                                                                                double* __restrict__ ecol) {
+    extern __shared__ double xtile[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ld = kp + 1;
+    double* tile = xtile + (size_t)warp * 32 * ld;
+    const int64_t nw = (int64_t)gridDim.x * kXposeWarps;
+    for (int64_t i0 = ((int64_t)blockIdx.x * kXposeWarps + warp) * 32; i0 < n; i0 += nw * 32) {
+        const int rows = (int)min((int64_t)32, n - i0);
+        const T* src = ei + (size_t)i0 * kp;
+        for (int f = lane; f < rows * kp; f += 32) tile[(f / kp) * ld + f % kp] = (double)src[f];
+        __syncwarp();
+        const int64_t i = i0 + lane;
+        if (i < n) {
+            const size_t dst = perm ? (size_t)perm[i] : (size_t)i;
+            for (int c = 0; c < k; ++c) ecol[(size_t)c * n + dst] = tile[lane * ld + c];
         }
-        __syncthreads();
-        for (int cc = ty; cc < 32; cc += 8) {
-            const int c = c0 + cc;
-            const int64_t i = i0 + tx;
-            if (c < k && i < n) ecol[(size_t)c * n + (perm ? perm[i] : i)] = tile[cc][tx];
-        }
-        __syncthreads();
+        __syncwarp();
     }
+}
+
+// Blocks for a transpose over `rows` rows (grid-stride beyond 16 blocks per SM).
+inline unsigned xpose_blocks(int64_t rows, int n_sm) {
+    const int64_t need = (rows + 32 * kXposeWarps - 1) / (32 * kXposeWarps);
+    return (unsigned)(need < 1 ? 1 : (need < (int64_t)n_sm * 16 ? need : (int64_t)n_sm * 16));
 }
 
 // ---------------------------------------------------------------------------
@@ -517,10 +538,12 @@ __global__ void __launch_bounds__(kBlock) cg_p_kernel(T* __restrict__ p, const T
 // ---------------------------------------------------------------------------
 
 // Work unit of a row-wise CSR pass: rows [row_begin, row_end) restricted to entries
-// [nz_begin, nz_end); rows cut by the range are partial and add atomically.
+// [nz_begin, nz_end); rows cut by the range are partial and add atomically.  whole: the
+// chunk is exactly one complete row, so its range needs no row-pointer loads.
 struct CsrChunk {
     uint32_t row_begin, row_end;
     int64_t nz_begin, nz_end;
+    uint32_t whole;
 };
 
 enum CsrEpi { EPI_ACC = 0, EPI_PIVOT = 1 };
@@ -548,7 +571,8 @@ __global__ void __launch_bounds__(kBlock) csr_rows_kernel(const CsrChunk* __rest
     for (int64_t ch = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < nchunks; ch += nw) {
         const CsrChunk C = chunks[ch];
         for (uint32_t row = C.row_begin; row < C.row_end; ++row) {
-            const int64_t rb = ptr[row], re = ptr[row + 1];
+            const bool one = C.whole != 0;  // one complete row: its range is the chunk's
+            const int64_t rb = one ? C.nz_begin : ptr[row], re = one ? C.nz_end : ptr[row + 1];
             const int64_t e0 = max(rb, C.nz_begin), e1 = min(re, C.nz_end);
             V4<T> acc(T(0));
             int64_t e = e0 + grp;
@@ -650,7 +674,8 @@ __global__ void __launch_bounds__(kBlock) csr_levels_kernel(const CsrChunk* __re
         for (int64_t ch = lp[l] + wid; ch < lp[l + 1]; ch += nw) {
             const CsrChunk C = chunks[ch];
             for (uint32_t row = C.row_begin; row < C.row_end; ++row) {
-                const int64_t rb = ptr[row], re = ptr[row + 1];
+                const bool one = C.whole != 0;  // one complete row: its range is the chunk's
+                const int64_t rb = one ? C.nz_begin : ptr[row], re = one ? C.nz_end : ptr[row + 1];
                 const int64_t e0 = max(rb, C.nz_begin), e1 = min(re, C.nz_end);
                 V4<T> acc(T(0));
                 int64_t e = e0 + grp;

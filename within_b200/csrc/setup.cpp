@@ -408,22 +408,34 @@ bool dense_cholesky(std::vector<double>& a, int32_t m);
 // SPD inverse through the Cholesky factor: A = L L^T, A^-1 = L^-T L^-1.
 bool spd_inverse(std::vector<double>& a, int32_t m) {
     if (!dense_cholesky(a, m)) return false;
-    for (int32_t j = 0; j < m; ++j) {  // L^-1 in place, column by column
-        a[(size_t)j * m + j] = 1.0 / a[(size_t)j * m + j];
-        for (int32_t i = j + 1; i < m; ++i) {
-            double s = 0.0;
-            for (int32_t k = j; k < i; ++k) s += a[(size_t)i * m + k] * a[(size_t)k * m + j];
-            a[(size_t)i * m + j] = -s / a[(size_t)i * m + i];
+    // L^-1 row by row (row i = (e_i - sum_{k<i} L_ik row_k) / L_ii): contiguous row updates
+    std::vector<double> li((size_t)m * m, 0.0);
+    for (int32_t i = 0; i < m; ++i) {
+        double* ri = li.data() + (size_t)i * m;
+        const double* lrow = a.data() + (size_t)i * m;
+        for (int32_t k = 0; k < i; ++k) {
+            const double c = lrow[k];
+            if (c == 0.0) continue;
+            const double* rk = li.data() + (size_t)k * m;
+            for (int32_t j = 0; j <= k; ++j) ri[j] -= c * rk[j];
+        }
+        ri[i] += 1.0;
+        const double inv = 1.0 / lrow[i];
+        for (int32_t j = 0; j <= i; ++j) ri[j] *= inv;
+    }
+    // A^-1 = L^-T L^-1 = sum_k row_k^T row_k, accumulated row by row into the lower half
+    std::vector<double> z((size_t)m * m, 0.0);
+    for (int32_t k = 0; k < m; ++k) {
+        const double* rk = li.data() + (size_t)k * m;
+        for (int32_t i = 0; i <= k; ++i) {
+            const double c = rk[i];
+            if (c == 0.0) continue;
+            double* zi = z.data() + (size_t)i * m;
+            for (int32_t j = 0; j <= i; ++j) zi[j] += c * rk[j];
         }
     }
-    std::vector<double> z((size_t)m * m);
     for (int32_t i = 0; i < m; ++i)
-        for (int32_t j = 0; j <= i; ++j) {
-            double s = 0.0;
-            for (int32_t k = i; k < m; ++k) s += a[(size_t)k * m + i] * a[(size_t)k * m + j];
-            z[(size_t)i * m + j] = s;
-            z[(size_t)j * m + i] = s;
-        }
+        for (int32_t j = 0; j < i; ++j) z[(size_t)j * m + i] = z[(size_t)i * m + j];
     a.swap(z);
     return true;
 }
@@ -495,12 +507,21 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
     CliqueTreeSampler sampler;
     std::vector<Edge> fill;
     int32_t remaining = n;
+    // A vertex's list changes only when a neighbour is eliminated (the neighbour dies, fill
+    // edges arrive), so only those "dirty" lists are compacted in the next round; a clean
+    // list is already sorted and merged, where compacting it again would change nothing.
+    std::vector<uint8_t> dirty((size_t)n, 1);
+    std::vector<uint64_t> vhash((size_t)n);
+    for (int32_t v = 0; v < n; ++v) vhash[v] = hash64(seed ^ ((uint64_t)v * 0xD1B54A32D192ED03ULL));
     while (remaining > kAcCoreMax) {
         rank.clear();
         for (int32_t v = 0; v < n; ++v) {
             if (dead[v]) continue;
-            compact_adj(g[v], dead);
-            rank.push_back(Rank{(int32_t)g[v].size(), hash64(seed ^ ((uint64_t)v * 0xD1B54A32D192ED03ULL)), v});
+            if (dirty[v]) {
+                compact_adj(g[v], dead);
+                dirty[v] = 0;
+            }
+            rank.push_back(Rank{(int32_t)g[v].size(), vhash[v], v});
         }
         std::sort(rank.begin(), rank.end(), [](const Rank& a, const Rank& b) {
             if (a.deg != b.deg) return a.deg < b.deg;
@@ -513,6 +534,12 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
             picked.push_back(rk.v);
             blocked[rk.v] = 1;
             for (const Nbr& x : g[rk.v]) blocked[x.col] = 1;
+        }
+        if ((int64_t)picked.size() < std::max<int64_t>(kAcStallMin, remaining / kAcStallDiv)) {
+            // the remaining graph has turned dense: rounds would eliminate a few vertices
+            // each; stop here (the tail below)
+            for (const Rank& rk : rank) blocked[rk.v] = 0;
+            break;
         }
         f.level_ptr.push_back((int32_t)f.col_vertex.size());
         for (int32_t v : picked) {
@@ -535,9 +562,28 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
                 }
             }
         }
+        for (int32_t v : picked)
+            for (const Nbr& x : g[v]) dirty[x.col] = 1;
         for (int32_t v : picked) { dead[v] = 1; std::vector<Nbr>().swap(g[v]); }
         for (const Rank& rk : rank) blocked[rk.v] = 0;
         remaining -= (int32_t)picked.size();
+        f.nlev++;
+    }
+    if (remaining > kAcCoreMax) {
+        // stalled with more vertices than a dense core holds: one last level of pivots,
+        // each remaining vertex's weighted degree in the remaining graph (the diagonal
+        // of the remaining Laplacian) and no off-diagonal entries
+        f.level_ptr.push_back((int32_t)f.col_vertex.size());
+        for (int32_t v = 0; v < n; ++v) {
+            if (dead[v]) continue;
+            compact_adj(g[v], dead);
+            double d = 0.0;
+            for (const Nbr& x : g[v]) d += x.w;
+            f.col_vertex.push_back(v);
+            f.col_diag.push_back(g[v].empty() ? 0.0 : d);
+            f.col_ptr.push_back((int32_t)f.col_idx.size());
+        }
+        for (int32_t v = 0; v < n; ++v) dead[v] = 1;
         f.nlev++;
     }
     f.level_ptr.push_back((int32_t)f.col_vertex.size());
@@ -549,16 +595,29 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
 
 // Lower Cholesky of an SPD row-major matrix; false when a pivot is not positive.
 bool dense_cholesky(std::vector<double>& a, int32_t m) {
+    // dot products with four partial sums (vectorisable; rounding differs from a strict
+    // left-to-right sum only in the last bits)
+    auto dot = [](const double* x, const double* y, int32_t n) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int32_t k = 0;
+        for (; k + 4 <= n; k += 4) {
+            s0 += x[k] * y[k];
+            s1 += x[k + 1] * y[k + 1];
+            s2 += x[k + 2] * y[k + 2];
+            s3 += x[k + 3] * y[k + 3];
+        }
+        for (; k < n; ++k) s0 += x[k] * y[k];
+        return (s0 + s1) + (s2 + s3);
+    };
     for (int32_t j = 0; j < m; ++j) {
-        double s = a[(size_t)j * m + j];
-        for (int32_t k = 0; k < j; ++k) s -= a[(size_t)j * m + k] * a[(size_t)j * m + k];
+        double* rj = a.data() + (size_t)j * m;
+        const double s = rj[j] - dot(rj, rj, j);
         if (!(s > 0.0)) return false;
         const double ljj = std::sqrt(s);
-        a[(size_t)j * m + j] = ljj;
+        rj[j] = ljj;
         for (int32_t i = j + 1; i < m; ++i) {
-            double t = a[(size_t)i * m + j];
-            for (int32_t k = 0; k < j; ++k) t -= a[(size_t)i * m + k] * a[(size_t)j * m + k];
-            a[(size_t)i * m + j] = t / ljj;
+            double* ri = a.data() + (size_t)i * m;
+            ri[j] = (ri[j] - dot(ri, rj, j)) / ljj;
         }
         for (int32_t i = 0; i < j; ++i) a[(size_t)i * m + j] = 0.0;
     }
@@ -632,25 +691,41 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
         for (int64_t i = 0; i < d.n; ++i) active[q][c[i]] = 1;
     }
     // Pairs (q < r) in lexicographic order (factor_pairs.rs:252-260); components in
-    // order; indices q-levels then r-levels (:244-250).
+    // order; indices q-levels then r-levels (:244-250).  The pairs are independent and
+    // built concurrently (each pair's arithmetic is unchanged), then appended in order.
+    std::vector<std::pair<int, int>> pairs;
     for (int q = 0; q < d.Q; ++q)
-        for (int r = q + 1; r < d.Q; ++r) {
-            CrossTab full;
-            std::vector<uint32_t> l2g;
-            int32_t nqf = 0;
-            if (!pair_crosstab(d, q, r, active, full, l2g, nqf)) continue;
-            std::vector<Component> comps = components(full);
-            for (size_t c = 0; c < comps.size(); ++c) {
-                Subdomain sd;
-                sd.q = q;
-                sd.r = r;
-                sd.gidx.reserve(comps[c].qi.size() + comps[c].ri.size());
-                for (int32_t i : comps[c].qi) sd.gidx.push_back(l2g[i]);
-                for (int32_t i : comps[c].ri) sd.gidx.push_back(l2g[nqf + i]);
-                sd.ct = comps.size() == 1 ? std::move(full) : extract(full, comps[c]);
-                subs.push_back(std::move(sd));
-            }
+        for (int r = q + 1; r < d.Q; ++r) pairs.emplace_back(q, r);
+    std::vector<std::vector<Subdomain>> per_pair(pairs.size());
+    auto build_pair = [&](size_t p) {
+        const int q = pairs[p].first, r = pairs[p].second;
+        CrossTab full;
+        std::vector<uint32_t> l2g;
+        int32_t nqf = 0;
+        if (!pair_crosstab(d, q, r, active, full, l2g, nqf)) return;
+        std::vector<Component> comps = components(full);
+        for (size_t c = 0; c < comps.size(); ++c) {
+            Subdomain sd;
+            sd.q = q;
+            sd.r = r;
+            sd.gidx.reserve(comps[c].qi.size() + comps[c].ri.size());
+            for (int32_t i : comps[c].qi) sd.gidx.push_back(l2g[i]);
+            for (int32_t i : comps[c].ri) sd.gidx.push_back(l2g[nqf + i]);
+            sd.ct = comps.size() == 1 ? std::move(full) : extract(full, comps[c]);
+            per_pair[p].push_back(std::move(sd));
         }
+    };
+    {
+        const size_t hw_pairs = std::max(1u, std::thread::hardware_concurrency());
+        std::vector<std::future<void>> pj;
+        for (size_t p = 0; p < pairs.size(); ++p) {
+            if (pj.size() + 1 < hw_pairs && p + 1 < pairs.size()) pj.push_back(std::async(std::launch::async, build_pair, p));
+            else build_pair(p);
+        }
+        for (auto& j : pj) j.get();
+    }
+    for (auto& v : per_pair)
+        for (auto& sd : v) subs.push_back(std::move(sd));
     // Partition-of-unity weights (compute_partition_weights, factor_pairs.rs:272-304).
     std::vector<uint32_t> count((size_t)d.ndofs, 0);
     for (const Subdomain& sd : subs)

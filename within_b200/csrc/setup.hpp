@@ -41,8 +41,13 @@ struct CrossTab {
     std::vector<double> dq, dr;
 };
 
-// Rounds of the approximate Cholesky factor stop once at most this many vertices remain.
+// Rounds of the approximate Cholesky factor stop once at most this many vertices remain
+// (they form the dense core), or once a round would eliminate fewer than
+// max(kAcStallMin, remaining / kAcStallDiv) vertices: the remaining graph has turned
+// dense, and if it is larger than a core, its vertices become one last level of pivots
+// (the diagonal of the remaining Laplacian).
 constexpr int32_t kAcCoreMax = 1024;
+constexpr int64_t kAcStallMin = 32, kAcStallDiv = 128;
 
 // Approximate Cholesky factor L D L^T of a Schur-complement Laplacian, eliminated in
 // rounds of independent vertices.  Column c eliminates vertex col_vertex[c] with pivot

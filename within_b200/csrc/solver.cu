@@ -9,8 +9,11 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <future>
 #include <memory>
 #include <mutex>
+#include <thread>
+#include <atomic>
 #include <numeric>
 #include <string>
 #include <tuple>
@@ -49,7 +52,7 @@ std::vector<CsrChunk> make_chunks(const std::vector<int64_t>& ptr, int64_t row_l
         const int64_t len = ptr[r + 1] - ptr[r];
         if (allow_split && len > max_nz) {
             for (int64_t a = ptr[r]; a < ptr[r + 1]; a += max_nz)
-                out.push_back(CsrChunk{(uint32_t)r, (uint32_t)(r + 1), a, std::min(a + max_nz, ptr[r + 1])});
+                out.push_back(CsrChunk{(uint32_t)r, (uint32_t)(r + 1), a, std::min(a + max_nz, ptr[r + 1]), 0u});
             ++r;
             continue;
         }
@@ -57,7 +60,7 @@ std::vector<CsrChunk> make_chunks(const std::vector<int64_t>& ptr, int64_t row_l
         while (r1 < row_hi && r1 - r < max_rows && ptr[r1 + 1] - ptr[r] <= max_nz &&
                !(allow_split && ptr[r1 + 1] - ptr[r1] > max_nz))
             ++r1;
-        out.push_back(CsrChunk{(uint32_t)r, (uint32_t)r1, ptr[r], ptr[r1]});
+        out.push_back(CsrChunk{(uint32_t)r, (uint32_t)r1, ptr[r], ptr[r1], r1 == r + 1 ? 1u : 0u});
         r = r1;
     }
     return out;
@@ -1464,7 +1467,7 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
     const int64_t n = S.d.n, m = S.d.ndofs;
     const uint32_t* perm = S.perm_identity ? nullptr : S.perm.p;
     // y -> interleaved, primary-sorted, padded to kp columns
-    gather_interleave_kernel<double><<<(unsigned)((n + 31) / 32), 256, 0, S.stream>>>(ycol, n, k, kp, perm, w.yi.p);
+    gather_interleave_kernel<double><<<xpose_blocks(n, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(ycol, n, k, kp, perm, w.yi.p);
     // b = D'W y (rmatvec_wdt, solver.rs:210-211)
     launch_obs<double, OBS_RHS>(S, kp, S.w64.p, nullptr, w.yi.p, w.b.p, nullptr);
     int nb = 0;
@@ -1564,8 +1567,8 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
     // final demeaned e = y - D x and ||D'W e|| / ||b|| (solver.rs:222-227, 335-339)
     launch_obs<double, OBS_RESID>(S, kp, S.w64.p, w.x.p, w.yi.p, w.r.p, w.e.p);
     launch_dot<double, double>(S, w.r.p, w.r.p, m, kp, w.part.p, nb);
-    scatter_deinterleave_kernel<double><<<(unsigned)((n + 31) / 32), 256, 0, S.stream>>>(w.e.p, n, k, kp, perm, demcol);
-    scatter_deinterleave_kernel<double><<<(unsigned)((m + 31) / 32), 256, 0, S.stream>>>(w.x.p, m, k, kp, nullptr, xcol);
+    scatter_deinterleave_kernel<double><<<xpose_blocks(n, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(w.e.p, n, k, kp, perm, demcol);
+    scatter_deinterleave_kernel<double><<<xpose_blocks(m, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(w.x.p, m, k, kp, nullptr, xcol);
     WB_CUDA(cudaGetLastError());
     S.gpu_launches += 3;
     std::vector<double> ee = host_reduce(S, nb, kp);
@@ -1639,10 +1642,10 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
         return wb::fail(WITHIN_ERR_CUDA, "no CUDA device is available (the solve phase has no CPU path)");
-    if (S->pc.kind != 0) {
-        st = wb::build_subdomains(S->d, S->pc, S->subs);
-        if (!st.ok()) return wb::fail(st.code, st.msg);
-    }
+    // the subdomains and their factors (host) are built while the design goes to the device
+    std::future<wb::Status> subs_job;
+    if (S->pc.kind != 0)
+        subs_job = std::async(std::launch::async, [&S]() { return wb::build_subdomains(S->d, S->pc, S->subs); });
     int dev = 0;
     WB_CUDA(cudaGetDevice(&dev));
     WB_CUDA(cudaDeviceGetAttribute(&S->n_sm, cudaDevAttrMultiProcessorCount, dev));
@@ -1652,6 +1655,10 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
     WB_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
     WB_CUDA(cudaMallocHost(&S->h_active, sizeof(int32_t)));
     wb::upload_design(*S);
+    if (subs_job.valid()) {
+        st = subs_job.get();
+        if (!st.ok()) return wb::fail(st.code, st.msg);
+    }
     if (S->pc.kind != 0 && !S->subs.empty()) {
         std::vector<std::vector<int32_t>> groups;
         if (S->pc.kind == 1) {
@@ -1866,7 +1873,7 @@ static int apply_common(within_solver* s, const double* in, size_t k, double* ou
         iout.alloc(out_rows * kp);
         WB_CUDA(cudaMemcpyAsync(din.p, in, sizeof(double) * in_rows * k, cudaMemcpyHostToDevice, S.stream));
         const uint32_t* perm = S.perm_identity ? nullptr : S.perm.p;
-        wb::gather_interleave_kernel<double><<<(unsigned)((in_rows + 31) / 32), 256, 0, S.stream>>>(
+        wb::gather_interleave_kernel<double><<<wb::xpose_blocks((int64_t)in_rows, S.n_sm), wb::kXposeWarps * 32, wb::xpose_smem(kp), S.stream>>>(
             din.p, (int64_t)in_rows, kk, kp, which == 3 ? perm : nullptr, iin.p);
         if (which == 0 || which == 1) {
             if (!S.mixed()) {
@@ -1895,7 +1902,7 @@ static int apply_common(within_solver* s, const double* in, size_t k, double* ou
         } else {  // D'W r
             wb::launch_obs<double, wb::OBS_RHS>(S, kp, S.w64.p, nullptr, iin.p, iout.p, nullptr);
         }
-        wb::scatter_deinterleave_kernel<double><<<(unsigned)((out_rows + 31) / 32), 256, 0, S.stream>>>(
+        wb::scatter_deinterleave_kernel<double><<<wb::xpose_blocks((int64_t)out_rows, S.n_sm), wb::kXposeWarps * 32, wb::xpose_smem(kp), S.stream>>>(
             iout.p, (int64_t)out_rows, kk, kp, which == 2 ? perm : nullptr, dout.p);
         WB_CUDA(cudaGetLastError());
         WB_CUDA(cudaMemcpyAsync(out, dout.p, sizeof(double) * out_rows * k, cudaMemcpyDeviceToHost, S.stream));
@@ -1947,6 +1954,48 @@ void within_solver_ac_arrays(const within_solver* s, int32_t i, int32_t* level_p
 }
 
 const char* within_last_error(void) { return wb::g_last_error.c_str(); }
+
+int within_solve_many(within_problem* problems, size_t n_problems, const within_params* params,
+                      const within_preconditioner* precond, int32_t concurrency) {
+    if (n_problems == 0) return WITHIN_OK;
+    if (!problems) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "problems is null");
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce != cudaSuccess) return wb::fail(WITHIN_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
+    const size_t nt = std::min<size_t>(n_problems, (size_t)(concurrency > 0 ? concurrency : 8));
+    std::atomic<size_t> next{0};
+    std::vector<std::string> msg(n_problems);
+    // each host thread drives one problem at a time: setup on the host, then the solve on
+    // the solver's own stream (the device is the caller's)
+    auto worker = [&]() {
+        cudaSetDevice(dev);
+        for (;;) {
+            const size_t i = next.fetch_add(1);
+            if (i >= n_problems) break;
+            within_problem& p = problems[i];
+            within_solver* sv = nullptr;
+            int rc = within_solver_new(p.codes, p.n_obs, p.n_factors, p.row_stride, p.col_stride, p.weights, params,
+                                       precond, &sv);
+            if (rc == WITHIN_OK) {
+                rc = within_solver_solve_batch(sv, p.ys, p.k, p.x, p.demeaned, p.stats);
+                if (rc != WITHIN_OK) msg[i] = within_last_error();
+                within_solver_free(sv);
+            } else {
+                msg[i] = within_last_error();
+            }
+            p.status = rc;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& t : pool) t.join();
+    for (size_t i = 0; i < n_problems; ++i)
+        if (problems[i].status != WITHIN_OK)
+            return wb::fail(problems[i].status, "problem " + std::to_string(i) + ": " + msg[i]);
+    wb::g_last_error.clear();
+    return WITHIN_OK;
+}
 
 int64_t within_solver_gpu_launches(const within_solver* s) { return s ? s->impl->gpu_launches : 0; }
 double within_solver_setup_time(const within_solver* s) { return s ? s->impl->setup_time : 0.0; }
@@ -2030,10 +2079,10 @@ extern "C" int within_solver_apply_gramian_noalloc(within_solver* s, const doubl
     S.stream = stream ? (cudaStream_t)stream : saved;
     int status = WITHIN_OK;
     try {  // no std::function wrapper here: nothing on this path allocates
-        wb::gather_interleave_kernel<double><<<(unsigned)((m + 31) / 32), 256, 0, S.stream>>>(d_x, (int64_t)m, kk, kp,
+        wb::gather_interleave_kernel<double><<<wb::xpose_blocks((int64_t)m, S.n_sm), wb::kXposeWarps * 32, wb::xpose_smem(kp), S.stream>>>(d_x, (int64_t)m, kk, kp,
                                                                                              nullptr, xi);
         wb::launch_obs<double, wb::OBS_GRAM>(S, kp, S.w64.p, xi, nullptr, yi, nullptr);
-        wb::scatter_deinterleave_kernel<double><<<(unsigned)((m + 31) / 32), 256, 0, S.stream>>>(yi, (int64_t)m, kk, kp,
+        wb::scatter_deinterleave_kernel<double><<<wb::xpose_blocks((int64_t)m, S.n_sm), wb::kXposeWarps * 32, wb::xpose_smem(kp), S.stream>>>(yi, (int64_t)m, kk, kp,
                                                                                                 nullptr, d_y);
         WB_CUDA(cudaGetLastError());
         S.gpu_launches += 2;

@@ -90,3 +90,20 @@ def config3(seed: int = 0, scale: float = 1.0):
     W = max(int(500_000 * scale), 10)
     F = max(int(100_000 * scale), 5)
     return akm_panel(W, F, 20, 20, 0.1, 15, True, seed)
+
+
+def config4(seed: int = 0, n_problems: int = 256, max_obs: int = 1_000_000):
+    """Uneven batch: n_problems independent designs, n_obs log-uniform on [1e3, max_obs],
+    2-4 factors with level counts log-uniform on [n/50, n/5] and uniform codes, 1-8
+    N(0,1) right-hand sides each.  Returns a list of (categories, Y)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_problems):
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(max_obs))))
+        q = int(rng.integers(2, 5))
+        lv = [max(2, int(np.exp(rng.uniform(np.log(n / 50), np.log(n / 5))))) for _ in range(q)]
+        cats = uniform_design(n, lv, seed=int(rng.integers(0, 2**31)))
+        k = int(rng.integers(1, 9))
+        Y = np.asfortranarray(rng.standard_normal((n, k)))
+        out.append((cats, Y))
+    return out
