@@ -174,12 +174,12 @@ def uneven(args):
     n_obs = sum(c.shape[0] for c, _ in probs)
     cfg = wb.CG(precision=args.precision)
     for _ in range(max(1, args.warmup)):
-        wb.solve_many(probs, cfg, concurrency=8)
+        wb.solve_many(probs, cfg)
     clocks = Clocks(0)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        res = wb.solve_many(probs, cfg, concurrency=8)
+        res = wb.solve_many(probs, cfg)
     torch.cuda.synchronize()
     el = time.perf_counter() - t0
     clk = clocks.stop()
@@ -194,7 +194,8 @@ def uneven(args):
             "config": {"workload": f"{len(probs)} independent problems, n_obs log-uniform on [1e3, 1e6] "
                                    f"(total {n_obs}), 2-4 factors with levels log-uniform on [n/50, n/5], "
                                    f"1-8 RHS each (total {n_rhs}), CG + additive Schwarz, tol 1e-8, "
-                                   "8 problems in flight", "timing": "host wall clock, device synchronised"},
+                                   f"{os.cpu_count()} problems in flight (one per host core)",
+                       "timing": "host wall clock, device synchronised"},
             "clocks": clk, "accuracy": {"converged": conv, "max_final_residual": worst}}
     print(json.dumps(line), flush=True)
 

@@ -153,7 +153,7 @@ typedef struct {
 } within_problem;
 
 /* Many independent problems of uneven size (orchestrate::solve_batch applied to each),
- * solved concurrently: up to `concurrency` problems (<= 0: 8) are in flight at once,
+ * solved concurrently: up to `concurrency` problems (<= 0: one per host core) are in flight at once,
  * each with its own solver and CUDA stream, so the kernels of small problems share the
  * GPU.  Every problem is attempted; the return value is WITHIN_OK or the code of the
  * first failed problem (its message in within_last_error), and each status says which.

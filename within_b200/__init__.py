@@ -399,12 +399,13 @@ def solve(categories, y, config=None, weights=None, preconditioner=None) -> Solv
     return r
 
 
-def solve_many(problems, config=None, preconditioner=None, concurrency: int = 8) -> list:
+def solve_many(problems, config=None, preconditioner=None, concurrency: int = 0) -> list:
     """Many independent problems of uneven size, each like ``solve_batch``.
 
     ``problems`` is a sequence of ``(categories, Y)`` or ``(categories, Y, weights)``
     with Y of shape (n_obs, k) (or (n_obs,) for one RHS).  Up to ``concurrency``
-    problems are solved at once, each with its own solver and CUDA stream, so that
+    problems (0: one per host core) are solved at once, each with its own solver and
+    CUDA stream, so that
     small problems share the GPU.  Returns one BatchSolveResult per problem; raises
     WithinError naming the first problem that failed.
     """

@@ -389,6 +389,35 @@ SymCsr schur_approx(const Elim& e, uint64_t seed, uint32_t split) {
 // ---------------------------------------------------------------------------
 
 // Sort neighbour records by column (stable) and merge duplicates, dropping dead ones.
+// compact_adj for a list whose first `sorted` entries are already sorted by column and
+// merged (the last compaction's output) and whose tail holds entries appended since:
+// the tail is sorted and merged into the prefix stably, which orders the entries exactly
+// as a stable sort of the whole list would.  Returns the list's new length (all sorted).
+size_t compact_adj_tail(std::vector<Nbr>& l, size_t sorted, const std::vector<uint8_t>& dead,
+                        std::vector<Nbr>& scratch) {
+    size_t m = 0, mp = 0;
+    for (size_t a = 0; a < l.size(); ++a) {
+        if (dead[l[a].col]) continue;
+        if (a < sorted) ++mp;
+        l[m++] = l[a];
+    }
+    l.resize(m);
+    auto by_col = [](const Nbr& a, const Nbr& b) { return a.col < b.col; };
+    if (mp < m) {
+        std::stable_sort(l.begin() + (ptrdiff_t)mp, l.end(), by_col);
+        scratch.resize(m);
+        std::merge(l.begin(), l.begin() + (ptrdiff_t)mp, l.begin() + (ptrdiff_t)mp, l.end(), scratch.begin(), by_col);
+        std::copy(scratch.begin(), scratch.begin() + (ptrdiff_t)m, l.begin());
+    }
+    size_t w = 0;
+    for (size_t a = 0; a < m; ++a) {
+        if (w > 0 && l[w - 1].col == l[a].col) l[w - 1].w += l[a].w;
+        else l[w++] = l[a];
+    }
+    l.resize(w);
+    return w;
+}
+
 void compact_adj(std::vector<Nbr>& l, const std::vector<uint8_t>& dead) {
     size_t m = 0;
     for (size_t a = 0; a < l.size(); ++a)
@@ -511,14 +540,17 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
     // edges arrive), so only those "dirty" lists are compacted in the next round; a clean
     // list is already sorted and merged, where compacting it again would change nothing.
     std::vector<uint8_t> dirty((size_t)n, 1);
+    std::vector<size_t> sorted_len((size_t)n, 0);  // leading entries already sorted and merged
     std::vector<uint64_t> vhash((size_t)n);
     for (int32_t v = 0; v < n; ++v) vhash[v] = hash64(seed ^ ((uint64_t)v * 0xD1B54A32D192ED03ULL));
+    std::vector<int32_t> live((size_t)n);  // live vertices, ascending
+    std::iota(live.begin(), live.end(), 0);
+    std::vector<Nbr> scratch;
     while (remaining > kAcCoreMax) {
         rank.clear();
-        for (int32_t v = 0; v < n; ++v) {
-            if (dead[v]) continue;
+        for (int32_t v : live) {
             if (dirty[v]) {
-                compact_adj(g[v], dead);
+                sorted_len[v] = compact_adj_tail(g[v], sorted_len[v], dead, scratch);
                 dirty[v] = 0;
             }
             rank.push_back(Rank{(int32_t)g[v].size(), vhash[v], v});
@@ -565,6 +597,7 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
         for (int32_t v : picked)
             for (const Nbr& x : g[v]) dirty[x.col] = 1;
         for (int32_t v : picked) { dead[v] = 1; std::vector<Nbr>().swap(g[v]); }
+        live.erase(std::remove_if(live.begin(), live.end(), [&](int32_t v) { return dead[v] != 0; }), live.end());
         for (const Rank& rk : rank) blocked[rk.v] = 0;
         remaining -= (int32_t)picked.size();
         f.nlev++;

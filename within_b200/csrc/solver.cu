@@ -1962,7 +1962,8 @@ int within_solve_many(within_problem* problems, size_t n_problems, const within_
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess) return wb::fail(WITHIN_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(ce));
-    const size_t nt = std::min<size_t>(n_problems, (size_t)(concurrency > 0 ? concurrency : 8));
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::min<size_t>(n_problems, concurrency > 0 ? (size_t)concurrency : hw);
     std::atomic<size_t> next{0};
     std::vector<std::string> msg(n_problems);
     // each host thread drives one problem at a time: setup on the host, then the solve on
