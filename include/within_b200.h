@@ -77,7 +77,8 @@ typedef struct {
     uint64_t approx_schur_seed;
     uint32_t approx_schur_split;
     int32_t dense_threshold;
-    int32_t reduction_strategy;    /* accepted for API parity; the device path has one reduction */
+    int32_t reduction_strategy;    /* ReductionStrategy: 0 Auto, 1 AtomicScatter, 2 ParallelReduction
+                                      (reported by the diagnostics; the device path has one reduction) */
 } within_preconditioner;
 
 typedef struct {
@@ -179,6 +180,31 @@ int32_t within_solver_n_subdomains(const within_solver *solver);
 void within_solver_subdomain_info(const within_solver *solver, int32_t i, int64_t *info);
 void within_solver_subdomain_indices(const within_solver *solver, int32_t i, uint32_t *gidx,
                                      double *pou);
+/* FePreconditioner::subdomain_inner_parallel_work (within/src/operator/preconditioner.rs:64-79):
+ * per subdomain, the work estimate of local_solver.rs:348-356 (2 nnz(C) + n_local when
+ * the larger side has more than 10,000 rows, else 0).  work has n_subdomains entries. */
+void within_solver_subdomain_inner_work(const within_solver *solver, int64_t *work);
+
+/* AdditiveSchwarzDiagnostics (schwarz-precond/src/schwarz/additive/planning.rs:141-210;
+ * within-py/src/lib.rs:200-260).  Strategies: 0 Auto, 1 AtomicScatter, 2
+ * ParallelReduction.  `resolved_reduction_strategy` is the reference CPU scheduler's
+ * choice for `threads` worker threads (planning.rs:71-135; <= 0: one per host core); the
+ * device executor always adds subdomain results with atomics. */
+typedef struct {
+    int32_t reduction_strategy;
+    int32_t resolved_reduction_strategy;
+    int64_t n_subdomains;
+    int64_t n_dofs;
+    int64_t total_inner_parallel_work;
+    int64_t max_inner_parallel_work;
+    int64_t total_scatter_dofs;
+    double outer_parallel_capacity;
+    double scatter_overlap;
+} within_additive_diagnostics;
+/* WITHIN_ERR_INVALID_ARGUMENT unless the solver was built with additive Schwarz
+ * (the reference returns None then: preconditioner.rs:98-106). */
+int within_solver_additive_diagnostics(const within_solver *solver, int32_t threads,
+                                       within_additive_diagnostics *out);
 /* AC factor of subdomain i: sizes[5] = n, n_levels, nnz, n_columns, n_core (zeros for
  * dense subdomains).  Arrays: level_ptr (n_levels+1), col_vertex/col_diag (n_columns),
  * col_ptr (n_columns+1), col_idx/col_coef (nnz), core_vertex (n_core),

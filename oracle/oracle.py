@@ -212,6 +212,72 @@ class OracleSolver:
             out.append(d)
         return out
 
+    def subdomain_inner_parallel_work(self):
+        """FePreconditioner::subdomain_inner_parallel_work (within/src/operator/preconditioner.rs:64-79)."""
+        L = lib()
+        out = []
+        for i in range(L.oracle_n_subdomains(self._h)):
+            info = np.zeros(8, np.int64)
+            L.oracle_subdomain_info(self._h, i, info)
+            out.append(inner_parallel_work(int(info[3]), int(info[4]), int(L.oracle_crosstab_nnz(self._h, i))))
+        return out
+
+    def additive_diagnostics(self, configured=0, threads=1):
+        """AdditiveSchwarzDiagnostics of this build (see ``additive_diagnostics``)."""
+        L = lib()
+        scatter = []
+        for i in range(L.oracle_n_subdomains(self._h)):
+            info = np.zeros(8, np.int64)
+            L.oracle_subdomain_info(self._h, i, info)
+            scatter.append(int(info[2]))
+        return additive_diagnostics(self.subdomain_inner_parallel_work(), scatter, self.n_dofs, configured, threads)
+
+
+# Subdomains go inner-parallel only above both thresholds (PAR_BACKSUB_THRESHOLD,
+# within/src/operator/local_solver.rs:78; PAR_SPMV_THRESHOLD, operator/csr_block.rs:4).
+PAR_THRESHOLD = 10_000
+# AdditiveScheduler constants (schwarz-precond/src/schwarz/additive/planning.rs:213-218).
+MIN_INNER_PARALLEL_WORK = 200_000
+OUTER_CAPACITY_TARGET = 0.75
+AUTO_REDUCTION_SWEEP_FACTOR = 1.1
+AUTO_INNER_REDUCTION_SWEEP_FACTOR = 6.0
+AUTO_OVERLAP_FOR_REDUCTION = 4.0
+
+
+def inner_parallel_work(n_q, n_r, cross_nnz):
+    """BlockElimSolver::estimated_inner_parallel_work (local_solver.rs:348-356)."""
+    if max(n_q, n_r) <= PAR_THRESHOLD:
+        return 0
+    return 2 * cross_nnz + n_q + n_r
+
+
+def additive_diagnostics(work, scatter, n_dofs, configured=0, threads=1):
+    """AdditiveSchwarzDiagnostics::from_entries and its accessors (planning.rs:151-210),
+    and the strategy AdditiveScheduler::reduction_plan resolves (planning.rs:71-135).
+    work: per-subdomain inner work; scatter: per-subdomain local sizes.  Strategies:
+    0 Auto, 1 AtomicScatter, 2 ParallelReduction."""
+    total, mx, tsc = sum(work), max(work, default=0), sum(scatter)
+    cap = 0.0 if mx == 0 else total / mx
+    overlap = tsc / max(n_dofs, 1)
+    threads = max(threads, 1)
+    inner = mx >= MIN_INNER_PARALLEL_WORK and cap < threads * OUTER_CAPACITY_TARGET
+    if configured in (1, 2):
+        resolved = configured
+    else:
+        active = max(min(threads, len(work)), 1)
+        ratio = (active * n_dofs) / max(tsc, 1)
+        if ratio <= AUTO_REDUCTION_SWEEP_FACTOR:
+            resolved = 2
+        elif inner and ratio <= AUTO_INNER_REDUCTION_SWEEP_FACTOR:
+            resolved = 2
+        elif overlap >= AUTO_OVERLAP_FOR_REDUCTION:
+            resolved = 2
+        else:
+            resolved = 1
+    return dict(reduction_strategy=configured, resolved_reduction_strategy=resolved, n_subdomains=len(work),
+                n_dofs=n_dofs, total_inner_parallel_work=total, max_inner_parallel_work=mx,
+                total_scatter_dofs=tsc, outer_parallel_capacity=cap, scatter_overlap=overlap)
+
 
 def csr_transpose(nrows, ncols, indptr, indices, data):
     indptr = np.ascontiguousarray(indptr, np.uint32); indices = np.ascontiguousarray(indices, np.uint32)

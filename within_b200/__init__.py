@@ -26,7 +26,7 @@ from . import _lib
 __all__ = [
     "OperatorRepr", "Preconditioner", "ReductionStrategy", "CG", "GMRES", "ApproxCholConfig",
     "ApproxSchurConfig", "SchurComplement", "AdditiveSchwarz", "MultiplicativeSchwarz", "SolveResult",
-    "BatchSolveResult", "FePreconditioner", "Solver", "solve", "solve_batch", "solve_many", "WithinError",
+    "BatchSolveResult", "AdditiveSchwarzDiagnostics", "FePreconditioner", "Solver", "solve", "solve_batch", "solve_many", "WithinError",
 ]
 
 
@@ -235,6 +235,35 @@ class BatchSolveResult:
         return f"BatchSolveResult(n_rhs={len(self.converged)}, converged={self.converged})"
 
 
+class AdditiveSchwarzDiagnostics:
+    """Build-time scheduling metrics of an additive Schwarz preconditioner
+    (within-py PyAdditiveSchwarzDiagnostics, lib.rs:200-260; planning.rs:141-210).
+
+    ``resolved_reduction_strategy`` is what the reference's CPU scheduler would pick for
+    this build with one worker thread per host core (planning.rs:71-135).  The device
+    executor has a single reduction (atomic adds of the subdomain results), whichever
+    strategy is configured.
+    """
+
+    def __init__(self, d: "_lib.AdditiveDiagnostics"):
+        self.reduction_strategy = ReductionStrategy(d.reduction_strategy)
+        self.resolved_reduction_strategy = ReductionStrategy(d.resolved_reduction_strategy)
+        self.total_inner_parallel_work = int(d.total_inner_parallel_work)
+        self.max_inner_parallel_work = int(d.max_inner_parallel_work)
+        self.total_scatter_dofs = int(d.total_scatter_dofs)
+        self.outer_parallel_capacity = float(d.outer_parallel_capacity)
+        self.scatter_overlap = float(d.scatter_overlap)
+
+    def __repr__(self):
+        return (f"AdditiveSchwarzDiagnostics(reduction_strategy={self.reduction_strategy.name}, "
+                f"resolved_reduction_strategy={self.resolved_reduction_strategy.name}, "
+                f"total_inner_parallel_work={self.total_inner_parallel_work}, "
+                f"max_inner_parallel_work={self.max_inner_parallel_work}, "
+                f"total_scatter_dofs={self.total_scatter_dofs}, "
+                f"outer_parallel_capacity={self.outer_parallel_capacity:.3f}, "
+                f"scatter_overlap={self.scatter_overlap:.3f})")
+
+
 class FePreconditioner:
     """Handle of a built preconditioner (within-py PyFePreconditioner, lib.rs:825-914).
 
@@ -261,6 +290,21 @@ class FePreconditioner:
     @property
     def n_subdomains(self) -> int:
         return int(_lib.load().within_solver_n_subdomains(self._solver._h))
+
+    @property
+    def subdomain_inner_parallel_work(self) -> list[int]:
+        """Per-subdomain inner parallel work estimate (preconditioner.rs:64-79)."""
+        work = np.zeros(self.n_subdomains, np.int64)
+        _lib.load().within_solver_subdomain_inner_work(self._solver._h, work)
+        return [int(v) for v in work]
+
+    def additive_schwarz_diagnostics(self) -> AdditiveSchwarzDiagnostics | None:
+        """Diagnostics if this is an additive preconditioner, else None (preconditioner.rs:98-106)."""
+        if self._cfg.kind != 1:
+            return None
+        d = _lib.AdditiveDiagnostics()
+        _check(_lib.load().within_solver_additive_diagnostics(self._solver._h, 0, C.byref(d)))
+        return AdditiveSchwarzDiagnostics(d)
 
     def __repr__(self):
         kind = {1: "Additive", 2: "Multiplicative"}.get(self._cfg.kind, "Off")

@@ -47,6 +47,13 @@ class Problem(C.Structure):
                 ("stats", C.c_void_p), ("status", C.c_int32)]
 
 
+class AdditiveDiagnostics(C.Structure):
+    _fields_ = [("reduction_strategy", C.c_int32), ("resolved_reduction_strategy", C.c_int32),
+                ("n_subdomains", C.c_int64), ("n_dofs", C.c_int64), ("total_inner_parallel_work", C.c_int64),
+                ("max_inner_parallel_work", C.c_int64), ("total_scatter_dofs", C.c_int64),
+                ("outer_parallel_capacity", C.c_double), ("scatter_overlap", C.c_double)]
+
+
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -62,7 +69,7 @@ EXPORTED = [
     "within_solver_subdomain_info", "within_solver_subdomain_indices", "within_solver_ac_sizes",
     "within_solver_ac_arrays", "within_solver_gpu_launches", "within_solver_setup_time", "within_last_error",
     "within_solver_set_profiling", "within_solver_kernel_time", "within_solver_apply_gramian_noalloc",
-    "within_solve_many",
+    "within_solve_many", "within_solver_subdomain_inner_work", "within_solver_additive_diagnostics",
 ]
 
 _lib = None
@@ -105,6 +112,9 @@ def load():
     L.within_solver_n_subdomains.restype = C.c_int32
     L.within_solver_subdomain_info.argtypes = [vp, C.c_int32, _i64p]
     L.within_solver_subdomain_indices.argtypes = [vp, C.c_int32, _u32p, _f64p]
+    L.within_solver_subdomain_inner_work.argtypes = [vp, _i64p]
+    L.within_solver_additive_diagnostics.argtypes = [vp, C.c_int32, C.POINTER(AdditiveDiagnostics)]
+    L.within_solver_additive_diagnostics.restype = C.c_int
     L.within_solver_ac_sizes.argtypes = [vp, C.c_int32, _i64p]
     L.within_solver_ac_arrays.argtypes = [vp, C.c_int32, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p, _i32p, _f64p]
     L.within_solver_gpu_launches.argtypes = [vp]

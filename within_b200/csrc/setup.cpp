@@ -836,4 +836,47 @@ void build_explicit_gramian(const Design& d, std::vector<int64_t>& ptr, std::vec
     }
 }
 
+// A subdomain's local solve goes inner-parallel in the reference only when its larger
+// side has more rows than both parallel thresholds (PAR_BACKSUB_THRESHOLD,
+// local_solver.rs:78, and PAR_SPMV_THRESHOLD, csr_block.rs:4: 10,000 each); its work is
+// then two passes over the cross block plus the local vector.
+int64_t inner_parallel_work(const Subdomain& sd) {
+    constexpr int32_t kParThreshold = 10000;
+    if (std::max(sd.n_q(), sd.n_r()) <= kParThreshold) return 0;
+    return 2 * sd.ct.c.nnz() + sd.n_local();
+}
+
+AdditiveDiagnostics additive_diagnostics(const std::vector<Subdomain>& subs, int64_t n_dofs, int32_t configured,
+                                         int64_t threads) {
+    // AdditiveScheduler constants (planning.rs:213-218)
+    constexpr int64_t kMinInnerWork = 200000;
+    constexpr double kOuterCapacityTarget = 0.75, kSweepFactor = 1.1, kInnerSweepFactor = 6.0, kOverlap = 4.0;
+    AdditiveDiagnostics g;
+    g.configured = configured;
+    g.n_subdomains = (int64_t)subs.size();
+    g.n_dofs = n_dofs;
+    for (const Subdomain& sd : subs) {  // from_entries (planning.rs:151-172)
+        const int64_t w = inner_parallel_work(sd);
+        g.total_inner_work += w;
+        g.max_inner_work = std::max(g.max_inner_work, w);
+        g.total_scatter_dofs += (int64_t)sd.gidx.size();
+    }
+    g.outer_parallel_capacity = g.max_inner_work == 0 ? 0.0 : (double)g.total_inner_work / (double)g.max_inner_work;
+    g.scatter_overlap = (double)g.total_scatter_dofs / (double)std::max<int64_t>(n_dofs, 1);
+    threads = std::max<int64_t>(threads, 1);
+    // allow_inner_parallelism (planning.rs:84-90)
+    const bool inner = g.max_inner_work >= kMinInnerWork && g.outer_parallel_capacity < (double)threads * kOuterCapacityTarget;
+    if (configured == 1 || configured == 2) {
+        g.resolved = configured;
+    } else {  // pick_auto_strategy, reduction_sweep_to_scatter (planning.rs:105-135)
+        const int64_t active = std::max<int64_t>(std::min<int64_t>(threads, g.n_subdomains), 1);
+        const double ratio = (double)(active * n_dofs) / (double)std::max<int64_t>(g.total_scatter_dofs, 1);
+        if (ratio <= kSweepFactor || (inner && ratio <= kInnerSweepFactor) || g.scatter_overlap >= kOverlap)
+            g.resolved = 2;
+        else
+            g.resolved = 1;
+    }
+    return g;
+}
+
 }  // namespace wb

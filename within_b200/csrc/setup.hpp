@@ -105,4 +105,20 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
 void build_explicit_gramian(const Design& d, std::vector<int64_t>& ptr, std::vector<uint32_t>& idx,
                             std::vector<double>& val);
 
+// LocalSolver::inner_parallelism_work_estimate of a block-elimination subdomain
+// (within/src/operator/local_solver.rs:348-356).
+int64_t inner_parallel_work(const Subdomain& sd);
+
+// AdditiveSchwarzDiagnostics (schwarz-precond/src/schwarz/additive/planning.rs:141-210) and
+// the strategy its scheduler resolves for `threads` worker threads (planning.rs:71-135).
+// Strategies: 0 Auto, 1 AtomicScatter, 2 ParallelReduction.
+struct AdditiveDiagnostics {
+    int32_t configured = 0, resolved = 0;
+    int64_t n_subdomains = 0, n_dofs = 0;
+    int64_t total_inner_work = 0, max_inner_work = 0, total_scatter_dofs = 0;
+    double outer_parallel_capacity = 0.0, scatter_overlap = 0.0;
+};
+AdditiveDiagnostics additive_diagnostics(const std::vector<Subdomain>& subs, int64_t n_dofs, int32_t configured,
+                                         int64_t threads);
+
 }  // namespace wb

@@ -326,6 +326,7 @@ struct SolverImpl {
     std::mutex mu;
     Design d;
     PrecondConfig pc;
+    int32_t reduction_strategy = 0;  // as configured (AdditiveSchwarz reduction)
     within_params params{};
     std::vector<Subdomain> subs;
     int primary = 0;
@@ -1638,6 +1639,9 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
         S->pc.schur_seed = precond->approx_schur_seed;
         S->pc.schur_split = precond->approx_schur_split < 1 ? 1 : precond->approx_schur_split;
         S->pc.dense_threshold = precond->dense_threshold;
+        if (precond->reduction_strategy < 0 || precond->reduction_strategy > 2)
+            return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "reduction strategy must be 0 (Auto), 1 (AtomicScatter) or 2 (ParallelReduction)");
+        S->reduction_strategy = precond->reduction_strategy;
     }
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
@@ -1926,6 +1930,28 @@ void within_solver_subdomain_info(const within_solver* s, int32_t i, int64_t* in
     const wb::Subdomain& sd = s->impl->subs[i];
     info[0] = sd.q; info[1] = sd.r; info[2] = sd.n_local(); info[3] = sd.n_q(); info[4] = sd.n_r();
     info[5] = sd.elim_q; info[6] = sd.kind; info[7] = sd.n_red;
+}
+void within_solver_subdomain_inner_work(const within_solver* s, int64_t* work) {
+    const auto& subs = s->impl->subs;
+    for (size_t i = 0; i < subs.size(); ++i) work[i] = wb::inner_parallel_work(subs[i]);
+}
+int within_solver_additive_diagnostics(const within_solver* s, int32_t threads, within_additive_diagnostics* out) {
+    if (!s || !out) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "solver and out must not be null");
+    const SolverImpl& S = *s->impl;
+    if (S.pc.kind != 1) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the solver has no additive Schwarz preconditioner");
+    const int64_t t = threads > 0 ? threads : (int64_t)std::max(1u, std::thread::hardware_concurrency());
+    const wb::AdditiveDiagnostics g = wb::additive_diagnostics(S.subs, S.d.ndofs, S.reduction_strategy, t);
+    out->reduction_strategy = g.configured;
+    out->resolved_reduction_strategy = g.resolved;
+    out->n_subdomains = g.n_subdomains;
+    out->n_dofs = g.n_dofs;
+    out->total_inner_parallel_work = g.total_inner_work;
+    out->max_inner_parallel_work = g.max_inner_work;
+    out->total_scatter_dofs = g.total_scatter_dofs;
+    out->outer_parallel_capacity = g.outer_parallel_capacity;
+    out->scatter_overlap = g.scatter_overlap;
+    wb::g_last_error.clear();
+    return WITHIN_OK;
 }
 void within_solver_subdomain_indices(const within_solver* s, int32_t i, uint32_t* gidx, double* pou) {
     const wb::Subdomain& sd = s->impl->subs[i];
