@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="problem scale (1.0 = 10M observations)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--operator", default="implicit", choices=["implicit", "explicit"],
+                    help="Krylov operator: the observation pass (default) or the assembled Gramian (CSR)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-dropin", action="store_true", help="skip the FP64 drop-in comparison run")
     ap.add_argument("--workload", default="panel", choices=["panel", "uneven"],
@@ -69,29 +71,89 @@ def workload(scale):
     return cats, np.asfortranarray(Y), w
 
 
-def config_dict(cats, k, scale, precision):
+def config_dict(cats, k, scale, precision, operator="implicit"):
     return {"workload": "weighted 3-FE worker-firm-year panel (10M obs: 500k workers x 20 years, 100k Zipf(1.1) "
                         "firms, p_switch 0.1, lognormal weights), 16 RHS, CG + additive Schwarz, tol 1e-8"
             if scale == 1.0 else f"weighted 3-FE panel at scale {scale}",
             "n_obs": int(cats.shape[0]), "n_factors": int(cats.shape[1]), "n_rhs": int(k),
-            "precision": precision, "l2": "inputs larger than L2 (Y is n_obs x 16 FP64 = 1.28 GB)"}
+            "precision": precision, "operator": operator,
+            "l2": "inputs larger than L2 (Y is n_obs x 16 FP64 = 1.28 GB)"}
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clocks, power and clock-event reasons sampled during the timed region.
+
+    NVML is read from a thread every 10 ms, with one sample when sampling starts and one
+    when it stops, so short timed regions still carry several samples; the device is
+    found by the UUID torch reports for cuda:`index` (CUDA_VISIBLE_DEVICES-safe).  Only
+    reads: no setting of the GPU is changed.  Without NVML, nvidia-smi is sampled instead.
+    """
+
+    # nvmlClocksEventReasons bits
+    _BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index):
+        import threading
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.p = self.nv = None
+        try:
+            import pynvml as nv
+            import torch
+            nv.nvmlInit()
+            try:
+                uuid = str(torch.cuda.get_device_properties(index).uuid)
+                h = nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(index)
+            self.nv, self.h = nv, h
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._sample()
+            self.done = threading.Event()
+            self.t = threading.Thread(target=self._loop, daemon=True)
+            self.t.start()
+        except Exception:
+            self.nv = None
+            self._smi(index)
+
+    def _sample(self):
+        nv, h = self.nv, self.h
+        self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+        try:
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        for name, bit in self._BITS.items():
+            if bits & bit:
+                self.reasons.add(name)
+
+    def _loop(self):
+        while not self.done.wait(0.01):
+            try:
+                self._sample()
+            except Exception:
+                return
+
+    def _smi(self, index):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
 
     def stop(self):
+        if self.nv is not None:
+            self.done.set()
+            self.t.join()
+            try:
+                self._sample()
+            except Exception:
+                pass
+            return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml, 10 ms"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -114,7 +176,7 @@ class Clocks:
                     reasons.add(nm)
         os.unlink(self.f.name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def cpu_baseline_run(cats, Y, w, n_rhs, threads):
@@ -218,7 +280,8 @@ def ours(args):
     cats, Y, w = workload(args.scale)
     n, k = Y.shape
     t0 = time.perf_counter()
-    solver = wb.Solver(cats, wb.CG(precision=args.precision), weights=w)
+    op = wb.OperatorRepr.Explicit if args.operator == "explicit" else wb.OperatorRepr.Implicit
+    solver = wb.Solver(cats, wb.CG(precision=args.precision, operator=op), weights=w)
     setup_s = time.perf_counter() - t0
     m = solver.n_dofs
     dY = torch.from_numpy(np.ascontiguousarray(Y.T)).cuda()       # (k, n) = RHS-major
@@ -311,9 +374,21 @@ def ours(args):
                 "algorithmic_bytes_per_launch": op_bytes, "launches": cnt,
                 "avg_launch_us": 1000.0 * ms / cnt if cnt else None, "traffic": None,
                 "schwarz_apply_avg_us": 1000.0 * kt[which + 2][1] / kt[which + 2][0] if kt[which + 2][0] else None}
+    if args.operator == "explicit":
+        # CSR SpMV of G: row pointers, column indices and values once, x read and y
+        # written once (nnz(G) = m + 2 x distinct level pairs of every factor pair)
+        nnz = m
+        for a in range(Q):
+            for b in range(a + 1, Q):
+                nnz += 2 * int(np.unique(cats[:, a].astype(np.int64) * (int(cats[:, b].max()) + 1) + cats[:, b]).size)
+        op_bytes = (m + 1) * 8 + nnz * (4 + s_b) + 2 * s_b * m * k
+        achieved = op_bytes / (ms / cnt / 1000.0) / 1e9 if cnt else None
+        roofline.update({"kernel": "csr_rows_kernel (explicit Gramian SpMV, %s)" % ("FP32" if which else "FP64"),
+                         "achieved": achieved, "frac": (achieved / peak) if achieved else None,
+                         "algorithmic_bytes_per_launch": op_bytes, "gramian_nnz": nnz})
     # DRAM bytes (dram__bytes_read.sum + write.sum) of one FP32 operator apply, from an ncu
     # capture of the same panel at half size (5M observations), scaled by the observations
-    if which == 1 and abs(args.scale - 1.0) < 1e-9:
+    if which == 1 and abs(args.scale - 1.0) < 1e-9 and args.operator == "implicit":
         roofline["traffic"] = int(2 * 111.6e6)
         roofline["traffic_source"] = "ncu dram__bytes_read+write at 5M observations, x2 (scales with n)"
 
@@ -322,7 +397,7 @@ def ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 inner / f64 refinement" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded generator with the reference benchmark's AKM shapes)",
-            "config": config_dict(cats, k, args.scale, args.precision),
+            "config": config_dict(cats, k, args.scale, args.precision, args.operator),
             "e2e": {"value": e2e_value, "unit": "RHS/s", "h2d_bytes_per_step": int(n * k * 8),
                     "d2h_bytes_per_step": int((m + n) * k * 8)},
             "gpu_launches": int(launches), "roofline": roofline, "clocks": clk,

@@ -355,6 +355,13 @@ struct SolverImpl {
     DArr<uint32_t> g_idx;
     DArr<double> g_val64;
     DArr<float> g_val32;
+    // The Krylov operator is the explicit G above (OperatorRepr::Explicit, or a
+    // multiplicative preconditioner, whose residual updates need G anyway): its rows in
+    // chunks for csr_rows_kernel (one warp per row, long rows in pieces).
+    bool explicit_op = false;
+    DArr<uint32_t> g_rows;
+    DArr<CsrChunk> g_chunks;
+    int64_t g_nchunks = 0;
     Workspace ws;
     DArr<double> host_y, host_x, host_dem;  // device side of the host-buffer entry points
     std::shared_ptr<void> gmres;  // GmresBufs, created on first GMRES solve
@@ -719,6 +726,25 @@ void launch_csr(SolverImpl& S, CsrDev<T>& c, int64_t ch0, int64_t ch1, const T* 
     S.gpu_launches++;
 }
 
+// y = G x for the Krylov methods and the refinement residual.  Implicit: one pass over
+// the observations.  Explicit (solver.rs:103-121, 350-360: when the solver holds the
+// assembled Gramian): y = 0, then the CSR rows of G, one warp per row, the pieces of
+// long rows added atomically.
+template <typename T>
+void launch_gram(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
+    if (!S.explicit_op) {
+        launch_obs<T, OBS_GRAM>(S, kp, w, x, nullptr, y, nullptr);
+        return;
+    }
+    WB_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * (size_t)S.d.ndofs * kp, S.stream));
+    const int G = group_for(kp);
+    const int grid = S.nblk(S.g_nchunks, 32);  // one warp per chunk
+    WB_DISPATCH_G(G, csr_rows_kernel<T, GV, EPI_ACC><<<grid, kBlock, 0, S.stream>>>(
+                         S.g_chunks.p, S.g_nchunks, S.g_rows.p, S.g_ptr.p, S.g_idx.p, gram_val<T>(S), nullptr, x, y, kp));
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches++;
+}
+
 // All levels of one AC sweep direction of a stage as one cooperative launch (grid
 // barriers between levels), when the device supports it; otherwise one launch per level.
 template <typename T, int EPI>
@@ -1058,7 +1084,7 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
     auto body = [&]() {
         cudaEvent_t e0 = nullptr;
         S.prof_begin(e0);
-        launch_obs<T, OBS_GRAM>(S, kp, w_t, p, nullptr, ap, nullptr);
+        launch_gram<T>(S, kp, w_t, p, ap);
         S.prof_end(kind, e0);
         launch_dot<T, T>(S, p, ap, m, kp, part, nb);
         launch_reduce(S, part, nb, kp, red);
@@ -1381,7 +1407,7 @@ void gmres_device(SolverImpl& S, GmresBufs& B, int kp, const double* rhs, double
     const int kind = std::is_same<T, double>::value ? 0 : 1;
     for (int cycle = 0; cycle < maxiter + 2; ++cycle) {
         // r = rhs - A x (FP64), beta, v_0 = r / beta
-        launch_obs<double, OBS_GRAM>(S, kp, S.w64.p, x, nullptr, B.w64.p, nullptr);
+        launch_gram<double>(S, kp, S.w64.p, x, B.w64.p);
         sub_kernel<<<gridv, kBlock, 0, S.stream>>>(rhs, B.w64.p, B.r64.p, (int64_t)mk);
         launch_dot<double, double>(S, B.r64.p, B.r64.p, m, kp, part, nb);
         launch_reduce(S, part, nb, kp, red);
@@ -1407,7 +1433,7 @@ void gmres_device(SolverImpl& S, GmresBufs& B, int kp, const double* rhs, double
             S.prof_end(kind + 2, e1);
             cudaEvent_t e0 = nullptr;
             S.prof_begin(e0);
-            launch_obs<T, OBS_GRAM>(S, kp, w_t, zj, nullptr, wv, nullptr);
+            launch_gram<T>(S, kp, w_t, zj, wv);
             S.prof_end(kind, e0);
             for (int i = 0; i <= j; ++i) {
                 const T* vi = V + (size_t)i * mk;
@@ -1534,7 +1560,7 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
         if (!first_mixed) {  // r = b - G x in FP64
             cudaEvent_t e0 = nullptr;
             S.prof_begin(e0);
-            launch_obs<double, OBS_GRAM>(S, kp, S.w64.p, w.x.p, nullptr, w.gx.p, nullptr);
+            launch_gram<double>(S, kp, S.w64.p, w.x.p, w.gx.p);
             S.prof_end(0, e0);
             const int grid = S.nblk(m * kp, 1);
             sub_kernel<<<grid, kBlock, 0, S.stream>>>(w.b.p, w.gx.p, w.r.p, m * kp);
@@ -1625,6 +1651,8 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
     if (precond && precond->kind == WITHIN_PRECOND_MULTIPLICATIVE && p.krylov == WITHIN_KRYLOV_CG)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT,
                         "CG requires a symmetric preconditioner; use 'additive' or switch to GMRES");
+    if (p.operator_repr != WITHIN_OPERATOR_IMPLICIT && p.operator_repr != WITHIN_OPERATOR_EXPLICIT)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "operator must be Implicit or Explicit");
     if (p.precision != WITHIN_PRECISION_FP64 && p.precision != WITHIN_PRECISION_MIXED)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "precision must be FP64 or MIXED");
     if (n_factors > (size_t)wb::kMaxQ) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "at most 16 factors are supported");
@@ -1688,16 +1716,26 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
                 wb::upload_stage(S->stages32.back(), h);
             }
         }
-        if (S->pc.kind == 2) {
-            std::vector<int64_t> gp;
-            std::vector<uint32_t> gi;
-            std::vector<double> gv;
-            wb::build_explicit_gramian(S->d, gp, gi, gv);
-            S->g_ptr.upload(gp);
-            S->g_idx.upload(gi);
-            S->g_val64.upload(gv);
-            if (S->mixed()) S->g_val32.upload_cast(gv);
-        }
+    }
+    // the assembled Gramian (solver.rs:103-121): for an explicit operator, and for the
+    // multiplicative residual updates, which then also use it as the Krylov operator
+    if (p.operator_repr == WITHIN_OPERATOR_EXPLICIT || S->pc.kind == 2) {
+        std::vector<int64_t> gp;
+        std::vector<uint32_t> gi;
+        std::vector<double> gv;
+        wb::build_explicit_gramian(S->d, gp, gi, gv);
+        S->g_ptr.upload(gp);
+        S->g_idx.upload(gi);
+        S->g_val64.upload(gv);
+        if (S->mixed()) S->g_val32.upload_cast(gv);
+        const int64_t m = S->d.ndofs;
+        std::vector<uint32_t> rows((size_t)m);
+        std::iota(rows.begin(), rows.end(), 0u);
+        S->g_rows.upload(rows);
+        const std::vector<wb::CsrChunk> ch = wb::make_chunks(gp, 0, m, 256, 1, true);
+        S->g_chunks.upload(ch);
+        S->g_nchunks = (int64_t)ch.size();
+        S->explicit_op = true;
     }
     WB_CUDA(cudaStreamSynchronize(S->stream));
     S->setup_time = wb::now_s() - t0;
@@ -1882,7 +1920,7 @@ static int apply_common(within_solver* s, const double* in, size_t k, double* ou
         if (which == 0 || which == 1) {
             if (!S.mixed()) {
                 if (which == 0) {
-                    wb::launch_obs<double, wb::OBS_GRAM>(S, kp, S.w64.p, iin.p, nullptr, iout.p, nullptr);
+                    wb::launch_gram<double>(S, kp, S.w64.p, iin.p, iout.p);
                 } else {
                     int nb = 0;
                     wb::apply_precond<double>(S, iin.p, iout.p, kp, nullptr, nb);
@@ -1893,7 +1931,7 @@ static int apply_common(within_solver* s, const double* in, size_t k, double* ou
                 fo.alloc(m * kp);
                 wb::convert_kernel<double, float><<<S.nblk(m * kp, 1), wb::kBlock, 0, S.stream>>>(iin.p, fi.p, m * kp);
                 if (which == 0) {
-                    wb::launch_obs<float, wb::OBS_GRAM>(S, kp, S.w32.p, fi.p, nullptr, fo.p, nullptr);
+                    wb::launch_gram<float>(S, kp, S.w32.p, fi.p, fo.p);
                 } else {
                     int nb = 0;
                     wb::apply_precond<float>(S, fi.p, fo.p, kp, nullptr, nb);
