@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="problem scale (1.0 = 10M observations)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--krylov", default="cg", choices=["cg", "lsmr"],
+                    help="cg (default): CG on the normal equations; lsmr: LSMR on W^(1/2) D (FP64)")
     ap.add_argument("--operator", default="implicit", choices=["implicit", "explicit"],
                     help="Krylov operator: the observation pass (default) or the assembled Gramian (CSR)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -281,7 +283,8 @@ def ours(args):
     n, k = Y.shape
     t0 = time.perf_counter()
     op = wb.OperatorRepr.Explicit if args.operator == "explicit" else wb.OperatorRepr.Implicit
-    solver = wb.Solver(cats, wb.CG(precision=args.precision, operator=op), weights=w)
+    cfg = wb.LSMR() if args.krylov == "lsmr" else wb.CG(precision=args.precision, operator=op)
+    solver = wb.Solver(cats, cfg, weights=w)
     setup_s = time.perf_counter() - t0
     m = solver.n_dofs
     dY = torch.from_numpy(np.ascontiguousarray(Y.T)).cuda()       # (k, n) = RHS-major
@@ -397,7 +400,7 @@ def ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 inner / f64 refinement" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded generator with the reference benchmark's AKM shapes)",
-            "config": config_dict(cats, k, args.scale, args.precision, args.operator),
+            "config": dict(config_dict(cats, k, args.scale, args.precision, args.operator), krylov=args.krylov),
             "e2e": {"value": e2e_value, "unit": "RHS/s", "h2d_bytes_per_step": int(n * k * 8),
                     "d2h_bytes_per_step": int((m + n) * k * 8)},
             "gpu_launches": int(launches), "roofline": roofline, "clocks": clk,
@@ -405,7 +408,7 @@ def ours(args):
             "setup_s": setup_s}
 
     # the plain FP64 drop-in on the same inputs (the metric's denominator)
-    if args.precision == "mixed" and not args.no_dropin:
+    if args.precision == "mixed" and not args.no_dropin and args.krylov == "cg":
         d64 = wb.Solver(cats, wb.CG(precision="fp64"), weights=w)
         for _ in range(max(1, args.warmup - 1)):
             L.within_solver_solve_batch_device(d64._h, C.c_void_p(dY.data_ptr()), k, C.c_void_p(dX.data_ptr()),

@@ -50,7 +50,7 @@ enum {
     WITHIN_ERR_CUDA = 10             /* device unavailable or a CUDA call failed */
 };
 
-enum { WITHIN_KRYLOV_CG = 0, WITHIN_KRYLOV_GMRES = 1 };
+enum { WITHIN_KRYLOV_CG = 0, WITHIN_KRYLOV_GMRES = 1, WITHIN_KRYLOV_LSMR = 2 };
 enum { WITHIN_OPERATOR_IMPLICIT = 0, WITHIN_OPERATOR_EXPLICIT = 1 };
 enum { WITHIN_PRECOND_OFF = 0, WITHIN_PRECOND_ADDITIVE = 1, WITHIN_PRECOND_MULTIPLICATIVE = 2 };
 /* Arithmetic of the inner Krylov solve.  FP64 is the plain drop-in; MIXED runs the
@@ -65,7 +65,9 @@ typedef struct {
     double tol;
     int32_t maxiter;
     int32_t max_refinements;
-    int32_t precision;       /* WITHIN_PRECISION_* */
+    int32_t precision;       /* WITHIN_PRECISION_* (LSMR always runs in FP64) */
+    int32_t lsmr_local_size; /* KrylovMethod::Lsmr { local_size }: windowed reorthogonalization
+                                against this many past v vectors; 0 = None (lsmr.rs:106-121) */
 } within_params;
 
 /* Preconditioner + LocalSolverConfig (within/src/config.rs:76-117, 174-183). */

@@ -1380,6 +1380,246 @@ static kres_t krylov_gmres(int64_t n, apply_fn A, apply_fn M, void *ctx, const d
     return out;
 }
 
+/* ------------------------------------------------------------------------- */
+/* LSMR: schwarz-precond/src/solve/lsmr.rs, lsmr/bidiag.rs, lsmr/recurrence.rs */
+/* (Fong & Saunders 2011, Algorithm 2.8; Modified Golub-Kahan with M ~ A'A)   */
+/* ------------------------------------------------------------------------- */
+
+/* WeightedDesignOperator, within/src/operator.rs:111-190: A = W^(1/2) D. */
+typedef struct { work_t *w; const double *sw; double *tmp; } rect_t;
+static void rect_apply(rect_t *R, const double *x, double *y) {
+    const design_t *d = &R->w->s->d;
+    design_matvec_d(d, x, y);
+    if (R->sw) for (int64_t i = 0; i < d->n; i++) y[i] *= R->sw[i];
+}
+static void rect_adjoint(rect_t *R, const double *u, double *x) {
+    const design_t *d = &R->w->s->d;
+    if (R->sw) {
+        for (int64_t i = 0; i < d->n; i++) R->tmp[i] = R->sw[i] * u[i];
+        design_rmatvec(d, R->tmp, x, 0);
+    } else {
+        design_rmatvec(d, u, x, 0);
+    }
+}
+
+/* Givens::new (recurrence.rs:24-31). */
+typedef struct { double c, s, r; } givens_t;
+static givens_t givens(double a, double b) {
+    givens_t g; g.r = hypot(a, b);
+    if (g.r > 0.0) { g.c = a / g.r; g.s = b / g.r; } else { g.c = 1.0; g.s = 0.0; }
+    return g;
+}
+typedef struct { double rho, rho_bar, theta_new, theta_bar, zeta; } rot_t;
+
+/* Ring of past v (and p~ = M v) vectors for windowed MGS (bidiag.rs:86-260): capacity
+ * min(local_size, rows, cols), swept oldest first. */
+typedef struct { double *v, *p; int64_t n; int cap, next, count; } ring_t;
+static void ring_sweep(const ring_t *g, double *v, double *p) {
+    int start = g->count < g->cap ? 0 : g->next;
+    for (int i = 0; i < g->count; i++) {
+        int idx = (start + i) % g->cap;
+        const double *vj = g->v + (size_t)idx * g->n;
+        if (p) {  /* M-weighted: c = <v, p_j>, v -= c v_j, p -= c p_j */
+            const double *pj = g->p + (size_t)idx * g->n;
+            double c = vdot(v, pj, g->n);
+            for (int64_t a = 0; a < g->n; a++) { v[a] += -c * vj[a]; p[a] += -c * pj[a]; }
+        } else {
+            double c = vdot(v, vj, g->n);
+            for (int64_t a = 0; a < g->n; a++) v[a] += -c * vj[a];
+        }
+    }
+}
+static void ring_push(ring_t *g, const double *v, const double *p, double pscale) {
+    memcpy(g->v + (size_t)g->next * g->n, v, sizeof(double) * (size_t)g->n);
+    if (p) for (int64_t a = 0; a < g->n; a++) g->p[(size_t)g->next * g->n + a] = p[a] * pscale;
+    g->next = (g->next + 1) % g->cap;
+    if (g->count < g->cap) g->count++;
+}
+
+/* A rectangular operator (rows x cols) and an optional preconditioner M^-1 (cols). */
+typedef struct {
+    void *ctx; int64_t rows, cols;
+    void (*apply)(void *, const double *, double *);
+    void (*adjoint)(void *, const double *, double *);
+    void (*minv)(void *, const double *, double *);   /* NULL: no preconditioner */
+} lsmr_op_t;
+static void cb_rect_apply(void *c, const double *x, double *y) { rect_apply((rect_t *)c, x, y); }
+static void cb_rect_adjoint(void *c, const double *u, double *x) { rect_adjoint((rect_t *)c, u, x); }
+static void cb_rect_minv(void *c, const double *r, double *z) { op_precond(((rect_t *)c)->w, r, z); }
+
+/* mlsmr (lsmr.rs:122-262): min ||b - A x||; with a preconditioner M ~ A'A, the Modified
+ * Golub-Kahan process (one M^-1 per iteration).  Returns x, converged, iterations;
+ * *stop_out (if given): 0 zero rhs, 1 A'b = 0, 2 residual tolerance, 3 normal-equation
+ * tolerance, 4 breakdown, 5 max iterations (LsmrStopReason, lsmr.rs:86-100). */
+static kres_t krylov_lsmr_op(const lsmr_op_t *A, const double *b, double tol, int maxiter, int local_size,
+                             int *stop_out) {
+    const int64_t no = A->rows, nd = A->cols;
+    const int precond = A->minv != NULL;
+    int stop_reason = 0;
+    kres_t out; out.x = xcalloc((size_t)nd + 1, sizeof(double));
+    out.converged = 1; out.iterations = 0; out.res = 0.0;
+    double bnorm = vnorm(b, no);
+    if (bnorm == 0.0) { if (stop_out) *stop_out = 0; return out; }   /* zero_rhs_result */
+    double *u = xcalloc((size_t)no + 1, sizeof(double)), *av = xcalloc((size_t)no + 1, sizeof(double));
+    double *v = xcalloc((size_t)nd + 1, sizeof(double)), *atu = xcalloc((size_t)nd + 1, sizeof(double));
+    double *pt = xcalloc((size_t)nd + 1, sizeof(double)), *h = xcalloc((size_t)nd + 1, sizeof(double));
+    double *hb = xcalloc((size_t)nd + 1, sizeof(double)), *x = out.x;
+    ring_t ring; ring.n = nd; ring.next = 0; ring.count = 0;
+    ring.cap = local_size; if (ring.cap > no) ring.cap = (int)no; if (ring.cap > nd) ring.cap = (int)nd;
+    if (ring.cap < 0) ring.cap = 0;
+    ring.v = ring.cap ? xcalloc((size_t)ring.cap * (size_t)nd, sizeof(double)) : NULL;
+    ring.p = (ring.cap && precond) ? xcalloc((size_t)ring.cap * (size_t)nd, sizeof(double)) : NULL;
+    /* init (bidiag.rs: GolubKahan::init, ModifiedGolubKahan::init) */
+    double beta = sqrt(vdot(b, b, no)), alpha, beta_prev_inv = 1.0;
+    if (beta > 0.0) for (int64_t i = 0; i < no; i++) u[i] = b[i] * (1.0 / beta);
+    if (!precond) {
+        A->adjoint(A->ctx, u, v);
+        alpha = sqrt(vdot(v, v, nd));
+        if (alpha > 0.0) for (int64_t j = 0; j < nd; j++) v[j] *= 1.0 / alpha;
+        if (ring.cap) ring_push(&ring, v, NULL, 0.0);
+    } else {
+        A->adjoint(A->ctx, u, pt);
+        A->minv(A->ctx, pt, v);
+        double vp = vdot(v, pt, nd);
+        alpha = vp > 0.0 ? sqrt(vp) : 0.0;
+        if (alpha > 0.0) for (int64_t j = 0; j < nd; j++) v[j] *= 1.0 / alpha;
+        if (ring.cap) ring_push(&ring, v, pt, alpha > 0.0 ? 1.0 / alpha : 0.0);
+    }
+    if (alpha == 0.0) { out.res = bnorm; stop_reason = 1; goto done; }   /* A'b = 0 */
+    /* lsmr_from_bidiag (lsmr.rs:204-262) */
+    double alpha_bar = alpha, phi_bar = beta, c_bar = 1.0, s_bar = 0.0, zeta_bar = alpha * beta;
+    double abs_tol = tol * bnorm, a2 = alpha * alpha;
+    rot_t prev = {1.0, 1.0, 0.0, 0.0, 0.0};
+    memcpy(h, v, sizeof(double) * (size_t)nd);
+    out.converged = 0; out.iterations = maxiter; stop_reason = 5;
+    for (int itn = 1; itn <= maxiter; itn++) {
+        /* one bidiagonalization step: (alpha, beta) and the normalized v */
+        double sa, sb;
+        if (!precond) {
+            A->apply(A->ctx, v, av);
+            double bsq = 0.0;
+            for (int64_t i = 0; i < no; i++) { u[i] = av[i] + (-alpha) * u[i]; bsq += u[i] * u[i]; }
+            sb = sqrt(bsq);
+            if (sb == 0.0) {
+                memset(v, 0, sizeof(double) * (size_t)nd); alpha = 0.0; sa = 0.0;
+            } else {
+                for (int64_t i = 0; i < no; i++) u[i] *= 1.0 / sb;
+                A->adjoint(A->ctx, u, atu);
+                double asq = 0.0;
+                for (int64_t j = 0; j < nd; j++) { v[j] = atu[j] + (-sb) * v[j]; asq += v[j] * v[j]; }
+                if (ring.cap) { ring_sweep(&ring, v, NULL); asq = vdot(v, v, nd); }
+                sa = sqrt(asq);
+                if (sa > 0.0) for (int64_t j = 0; j < nd; j++) v[j] *= 1.0 / sa;
+                if (ring.cap) ring_push(&ring, v, NULL, 0.0);
+                alpha = sa;
+            }
+        } else {
+            double scale = -(alpha * beta_prev_inv);
+            A->apply(A->ctx, v, av);
+            double bsq = 0.0;
+            for (int64_t i = 0; i < no; i++) { u[i] = av[i] + scale * u[i]; bsq += u[i] * u[i]; }
+            sb = sqrt(bsq);
+            if (sb == 0.0) {
+                memset(v, 0, sizeof(double) * (size_t)nd); memset(pt, 0, sizeof(double) * (size_t)nd);
+                alpha = 0.0; beta_prev_inv = 0.0; sa = 0.0;
+            } else {
+                double binv = 1.0 / sb, pc = sb / alpha;
+                A->adjoint(A->ctx, u, atu);
+                for (int64_t j = 0; j < nd; j++) pt[j] = binv * atu[j] + (-pc) * pt[j];
+                A->minv(A->ctx, pt, v);
+                if (ring.cap) ring_sweep(&ring, v, pt);
+                double vp = vdot(v, pt, nd);
+                sa = vp > 0.0 ? sqrt(vp) : 0.0;
+                if (sa > 0.0) for (int64_t j = 0; j < nd; j++) v[j] *= 1.0 / sa;
+                if (ring.cap) ring_push(&ring, v, pt, sa > 0.0 ? 1.0 / sa : 0.0);
+                alpha = sa; beta_prev_inv = binv;
+            }
+        }
+        a2 += sa * sa + sb * sb;                                     /* ConvergenceState::observe */
+        /* LsmrRecurrenceState::step (recurrence.rs:92-140) */
+        givens_t ph = givens(alpha_bar, sb);
+        double theta_new = ph.s * sa, alpha_bar_new = -ph.c * sa, phi_bar_new = ph.s * phi_bar;
+        double theta_bar = s_bar * ph.r;
+        givens_t pb = givens(c_bar * ph.r, theta_new);
+        double zeta = pb.c * zeta_bar, zeta_bar_new = -pb.s * zeta_bar;
+        alpha_bar = alpha_bar_new; phi_bar = phi_bar_new; c_bar = pb.c; s_bar = pb.s; zeta_bar = zeta_bar_new;
+        rot_t cur = {ph.r, pb.r, theta_new, theta_bar, zeta};
+        /* SolutionState::update (recurrence.rs:186-240) */
+        double dx = cur.rho * cur.rho_bar, dh = prev.rho * prev.rho_bar;
+        double t_x = fabs(dx) > DBL_EPSILON ? cur.zeta / dx : 0.0;
+        double t_hbar = fabs(dh) > DBL_EPSILON ? cur.theta_bar * cur.rho / dh : 0.0;
+        double t_h = fabs(cur.rho) > DBL_EPSILON ? cur.theta_new / cur.rho : 0.0;
+        for (int64_t j = 0; j < nd; j++) {
+            double h_old = h[j], hbj = h_old - t_hbar * hb[j];
+            hb[j] = hbj; x[j] += t_x * hbj; h[j] = v[j] - t_h * h_old;
+        }
+        /* ConvergenceState::check (recurrence.rs:272-284) */
+        double residual = fabs(phi_bar);
+        int stop = residual <= abs_tol;
+        if (!stop) {
+            double an = fmax(sqrt(a2), DBL_MIN), normar = fabs(zeta_bar);
+            stop = normar / (an * fmax(residual, DBL_MIN)) <= tol;
+        }
+        out.res = residual;
+        if (stop || sa == 0.0) {
+            out.converged = 1; out.iterations = itn;
+            stop_reason = stop ? (residual <= abs_tol ? 2 : 3) : 4;
+            break;
+        }
+        prev = cur;
+    }
+done:
+    if (stop_out) *stop_out = stop_reason;
+    free(u); free(av); free(v); free(atu); free(pt); free(h); free(hb); free(ring.v); free(ring.p);
+    return out;
+}
+
+/* The design operator A = W^(1/2) D with the solver's preconditioner. */
+static kres_t krylov_lsmr(rect_t *R, int precond, const double *b, double tol, int maxiter, int local_size) {
+    lsmr_op_t A = {R, R->w->s->d.n, R->w->s->d.ndofs, cb_rect_apply, cb_rect_adjoint, precond ? cb_rect_minv : NULL};
+    return krylov_lsmr_op(&A, b, tol, maxiter, local_size, NULL);
+}
+
+/* Dense operators for the known-answer tests of the LSMR recurrences: A row-major
+ * rows x cols, minv (optional) row-major cols x cols. */
+typedef struct { const double *a, *minv; int64_t rows, cols; } dense_op_t;
+static void dense_apply(void *c, const double *x, double *y) {
+    const dense_op_t *d = (const dense_op_t *)c;
+    for (int64_t i = 0; i < d->rows; i++) {
+        double t = 0.0;
+        for (int64_t j = 0; j < d->cols; j++) t += d->a[i * d->cols + j] * x[j];
+        y[i] = t;
+    }
+}
+static void dense_adjoint(void *c, const double *u, double *x) {
+    const dense_op_t *d = (const dense_op_t *)c;
+    for (int64_t j = 0; j < d->cols; j++) {
+        double t = 0.0;
+        for (int64_t i = 0; i < d->rows; i++) t += d->a[i * d->cols + j] * u[i];
+        x[j] = t;
+    }
+}
+static void dense_minv(void *c, const double *r, double *z) {
+    const dense_op_t *d = (const dense_op_t *)c;
+    for (int64_t i = 0; i < d->cols; i++) {
+        double t = 0.0;
+        for (int64_t j = 0; j < d->cols; j++) t += d->minv[i * d->cols + j] * r[j];
+        z[i] = t;
+    }
+}
+int oracle_lsmr_dense(const double *a, int64_t rows, int64_t cols, const double *minv, const double *b, double tol,
+                      int32_t maxiter, int32_t local_size, double *x, int32_t *converged, int32_t *iterations,
+                      int32_t *stop_reason) {
+    dense_op_t d = {a, minv, rows, cols};
+    lsmr_op_t A = {&d, rows, cols, dense_apply, dense_adjoint, minv ? dense_minv : NULL};
+    int stop = 0;
+    kres_t r = krylov_lsmr_op(&A, b, tol, maxiter, local_size, &stop);
+    memcpy(x, r.x, sizeof(double) * (size_t)cols);
+    *converged = r.converged; *iterations = r.iterations; *stop_reason = stop;
+    free(r.x);
+    return 0;
+}
+
 static void cb_gramian(void *ctx, const double *x, double *y) { op_gramian((work_t *)ctx, x, y); }
 static void cb_precond(void *ctx, const double *x, double *y) { op_precond((work_t *)ctx, x, y); }
 
@@ -1398,6 +1638,28 @@ static void solve_one(work_t *w, const double *y, double *x_out, double *dem, in
     double *rhs = xcalloc((size_t)m + 1, sizeof(double));
     design_rmatvec(&s->d, y, rhs, 1);
     double rn = vnorm(rhs, m); if (rn < 1e-15) rn = 1e-15;
+    if (s->p.krylov == 2) {
+        /* Solver::solve, LSMR branch (solver.rs:162-203): b = W^(1/2) y, mlsmr, then the
+         * demeaning and the normal-equation residual; no refinement */
+        rect_t R; R.w = w; R.sw = NULL; R.tmp = NULL;
+        double *sw = NULL, *b = xcalloc((size_t)n + 1, sizeof(double));
+        if (s->d.w) {
+            sw = xcalloc((size_t)n + 1, sizeof(double));
+            for (int64_t i = 0; i < n; i++) sw[i] = sqrt(s->d.w[i]);
+            R.sw = sw; R.tmp = xcalloc((size_t)n + 1, sizeof(double));
+        }
+        for (int64_t i = 0; i < n; i++) b[i] = sw ? sw[i] * y[i] : y[i];
+        kres_t r = krylov_lsmr(&R, s->p.precond_kind != 0, b, s->p.tol, s->p.maxiter, s->p.lsmr_local_size);
+        design_matvec_d(&s->d, r.x, dem);
+        for (int64_t i = 0; i < n; i++) dem[i] = y[i] - dem[i];
+        double *corr = xcalloc((size_t)m + 1, sizeof(double));
+        design_rmatvec(&s->d, dem, corr, 1);
+        *fres = vnorm(corr, m) / rn;
+        *conv = r.converged; *iters = r.iterations;
+        memcpy(x_out, r.x, sizeof(double) * (size_t)m);
+        free(r.x); free(corr); free(b); free(sw); free(R.tmp); free(rhs);
+        return;
+    }
     double abs_tol = s->p.tol * rn;
     kres_t k0 = krylov_solve(w, rhs, s->p.tol);
     double *x = k0.x;

@@ -27,7 +27,7 @@ extern "C" {
 
 typedef struct oracle_solver oracle_solver;
 
-/* krylov: 0 = CG, 1 = GMRES.  precond_kind: 0 = off, 1 = additive, 2 = multiplicative.
+/* krylov: 0 = CG, 1 = GMRES, 2 = LSMR.  precond_kind: 0 = off, 1 = additive, 2 = multiplicative.
  * approx_schur_enabled: 0 = exact Schur complement, 1 = sampled (clique tree). */
 typedef struct {
     int32_t krylov;
@@ -42,6 +42,7 @@ typedef struct {
     uint64_t approx_schur_seed;
     uint32_t approx_schur_split;
     int32_t dense_threshold;
+    int32_t lsmr_local_size;      /* krylov 2 (LSMR): windowed reorthogonalization, 0 = off */
 } oracle_params;
 
 /* codes: element (i, q) at codes[i*row_stride + q*col_stride].  weights may be NULL. */
@@ -71,6 +72,14 @@ void oracle_rmatvec_dt(const oracle_solver *s, const double *r, double *x);
 void oracle_gramian_diagonal(const oracle_solver *s, double *diag);
 void oracle_apply_gramian(const oracle_solver *s, const double *x, double *y);
 int oracle_apply_precond(oracle_solver *s, const double *r, double *z);
+
+/* LSMR on a dense row-major operator a (rows x cols) with an optional dense M^-1
+ * (cols x cols), for known-answer tests of the recurrences (lsmr/tests.rs).
+ * stop_reason: 0 zero rhs, 1 A'b = 0, 2 residual tolerance, 3 normal-equation
+ * tolerance, 4 breakdown, 5 max iterations. */
+int oracle_lsmr_dense(const double *a, int64_t rows, int64_t cols, const double *minv, const double *b, double tol,
+                      int32_t maxiter, int32_t local_size, double *x, int32_t *converged, int32_t *iterations,
+                      int32_t *stop_reason);
 
 /* Setup structure, for bit-exact checks of the integer setup. */
 int32_t oracle_n_subdomains(const oracle_solver *s);

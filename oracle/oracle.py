@@ -37,6 +37,7 @@ class OracleParams(C.Structure):
         ("approx_schur_seed", C.c_uint64),
         ("approx_schur_split", C.c_uint32),
         ("dense_threshold", C.c_int32),
+        ("lsmr_local_size", C.c_int32),
     ]
 
 
@@ -78,17 +79,36 @@ def lib():
                                       i32p, i32p, f64p]
         L.oracle_dense_gmres.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, f64p, C.c_double, C.c_int32,
                                          C.c_int32, f64p, i32p, i32p, f64p]
+        L.oracle_lsmr_dense.argtypes = [f64p, C.c_int64, C.c_int64, C.c_void_p, f64p, C.c_double, C.c_int32,
+                                        C.c_int32, f64p, i32p, i32p, i32p]
         _lib = L
     return _lib
 
 
+LSMR_STOPS = ("ZeroRhs", "InitialNormalEquationResidualZero", "ResidualTolerance", "NormalEquationTolerance",
+              "BidiagonalizationBreakdown", "MaxIterations")
+
+
+def lsmr_dense(a, b, minv=None, tol=1e-10, maxiter=100, local_size=0):
+    """The oracle's LSMR (lsmr.rs) on a dense operator: (x, converged, iterations, stop reason)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    rows, cols = a.shape
+    mi = None if minv is None else np.ascontiguousarray(minv, dtype=np.float64)
+    x = np.zeros(cols)
+    cv, it, st = np.zeros(1, np.int32), np.zeros(1, np.int32), np.zeros(1, np.int32)
+    lib().oracle_lsmr_dense(a.ravel(), rows, cols, None if mi is None else mi.ctypes.data_as(C.c_void_p),
+                            np.ascontiguousarray(b, dtype=np.float64), tol, maxiter, local_size, x, cv, it, st)
+    return x, bool(cv[0]), int(it[0]), LSMR_STOPS[int(st[0])]
+
+
 def make_params(krylov="cg", tol=1e-8, maxiter=1000, max_refinements=2, restart=30,
                 preconditioner="additive", approx_chol_seed=0, approx_chol_split=2,
-                approx_schur=(0, 1), dense_threshold=24) -> OracleParams:
+                approx_schur=(0, 1), dense_threshold=24, local_size=None) -> OracleParams:
     """Reference defaults: CG, tol 1e-8, maxiter 1000, 2 refinements (within/src/config.rs:227-236),
     additive Schwarz with LocalSolverConfig::solver_default() (config.rs:108-117)."""
     p = OracleParams()
-    p.krylov = {"cg": 0, "gmres": 1}[krylov]
+    p.krylov = {"cg": 0, "gmres": 1, "lsmr": 2}[krylov]
+    p.lsmr_local_size = 0 if local_size is None else int(local_size)
     p.gmres_restart = restart
     p.tol = tol
     p.maxiter = maxiter

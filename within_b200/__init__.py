@@ -24,7 +24,7 @@ import numpy as np
 from . import _lib
 
 __all__ = [
-    "OperatorRepr", "Preconditioner", "ReductionStrategy", "CG", "GMRES", "ApproxCholConfig",
+    "OperatorRepr", "Preconditioner", "ReductionStrategy", "CG", "GMRES", "LSMR", "ApproxCholConfig",
     "ApproxSchurConfig", "SchurComplement", "AdditiveSchwarz", "MultiplicativeSchwarz", "SolveResult",
     "BatchSolveResult", "AdditiveSchwarzDiagnostics", "FePreconditioner", "Solver", "solve", "solve_batch", "solve_many", "WithinError",
 ]
@@ -86,6 +86,21 @@ class GMRES:
 
     def __repr__(self):
         return f"GMRES(tol={self.tol}, maxiter={self.maxiter}, restart={self.restart})"
+
+
+class LSMR:
+    """Modified LSMR on the rectangular problem min ||W^(1/2)(y - D x)|| (within-py LSMR,
+    lib.rs:399-425; schwarz-precond/src/solve/lsmr.rs).  Runs in FP64 with no iterative
+    refinement; with a preconditioner, one M^-1 apply per iteration."""
+
+    def __init__(self, tol: float = 1e-8, maxiter: int = 1000, local_size: int | None = None):
+        if local_size is not None and int(local_size) < 0:
+            raise OverflowError("local_size must be a non-negative integer")
+        self.tol, self.maxiter = float(tol), int(maxiter)
+        self.local_size = None if local_size is None else int(local_size)
+
+    def __repr__(self):
+        return f"LSMR(tol={self.tol}, maxiter={self.maxiter}, local_size={self.local_size})"
 
 
 class ApproxCholConfig:
@@ -176,6 +191,10 @@ def _params_struct(config):
     _lib.load().within_default_params(C.byref(p))
     if config is None:
         return p
+    if isinstance(config, LSMR):  # extract_solver_params (lib.rs:621-632)
+        p.krylov, p.lsmr_local_size = 2, config.local_size or 0
+        p.tol, p.maxiter, p.max_refinements = config.tol, config.maxiter, 0
+        return p
     if isinstance(config, CG):
         p.krylov = 0
     elif isinstance(config, GMRES):
@@ -189,8 +208,9 @@ def _params_struct(config):
 
 def _validate(params, pre) -> None:
     """validate_cg_preconditioner (within-py/src/lib.rs:639-656)."""
-    if params.krylov == 0 and pre.kind == 2:
-        raise ValueError("CG requires a symmetric preconditioner; use 'additive' or switch to GMRES")
+    if params.krylov in (0, 2) and pre.kind == 2:
+        method = "CG" if params.krylov == 0 else "LSMR"
+        raise ValueError(f"{method} requires a symmetric preconditioner; use 'additive' or switch to GMRES")
 
 
 def _categories(categories) -> np.ndarray:

@@ -25,7 +25,7 @@ ERR_NAMES = {
 class Params(C.Structure):
     _fields_ = [("krylov", C.c_int32), ("gmres_restart", C.c_int32), ("operator_repr", C.c_int32),
                 ("tol", C.c_double), ("maxiter", C.c_int32), ("max_refinements", C.c_int32),
-                ("precision", C.c_int32)]
+                ("precision", C.c_int32), ("lsmr_local_size", C.c_int32)]
 
 
 class Precond(C.Structure):

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <array>
 #include <chrono>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -365,6 +366,7 @@ struct SolverImpl {
     Workspace ws;
     DArr<double> host_y, host_x, host_dem;  // device side of the host-buffer entry points
     std::shared_ptr<void> gmres;  // GmresBufs, created on first GMRES solve
+    std::shared_ptr<void> lsmr;   // LsmrBufs, created on first LSMR solve
     int32_t* h_active = nullptr;  // pinned
     double setup_time = 0.0;
     int64_t gpu_launches = 0;
@@ -1462,6 +1464,409 @@ void gmres_device(SolverImpl& S, GmresBufs& B, int kp, const double* rhs, double
     WB_CUDA(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------------------
+// LSMR (schwarz-precond/src/solve/lsmr.rs, lsmr/bidiag.rs, lsmr/recurrence.rs):
+// min ||b - A x|| with A = W^(1/2) D (within/src/operator.rs:111-190), b = W^(1/2) y,
+// batched over the RHS columns.  Every column runs its own Golub-Kahan process and
+// Givens recurrences; their scalars live on the device (one thread per column), the
+// vectors are the interleaved n x kp / m x kp layout of the other solvers.  With a
+// preconditioner M ~ A'A the Modified Golub-Kahan process applies M^-1 once per step.
+// ---------------------------------------------------------------------------
+
+struct LsmrBufs {
+    int kp = 0, cap = 0;
+    int64_t n = 0, m = 0;
+    DArr<double> u, av, sw;                      // observation space (n x kp; sw: n)
+    DArr<double> v, atu, pt, h, hb;              // dof space (m x kp)
+    DArr<double> ring_v, ring_p;                 // cap x m x kp
+    // per-column scalars (kp each)
+    DArr<double> bnorm, beta, alpha, bpi, scale, pa, pb, inv_alpha;
+    DArr<double> abar, phibar, cbar, sbar, zbar, a2, prho, prhob, coef, zeros;
+    DArr<int32_t> active, conv, iters, part_of, brk, n_active;
+};
+
+struct LsmrState {
+    double *bnorm, *beta, *alpha, *bpi, *scale, *pa, *pb, *inv_alpha;
+    double *abar, *phibar, *cbar, *sbar, *zbar, *a2, *prho, *prhob, *coef;
+    int32_t *active, *conv, *iters, *part_of, *brk, *n_active;
+    double tol;
+    int maxiter, precond;
+};
+
+LsmrState lsmr_state(LsmrBufs& B, double tol, int maxiter, int precond) {
+    return LsmrState{B.bnorm.p, B.beta.p, B.alpha.p, B.bpi.p, B.scale.p, B.pa.p, B.pb.p, B.inv_alpha.p,
+                     B.abar.p, B.phibar.p, B.cbar.p, B.sbar.p, B.zbar.p, B.a2.p, B.prho.p, B.prhob.p, B.coef.p,
+                     B.active.p, B.conv.p, B.iters.p, B.part_of.p, B.brk.p, B.n_active.p, tol, maxiter, precond};
+}
+
+__device__ void lsmr_count(const LsmrState& s, int kp) {
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        int na = 0;
+        for (int j = 0; j < kp; ++j) na += s.active[j];
+        *s.n_active = na;
+    }
+}
+
+// u = sw .* x + scale[c] u (u not read where scale is 0), with partial sums of u^2.
+template <int G>
+__global__ void __launch_bounds__(kBlock) lsmr_obs_axpy_kernel(double* __restrict__ u, const double* __restrict__ x,
+                                                               const double* __restrict__ sw,
+                                                               const double* __restrict__ scale, int64_t rows, int kp,
+                                                               double* __restrict__ part) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const V4<double> sc(scale[c4], scale[c4 + 1], scale[c4 + 2], scale[c4 + 3]);
+    V4<double> acc(0.0);
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t r = (int64_t)blockIdx.x * rpb + threadIdx.x / G; r < rows; r += (int64_t)gridDim.x * rpb) {
+        const size_t e = (size_t)r * kp + c4;
+        const double wr = sw ? sw[r] : 1.0;
+        V4<double> xv = ld4(x + e);
+        const V4<double> uv = ld4(u + e);
+        xv.a = wr * xv.a + (sc.a != 0.0 ? sc.a * uv.a : 0.0);
+        xv.b = wr * xv.b + (sc.b != 0.0 ? sc.b * uv.b : 0.0);
+        xv.c = wr * xv.c + (sc.c != 0.0 ? sc.c * uv.c : 0.0);
+        xv.d = wr * xv.d + (sc.d != 0.0 ? sc.d * uv.d : 0.0);
+        st4(u + e, xv);
+        acc.a += xv.a * xv.a; acc.b += xv.b * xv.b; acc.c += xv.c * xv.c; acc.d += xv.d * xv.d;
+    }
+    block_reduce_store4<G>(acc, kp, part);
+}
+
+// y = sa * a[c] x + b[c] y per column (b == nullptr: 1; y not read where b[c] is 0),
+// with partial sums of y^2 when part is given.
+template <int G>
+__global__ void __launch_bounds__(kBlock) lsmr_axpby_kernel(double* y, const double* x,
+                                                            const double* __restrict__ a, double sa,
+                                                            const double* __restrict__ b, int64_t rows, int kp,
+                                                            double* __restrict__ part) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const V4<double> av(sa * a[c4], sa * a[c4 + 1], sa * a[c4 + 2], sa * a[c4 + 3]);
+    const V4<double> bv = b ? V4<double>(b[c4], b[c4 + 1], b[c4 + 2], b[c4 + 3]) : V4<double>(1.0);
+    V4<double> acc(0.0);
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t r = (int64_t)blockIdx.x * rpb + threadIdx.x / G; r < rows; r += (int64_t)gridDim.x * rpb) {
+        const size_t e = (size_t)r * kp + c4;
+        const V4<double> xv = ld4(x + e), yv = ld4(y + e);
+        V4<double> o;
+        o.a = av.a * xv.a + (bv.a != 0.0 ? bv.a * yv.a : 0.0);
+        o.b = av.b * xv.b + (bv.b != 0.0 ? bv.b * yv.b : 0.0);
+        o.c = av.c * xv.c + (bv.c != 0.0 ? bv.c * yv.c : 0.0);
+        o.d = av.d * xv.d + (bv.d != 0.0 ? bv.d * yv.d : 0.0);
+        st4(y + e, o);
+        acc.a += o.a * o.a; acc.b += o.b * o.b; acc.c += o.c * o.c; acc.d += o.d * o.d;
+    }
+    if (part) block_reduce_store4<G>(acc, kp, part);
+}
+
+// SolutionState::update (recurrence.rs:186-240): hb = h - t_hbar hb; x += t_x hb;
+// h = v - t_h h, with coef = [t_x | t_hbar | t_h] per column (zeros freeze a column's x).
+template <int G>
+__global__ void __launch_bounds__(kBlock) lsmr_update_kernel(double* __restrict__ x, double* __restrict__ h,
+                                                             double* __restrict__ hb, const double* __restrict__ v,
+                                                             const double* __restrict__ coef, int64_t rows, int kp) {
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const V4<double> tx(coef[c4], coef[c4 + 1], coef[c4 + 2], coef[c4 + 3]);
+    const V4<double> thb(coef[kp + c4], coef[kp + c4 + 1], coef[kp + c4 + 2], coef[kp + c4 + 3]);
+    const V4<double> th(coef[2 * kp + c4], coef[2 * kp + c4 + 1], coef[2 * kp + c4 + 2], coef[2 * kp + c4 + 3]);
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t r = (int64_t)blockIdx.x * rpb + threadIdx.x / G; r < rows; r += (int64_t)gridDim.x * rpb) {
+        const size_t e = (size_t)r * kp + c4;
+        const V4<double> ho = ld4(h + e), hbo = ld4(hb + e), vv = ld4(v + e);
+        V4<double> xv = ld4(x + e), hn, hbn;
+        hbn.a = ho.a - thb.a * hbo.a; hbn.b = ho.b - thb.b * hbo.b; hbn.c = ho.c - thb.c * hbo.c; hbn.d = ho.d - thb.d * hbo.d;
+        xv.a += tx.a * hbn.a; xv.b += tx.b * hbn.b; xv.c += tx.c * hbn.c; xv.d += tx.d * hbn.d;
+        hn.a = vv.a - th.a * ho.a; hn.b = vv.b - th.b * ho.b; hn.c = vv.c - th.c * ho.c; hn.d = vv.d - th.d * ho.d;
+        st4(hb + e, hbn);
+        st4(x + e, xv);
+        st4(h + e, hn);
+    }
+}
+
+__global__ void lsmr_sqrt_kernel(const double* __restrict__ w, double* __restrict__ sw, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        sw[i] = sqrt(w[i]);
+}
+
+// beta_1 = ||b|| (GolubKahan::init / ModifiedGolubKahan::init); zero right-hand sides
+// are solved at iteration 0 (zero_rhs_result).  inv_alpha holds 1 / beta_1 for u.
+__global__ void lsmr_init_kernel(LsmrState s, const double* __restrict__ red, int kp) {
+    const int c = threadIdx.x;
+    if (c < kp) {
+        const double bn = sqrt(red[c]);
+        s.bnorm[c] = bn;
+        s.beta[c] = bn;
+        s.inv_alpha[c] = bn > 0.0 ? 1.0 / bn : 0.0;
+        const int on = s.part_of[c] && bn != 0.0;
+        s.active[c] = on;
+        s.conv[c] = s.part_of[c] && !on;
+        s.iters[c] = 0;
+        s.brk[c] = 0;
+    }
+    lsmr_count(s, kp);
+}
+
+// alpha_1 (Euclidean or M-norm of A'u_1), then the recurrence and convergence state
+// (LsmrRecurrenceState::init, ConvergenceState::new, RotationStep::initial); A'b = 0
+// stops at iteration 0.  inv_alpha = 1 / alpha_1 normalizes v_1.
+__global__ void lsmr_alpha1_kernel(LsmrState s, const double* __restrict__ red, int kp) {
+    const int c = threadIdx.x;
+    if (c < kp) {
+        const double q = red[c];
+        const double al = s.precond ? (q > 0.0 ? sqrt(q) : 0.0) : sqrt(q);
+        s.alpha[c] = al;
+        s.inv_alpha[c] = al > 0.0 ? 1.0 / al : 0.0;
+        if (s.active[c] && al == 0.0) {
+            s.active[c] = 0;
+            s.conv[c] = 1;
+        }
+        const double be = s.beta[c];
+        s.abar[c] = al; s.phibar[c] = be; s.cbar[c] = 1.0; s.sbar[c] = 0.0; s.zbar[c] = al * be;
+        s.a2[c] = al * al; s.prho[c] = 1.0; s.prhob[c] = 1.0; s.bpi[c] = 1.0;
+        // the first step's u-update scale: -alpha (GK) or -alpha / beta_prev (MGK, u normalized)
+        s.scale[c] = s.active[c] ? -al : 0.0;
+    }
+    lsmr_count(s, kp);
+}
+
+// beta_{k+1} = ||u||: the breakdown flag, and the coefficients of the next vector update:
+// GK: u *= 1/beta (pa), v = A'u - beta v (pb = -beta);  MGK: p~ = (1/beta) A'u - (beta/alpha) p~.
+// Inactive or broken-down columns get zeros, which zero their v (and p~).
+__global__ void lsmr_beta_kernel(LsmrState s, const double* __restrict__ red, int kp) {
+    const int c = threadIdx.x;
+    if (c < kp) {
+        const double be = sqrt(red[c]);
+        const int on = s.active[c];
+        s.beta[c] = be;
+        s.brk[c] = on && be == 0.0;
+        const int go = on && be != 0.0;
+        const double binv = be > 0.0 ? 1.0 / be : 0.0;
+        if (!s.precond) {
+            s.inv_alpha[c] = go ? binv : 0.0;  // scale of u
+            s.pa[c] = go ? 1.0 : 0.0;
+            s.pb[c] = go ? -be : 0.0;
+        } else {
+            const double al = s.alpha[c];
+            s.pa[c] = go ? binv : 0.0;
+            s.pb[c] = (go && al > 0.0) ? -(be / al) : 0.0;
+            s.bpi[c] = go ? binv : 0.0;
+        }
+    }
+}
+
+// One LSMR step's scalars after the new v: alpha_{k+1}, the ||A||_F^2 estimate, both
+// Givens rotations, the solution-update coefficients and the stop tests
+// (lsmr.rs:225-262, recurrence.rs:92-140, 186-240, 265-284).  red: GK ||v||^2, MGK <v, p~>.
+__global__ void lsmr_step_kernel(LsmrState s, const double* __restrict__ red, int kp, int itn) {
+    const int c = threadIdx.x;
+    if (c < kp) {
+        double* coef = s.coef;
+        coef[c] = 0.0; coef[kp + c] = 0.0; coef[2 * kp + c] = 0.0;
+        if (s.active[c]) {
+            const double q = red[c];
+            const double sb = s.beta[c];
+            double sa = s.precond ? (q > 0.0 ? sqrt(q) : 0.0) : sqrt(q);
+            if (s.brk[c]) sa = 0.0;
+            s.inv_alpha[c] = sa > 0.0 ? 1.0 / sa : 0.0;
+            s.a2[c] += sa * sa + sb * sb;
+            // P-hat: eliminate beta_{k+1} against alpha_bar
+            const double ab = s.abar[c];
+            const double r1 = hypot(ab, sb);
+            const double c1 = r1 > 0.0 ? ab / r1 : 1.0, s1 = r1 > 0.0 ? sb / r1 : 0.0;
+            const double theta_new = s1 * sa;
+            s.abar[c] = -c1 * sa;
+            s.phibar[c] = s1 * s.phibar[c];
+            // P-bar: eliminate theta_{k+1} against c_bar rho (theta_bar uses the old s_bar)
+            const double theta_bar = s.sbar[c] * r1;
+            const double a_ = s.cbar[c] * r1;
+            const double r2 = hypot(a_, theta_new);
+            const double c2 = r2 > 0.0 ? a_ / r2 : 1.0, s2 = r2 > 0.0 ? theta_new / r2 : 0.0;
+            const double zeta = c2 * s.zbar[c];
+            s.zbar[c] = -s2 * s.zbar[c];
+            s.cbar[c] = c2;
+            s.sbar[c] = s2;
+            // solution-update coefficients
+            const double dx = r1 * r2, dh = s.prho[c] * s.prhob[c];
+            coef[c] = fabs(dx) > DBL_EPSILON ? zeta / dx : 0.0;
+            coef[kp + c] = fabs(dh) > DBL_EPSILON ? theta_bar * r1 / dh : 0.0;
+            coef[2 * kp + c] = fabs(r1) > DBL_EPSILON ? theta_new / r1 : 0.0;
+            s.prho[c] = r1;
+            s.prhob[c] = r2;
+            // stop tests: ||r|| <= tol ||b||, or ||A'r|| / (||A|| ||r||) <= tol
+            const double res = fabs(s.phibar[c]);
+            bool stop = res <= s.tol * s.bnorm[c];
+            if (!stop) {
+                const double an = fmax(sqrt(s.a2[c]), DBL_MIN);
+                stop = fabs(s.zbar[c]) / (an * fmax(res, DBL_MIN)) <= s.tol;
+            }
+            s.iters[c] = itn;
+            s.alpha[c] = sa;
+            if (stop || sa == 0.0) {
+                s.conv[c] = 1;
+                s.active[c] = 0;
+            } else if (itn >= s.maxiter) {
+                s.active[c] = 0;
+            }
+            s.scale[c] = s.active[c] ? (s.precond ? -(sa * s.bpi[c]) : -sa) : 0.0;
+        } else {
+            s.inv_alpha[c] = 0.0;
+            s.scale[c] = 0.0;
+        }
+    }
+    lsmr_count(s, kp);
+}
+
+// LSMR for the columns in part_of, into x (m x kp, FP64).  y_i: interleaved n x kp.
+void lsmr_device(SolverImpl& S, LsmrBufs& B, int kp, const double* yi, double* x, const std::vector<int32_t>& part_of,
+                 std::vector<int32_t>& conv, std::vector<int32_t>& iters) {
+    const int64_t n = S.d.n, m = S.d.ndofs;
+    const int precond = S.pc.kind != 0 ? 1 : 0;
+    const int cap = (int)std::max<int64_t>(0, std::min<int64_t>(S.params.lsmr_local_size, std::min(n, m)));
+    if (B.kp != kp || B.n != n || B.m != m || B.cap != cap) {
+        B.kp = kp; B.n = n; B.m = m; B.cap = cap;
+        B.u.alloc((size_t)n * kp); B.av.alloc((size_t)n * kp);
+        for (DArr<double>* a : {&B.v, &B.atu, &B.pt, &B.h, &B.hb}) a->alloc((size_t)m * kp);
+        if (cap) {
+            B.ring_v.alloc((size_t)cap * m * kp);
+            if (precond) B.ring_p.alloc((size_t)cap * m * kp);
+        }
+        for (DArr<double>* a : {&B.bnorm, &B.beta, &B.alpha, &B.bpi, &B.scale, &B.pa, &B.pb, &B.inv_alpha, &B.abar,
+                                &B.phibar, &B.cbar, &B.sbar, &B.zbar, &B.a2, &B.prho, &B.prhob, &B.zeros})
+            a->alloc(32);
+        B.coef.alloc(96);
+        for (DArr<int32_t>* a : {&B.active, &B.conv, &B.iters, &B.part_of, &B.brk, &B.n_active}) a->alloc(32);
+        B.sw.release();
+        if (S.w64.p) {
+            B.sw.alloc((size_t)n);
+            lsmr_sqrt_kernel<<<S.nblk(n, 1, 4), kBlock, 0, S.stream>>>(S.w64.p, B.sw.p, n);
+            WB_CUDA(cudaGetLastError());
+            S.gpu_launches++;
+        }
+        WB_CUDA(cudaMemsetAsync(B.zeros.p, 0, 32 * sizeof(double), S.stream));
+    }
+    LsmrState s = lsmr_state(B, S.params.tol, S.params.maxiter, precond);
+    WB_CUDA(cudaMemcpyAsync(B.part_of.p, part_of.data(), sizeof(int32_t) * kp, cudaMemcpyHostToDevice, S.stream));
+    const int G = group_for(kp);
+    const double* sw = B.sw.p;
+    double* part = S.ws.part.p;
+    double* red = S.ws.red.p;
+    const int gn = S.nblk(n, G, 2), gm = S.nblk(m, G, 2);
+    const size_t mk = (size_t)m * kp;
+    int nb = 0;
+    auto axpby = [&](double* y, const double* xx, const double* a, double sa, const double* b, bool sq) {
+        WB_DISPATCH_G(G, lsmr_axpby_kernel<GV><<<gm, kBlock, 0, S.stream>>>(y, xx, a, sa, b, m, kp, sq ? part : nullptr));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+        if (sq) launch_reduce(S, part, gm, kp, red);
+    };
+    auto dot = [&](const double* a, const double* b) {
+        launch_dot<double, double>(S, a, b, m, kp, part, nb);
+        launch_reduce(S, part, nb, kp, red);
+    };
+    auto obs_axpy = [&](const double* xx, const double* scale) {  // u = sw .* xx + scale u, red = ||u||^2
+        WB_DISPATCH_G(G, lsmr_obs_axpy_kernel<GV><<<gn, kBlock, 0, S.stream>>>(B.u.p, xx, sw, scale, n, kp, part));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+        launch_reduce(S, part, gn, kp, red);
+    };
+    auto scale_u = [&]() {  // u *= inv_alpha (a = inv_alpha, b = 0)
+        WB_DISPATCH_G(G, lsmr_axpby_kernel<GV><<<gn, kBlock, 0, S.stream>>>(B.u.p, B.u.p, B.inv_alpha.p, 1.0, B.zeros.p,
+                                                                             n, kp, nullptr));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+    };
+    auto adjoint = [&](double* out) {  // out = D' (sw .* u)
+        launch_obs<double, OBS_RHS>(S, kp, sw, nullptr, B.u.p, out, nullptr);
+    };
+    // ring of past (v, M v) pairs for the windowed reorthogonalization
+    int r_next = 0, r_count = 0;
+    auto ring_sweep = [&]() {
+        const int start = r_count < cap ? 0 : r_next;
+        for (int i = 0; i < r_count; ++i) {
+            const int idx = (start + i) % cap;
+            const double* vj = B.ring_v.p + (size_t)idx * mk;
+            if (precond) {
+                const double* pj = B.ring_p.p + (size_t)idx * mk;
+                dot(B.v.p, pj);
+                axpby(B.v.p, vj, red, -1.0, nullptr, false);
+                axpby(B.pt.p, pj, red, -1.0, nullptr, false);
+            } else {
+                dot(B.v.p, vj);
+                axpby(B.v.p, vj, red, -1.0, nullptr, false);
+            }
+        }
+    };
+    auto ring_push = [&]() {  // v (normalized) and p~ / alpha
+        WB_CUDA(cudaMemcpyAsync(B.ring_v.p + (size_t)r_next * mk, B.v.p, sizeof(double) * mk, cudaMemcpyDeviceToDevice,
+                                S.stream));
+        if (precond) {
+            double* pj = B.ring_p.p + (size_t)r_next * mk;
+            axpby(pj, B.pt.p, B.inv_alpha.p, 1.0, B.zeros.p, false);
+        }
+        r_next = (r_next + 1) % cap;
+        if (r_count < cap) ++r_count;
+    };
+    // --- init: beta_1 u_1 = b, alpha_1 v_1 = A'u_1 (or M^-1 A'u_1 with the M-norm)
+    obs_axpy(yi, B.zeros.p);
+    lsmr_init_kernel<<<1, 32, 0, S.stream>>>(s, red, kp);
+    scale_u();
+    if (!precond) {
+        adjoint(B.v.p);
+        dot(B.v.p, B.v.p);
+    } else {
+        adjoint(B.pt.p);
+        int nbp = 0;
+        apply_precond<double>(S, B.pt.p, B.v.p, kp, nullptr, nbp);
+        dot(B.v.p, B.pt.p);
+    }
+    lsmr_alpha1_kernel<<<1, 32, 0, S.stream>>>(s, red, kp);
+    axpby(B.v.p, B.v.p, B.inv_alpha.p, 1.0, B.zeros.p, false);  // v /= alpha_1
+    if (cap) ring_push();
+    WB_CUDA(cudaMemcpyAsync(B.h.p, B.v.p, sizeof(double) * mk, cudaMemcpyDeviceToDevice, S.stream));
+    WB_CUDA(cudaMemsetAsync(B.hb.p, 0, sizeof(double) * mk, S.stream));
+    WB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * mk, S.stream));
+    WB_CUDA(cudaMemcpyAsync(S.h_active, B.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    S.gpu_launches += 2;
+    for (int itn = 1; itn <= S.params.maxiter && *S.h_active > 0; ++itn) {
+        // beta_{k+1} u_{k+1} = A v_k + scale u_k
+        launch_obs<double, OBS_DX>(S, kp, nullptr, B.v.p, nullptr, nullptr, B.av.p);
+        obs_axpy(B.av.p, B.scale.p);
+        lsmr_beta_kernel<<<1, 32, 0, S.stream>>>(s, red, kp);
+        S.gpu_launches++;
+        if (!precond) {
+            scale_u();
+            adjoint(B.atu.p);
+            axpby(B.v.p, B.atu.p, B.pa.p, 1.0, B.pb.p, !cap);  // v = A'u - beta v, red = ||v||^2
+            if (cap) {
+                ring_sweep();
+                dot(B.v.p, B.v.p);
+            }
+        } else {
+            adjoint(B.atu.p);
+            axpby(B.pt.p, B.atu.p, B.pa.p, 1.0, B.pb.p, false);  // p~ = A'u / beta - (beta / alpha) p~
+            int nbp = 0;
+            apply_precond<double>(S, B.pt.p, B.v.p, kp, nullptr, nbp);
+            if (cap) ring_sweep();
+            dot(B.v.p, B.pt.p);
+        }
+        lsmr_step_kernel<<<1, 32, 0, S.stream>>>(s, red, kp, itn);
+        S.gpu_launches++;
+        axpby(B.v.p, B.v.p, B.inv_alpha.p, 1.0, B.zeros.p, false);  // v /= alpha_{k+1}
+        if (cap) ring_push();
+        WB_DISPATCH_G(G, lsmr_update_kernel<GV><<<gm, kBlock, 0, S.stream>>>(x, B.h.p, B.hb.p, B.v.p, B.coef.p, m, kp));
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+        WB_CUDA(cudaMemcpyAsync(S.h_active, B.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+        WB_CUDA(cudaStreamSynchronize(S.stream));
+    }
+    conv.assign(kp, 0);
+    iters.assign(kp, 0);
+    WB_CUDA(cudaMemcpyAsync(conv.data(), B.conv.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaMemcpyAsync(iters.data(), B.iters.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1508,88 +1913,95 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
     std::vector<int32_t> conv(kp, 0), iters(kp, 0), part_of(kp, 0);
     for (int c = 0; c < k; ++c) part_of[c] = 1;
     std::vector<double> tol(kp, S.params.tol);
-    // One inner Krylov solve of G d = rhs on the RHS in `who` to relative tolerances tl,
-    // then x += d on those RHS.
-    auto run_inner = [&](const double* rhs, const std::vector<int32_t>& who, const std::vector<double>& tl,
-                         std::vector<int32_t>& cv, std::vector<int32_t>& it) {
-        WB_CUDA(cudaMemcpyAsync(w.st_part.p, who.data(), sizeof(int32_t) * kp, cudaMemcpyHostToDevice, S.stream));
-        WB_CUDA(cudaMemcpyAsync(w.st_tol.p, tl.data(), sizeof(double) * kp, cudaMemcpyHostToDevice, S.stream));
-        WB_CUDA(cudaMemsetAsync(w.st_conv.p, 0, sizeof(int32_t) * 32, S.stream));
-        const int grid = S.nblk(m * kp, 1);
-        if (S.params.krylov == WITHIN_KRYLOV_GMRES) {
-            if (!S.gmres) S.gmres = std::make_shared<GmresBufs>();
-            GmresBufs& B = *std::static_pointer_cast<GmresBufs>(S.gmres);
-            if (!S.mixed()) gmres_device<double>(S, B, kp, rhs, w.cx.p, S.params.maxiter);
-            else gmres_device<float>(S, B, kp, rhs, w.cx.p, S.params.maxiter);
-            masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, kp);
-            WB_CUDA(cudaMemcpyAsync(w.st_conv.p, B.conv.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToDevice, S.stream));
-            WB_CUDA(cudaMemcpyAsync(w.st_iters.p, B.iters.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToDevice, S.stream));
-        } else if (!S.mixed()) {
-            cg_device<double>(S, kp, rhs, w.cx.p, w.cr.p, w.dz.p, w.dp.p, w.dap.p, S.params.maxiter);
-            masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, kp);
-        } else {
-            convert_kernel<double, float><<<grid, kBlock, 0, S.stream>>>(rhs, w.frhs.p, m * kp);
-            cg_device<float>(S, kp, w.frhs.p, w.fx.p, w.fr.p, w.fz.p, w.fp.p, w.fap.p, S.params.maxiter);
-            masked_axpy_kernel<float><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.fx.p, w.st_part.p, m, kp);
-        }
-        WB_CUDA(cudaGetLastError());
-        S.gpu_launches += 2;
-        cv.assign(kp, 0);
-        it.assign(kp, 0);
-        WB_CUDA(cudaMemcpyAsync(cv.data(), w.st_conv.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
-        WB_CUDA(cudaMemcpyAsync(it.data(), w.st_iters.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
-        WB_CUDA(cudaStreamSynchronize(S.stream));
-    };
-    WB_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * m * kp, S.stream));
-    std::vector<int32_t> cv, it;
-    // FP64: initial solve + max_refinements corrections (solver.rs:215-216, 296-333).
-    // Mixed: FP32 inner solves to >= 1e-5 relative inside an FP64 refinement loop of up to
-    // max_refinements + 4 corrections, stopping when ||b - G x|| <= tol ||b||.
-    const int n_corr = S.mixed() ? S.params.max_refinements + 4 : S.params.max_refinements;
-    if (!S.mixed()) {
-        run_inner(w.b.p, part_of, tol, cv, it);
-        conv = cv;
-        iters = it;
-    }
-    std::vector<int32_t> done(kp, 0);
-    for (int c = k; c < kp; ++c) done[c] = 1;
-    for (int ref = 0; ref <= n_corr; ++ref) {
-        if (!S.mixed() && ref == n_corr) break;
-        const bool first_mixed = S.mixed() && ref == 0;
-        const double* rhs = w.b.p;
-        if (!first_mixed) {  // r = b - G x in FP64
-            cudaEvent_t e0 = nullptr;
-            S.prof_begin(e0);
-            launch_gram<double>(S, kp, S.w64.p, w.x.p, w.gx.p);
-            S.prof_end(0, e0);
+    if (S.params.krylov == WITHIN_KRYLOV_LSMR) {
+        // Solver::solve, LSMR branch (solver.rs:162-203): mlsmr on W^(1/2) D, FP64, no
+        // refinement; converged and iterations are LSMR's own
+        if (!S.lsmr) S.lsmr = std::make_shared<LsmrBufs>();
+        lsmr_device(S, *std::static_pointer_cast<LsmrBufs>(S.lsmr), kp, w.yi.p, w.x.p, part_of, conv, iters);
+    } else {
+        // One inner Krylov solve of G d = rhs on the RHS in `who` to relative tolerances tl,
+        // then x += d on those RHS.
+        auto run_inner = [&](const double* rhs, const std::vector<int32_t>& who, const std::vector<double>& tl,
+                             std::vector<int32_t>& cv, std::vector<int32_t>& it) {
+            WB_CUDA(cudaMemcpyAsync(w.st_part.p, who.data(), sizeof(int32_t) * kp, cudaMemcpyHostToDevice, S.stream));
+            WB_CUDA(cudaMemcpyAsync(w.st_tol.p, tl.data(), sizeof(double) * kp, cudaMemcpyHostToDevice, S.stream));
+            WB_CUDA(cudaMemsetAsync(w.st_conv.p, 0, sizeof(int32_t) * 32, S.stream));
             const int grid = S.nblk(m * kp, 1);
-            sub_kernel<<<grid, kBlock, 0, S.stream>>>(w.b.p, w.gx.p, w.r.p, m * kp);
+            if (S.params.krylov == WITHIN_KRYLOV_GMRES) {
+                if (!S.gmres) S.gmres = std::make_shared<GmresBufs>();
+                GmresBufs& B = *std::static_pointer_cast<GmresBufs>(S.gmres);
+                if (!S.mixed()) gmres_device<double>(S, B, kp, rhs, w.cx.p, S.params.maxiter);
+                else gmres_device<float>(S, B, kp, rhs, w.cx.p, S.params.maxiter);
+                masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, kp);
+                WB_CUDA(cudaMemcpyAsync(w.st_conv.p, B.conv.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToDevice, S.stream));
+                WB_CUDA(cudaMemcpyAsync(w.st_iters.p, B.iters.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToDevice, S.stream));
+            } else if (!S.mixed()) {
+                cg_device<double>(S, kp, rhs, w.cx.p, w.cr.p, w.dz.p, w.dp.p, w.dap.p, S.params.maxiter);
+                masked_axpy_kernel<double><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.cx.p, w.st_part.p, m, kp);
+            } else {
+                convert_kernel<double, float><<<grid, kBlock, 0, S.stream>>>(rhs, w.frhs.p, m * kp);
+                cg_device<float>(S, kp, w.frhs.p, w.fx.p, w.fr.p, w.fz.p, w.fp.p, w.fap.p, S.params.maxiter);
+                masked_axpy_kernel<float><<<grid, kBlock, 0, S.stream>>>(w.x.p, w.fx.p, w.st_part.p, m, kp);
+            }
             WB_CUDA(cudaGetLastError());
-            S.gpu_launches++;
-            rhs = w.r.p;
+            S.gpu_launches += 2;
+            cv.assign(kp, 0);
+            it.assign(kp, 0);
+            WB_CUDA(cudaMemcpyAsync(cv.data(), w.st_conv.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
+            WB_CUDA(cudaMemcpyAsync(it.data(), w.st_iters.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
+            WB_CUDA(cudaStreamSynchronize(S.stream));
+        };
+        WB_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * m * kp, S.stream));
+        std::vector<int32_t> cv, it;
+        // FP64: initial solve + max_refinements corrections (solver.rs:215-216, 296-333).
+        // Mixed: FP32 inner solves to >= 1e-5 relative inside an FP64 refinement loop of up to
+        // max_refinements + 4 corrections, stopping when ||b - G x|| <= tol ||b||.
+        const int n_corr = S.mixed() ? S.params.max_refinements + 4 : S.params.max_refinements;
+        if (!S.mixed()) {
+            run_inner(w.b.p, part_of, tol, cv, it);
+            conv = cv;
+            iters = it;
         }
-        launch_dot<double, double>(S, rhs, rhs, m, kp, w.part.p, nb);
-        std::vector<double> rr = host_reduce(S, nb, kp);
-        std::vector<int32_t> who(kp, 0);
-        std::vector<double> ctol(kp, 1.0);
-        int nwho = 0;
-        for (int c = 0; c < k; ++c) {
-            if (done[c]) continue;
-            const double cn = std::sqrt(rr[c]);
-            if (cn <= abs_tol[c]) { done[c] = 1; continue; }
-            ctol[c] = std::min(abs_tol[c] / cn, 1.0);  // corr_tol (solver.rs:319-320)
-            if (S.mixed()) ctol[c] = std::max(ctol[c], 1e-5);
-            who[c] = 1;
-            ++nwho;
+        std::vector<int32_t> done(kp, 0);
+        for (int c = k; c < kp; ++c) done[c] = 1;
+        for (int ref = 0; ref <= n_corr; ++ref) {
+            if (!S.mixed() && ref == n_corr) break;
+            const bool first_mixed = S.mixed() && ref == 0;
+            const double* rhs = w.b.p;
+            if (!first_mixed) {  // r = b - G x in FP64
+                cudaEvent_t e0 = nullptr;
+                S.prof_begin(e0);
+                launch_gram<double>(S, kp, S.w64.p, w.x.p, w.gx.p);
+                S.prof_end(0, e0);
+                const int grid = S.nblk(m * kp, 1);
+                sub_kernel<<<grid, kBlock, 0, S.stream>>>(w.b.p, w.gx.p, w.r.p, m * kp);
+                WB_CUDA(cudaGetLastError());
+                S.gpu_launches++;
+                rhs = w.r.p;
+            }
+            launch_dot<double, double>(S, rhs, rhs, m, kp, w.part.p, nb);
+            std::vector<double> rr = host_reduce(S, nb, kp);
+            std::vector<int32_t> who(kp, 0);
+            std::vector<double> ctol(kp, 1.0);
+            int nwho = 0;
+            for (int c = 0; c < k; ++c) {
+                if (done[c]) continue;
+                const double cn = std::sqrt(rr[c]);
+                if (cn <= abs_tol[c]) { done[c] = 1; continue; }
+                ctol[c] = std::min(abs_tol[c] / cn, 1.0);  // corr_tol (solver.rs:319-320)
+                if (S.mixed()) ctol[c] = std::max(ctol[c], 1e-5);
+                who[c] = 1;
+                ++nwho;
+            }
+            if (nwho == 0 || ref == n_corr) break;
+            run_inner(rhs, who, ctol, cv, it);
+            for (int c = 0; c < k; ++c)
+                if (who[c]) { iters[c] += it[c]; conv[c] = cv[c]; }
         }
-        if (nwho == 0 || ref == n_corr) break;
-        run_inner(rhs, who, ctol, cv, it);
-        for (int c = 0; c < k; ++c)
-            if (who[c]) { iters[c] += it[c]; conv[c] = cv[c]; }
-    }
-    if (S.mixed()) {
-        // converged when the FP64 residual met the tolerance
-        for (int c = 0; c < k; ++c) conv[c] = done[c] ? 1 : 0;
+        if (S.mixed()) {
+            // converged when the FP64 residual met the tolerance
+            for (int c = 0; c < k; ++c) conv[c] = done[c] ? 1 : 0;
+        }
     }
     // final demeaned e = y - D x and ||D'W e|| / ||b|| (solver.rs:222-227, 335-339)
     launch_obs<double, OBS_RESID>(S, kp, S.w64.p, w.x.p, w.yi.p, w.r.p, w.e.p);
@@ -1644,13 +2056,18 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
     within_default_params(&S->params);
     if (params) S->params = *params;
     const within_params& p = S->params;
-    if (p.krylov != WITHIN_KRYLOV_CG && p.krylov != WITHIN_KRYLOV_GMRES)
-        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "config must be CG or GMRES");
+    if (p.krylov != WITHIN_KRYLOV_CG && p.krylov != WITHIN_KRYLOV_GMRES && p.krylov != WITHIN_KRYLOV_LSMR)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "config must be CG, GMRES, or LSMR");
+    if (p.krylov == WITHIN_KRYLOV_LSMR && p.lsmr_local_size < 0)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "LSMR local_size must be >= 0");
     if (p.krylov == WITHIN_KRYLOV_GMRES && p.gmres_restart < 1)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "GMRES restart must be >= 1");
     if (precond && precond->kind == WITHIN_PRECOND_MULTIPLICATIVE && p.krylov == WITHIN_KRYLOV_CG)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT,
                         "CG requires a symmetric preconditioner; use 'additive' or switch to GMRES");
+    if (precond && precond->kind == WITHIN_PRECOND_MULTIPLICATIVE && p.krylov == WITHIN_KRYLOV_LSMR)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT,
+                        "LSMR requires a symmetric preconditioner; use 'additive' or switch to GMRES");
     if (p.operator_repr != WITHIN_OPERATOR_IMPLICIT && p.operator_repr != WITHIN_OPERATOR_EXPLICIT)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "operator must be Implicit or Explicit");
     if (p.precision != WITHIN_PRECISION_FP64 && p.precision != WITHIN_PRECISION_MIXED)
@@ -1774,6 +2191,7 @@ void within_default_params(within_params* p) {
     p->krylov = WITHIN_KRYLOV_CG;
     p->gmres_restart = 30;
     p->operator_repr = WITHIN_OPERATOR_IMPLICIT;
+    p->lsmr_local_size = 0;
     p->tol = 1e-8;
     p->maxiter = 1000;
     p->max_refinements = 2;
