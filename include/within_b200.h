@@ -182,6 +182,29 @@ int32_t within_solver_n_subdomains(const within_solver *solver);
 void within_solver_subdomain_info(const within_solver *solver, int32_t i, int64_t *info);
 void within_solver_subdomain_indices(const within_solver *solver, int32_t i, uint32_t *gidx,
                                      double *pou);
+/* Preconditioner persistence (FePreconditioner pickling and FePreconditioner(bytes),
+ * within-py/src/lib.rs:890-913; Solver::with_preconditioner, within/src/solver.rs:433-446).
+ * The bytes are this library's own format (magic "WB200PC", version, checksum); they
+ * hold the configuration, every subdomain with its local factor and, for multiplicative
+ * Schwarz, the explicit Gramian of its residual updates.  Reading rejects corrupted or
+ * inconsistent bytes with WITHIN_ERR_INVALID_ARGUMENT before anything reaches the GPU.
+ *
+ * preconditioner_bytes: with buf NULL, *len receives the size; otherwise buf (of *len
+ * bytes) receives the bytes.  WITHIN_ERR_INVALID_ARGUMENT when the solver has none.
+ * new_with_preconditioner: a solver on a design that reuses the preconditioner instead of
+ * building one (its dof count must equal the design's).
+ * preconditioner_from_bytes: a handle holding only the preconditioner; it supports
+ * apply_preconditioner, n_dofs, the subdomain queries and the diagnostics, and rejects
+ * solves and the operator applies.  Free it with within_solver_free.
+ * preconditioner_kind: 0 none, 1 additive, 2 multiplicative. */
+int within_solver_preconditioner_bytes(within_solver *solver, uint8_t *buf, size_t *len);
+int within_solver_new_with_preconditioner(const uint32_t *codes, size_t n_obs, size_t n_factors,
+                                          int64_t row_stride, int64_t col_stride, const double *weights,
+                                          const within_params *params, const uint8_t *data, size_t len,
+                                          within_solver **out);
+int within_preconditioner_from_bytes(const uint8_t *data, size_t len, within_solver **out);
+int32_t within_solver_preconditioner_kind(const within_solver *solver);
+
 /* FePreconditioner::subdomain_inner_parallel_work (within/src/operator/preconditioner.rs:64-79):
  * per subdomain, the work estimate of local_solver.rs:348-356 (2 nnz(C) + n_local when
  * the larger side has more than 10,000 rows, else 0).  work has n_subdomains entries. */

@@ -164,7 +164,7 @@ def _local_config(p: _lib.Precond, local) -> None:
 def _precond_struct(preconditioner):
     """extract_preconditioner_config (within-py/src/lib.rs:542-594)."""
     if isinstance(preconditioner, FePreconditioner):
-        return preconditioner._cfg
+        raise TypeError("a built FePreconditioner applies to one design: pass it to Solver(...)")
     p = _default_local()
     if preconditioner is None:
         return p
@@ -285,50 +285,94 @@ class AdditiveSchwarzDiagnostics:
 
 
 class FePreconditioner:
-    """Handle of a built preconditioner (within-py PyFePreconditioner, lib.rs:825-914).
+    """A built Schwarz preconditioner (within-py PyFePreconditioner, lib.rs:825-914).
 
-    It records the configuration it was built with; passing it back to
-    ``Solver(..., preconditioner=p)`` rebuilds the same factors (the build is
-    deterministic for a given design and seed).
+    Obtained from ``Solver.preconditioner()``, or rebuilt from bytes with
+    ``FePreconditioner(data)``, which is what ``pickle`` calls (``__reduce__``).  Passing
+    it to ``Solver(..., preconditioner=p)`` reuses its factors instead of building them
+    (``Solver::with_preconditioner``); the design must have the same number of dofs.  The
+    bytes are this library's own format (see ``within_solver_preconditioner_bytes``).
     """
 
-    def __init__(self, solver: "Solver"):
-        self._solver = solver
-        self._cfg = solver._pre
+    def __init__(self, data: bytes):
+        data = bytes(data)
+        h = C.c_void_p()
+        buf = (C.c_ubyte * len(data)).from_buffer_copy(data) if data else None
+        rc = _lib.load().within_preconditioner_from_bytes(buf, len(data), C.byref(h))
+        if rc != _lib.WITHIN_OK:
+            raise ValueError(_lib.last_error())
+        self._h, self._solver, self._own, self._data = h, None, True, data
+
+    @classmethod
+    def _of(cls, solver: "Solver") -> "FePreconditioner":
+        p = cls.__new__(cls)
+        p._h, p._solver, p._own, p._data = solver._h, solver, False, None
+        return p
+
+    def __del__(self):
+        if getattr(self, "_own", False) and getattr(self, "_h", None):
+            _lib.load().within_solver_free(self._h)
+            self._h = None
+
+    def _bytes(self) -> bytes:
+        if self._data is None:
+            L = _lib.load()
+            n = C.c_size_t(0)
+            _check(L.within_solver_preconditioner_bytes(self._h, None, C.byref(n)))
+            buf = (C.c_ubyte * n.value)()
+            _check(L.within_solver_preconditioner_bytes(self._h, buf, C.byref(n)))
+            self._data = bytes(buf)
+        return self._data
+
+    def __reduce__(self):
+        return (FePreconditioner, (self._bytes(),))
+
+    @property
+    def _kind(self) -> int:
+        return int(_lib.load().within_solver_preconditioner_kind(self._h))
 
     def apply(self, x) -> np.ndarray:
-        return self._solver._apply("within_solver_apply_preconditioner", x)
+        return _apply_handle(self._h, "within_solver_apply_preconditioner", x, self.nrows)
 
     @property
     def nrows(self) -> int:
-        return self._solver.n_dofs
+        return int(_lib.load().within_solver_n_dofs(self._h))
 
     @property
     def ncols(self) -> int:
-        return self._solver.n_dofs
+        return self.nrows
 
     @property
     def n_subdomains(self) -> int:
-        return int(_lib.load().within_solver_n_subdomains(self._solver._h))
+        return int(_lib.load().within_solver_n_subdomains(self._h))
 
     @property
     def subdomain_inner_parallel_work(self) -> list[int]:
         """Per-subdomain inner parallel work estimate (preconditioner.rs:64-79)."""
         work = np.zeros(self.n_subdomains, np.int64)
-        _lib.load().within_solver_subdomain_inner_work(self._solver._h, work)
+        _lib.load().within_solver_subdomain_inner_work(self._h, work)
         return [int(v) for v in work]
 
     def additive_schwarz_diagnostics(self) -> AdditiveSchwarzDiagnostics | None:
         """Diagnostics if this is an additive preconditioner, else None (preconditioner.rs:98-106)."""
-        if self._cfg.kind != 1:
+        if self._kind != 1:
             return None
         d = _lib.AdditiveDiagnostics()
-        _check(_lib.load().within_solver_additive_diagnostics(self._solver._h, 0, C.byref(d)))
+        _check(_lib.load().within_solver_additive_diagnostics(self._h, 0, C.byref(d)))
         return AdditiveSchwarzDiagnostics(d)
 
     def __repr__(self):
-        kind = {1: "Additive", 2: "Multiplicative"}.get(self._cfg.kind, "Off")
-        return f"FePreconditioner({kind}, n_subdomains={self.n_subdomains})"
+        kind = {1: "Additive", 2: "Multiplicative"}.get(self._kind, "Off")
+        return f"FePreconditioner({kind}, n={self.nrows})"
+
+
+def _apply_handle(h, fn, v, rows):
+    v = np.asarray(v, dtype=np.float64)
+    one = v.ndim == 1
+    V = np.asfortranarray(v.reshape(v.shape[0], -1))
+    out = np.empty((rows, V.shape[1]), order="F")
+    _check(getattr(_lib.load(), fn)(h, _lib.ptr(V), V.shape[1], _lib.ptr(out)))
+    return out[:, 0] if one else out
 
 
 class Solver:
@@ -339,8 +383,10 @@ class Solver:
         L = _lib.load()
         cats = _categories(categories)
         self._params = _params_struct(config)
-        self._pre = _precond_struct(preconditioner)
-        _validate(self._params, self._pre)
+        built = isinstance(preconditioner, FePreconditioner)
+        if not built:  # a built preconditioner skips the configuration checks (lib.rs:963-972)
+            self._pre = _precond_struct(preconditioner)
+            _validate(self._params, self._pre)
         n, q = cats.shape
         self._w = None
         if weights is not None:
@@ -349,9 +395,17 @@ class Solver:
                 raise WithinError(3, f"weights has length {self._w.shape[0] if self._w.ndim else 0}, expected {n}")
         isz = cats.itemsize
         h = C.c_void_p()
-        pre = None if self._pre.kind == 0 else C.byref(self._pre)
-        rc = L.within_solver_new(cats.ctypes.data_as(C.c_void_p), n, q, cats.strides[0] // isz,
-                                 cats.strides[1] // isz, _lib.ptr(self._w), C.byref(self._params), pre, C.byref(h))
+        if built:  # Solver::with_preconditioner (solver.rs:433-446)
+            data = preconditioner._bytes()
+            buf = (C.c_ubyte * len(data)).from_buffer_copy(data)
+            rc = L.within_solver_new_with_preconditioner(cats.ctypes.data_as(C.c_void_p), n, q, cats.strides[0] // isz,
+                                                         cats.strides[1] // isz, _lib.ptr(self._w),
+                                                         C.byref(self._params), buf, len(data), C.byref(h))
+        else:
+            pre = None if self._pre.kind == 0 else C.byref(self._pre)
+            rc = L.within_solver_new(cats.ctypes.data_as(C.c_void_p), n, q, cats.strides[0] // isz,
+                                     cats.strides[1] // isz, _lib.ptr(self._w), C.byref(self._params), pre,
+                                     C.byref(h))
         _check(rc)
         self._h = h
         self.n_obs, self.n_dofs, self.n_factors = n, int(L.within_solver_n_dofs(h)), q
@@ -393,17 +447,11 @@ class Solver:
                                 [float(st[c].time_solve) for c in range(k)], float(st[0].time_total) if k else 0.0)
 
     def preconditioner(self) -> FePreconditioner | None:
-        return None if self._pre.kind == 0 else FePreconditioner(self)
+        return None if _lib.load().within_solver_preconditioner_kind(self._h) == 0 else FePreconditioner._of(self)
 
     # --- operator access (kernel-level parity checks) ---
     def _apply(self, fn, v, out_rows=None):
-        v = np.asarray(v, dtype=np.float64)
-        one = v.ndim == 1
-        V = np.asfortranarray(v.reshape(v.shape[0], -1))
-        out_rows = out_rows or self.n_dofs
-        out = np.empty((out_rows, V.shape[1]), order="F")
-        _check(getattr(_lib.load(), fn)(self._h, _lib.ptr(V), V.shape[1], _lib.ptr(out)))
-        return out[:, 0] if one else out
+        return _apply_handle(self._h, fn, v, out_rows or self.n_dofs)
 
     def apply_gramian(self, x):
         return self._apply("within_solver_apply_gramian", x)

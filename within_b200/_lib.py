@@ -70,6 +70,8 @@ EXPORTED = [
     "within_solver_ac_arrays", "within_solver_gpu_launches", "within_solver_setup_time", "within_last_error",
     "within_solver_set_profiling", "within_solver_kernel_time", "within_solver_apply_gramian_noalloc",
     "within_solve_many", "within_solver_subdomain_inner_work", "within_solver_additive_diagnostics",
+    "within_solver_preconditioner_bytes", "within_solver_new_with_preconditioner",
+    "within_preconditioner_from_bytes", "within_solver_preconditioner_kind",
 ]
 
 _lib = None
@@ -112,6 +114,15 @@ def load():
     L.within_solver_n_subdomains.restype = C.c_int32
     L.within_solver_subdomain_info.argtypes = [vp, C.c_int32, _i64p]
     L.within_solver_subdomain_indices.argtypes = [vp, C.c_int32, _u32p, _f64p]
+    L.within_solver_preconditioner_bytes.argtypes = [vp, vp, C.POINTER(C.c_size_t)]
+    L.within_solver_preconditioner_bytes.restype = C.c_int
+    L.within_solver_new_with_preconditioner.argtypes = [vp, C.c_size_t, C.c_size_t, C.c_int64, C.c_int64, vp,
+                                                        C.POINTER(Params), vp, C.c_size_t, C.POINTER(vp)]
+    L.within_solver_new_with_preconditioner.restype = C.c_int
+    L.within_preconditioner_from_bytes.argtypes = [vp, C.c_size_t, C.POINTER(vp)]
+    L.within_preconditioner_from_bytes.restype = C.c_int
+    L.within_solver_preconditioner_kind.argtypes = [vp]
+    L.within_solver_preconditioner_kind.restype = C.c_int32
     L.within_solver_subdomain_inner_work.argtypes = [vp, _i64p]
     L.within_solver_additive_diagnostics.argtypes = [vp, C.c_int32, C.POINTER(AdditiveDiagnostics)]
     L.within_solver_additive_diagnostics.restype = C.c_int

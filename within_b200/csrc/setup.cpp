@@ -836,6 +836,200 @@ void build_explicit_gramian(const Design& d, std::vector<int64_t>& ptr, std::vec
     }
 }
 
+namespace {
+
+constexpr char kPcMagic[8] = {'W', 'B', '2', '0', '0', 'P', 'C', '\0'};
+constexpr uint32_t kPcVersion = 1;
+
+uint64_t fnv1a(const uint8_t* p, size_t n) {
+    uint64_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < n; ++i) { h ^= p[i]; h *= 1099511628211ull; }
+    return h;
+}
+
+struct Writer {
+    std::vector<uint8_t> b;
+    template <typename T> void put(T v) {
+        const uint8_t* p = reinterpret_cast<const uint8_t*>(&v);
+        b.insert(b.end(), p, p + sizeof(T));
+    }
+    template <typename T> void vec(const std::vector<T>& v) {
+        put<uint64_t>(v.size());
+        const uint8_t* p = reinterpret_cast<const uint8_t*>(v.data());
+        b.insert(b.end(), p, p + sizeof(T) * v.size());
+    }
+    void csr(const Csr& c) { put<int32_t>(c.nrows); put<int32_t>(c.ncols); vec(c.ptr); vec(c.idx); vec(c.val); }
+};
+
+struct Reader {
+    const uint8_t* p;
+    size_t left;
+    bool ok = true;
+    template <typename T> T get() {
+        T v{};
+        if (!ok || left < sizeof(T)) { ok = false; return v; }
+        std::memcpy(&v, p, sizeof(T));
+        p += sizeof(T);
+        left -= sizeof(T);
+        return v;
+    }
+    template <typename T> void vec(std::vector<T>& v) {
+        const uint64_t n = get<uint64_t>();
+        if (!ok || n > left / sizeof(T)) { ok = false; v.clear(); return; }
+        v.resize((size_t)n);
+        if (n) std::memcpy(v.data(), p, sizeof(T) * (size_t)n);
+        p += sizeof(T) * (size_t)n;
+        left -= sizeof(T) * (size_t)n;
+    }
+    void csr(Csr& c) { c.nrows = get<int32_t>(); c.ncols = get<int32_t>(); vec(c.ptr); vec(c.idx); vec(c.val); }
+};
+
+// CSR structure: rows + 1 non-decreasing pointers from 0 to nnz, columns below ncols.
+bool csr_valid(const Csr& c) {
+    if (c.nrows < 0 || c.ncols < 0 || c.ptr.size() != (size_t)c.nrows + 1 || c.ptr[0] != 0) return false;
+    for (int32_t i = 0; i < c.nrows; ++i)
+        if (c.ptr[i + 1] < c.ptr[i]) return false;
+    if ((size_t)c.ptr[c.nrows] != c.idx.size() || c.idx.size() != c.val.size()) return false;
+    for (uint32_t j : c.idx)
+        if ((int64_t)j >= c.ncols) return false;
+    return true;
+}
+template <typename I> bool ptr_valid(const std::vector<I>& ptr, size_t rows, size_t total) {
+    if (ptr.size() != rows + 1 || ptr[0] != 0) return false;
+    for (size_t i = 0; i < rows; ++i)
+        if (ptr[i + 1] < ptr[i]) return false;
+    return (size_t)ptr[rows] == total;
+}
+template <typename I> bool all_below(const std::vector<I>& v, int64_t bound) {
+    for (I x : v)
+        if ((int64_t)x < 0 || (int64_t)x >= bound) return false;
+    return true;
+}
+
+// Everything the device layout is built from (build_stage) indexes within its arrays.
+std::string subdomain_invalid(const Subdomain& sd, int64_t ndofs) {
+    const int64_t nq = sd.ct.c.nrows, nr = sd.ct.c.ncols;
+    if (sd.q < 0 || sd.r <= sd.q || sd.r >= 64) return "factor pair";
+    if (!csr_valid(sd.ct.c) || !csr_valid(sd.ct.ct) || sd.ct.ct.nrows != nr || sd.ct.ct.ncols != nq)
+        return "cross-tab structure";
+    if (sd.ct.c.idx.size() != sd.ct.ct.idx.size()) return "cross-tab transpose size";
+    if ((int64_t)sd.gidx.size() != nq + nr || !all_below(sd.gidx, ndofs)) return "global indices";
+    if (!sd.pou.empty() && (int64_t)sd.pou.size() != nq + nr) return "partition-of-unity weights";
+    if ((int64_t)sd.ct.dq.size() != nq || (int64_t)sd.ct.dr.size() != nr) return "cross-tab diagonals";
+    const int64_t n_keep = sd.elim_q ? nr : nq, n_elim = sd.elim_q ? nq : nr;
+    if ((int64_t)sd.inv_diag.size() != n_elim) return "eliminated-block diagonal";
+    if (sd.n_red != n_keep) return "reduced size";
+    if (sd.kind == 0) {
+        const int64_t m1 = n_keep >= 1 ? n_keep - 1 : 0;
+        if ((int64_t)sd.L.size() != m1 * m1) return "dense factor size";
+    } else if (sd.kind == 1) {
+        const AcFactor& f = sd.ac;
+        if (f.n != n_keep || f.nlev < 0 || f.ncol < 0 || f.ncore < 0 || f.ncore > kAcCoreMax) return "factor sizes";
+        if (!ptr_valid(f.level_ptr, (size_t)f.nlev, (size_t)f.ncol)) return "factor levels";
+        if (f.col_vertex.size() != (size_t)f.ncol || f.col_diag.size() != (size_t)f.ncol || !all_below(f.col_vertex, f.n))
+            return "factor columns";
+        if (!ptr_valid(f.col_ptr, (size_t)f.ncol, f.col_idx.size()) || f.col_idx.size() != f.col_coef.size() ||
+            !all_below(f.col_idx, f.n))
+            return "factor entries";
+        if (f.core_vertex.size() != (size_t)f.ncore || !all_below(f.core_vertex, f.n) ||
+            f.core_z.size() != (size_t)f.ncore * (size_t)f.ncore)
+            return "factor core";
+    } else {
+        return "local solver kind";
+    }
+    return {};
+}
+
+}  // namespace
+
+std::vector<uint8_t> serialize_preconditioner(const PrecondImage& img, const std::vector<Subdomain>& subs) {
+    Writer w;
+    for (char c : kPcMagic) w.put<char>(c);
+    w.put<uint32_t>(kPcVersion);
+    w.put<int64_t>(img.ndofs);
+    w.put<int32_t>(img.kind);
+    w.put<int32_t>(img.reduction);
+    w.put<uint64_t>(img.cfg.ac_seed);
+    w.put<uint32_t>(img.cfg.ac_split);
+    w.put<int32_t>(img.cfg.approx_schur ? 1 : 0);
+    w.put<uint64_t>(img.cfg.schur_seed);
+    w.put<uint32_t>(img.cfg.schur_split);
+    w.put<int32_t>(img.cfg.dense_threshold);
+    w.put<uint64_t>(subs.size());
+    for (const Subdomain& sd : subs) {
+        w.put<int32_t>(sd.q); w.put<int32_t>(sd.r); w.put<int32_t>(sd.elim_q ? 1 : 0);
+        w.put<int32_t>(sd.kind); w.put<int32_t>(sd.n_red);
+        w.vec(sd.gidx); w.vec(sd.pou);
+        w.csr(sd.ct.c); w.csr(sd.ct.ct);
+        w.vec(sd.ct.dq); w.vec(sd.ct.dr); w.vec(sd.inv_diag); w.vec(sd.L);
+        const AcFactor& f = sd.ac;
+        w.put<int32_t>(f.n); w.put<int32_t>(f.nlev); w.put<int32_t>(f.ncol); w.put<int32_t>(f.ncore);
+        w.vec(f.level_ptr); w.vec(f.col_vertex); w.vec(f.col_ptr); w.vec(f.col_idx);
+        w.vec(f.col_diag); w.vec(f.col_coef); w.vec(f.core_vertex); w.vec(f.core_z);
+    }
+    w.vec(img.g_ptr); w.vec(img.g_idx); w.vec(img.g_val);
+    w.put<uint64_t>(fnv1a(w.b.data(), w.b.size()));
+    return std::move(w.b);
+}
+
+Status deserialize_preconditioner(const uint8_t* data, size_t len, PrecondImage& img) {
+    Status st;
+    auto bad = [&](const std::string& what) {
+        st.code = WITHIN_ERR_INVALID_ARGUMENT;
+        st.msg = "failed to deserialize preconditioner: " + what;
+        return st;
+    };
+    if (!data || len < sizeof(kPcMagic) + sizeof(uint32_t) + sizeof(uint64_t)) return bad("too short");
+    if (std::memcmp(data, kPcMagic, sizeof(kPcMagic)) != 0) return bad("not a serialized preconditioner");
+    uint64_t sum = 0;
+    std::memcpy(&sum, data + len - sizeof(uint64_t), sizeof(uint64_t));
+    if (sum != fnv1a(data, len - sizeof(uint64_t))) return bad("checksum mismatch (corrupted bytes)");
+    Reader r{data + sizeof(kPcMagic), len - sizeof(kPcMagic) - sizeof(uint64_t)};
+    if (r.get<uint32_t>() != kPcVersion) return bad("unsupported version");
+    img.ndofs = r.get<int64_t>();
+    img.kind = r.get<int32_t>();
+    img.reduction = r.get<int32_t>();
+    img.cfg.kind = img.kind;
+    img.cfg.ac_seed = r.get<uint64_t>();
+    img.cfg.ac_split = r.get<uint32_t>();
+    img.cfg.approx_schur = r.get<int32_t>() != 0;
+    img.cfg.schur_seed = r.get<uint64_t>();
+    img.cfg.schur_split = r.get<uint32_t>();
+    img.cfg.dense_threshold = r.get<int32_t>();
+    const uint64_t nsub = r.get<uint64_t>();
+    if (!r.ok) return bad("truncated header");
+    if (img.ndofs <= 0 || img.ndofs > 0xFFFFFFFFll) return bad("dof count");
+    if (img.kind != 1 && img.kind != 2) return bad("preconditioner kind");
+    if (img.reduction < 0 || img.reduction > 2) return bad("reduction strategy");
+    if (nsub > r.left / 64) return bad("subdomain count");
+    img.subs.resize((size_t)nsub);
+    for (uint64_t i = 0; i < nsub; ++i) {
+        Subdomain& sd = img.subs[i];
+        sd.q = r.get<int32_t>(); sd.r = r.get<int32_t>(); sd.elim_q = r.get<int32_t>() != 0;
+        sd.kind = r.get<int32_t>(); sd.n_red = r.get<int32_t>();
+        r.vec(sd.gidx); r.vec(sd.pou);
+        r.csr(sd.ct.c); r.csr(sd.ct.ct);
+        r.vec(sd.ct.dq); r.vec(sd.ct.dr); r.vec(sd.inv_diag); r.vec(sd.L);
+        AcFactor& f = sd.ac;
+        f.n = r.get<int32_t>(); f.nlev = r.get<int32_t>(); f.ncol = r.get<int32_t>(); f.ncore = r.get<int32_t>();
+        r.vec(f.level_ptr); r.vec(f.col_vertex); r.vec(f.col_ptr); r.vec(f.col_idx);
+        r.vec(f.col_diag); r.vec(f.col_coef); r.vec(f.core_vertex); r.vec(f.core_z);
+        if (!r.ok) return bad("truncated subdomain " + std::to_string(i));
+        const std::string why = subdomain_invalid(sd, img.ndofs);
+        if (!why.empty()) return bad("subdomain " + std::to_string(i) + ": " + why);
+    }
+    r.vec(img.g_ptr); r.vec(img.g_idx); r.vec(img.g_val);
+    if (!r.ok || r.left != 0) return bad("trailing or truncated data");
+    if (img.kind == 2) {
+        if (!ptr_valid(img.g_ptr, (size_t)img.ndofs, img.g_idx.size()) || img.g_idx.size() != img.g_val.size() ||
+            !all_below(img.g_idx, img.ndofs))
+            return bad("explicit Gramian");
+    } else if (!img.g_ptr.empty() || !img.g_idx.empty() || !img.g_val.empty()) {
+        return bad("explicit Gramian of an additive preconditioner");
+    }
+    return st;
+}
+
 // A subdomain's local solve goes inner-parallel in the reference only when its larger
 // side has more rows than both parallel thresholds (PAR_BACKSUB_THRESHOLD,
 // local_solver.rs:78, and PAR_SPMV_THRESHOLD, csr_block.rs:4: 10,000 each); its work is

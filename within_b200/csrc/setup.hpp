@@ -105,6 +105,27 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
 void build_explicit_gramian(const Design& d, std::vector<int64_t>& ptr, std::vector<uint32_t>& idx,
                             std::vector<double>& val);
 
+// A built preconditioner as bytes (FePreconditioner pickling, within-py/src/lib.rs:890-913):
+// the configuration, the subdomains with their local factors and, for multiplicative
+// Schwarz, the explicit Gramian of its residual updates.  The format is this library's
+// own: magic "WB200PC\0", a version, little-endian fields, length-prefixed arrays, an
+// FNV-1a 64 checksum at the end.  Reading validates every count against the bytes left
+// and every index against the sizes it addresses, so that nothing built from the bytes
+// can address outside its arrays.
+struct PrecondImage {
+    int64_t ndofs = 0;
+    int32_t kind = 1;       // 1 additive, 2 multiplicative
+    int32_t reduction = 0;  // ReductionStrategy as configured
+    PrecondConfig cfg;
+    std::vector<Subdomain> subs;
+    std::vector<int64_t> g_ptr;  // multiplicative only
+    std::vector<uint32_t> g_idx;
+    std::vector<double> g_val;
+};
+// img's subdomains are ignored in favour of `subs` (so that a solver's need not be copied).
+std::vector<uint8_t> serialize_preconditioner(const PrecondImage& img, const std::vector<Subdomain>& subs);
+Status deserialize_preconditioner(const uint8_t* data, size_t len, PrecondImage& img);
+
 // LocalSolver::inner_parallelism_work_estimate of a block-elimination subdomain
 // (within/src/operator/local_solver.rs:348-356).
 int64_t inner_parallel_work(const Subdomain& sd);

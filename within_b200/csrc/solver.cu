@@ -367,6 +367,8 @@ struct SolverImpl {
     DArr<double> host_y, host_x, host_dem;  // device side of the host-buffer entry points
     std::shared_ptr<void> gmres;  // GmresBufs, created on first GMRES solve
     std::shared_ptr<void> lsmr;   // LsmrBufs, created on first LSMR solve
+    bool precond_only = false;    // built from a serialized preconditioner: no design
+    std::vector<uint8_t> pc_bytes;  // serialized preconditioner, made on first request
     int32_t* h_active = nullptr;  // pinned
     double setup_time = 0.0;
     int64_t gpu_launches = 0;
@@ -2048,9 +2050,69 @@ int guard(const std::function<int()>& f) {
     }
 }
 
+// Device attributes, the solver's stream and its pinned status word.
+void init_device(SolverImpl& S) {
+    int dev = 0;
+    WB_CUDA(cudaGetDevice(&dev));
+    WB_CUDA(cudaDeviceGetAttribute(&S.n_sm, cudaDevAttrMultiProcessorCount, dev));
+    int coop = 0;
+    WB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    S.coop = coop != 0;
+    WB_CUDA(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
+    WB_CUDA(cudaMallocHost(&S.h_active, sizeof(int32_t)));
+}
+
+// The device stages of the Schwarz preconditioner from the host subdomains: one stage of
+// all subdomains (additive), or one per factor pair (multiplicative).
+void build_precond_stages(SolverImpl& S) {
+    if (S.pc.kind == 0 || S.subs.empty()) return;
+    std::vector<std::vector<int32_t>> groups;
+    if (S.pc.kind == 1) {
+        groups.emplace_back(S.subs.size());
+        std::iota(groups[0].begin(), groups[0].end(), 0);
+    } else {
+        for (int32_t i = 0; i < (int32_t)S.subs.size(); ++i) {
+            if (groups.empty() || S.subs[groups.back()[0]].q != S.subs[i].q || S.subs[groups.back()[0]].r != S.subs[i].r)
+                groups.emplace_back();
+            groups.back().push_back(i);
+        }
+    }
+    for (auto& g : groups) {
+        const wb::StageHost h = wb::build_stage(S.subs, g, S.d.ndofs, S.pc.kind == 1);
+        S.max_nsub = std::max(S.max_nsub, h.nsub);
+        S.max_slots = std::max(S.max_slots, h.nslots);
+        S.max_core_total = std::max(S.max_core_total, (int64_t)h.core_slot.size());
+        S.stages64.emplace_back();
+        wb::upload_stage(S.stages64.back(), h);
+        if (S.mixed()) {
+            S.stages32.emplace_back();
+            wb::upload_stage(S.stages32.back(), h);
+        }
+    }
+}
+
+// The assembled Gramian on the device, with its row chunks for the explicit operator.
+void install_gramian(SolverImpl& S, const std::vector<int64_t>& gp, const std::vector<uint32_t>& gi,
+                     const std::vector<double>& gv) {
+    S.g_ptr.upload(gp);
+    S.g_idx.upload(gi);
+    S.g_val64.upload(gv);
+    if (S.mixed()) S.g_val32.upload_cast(gv);
+    const int64_t m = S.d.ndofs;
+    std::vector<uint32_t> rows((size_t)m);
+    std::iota(rows.begin(), rows.end(), 0u);
+    S.g_rows.upload(rows);
+    const std::vector<wb::CsrChunk> ch = wb::make_chunks(gp, 0, m, 256, 1, true);
+    S.g_chunks.upload(ch);
+    S.g_nchunks = (int64_t)ch.size();
+    S.explicit_op = true;
+}
+
+// img: a deserialized preconditioner to use instead of building one (Solver::with_preconditioner,
+// solver.rs:433-446, from_design_with_preconditioner :137-154).
 int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t row_stride, int64_t col_stride,
                  const double* weights, const within_params* params, const within_preconditioner* precond,
-                 std::unique_ptr<SolverImpl>& out) {
+                 std::unique_ptr<SolverImpl>& out, wb::PrecondImage* img = nullptr) {
     const double t0 = wb::now_s();
     auto S = std::make_unique<SolverImpl>();
     within_default_params(&S->params);
@@ -2088,71 +2150,41 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
             return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "reduction strategy must be 0 (Auto), 1 (AtomicScatter) or 2 (ParallelReduction)");
         S->reduction_strategy = precond->reduction_strategy;
     }
+    if (img) {
+        if (img->ndofs != S->d.ndofs)
+            return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the preconditioner has " + std::to_string(img->ndofs) +
+                                                             " dofs, the design has " + std::to_string(S->d.ndofs));
+        S->pc = img->cfg;
+        S->pc.kind = img->kind;
+        S->reduction_strategy = img->reduction;
+        S->subs = std::move(img->subs);
+    }
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
         return wb::fail(WITHIN_ERR_CUDA, "no CUDA device is available (the solve phase has no CPU path)");
     // the subdomains and their factors (host) are built while the design goes to the device
     std::future<wb::Status> subs_job;
-    if (S->pc.kind != 0)
+    if (S->pc.kind != 0 && !img)
         subs_job = std::async(std::launch::async, [&S]() { return wb::build_subdomains(S->d, S->pc, S->subs); });
-    int dev = 0;
-    WB_CUDA(cudaGetDevice(&dev));
-    WB_CUDA(cudaDeviceGetAttribute(&S->n_sm, cudaDevAttrMultiProcessorCount, dev));
-    int coop = 0;
-    WB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-    S->coop = coop != 0;
-    WB_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
-    WB_CUDA(cudaMallocHost(&S->h_active, sizeof(int32_t)));
+    init_device(*S);
     wb::upload_design(*S);
     if (subs_job.valid()) {
         st = subs_job.get();
         if (!st.ok()) return wb::fail(st.code, st.msg);
     }
-    if (S->pc.kind != 0 && !S->subs.empty()) {
-        std::vector<std::vector<int32_t>> groups;
-        if (S->pc.kind == 1) {
-            groups.emplace_back(S->subs.size());
-            std::iota(groups[0].begin(), groups[0].end(), 0);
-        } else {
-            for (int32_t i = 0; i < (int32_t)S->subs.size(); ++i) {
-                if (groups.empty() || S->subs[groups.back()[0]].q != S->subs[i].q ||
-                    S->subs[groups.back()[0]].r != S->subs[i].r)
-                    groups.emplace_back();
-                groups.back().push_back(i);
-            }
-        }
-        for (auto& g : groups) {
-            const wb::StageHost h = wb::build_stage(S->subs, g, S->d.ndofs, S->pc.kind == 1);
-            S->max_nsub = std::max(S->max_nsub, h.nsub);
-            S->max_slots = std::max(S->max_slots, h.nslots);
-            S->max_core_total = std::max(S->max_core_total, (int64_t)h.core_slot.size());
-            S->stages64.emplace_back();
-            wb::upload_stage(S->stages64.back(), h);
-            if (S->mixed()) {
-                S->stages32.emplace_back();
-                wb::upload_stage(S->stages32.back(), h);
-            }
-        }
-    }
+    build_precond_stages(*S);
     // the assembled Gramian (solver.rs:103-121): for an explicit operator, and for the
     // multiplicative residual updates, which then also use it as the Krylov operator
     if (p.operator_repr == WITHIN_OPERATOR_EXPLICIT || S->pc.kind == 2) {
-        std::vector<int64_t> gp;
-        std::vector<uint32_t> gi;
-        std::vector<double> gv;
-        wb::build_explicit_gramian(S->d, gp, gi, gv);
-        S->g_ptr.upload(gp);
-        S->g_idx.upload(gi);
-        S->g_val64.upload(gv);
-        if (S->mixed()) S->g_val32.upload_cast(gv);
-        const int64_t m = S->d.ndofs;
-        std::vector<uint32_t> rows((size_t)m);
-        std::iota(rows.begin(), rows.end(), 0u);
-        S->g_rows.upload(rows);
-        const std::vector<wb::CsrChunk> ch = wb::make_chunks(gp, 0, m, 256, 1, true);
-        S->g_chunks.upload(ch);
-        S->g_nchunks = (int64_t)ch.size();
-        S->explicit_op = true;
+        if (img && !img->g_ptr.empty()) {
+            install_gramian(*S, img->g_ptr, img->g_idx, img->g_val);
+        } else {
+            std::vector<int64_t> gp;
+            std::vector<uint32_t> gi;
+            std::vector<double> gv;
+            wb::build_explicit_gramian(S->d, gp, gi, gv);
+            install_gramian(*S, gp, gi, gv);
+        }
     }
     WB_CUDA(cudaStreamSynchronize(S->stream));
     S->setup_time = wb::now_s() - t0;
@@ -2160,7 +2192,31 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
     return WITHIN_OK;
 }
 
+// A handle that holds only a deserialized preconditioner (FePreconditioner::new from
+// bytes, within-py/src/lib.rs:903-913): its apply, sizes and diagnostics, no design.
+int build_precond_only(wb::PrecondImage& img, std::unique_ptr<SolverImpl>& out) {
+    auto S = std::make_unique<SolverImpl>();
+    within_default_params(&S->params);
+    S->precond_only = true;
+    S->d.ndofs = img.ndofs;
+    S->pc = img.cfg;
+    S->pc.kind = img.kind;
+    S->reduction_strategy = img.reduction;
+    S->subs = std::move(img.subs);
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        return wb::fail(WITHIN_ERR_CUDA, "no CUDA device is available (the solve phase has no CPU path)");
+    init_device(*S);
+    build_precond_stages(*S);
+    if (S->pc.kind == 2) install_gramian(*S, img.g_ptr, img.g_idx, img.g_val);
+    WB_CUDA(cudaStreamSynchronize(S->stream));
+    out = std::move(S);
+    return WITHIN_OK;
+}
+
 int solve_device(SolverImpl& S, const double* d_ys, size_t k, double* d_x, double* d_dem, within_solve_stats* stats) {
+    if (S.precond_only)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "this handle holds only a preconditioner; build a Solver to solve");
     const int64_t n = S.d.n, m = S.d.ndofs;
     for (size_t c0 = 0; c0 < k; c0 += 32) {
         const int kc = (int)std::min<size_t>(32, k - c0);
@@ -2208,6 +2264,75 @@ void within_default_preconditioner(within_preconditioner* p) {
     p->dense_threshold = 24;
     p->reduction_strategy = 0;
 }
+
+int within_solver_new_with_preconditioner(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t row_stride,
+                                          int64_t col_stride, const double* weights, const within_params* params,
+                                          const uint8_t* data, size_t len, within_solver** out) {
+    if (!out) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "out pointer is null");
+    *out = nullptr;
+    return guard([&]() -> int {
+        wb::PrecondImage img;
+        const wb::Status st = wb::deserialize_preconditioner(data, len, img);
+        if (!st.ok()) return wb::fail(st.code, st.msg);
+        std::unique_ptr<SolverImpl> S;
+        const int rc = build_solver(codes, n_obs, n_factors, row_stride, col_stride, weights, params, nullptr, S, &img);
+        if (rc != WITHIN_OK) return rc;
+        *out = new within_solver{std::move(S)};
+        return WITHIN_OK;
+    });
+}
+
+int within_preconditioner_from_bytes(const uint8_t* data, size_t len, within_solver** out) {
+    if (!out) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "out pointer is null");
+    *out = nullptr;
+    return guard([&]() -> int {
+        wb::PrecondImage img;
+        const wb::Status st = wb::deserialize_preconditioner(data, len, img);
+        if (!st.ok()) return wb::fail(st.code, st.msg);
+        std::unique_ptr<SolverImpl> S;
+        const int rc = build_precond_only(img, S);
+        if (rc != WITHIN_OK) return rc;
+        *out = new within_solver{std::move(S)};
+        return WITHIN_OK;
+    });
+}
+
+int within_solver_preconditioner_bytes(within_solver* s, uint8_t* buf, size_t* len) {
+    if (!s || !len) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "solver and len must not be null");
+    SolverImpl& S = *s->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    return guard([&]() -> int {
+        if (S.pc.kind == 0) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the solver has no preconditioner");
+        if (S.pc_bytes.empty()) {
+            wb::PrecondImage img;
+            img.ndofs = S.d.ndofs;
+            img.kind = S.pc.kind;
+            img.reduction = S.reduction_strategy;
+            img.cfg = S.pc;
+            if (S.pc.kind == 2) {  // the residual updater's Gramian, from the device copy
+                img.g_ptr.resize(S.g_ptr.n);
+                img.g_idx.resize(S.g_idx.n);
+                img.g_val.resize(S.g_val64.n);
+                WB_CUDA(cudaMemcpy(img.g_ptr.data(), S.g_ptr.p, sizeof(int64_t) * S.g_ptr.n, cudaMemcpyDeviceToHost));
+                WB_CUDA(cudaMemcpy(img.g_idx.data(), S.g_idx.p, sizeof(uint32_t) * S.g_idx.n, cudaMemcpyDeviceToHost));
+                WB_CUDA(cudaMemcpy(img.g_val.data(), S.g_val64.p, sizeof(double) * S.g_val64.n, cudaMemcpyDeviceToHost));
+            }
+            S.pc_bytes = wb::serialize_preconditioner(img, S.subs);
+        }
+        const size_t need = S.pc_bytes.size();
+        if (buf) {
+            if (*len < need) {
+                *len = need;
+                return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "buffer too small for the serialized preconditioner");
+            }
+            std::memcpy(buf, S.pc_bytes.data(), need);
+        }
+        *len = need;
+        return WITHIN_OK;
+    });
+}
+
+int32_t within_solver_preconditioner_kind(const within_solver* s) { return s ? (int32_t)s->impl->pc.kind : 0; }
 
 int within_solver_new(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t row_stride, int64_t col_stride,
                       const double* weights, const within_params* params, const within_preconditioner* precond,
@@ -2321,6 +2446,8 @@ static int apply_common(within_solver* s, const double* in, size_t k, double* ou
     return guard([&]() -> int {
         if (k == 0) return WITHIN_OK;
         if (k > 32) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "at most 32 vectors per call");
+        if (S.precond_only && which != 1)
+            return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "this handle holds only a preconditioner");
         const int kk = (int)k, kp = wb::pad_kp(kk);
         wb::ensure_ws(S, kp);
         const size_t n = (size_t)S.d.n, m = (size_t)S.d.ndofs;
