@@ -3,6 +3,7 @@
 #include "setup.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <future>
@@ -726,10 +727,34 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
     // Pairs (q < r) in lexicographic order (factor_pairs.rs:252-260); components in
     // order; indices q-levels then r-levels (:244-250).  The pairs are independent and
     // built concurrently (each pair's arithmetic is unchanged), then appended in order.
+    // A pair's local factors (which do not depend on the partition of unity) are built
+    // as soon as its subdomains exist: the large ones on threads of their own, the rest
+    // on the pair's thread.
     std::vector<std::pair<int, int>> pairs;
     for (int q = 0; q < d.Q; ++q)
         for (int r = q + 1; r < d.Q; ++r) pairs.emplace_back(q, r);
     std::vector<std::vector<Subdomain>> per_pair(pairs.size());
+    std::vector<std::vector<Status>> per_status(pairs.size());
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<unsigned> busy{(unsigned)std::min<size_t>(pairs.size(), hw)};
+    auto factor_pair = [&](size_t p) {
+        std::vector<Subdomain>& v = per_pair[p];
+        std::vector<Status>& status = per_status[p];
+        status.assign(v.size(), Status{});
+        std::vector<std::future<void>> jobs;
+        for (size_t i = 0; i < v.size(); ++i) {
+            if (v[i].n_local() > 4096 && busy.fetch_add(1) < hw) {
+                jobs.push_back(std::async(std::launch::async, [&, i] {
+                    status[i] = build_local_factor(v[i], cfg);
+                    busy.fetch_sub(1);
+                }));
+            } else {
+                if (v[i].n_local() > 4096) busy.fetch_sub(1);
+                status[i] = build_local_factor(v[i], cfg);
+            }
+        }
+        for (auto& j : jobs) j.get();
+    };
     auto build_pair = [&](size_t p) {
         const int q = pairs[p].first, r = pairs[p].second;
         CrossTab full;
@@ -747,16 +772,19 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
             sd.ct = comps.size() == 1 ? std::move(full) : extract(full, comps[c]);
             per_pair[p].push_back(std::move(sd));
         }
+        factor_pair(p);
     };
     {
-        const size_t hw_pairs = std::max(1u, std::thread::hardware_concurrency());
         std::vector<std::future<void>> pj;
         for (size_t p = 0; p < pairs.size(); ++p) {
-            if (pj.size() + 1 < hw_pairs && p + 1 < pairs.size()) pj.push_back(std::async(std::launch::async, build_pair, p));
+            if (pj.size() + 1 < hw && p + 1 < pairs.size()) pj.push_back(std::async(std::launch::async, build_pair, p));
             else build_pair(p);
         }
         for (auto& j : pj) j.get();
     }
+    for (const auto& v : per_status)
+        for (const Status& st : v)
+            if (!st.ok()) return st;
     for (auto& v : per_pair)
         for (auto& sd : v) subs.push_back(std::move(sd));
     // Partition-of-unity weights (compute_partition_weights, factor_pairs.rs:272-304).
@@ -771,20 +799,6 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
             for (size_t a = 0; a < sd.gidx.size(); ++a) sd.pou[a] = 1.0 / std::sqrt((double)count[sd.gidx[a]]);
         }
     }
-    // Local factors: independent per subdomain; large ones on worker threads.
-    std::vector<Status> status(subs.size());
-    std::vector<std::future<void>> jobs;
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    for (size_t i = 0; i < subs.size(); ++i) {
-        if (subs[i].n_local() > 4096 && jobs.size() + 1 < hw) {
-            jobs.push_back(std::async(std::launch::async, [&, i] { status[i] = build_local_factor(subs[i], cfg); }));
-        } else {
-            status[i] = build_local_factor(subs[i], cfg);
-        }
-    }
-    for (auto& j : jobs) j.get();
-    for (const Status& s : status)
-        if (!s.ok()) return s;
     return {};
 }
 

@@ -67,62 +67,144 @@ std::vector<CsrChunk> make_chunks(const std::vector<int64_t>& ptr, int64_t row_l
     return out;
 }
 
-// Flatten the subdomains `ids` into one stage (see StageHost and kernels.cuh).
+// Runs fn(t) for t in [0, ntasks) on up to one thread per host core.
+void parallel_tasks(size_t ntasks, const std::function<void(size_t)>& fn) {
+    const size_t nt = std::min<size_t>(ntasks, std::max(1u, std::thread::hardware_concurrency()));
+    if (nt <= 1) {
+        for (size_t t = 0; t < ntasks; ++t) fn(t);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+        for (size_t t; (t = next.fetch_add(1)) < ntasks;) fn(t);
+    };
+    std::vector<std::thread> th;
+    for (size_t i = 1; i < nt; ++i) th.emplace_back(worker);
+    worker();
+    for (auto& x : th) x.join();
+}
+
+// Flatten the subdomains `ids` into one stage (see StageHost and kernels.cuh).  The
+// per-slot arrays, the keep rows and the back-substitution rows are sized first and then
+// filled in parallel over ranges of slots and rows (every range writes its own part, with
+// the same arithmetic as a sequential fill); the dense and AC factors follow in order.
 StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int32_t>& ids, int64_t ndofs,
                       bool with_gather) {
     StageHost st;
     st.nsub = (int32_t)ids.size();
+    const int32_t ns = st.nsub;
     std::vector<std::vector<std::pair<uint32_t, std::vector<std::pair<uint32_t, double>>>>> afwd;
     std::vector<std::vector<std::tuple<uint32_t, double, std::vector<std::pair<uint32_t, double>>>>> abwd;
-    int64_t o = 0;
-    for (int32_t si = 0; si < st.nsub; ++si) {
+    // offsets per subdomain: slots, keep rows, keep entries, back-substitution entries
+    std::vector<int64_t> so(ns + 1, 0), kro(ns + 1, 0), kno(ns + 1, 0), bno(ns + 1, 0);
+    auto k2e_of = [&](const Subdomain& sd) -> const Csr& { return sd.elim_q ? sd.ct.ct : sd.ct.c; };
+    auto e2k_of = [&](const Subdomain& sd) -> const Csr& { return sd.elim_q ? sd.ct.c : sd.ct.ct; };
+    for (int32_t si = 0; si < ns; ++si) {
+        const Subdomain& sd = subs[ids[si]];
+        so[si + 1] = so[si] + sd.n_local();
+        kro[si + 1] = kro[si] + (sd.elim_q ? sd.n_r() : sd.n_q());
+        kno[si + 1] = kno[si] + k2e_of(sd).nnz();
+        bno[si + 1] = bno[si] + e2k_of(sd).nnz();
+    }
+    const int64_t nslots = so[ns], nkeep = kro[ns];
+    st.sub_nloc.resize(ns);
+    st.sub_nkeep.resize(ns);
+    st.sub_I.resize(ns);
+    st.gidx.resize(nslots);
+    st.sub_of.resize(nslots);
+    st.spou.resize(nslots);
+    st.invd.assign(nslots, 0.0);
+    st.keep_slots.resize(nkeep);
+    st.keep.row_slot.resize(nkeep);
+    st.keep.rscale.assign(nkeep, 1.0);
+    st.rho.resize(nkeep);
+    st.keep.ptr.assign(nkeep + 1, 0);
+    st.keep.col.resize(kno[ns]);
+    st.keep.val.resize(kno[ns]);
+    st.bs_ptr.assign(nslots + 1, 0);
+    st.bs_col.resize(bno[ns]);
+    st.bs_val.resize(bno[ns]);
+    // tasks: (subdomain, kind 0 = slots / 1 = keep rows, begin, end)
+    struct Task { int32_t si, kind; int64_t b, e; };
+    std::vector<Task> tasks;
+    constexpr int64_t kSlotsPerTask = 1 << 16, kEntriesPerTask = 1 << 18;
+    for (int32_t si = 0; si < ns; ++si) {
+        const Subdomain& sd = subs[ids[si]];
+        const int64_t nl = sd.n_local();
+        for (int64_t b0 = 0; b0 < nl; b0 += kSlotsPerTask) tasks.push_back({si, 0, b0, std::min(nl, b0 + kSlotsPerTask)});
+        const Csr& k2e = k2e_of(sd);
+        int64_t r0 = 0;
+        for (int64_t r = 0; r < k2e.nrows; ++r)
+            if ((int64_t)k2e.ptr[r + 1] - (int64_t)k2e.ptr[r0] >= kEntriesPerTask || r + 1 == k2e.nrows) {
+                tasks.push_back({si, 1, r0, r + 1});
+                r0 = r + 1;
+            }
+    }
+    parallel_tasks(tasks.size(), [&](size_t t) {
+        const Task& T = tasks[t];
+        const Subdomain& sd = subs[ids[T.si]];
+        const int32_t nq = sd.n_q();
+        const int64_t o = so[T.si];
+        const int64_t keep0 = o + (sd.elim_q ? nq : 0), elim0 = o + (sd.elim_q ? 0 : nq);
+        const int64_t le0 = elim0 - o;  // first eliminated slot, local
+        const int32_t n_elim = sd.elim_q ? nq : sd.n_r();
+        auto spou_of = [&](int64_t a) {  // r-block sign flip (local_solver.rs:83-87, 362, 447)
+            const double pw = sd.pou.empty() ? 1.0 : sd.pou[a];
+            return a < nq ? pw : -pw;
+        };
+        if (T.kind == 0) {
+            const Csr& e2k = e2k_of(sd);
+            for (int64_t a = T.b; a < T.e; ++a) {
+                const int64_t l = o + a;
+                st.gidx[l] = sd.gidx[a];
+                st.sub_of[l] = (uint32_t)T.si;
+                st.spou[l] = spou_of(a);
+                // back substitution rows over all slots of the subdomain (local_solver.rs:111-151)
+                int64_t end = 0;
+                if (a >= le0 && a < le0 + n_elim) {
+                    const int64_t e = a - le0;
+                    st.invd[l] = sd.inv_diag[e];
+                    for (uint32_t x = e2k.ptr[e]; x < e2k.ptr[e + 1]; ++x) {
+                        st.bs_col[bno[T.si] + x] = (uint32_t)(keep0 + e2k.idx[x]);
+                        st.bs_val[bno[T.si] + x] = e2k.val[x];
+                    }
+                    end = e2k.ptr[e + 1];
+                } else {
+                    end = a < le0 ? 0 : e2k.nnz();
+                }
+                st.bs_ptr[l + 1] = bno[T.si] + end;
+            }
+        } else {
+            // reduced rhs rows (local_solver.rs:374-381, 410-417), premultiplied by the restriction
+            const Csr& k2e = k2e_of(sd);
+            for (int64_t i = T.b; i < T.e; ++i) {
+                const int64_t row = kro[T.si] + i;
+                st.keep_slots[row] = (uint32_t)(keep0 + i);
+                st.keep.row_slot[row] = (uint32_t)(keep0 + i);
+                double rho = 0.0;
+                for (uint32_t e = k2e.ptr[i]; e < k2e.ptr[i + 1]; ++e) {
+                    const int64_t a = le0 + k2e.idx[e];
+                    const double ci = k2e.val[e] * sd.inv_diag[k2e.idx[e]];
+                    rho += ci;
+                    st.keep.col[kno[T.si] + e] = sd.gidx[a];
+                    st.keep.val[kno[T.si] + e] = ci * spou_of(a);
+                }
+                st.rho[row] = rho;
+                st.keep.ptr[row + 1] = kno[T.si] + k2e.ptr[i + 1];
+            }
+        }
+    });
+    for (int32_t si = 0; si < ns; ++si) {
         const Subdomain& sd = subs[ids[si]];
         const int32_t nq = sd.n_q(), nr = sd.n_r(), nl = nq + nr;
-        const int64_t keep0 = o + (sd.elim_q ? nq : 0), elim0 = o + (sd.elim_q ? 0 : nq);
+        const int64_t o = so[si];
+        const int64_t keep0 = o + (sd.elim_q ? nq : 0);
         const int32_t n_keep = sd.elim_q ? nr : nq, n_elim = sd.elim_q ? nq : nr;
-        st.sub_nloc.push_back(nl);
-        st.sub_nkeep.push_back(n_keep);
+        st.sub_nloc[si] = nl;
+        st.sub_nkeep[si] = n_keep;
         double I = 0.0;
         for (int32_t e = 0; e < n_elim; ++e) I += sd.inv_diag[e];
-        st.sub_I.push_back(I);
-        for (int32_t a = 0; a < nl; ++a) {
-            st.gidx.push_back(sd.gidx[a]);
-            st.sub_of.push_back((uint32_t)si);
-            const double pw = sd.pou.empty() ? 1.0 : sd.pou[a];
-            st.spou.push_back(a < nq ? pw : -pw);  // r-block sign flip (local_solver.rs:83-87, 362, 447)
-            st.invd.push_back(0.0);
-        }
-        for (int32_t e = 0; e < n_elim; ++e) st.invd[elim0 + e] = sd.inv_diag[e];
-        const Csr& k2e = sd.elim_q ? sd.ct.ct : sd.ct.c;
-        const Csr& e2k = sd.elim_q ? sd.ct.c : sd.ct.ct;
-        // reduced rhs rows (local_solver.rs:374-381, 410-417), premultiplied by the restriction
-        for (int32_t i = 0; i < n_keep; ++i) {
-            st.keep_slots.push_back((uint32_t)(keep0 + i));
-            st.keep.row_slot.push_back((uint32_t)(keep0 + i));
-            st.keep.rscale.push_back(1.0);
-            double rho = 0.0;
-            for (uint32_t e = k2e.ptr[i]; e < k2e.ptr[i + 1]; ++e) {
-                const int64_t es = elim0 + k2e.idx[e];
-                const double ci = k2e.val[e] * sd.inv_diag[k2e.idx[e]];
-                rho += ci;
-                st.keep.col.push_back(st.gidx[es]);
-                st.keep.val.push_back(ci * st.spou[es]);
-            }
-            st.rho.push_back(rho);
-            st.keep.ptr.push_back((int64_t)st.keep.col.size());
-        }
-        // back substitution rows over all slots of the subdomain (local_solver.rs:111-151)
-        for (int32_t a = 0; a < nl; ++a) {
-            const int64_t l = o + a;
-            if (l >= elim0 && l < elim0 + n_elim) {
-                const int32_t e = (int32_t)(l - elim0);
-                for (uint32_t x = e2k.ptr[e]; x < e2k.ptr[e + 1]; ++x) {
-                    st.bs_col.push_back((uint32_t)(keep0 + e2k.idx[x]));
-                    st.bs_val.push_back(e2k.val[x]);
-                }
-            }
-            st.bs_ptr.push_back((int64_t)st.bs_col.size());
-        }
+        st.sub_I[si] = I;
         if (sd.kind == 0) {
             st.dn_keep0.push_back(keep0);
             st.dn_n.push_back(sd.n_red);
@@ -171,9 +253,8 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
                 }
             }
         }
-        o += nl;
     }
-    st.nslots = o;
+    st.nslots = nslots;
     // level-major AC rows: fwd (targets, may split) and bwd (columns, never split)
     st.fwd_lp.push_back(0);
     st.bwd_lp.push_back(0);
@@ -212,20 +293,26 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
         st.gsub.resize(ng);
         st.gspou.resize(ng);
         st.ginvd.resize(ng);
-        st.gbs_ptr.assign(1, 0);
-        st.gbs_col.reserve(st.bs_col.size());
-        st.gbs_val.reserve(st.bs_val.size());
+        st.gbs_ptr.assign(ng + 1, 0);
         for (size_t e = 0; e < ng; ++e) {
             const uint32_t l = st.gslot[e];
-            st.gsub[e] = st.sub_of[l];
-            st.gspou[e] = st.spou[l];
-            st.ginvd[e] = st.invd[l];
-            for (int64_t t = st.bs_ptr[l]; t < st.bs_ptr[l + 1]; ++t) {
-                st.gbs_col.push_back(st.bs_col[t]);
-                st.gbs_val.push_back(st.bs_val[t]);
-            }
-            st.gbs_ptr.push_back((int64_t)st.gbs_col.size());
+            st.gbs_ptr[e + 1] = st.gbs_ptr[e] + (st.bs_ptr[l + 1] - st.bs_ptr[l]);
         }
+        st.gbs_col.resize((size_t)st.gbs_ptr[ng]);
+        st.gbs_val.resize((size_t)st.gbs_ptr[ng]);
+        constexpr size_t kPer = 1 << 16;
+        parallel_tasks((ng + kPer - 1) / kPer, [&](size_t t) {
+            for (size_t e = t * kPer; e < std::min(ng, (t + 1) * kPer); ++e) {
+                const uint32_t l = st.gslot[e];
+                st.gsub[e] = st.sub_of[l];
+                st.gspou[e] = st.spou[l];
+                st.ginvd[e] = st.invd[l];
+                std::copy(st.bs_col.begin() + st.bs_ptr[l], st.bs_col.begin() + st.bs_ptr[l + 1],
+                          st.gbs_col.begin() + st.gbs_ptr[e]);
+                std::copy(st.bs_val.begin() + st.bs_ptr[l], st.bs_val.begin() + st.bs_ptr[l + 1],
+                          st.gbs_val.begin() + st.gbs_ptr[e]);
+            }
+        });
     }
     return st;
 }
