@@ -51,7 +51,7 @@ def test_config_validation_before_device():
         wb.ApproxCholConfig(split=0)
     with pytest.raises(ValueError):
         wb.CG(precision="fp16")
-    with pytest.raises(ValueError):
+    with pytest.raises(TypeError):  # 1-D categories (reference tests/test_error_handling.py:51-56)
         wb.Solver(np.zeros(4, np.uint32))
     with pytest.raises(wb.WithinError, match="weights has length 3, expected 4"):
         wb.Solver(cats, weights=np.ones(3))

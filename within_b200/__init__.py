@@ -215,14 +215,22 @@ def _validate(params, pre) -> None:
 
 def _categories(categories) -> np.ndarray:
     cats = np.asarray(categories)
-    if cats.ndim != 2:
-        raise ValueError("categories must be a 2-D array of shape (n_obs, n_factors)")
+    if cats.ndim != 2:  # within-py extracts a 2-D uint32 array (a TypeError otherwise)
+        raise TypeError("categories must be a 2-D array of shape (n_obs, n_factors)")
     if cats.dtype != np.uint32:
         raise TypeError("categories must have dtype uint32")
     if cats.strides[0] != cats.itemsize and cats.shape[0] > 1 and cats.shape[1] > 1:
         warnings.warn("categories array is not F-contiguous (column-major). "
                       "Use np.asfortranarray(categories) for faster solves.", UserWarning, stacklevel=3)
     return cats
+
+
+def _f64(a, name):
+    """A float64 array; other numpy dtypes are a TypeError, as within-py's float64 array
+    arguments are (lists and scalars are converted)."""
+    if isinstance(a, np.ndarray) and a.dtype != np.float64:
+        raise TypeError(f"{name} must have dtype float64, got {a.dtype}")
+    return np.asarray(a, dtype=np.float64)
 
 
 def _check(rc: int) -> None:
@@ -366,9 +374,13 @@ class FePreconditioner:
         return f"FePreconditioner({kind}, n={self.nrows})"
 
 
-def _apply_handle(h, fn, v, rows):
+def _apply_handle(h, fn, v, rows, in_rows=None):
+    """out (rows x k) = fn(v); v has in_rows rows (default: rows), else a ValueError."""
     v = np.asarray(v, dtype=np.float64)
     one = v.ndim == 1
+    want = rows if in_rows is None else in_rows
+    if v.ndim not in (1, 2) or v.shape[0] != want:
+        raise ValueError(f"expected {want} rows, got shape {v.shape}")
     V = np.asfortranarray(v.reshape(v.shape[0], -1))
     out = np.empty((rows, V.shape[1]), order="F")
     _check(getattr(_lib.load(), fn)(h, _lib.ptr(V), V.shape[1], _lib.ptr(out)))
@@ -390,7 +402,7 @@ class Solver:
         n, q = cats.shape
         self._w = None
         if weights is not None:
-            self._w = np.ascontiguousarray(weights, dtype=np.float64)
+            self._w = np.ascontiguousarray(_f64(weights, "weights"))
             if self._w.ndim != 1 or self._w.shape[0] != n:
                 raise WithinError(3, f"weights has length {self._w.shape[0] if self._w.ndim else 0}, expected {n}")
         isz = cats.itemsize
@@ -418,7 +430,7 @@ class Solver:
             self._h = None
 
     def _y(self, y, ndim):
-        y = np.asarray(y, dtype=np.float64)
+        y = _f64(y, "y")
         if y.ndim != ndim:
             raise ValueError(f"expected a {ndim}-D array")
         if y.shape[0] != self.n_obs:
@@ -450,8 +462,8 @@ class Solver:
         return None if _lib.load().within_solver_preconditioner_kind(self._h) == 0 else FePreconditioner._of(self)
 
     # --- operator access (kernel-level parity checks) ---
-    def _apply(self, fn, v, out_rows=None):
-        return _apply_handle(self._h, fn, v, out_rows or self.n_dofs)
+    def _apply(self, fn, v, out_rows=None, in_rows=None):
+        return _apply_handle(self._h, fn, v, out_rows or self.n_dofs, in_rows or self.n_dofs)
 
     def apply_gramian(self, x):
         return self._apply("within_solver_apply_gramian", x)
@@ -460,7 +472,7 @@ class Solver:
         return self._apply("within_solver_matvec_d", x, self.n_obs)
 
     def rmatvec_wdt(self, r):
-        return self._apply("within_solver_rmatvec_wdt", r)
+        return self._apply("within_solver_rmatvec_wdt", r, self.n_dofs, self.n_obs)
 
     def factor_meta(self):
         nl = np.zeros(self.n_factors, np.int64)
@@ -504,6 +516,7 @@ class Solver:
 def solve(categories, y, config=None, weights=None, preconditioner=None) -> SolveResult:
     """orchestrate::solve (within/src/orchestrate.rs:151-166)."""
     t0 = time.perf_counter()
+    y = _f64(y, "y")  # argument types are checked before anything is built
     s = Solver(categories, config, weights, preconditioner)
     r = s.solve(y)
     r.time_setup = s.time_setup
@@ -566,6 +579,7 @@ def solve_many(problems, config=None, preconditioner=None, concurrency: int = 0)
 def solve_batch(categories, Y, config=None, weights=None, preconditioner=None) -> BatchSolveResult:
     """orchestrate::solve_batch (within/src/orchestrate.rs:172-184)."""
     t0 = time.perf_counter()
+    Y = _f64(Y, "Y")
     s = Solver(categories, config, weights, preconditioner)
     r = s.solve_batch(Y)
     r.time_total = time.perf_counter() - t0
