@@ -534,8 +534,6 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
     f.col_vertex.reserve((size_t)n);
     f.col_diag.reserve((size_t)n);
     f.col_ptr.reserve((size_t)n + 1);
-    CliqueTreeSampler sampler;
-    std::vector<Edge> fill;
     int32_t remaining = n;
     // A vertex's list changes only when a neighbour is eliminated (the neighbour dies, fill
     // edges arrive), so only those "dirty" lists are compacted in the next round; a clean
@@ -546,16 +544,24 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
     for (int32_t v = 0; v < n; ++v) vhash[v] = hash64(seed ^ ((uint64_t)v * 0xD1B54A32D192ED03ULL));
     std::vector<int32_t> live((size_t)n);  // live vertices, ascending
     std::iota(live.begin(), live.end(), 0);
-    std::vector<Nbr> scratch;
+    std::vector<int32_t> todo;
+    std::vector<std::vector<Edge>> fills;
+    constexpr size_t kPerTask = 512;  // vertices per task of the parallel phases
     while (remaining > kAcCoreMax) {
-        rank.clear();
-        for (int32_t v : live) {
-            if (dirty[v]) {
-                sorted_len[v] = compact_adj_tail(g[v], sorted_len[v], dead, scratch);
+        // compact the dirty lists (each list alone: independent across vertices)
+        todo.clear();
+        for (int32_t v : live)
+            if (dirty[v]) todo.push_back(v);
+        parallel_tasks((todo.size() + kPerTask - 1) / kPerTask, [&](size_t t) {
+            std::vector<Nbr> scr;
+            for (size_t a = t * kPerTask; a < std::min(todo.size(), (t + 1) * kPerTask); ++a) {
+                const int32_t v = todo[a];
+                sorted_len[v] = compact_adj_tail(g[v], sorted_len[v], dead, scr);
                 dirty[v] = 0;
             }
-            rank.push_back(Rank{(int32_t)g[v].size(), vhash[v], v});
-        }
+        });
+        rank.clear();
+        for (int32_t v : live) rank.push_back(Rank{(int32_t)g[v].size(), vhash[v], v});
         std::sort(rank.begin(), rank.end(), [](const Rank& a, const Rank& b) {
             if (a.deg != b.deg) return a.deg < b.deg;
             if (a.h != b.h) return a.h < b.h;
@@ -575,7 +581,24 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
             break;
         }
         f.level_ptr.push_back((int32_t)f.col_vertex.size());
-        for (int32_t v : picked) {
+        // the picked vertices are independent: no fill edge touches another picked vertex's
+        // list, so every clique tree is sampled from the lists as they are now (in parallel,
+        // each with its own seed) and the fill is then added in pick order
+        fills.resize(picked.size());
+        parallel_tasks((picked.size() + kPerTask - 1) / kPerTask, [&](size_t t) {
+            CliqueTreeSampler smp;
+            for (size_t a = t * kPerTask; a < std::min(picked.size(), (t + 1) * kPerTask); ++a) {
+                const int32_t v = picked[a];
+                const std::vector<Nbr>& L = g[v];
+                fills[a].clear();
+                if (L.size() <= 1) continue;
+                double d = 0.0;
+                for (const Nbr& x : L) d += x.w;
+                smp.sample(L.data(), (int32_t)L.size(), split, d, seed + (uint64_t)v, fills[a]);
+            }
+        });
+        for (size_t a = 0; a < picked.size(); ++a) {
+            const int32_t v = picked[a];
             const std::vector<Nbr>& L = g[v];
             double d = 0.0;
             for (const Nbr& x : L) d += x.w;
@@ -586,13 +609,9 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
                 f.col_idx.push_back((int32_t)x.col);
                 f.col_coef.push_back(x.w / d);
             }
-            if (L.size() > 1) {
-                fill.clear();
-                sampler.sample(L.data(), (int32_t)L.size(), split, d, seed + (uint64_t)v, fill);
-                for (const Edge& e : fill) {
-                    g[e.lo].push_back(Nbr{e.hi, e.w});
-                    g[e.hi].push_back(Nbr{e.lo, e.w});
-                }
+            for (const Edge& e : fills[a]) {
+                g[e.lo].push_back(Nbr{e.hi, e.w});
+                g[e.hi].push_back(Nbr{e.lo, e.w});
             }
         }
         for (int32_t v : picked)
@@ -735,21 +754,19 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
         for (int r = q + 1; r < d.Q; ++r) pairs.emplace_back(q, r);
     std::vector<std::vector<Subdomain>> per_pair(pairs.size());
     std::vector<std::vector<Status>> per_status(pairs.size());
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    std::atomic<unsigned> busy{(unsigned)std::min<size_t>(pairs.size(), hw)};
+    // (threads come from the process-wide budget: try_take_helper)
     auto factor_pair = [&](size_t p) {
         std::vector<Subdomain>& v = per_pair[p];
         std::vector<Status>& status = per_status[p];
         status.assign(v.size(), Status{});
         std::vector<std::future<void>> jobs;
         for (size_t i = 0; i < v.size(); ++i) {
-            if (v[i].n_local() > 4096 && busy.fetch_add(1) < hw) {
+            if (v[i].n_local() > 4096 && try_take_helper()) {
                 jobs.push_back(std::async(std::launch::async, [&, i] {
                     status[i] = build_local_factor(v[i], cfg);
-                    busy.fetch_sub(1);
+                    release_helper();
                 }));
             } else {
-                if (v[i].n_local() > 4096) busy.fetch_sub(1);
                 status[i] = build_local_factor(v[i], cfg);
             }
         }
@@ -777,8 +794,13 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
     {
         std::vector<std::future<void>> pj;
         for (size_t p = 0; p < pairs.size(); ++p) {
-            if (pj.size() + 1 < hw && p + 1 < pairs.size()) pj.push_back(std::async(std::launch::async, build_pair, p));
-            else build_pair(p);
+            if (p + 1 < pairs.size() && try_take_helper())
+                pj.push_back(std::async(std::launch::async, [&, p] {
+                    build_pair(p);
+                    release_helper();
+                }));
+            else
+                build_pair(p);
         }
         for (auto& j : pj) j.get();
     }

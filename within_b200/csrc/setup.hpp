@@ -4,11 +4,61 @@
 // reference exactly; the device layout is built from these in solver.cu.
 #pragma once
 
+#include <algorithm>
+#include <atomic>
 #include <cstdint>
+#include <functional>
+#include <thread>
 #include <string>
 #include <vector>
 
 namespace wb {
+
+// Host threads busy with setup work across the process: the workers of concurrent
+// solves (which hold one each while they work) and the helpers of parallel_tasks.
+// Nested parallel phases only take helpers while this stays below the core count, so
+// that many concurrent solves do not oversubscribe the host.
+inline std::atomic<int>& busy_threads() {
+    static std::atomic<int> n{0};
+    return n;
+}
+
+// One helper thread from the budget, if a core is idle (release it with release_helper).
+inline bool try_take_helper() {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<int>& busy = busy_threads();
+    for (int cur = busy.load(); cur + 1 < hw;)
+        if (busy.compare_exchange_weak(cur, cur + 1)) return true;
+    return false;
+}
+inline void release_helper() { busy_threads().fetch_sub(1); }
+
+// Runs fn(t) for t in [0, ntasks) on the calling thread and as many helper threads as
+// there are idle cores (at most one per task).
+inline void parallel_tasks(size_t ntasks, const std::function<void(size_t)>& fn) {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int want = (int)std::min<size_t>(ntasks, (size_t)hw) - 1;
+    int got = 0;
+    std::atomic<int>& busy = busy_threads();
+    while (got < want) {
+        int cur = busy.load();
+        if (cur + 1 >= hw) break;  // the calling thread keeps one core
+        if (busy.compare_exchange_weak(cur, cur + 1)) ++got;
+    }
+    if (got == 0) {
+        for (size_t t = 0; t < ntasks; ++t) fn(t);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+        for (size_t t; (t = next.fetch_add(1)) < ntasks;) fn(t);
+    };
+    std::vector<std::thread> th;
+    for (int i = 0; i < got; ++i) th.emplace_back(worker);
+    worker();
+    for (auto& x : th) x.join();
+    busy.fetch_sub(got);
+}
 
 struct Status {
     int code = 0;  // WITHIN_OK or a WITHIN_ERR_* value

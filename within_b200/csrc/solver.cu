@@ -67,23 +67,6 @@ std::vector<CsrChunk> make_chunks(const std::vector<int64_t>& ptr, int64_t row_l
     return out;
 }
 
-// Runs fn(t) for t in [0, ntasks) on up to one thread per host core.
-void parallel_tasks(size_t ntasks, const std::function<void(size_t)>& fn) {
-    const size_t nt = std::min<size_t>(ntasks, std::max(1u, std::thread::hardware_concurrency()));
-    if (nt <= 1) {
-        for (size_t t = 0; t < ntasks; ++t) fn(t);
-        return;
-    }
-    std::atomic<size_t> next{0};
-    auto worker = [&]() {
-        for (size_t t; (t = next.fetch_add(1)) < ntasks;) fn(t);
-    };
-    std::vector<std::thread> th;
-    for (size_t i = 1; i < nt; ++i) th.emplace_back(worker);
-    worker();
-    for (auto& x : th) x.join();
-}
-
 // Flatten the subdomains `ids` into one stage (see StageHost and kernels.cuh).  The
 // per-slot arrays, the keep rows and the back-substitution rows are sized first and then
 // filled in parallel over ranges of slots and rows (every range writes its own part, with
@@ -93,8 +76,8 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
     StageHost st;
     st.nsub = (int32_t)ids.size();
     const int32_t ns = st.nsub;
-    std::vector<std::vector<std::pair<uint32_t, std::vector<std::pair<uint32_t, double>>>>> afwd;
-    std::vector<std::vector<std::tuple<uint32_t, double, std::vector<std::pair<uint32_t, double>>>>> abwd;
+    std::vector<int32_t> ac_subs;  // stage-local indices of the AC subdomains, in order
+    int32_t max_lev = 0;
     // offsets per subdomain: slots, keep rows, keep entries, back-substitution entries
     std::vector<int64_t> so(ns + 1, 0), kro(ns + 1, 0), kno(ns + 1, 0), bno(ns + 1, 0);
     auto k2e_of = [&](const Subdomain& sd) -> const Csr& { return sd.elim_q ? sd.ct.ct : sd.ct.c; };
@@ -212,34 +195,8 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
             st.dn_L.insert(st.dn_L.end(), sd.L.begin(), sd.L.end());
         } else {
             const AcFactor& f = sd.ac;
-            if ((int32_t)afwd.size() < f.nlev) { afwd.resize(f.nlev); abwd.resize(f.nlev); }
-            for (int32_t lv = 0; lv < f.nlev; ++lv) {
-                std::vector<std::tuple<uint32_t, uint32_t, double>> trip;  // (target, source, coef)
-                for (int32_t c = f.level_ptr[lv]; c < f.level_ptr[lv + 1]; ++c) {
-                    const uint32_t v = (uint32_t)(keep0 + f.col_vertex[c]);
-                    std::vector<std::pair<uint32_t, double>> ent;
-                    for (int32_t e = f.col_ptr[c]; e < f.col_ptr[c + 1]; ++e) {
-                        const uint32_t u = (uint32_t)(keep0 + f.col_idx[e]);
-                        ent.push_back({u, f.col_coef[e]});
-                        trip.emplace_back(u, v, f.col_coef[e]);
-                    }
-                    const double dd = f.col_diag[c];
-                    abwd[lv].emplace_back(v, dd > 0.0 ? 1.0 / dd : 0.0, std::move(ent));
-                }
-                std::stable_sort(trip.begin(), trip.end(), [](const auto& a, const auto& b) {
-                    return std::get<0>(a) != std::get<0>(b) ? std::get<0>(a) < std::get<0>(b)
-                                                              : std::get<1>(a) < std::get<1>(b);
-                });
-                for (size_t a = 0; a < trip.size();) {
-                    const uint32_t u = std::get<0>(trip[a]);
-                    std::vector<std::pair<uint32_t, double>> ent;
-                    while (a < trip.size() && std::get<0>(trip[a]) == u) {
-                        ent.push_back({std::get<1>(trip[a]), std::get<2>(trip[a])});
-                        ++a;
-                    }
-                    afwd[lv].push_back({u, std::move(ent)});
-                }
-            }
+            ac_subs.push_back(si);
+            max_lev = std::max(max_lev, f.nlev);
             if (f.ncore > 0) {
                 const int32_t g = (int32_t)st.core_n.size();
                 st.core_n.push_back(f.ncore);
@@ -255,27 +212,84 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
         }
     }
     st.nslots = nslots;
+    // AC rows per (AC subdomain, level), built in parallel: bwd rows are the level's
+    // columns in order (pivot slot, 1/pivot, entries in column order); fwd rows are the
+    // level's targets in ascending slot order, each with its sources in ascending order
+    // (within one level every (target, source) pair occurs once).
+    struct LevelRows {
+        std::vector<uint32_t> slot;
+        std::vector<double> scale;
+        std::vector<int64_t> len;
+        std::vector<uint32_t> col;
+        std::vector<double> val;
+    };
+    const size_t nac = ac_subs.size();
+    std::vector<std::vector<LevelRows>> fwd_sl(nac), bwd_sl(nac);
+    std::vector<std::pair<int32_t, int32_t>> ac_tasks;
+    for (size_t i = 0; i < nac; ++i) {
+        const int32_t nlev = subs[ids[ac_subs[i]]].ac.nlev;
+        fwd_sl[i].resize(nlev);
+        bwd_sl[i].resize(nlev);
+        for (int32_t lv = 0; lv < nlev; ++lv) ac_tasks.push_back({(int32_t)i, lv});
+    }
+    parallel_tasks(ac_tasks.size(), [&](size_t t) {
+        const int32_t i = ac_tasks[t].first, lv = ac_tasks[t].second;
+        const int32_t si = ac_subs[i];
+        const Subdomain& sd = subs[ids[si]];
+        const AcFactor& f = sd.ac;
+        const int64_t keep0 = so[si] + (sd.elim_q ? sd.n_q() : 0);
+        LevelRows& B = bwd_sl[i][lv];
+        LevelRows& F = fwd_sl[i][lv];
+        std::vector<std::tuple<uint32_t, uint32_t, double>> trip;  // (target, source, coef)
+        for (int32_t c = f.level_ptr[lv]; c < f.level_ptr[lv + 1]; ++c) {
+            const uint32_t v = (uint32_t)(keep0 + f.col_vertex[c]);
+            for (int32_t e = f.col_ptr[c]; e < f.col_ptr[c + 1]; ++e) {
+                const uint32_t u = (uint32_t)(keep0 + f.col_idx[e]);
+                B.col.push_back(u);
+                B.val.push_back(f.col_coef[e]);
+                trip.emplace_back(u, v, f.col_coef[e]);
+            }
+            const double dd = f.col_diag[c];
+            B.slot.push_back(v);
+            B.scale.push_back(dd > 0.0 ? 1.0 / dd : 0.0);
+            B.len.push_back(f.col_ptr[c + 1] - f.col_ptr[c]);
+        }
+        std::sort(trip.begin(), trip.end(), [](const auto& x, const auto& y) {
+            return std::get<0>(x) != std::get<0>(y) ? std::get<0>(x) < std::get<0>(y) : std::get<1>(x) < std::get<1>(y);
+        });
+        for (size_t a = 0; a < trip.size();) {
+            const uint32_t u = std::get<0>(trip[a]);
+            const size_t a0 = a;
+            while (a < trip.size() && std::get<0>(trip[a]) == u) {
+                F.col.push_back(std::get<1>(trip[a]));
+                F.val.push_back(std::get<2>(trip[a]));
+                ++a;
+            }
+            F.slot.push_back(u);
+            F.scale.push_back(1.0);
+            F.len.push_back((int64_t)(a - a0));
+        }
+    });
     // level-major AC rows: fwd (targets, may split) and bwd (columns, never split)
     st.fwd_lp.push_back(0);
     st.bwd_lp.push_back(0);
-    for (size_t lv = 0; lv < afwd.size(); ++lv) {
+    auto append = [](CsrHost& c, const LevelRows& R) {
+        c.row_slot.insert(c.row_slot.end(), R.slot.begin(), R.slot.end());
+        c.rscale.insert(c.rscale.end(), R.scale.begin(), R.scale.end());
+        c.col.insert(c.col.end(), R.col.begin(), R.col.end());
+        c.val.insert(c.val.end(), R.val.begin(), R.val.end());
+        for (int64_t l : R.len) c.ptr.push_back(c.ptr.back() + l);
+    };
+    for (int32_t lv = 0; lv < max_lev; ++lv) {
         const int64_t r0 = st.fwd.nrows();
-        for (auto& row : afwd[lv]) {
-            st.fwd.row_slot.push_back(row.first);
-            st.fwd.rscale.push_back(1.0);
-            for (auto& e : row.second) { st.fwd.col.push_back(e.first); st.fwd.val.push_back(e.second); }
-            st.fwd.ptr.push_back((int64_t)st.fwd.col.size());
-        }
+        for (size_t i = 0; i < nac; ++i)
+            if (lv < (int32_t)fwd_sl[i].size()) append(st.fwd, fwd_sl[i][lv]);
         auto fc = make_chunks(st.fwd.ptr, r0, st.fwd.nrows(), 64, 1, true);  // long rows in pieces (atomics)
         st.fwd.chunks.insert(st.fwd.chunks.end(), fc.begin(), fc.end());
         st.fwd_lp.push_back((int64_t)st.fwd.chunks.size());
         const int64_t b0 = st.bwd.nrows();
-        for (auto& row : abwd[lv]) {
-            st.bwd.row_slot.push_back(std::get<0>(row));
-            st.bwd.rscale.push_back(std::get<1>(row));
-            for (auto& e : std::get<2>(row)) { st.bwd.col.push_back(e.first); st.bwd.val.push_back(e.second); }
-            st.bwd.ptr.push_back((int64_t)st.bwd.col.size());
-        }
+        for (size_t i = 0; i < nac; ++i)
+            if (lv < (int32_t)bwd_sl[i].size()) append(st.bwd, bwd_sl[i][lv]);
         auto bc = make_chunks(st.bwd.ptr, b0, st.bwd.nrows(), 256, 1, false);
         st.bwd.chunks.insert(st.bwd.chunks.end(), bc.begin(), bc.end());
         st.bwd_lp.push_back((int64_t)st.bwd.chunks.size());
@@ -2666,6 +2680,7 @@ int within_solve_many(within_problem* problems, size_t n_problems, const within_
     // the solver's own stream (the device is the caller's)
     auto worker = [&]() {
         cudaSetDevice(dev);
+        wb::busy_threads().fetch_add(1);  // nested setup phases see this core as taken
         for (;;) {
             const size_t i = next.fetch_add(1);
             if (i >= n_problems) break;
@@ -2682,6 +2697,7 @@ int within_solve_many(within_problem* problems, size_t n_problems, const within_
             }
             p.status = rc;
         }
+        wb::busy_threads().fetch_sub(1);
     };
     std::vector<std::thread> pool;
     for (size_t t = 1; t < nt; ++t) pool.emplace_back(worker);
