@@ -217,7 +217,10 @@ def reference_arm(args):
     line = {"metric": METRIC, "value": value, "unit": "RHS/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * total / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": config_dict(cats, threads, args.scale, "fp64"), "impl": "reference",
+            # the workload is our arm's (all its RHS); each step is a bounded sample of it
+            "config": dict(config_dict(cats, Y.shape[1], args.scale, args.precision, args.operator),
+                           krylov=args.krylov),
+            "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "RHS/s", "cores": threads, "kind": "port",
                              "sample": f"each step solves {threads} of the 16 RHS, one per host thread"},
             "e2e": {"value": value, "unit": "RHS/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
