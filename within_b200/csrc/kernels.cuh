@@ -92,7 +92,7 @@ __device__ __forceinline__ V4<T> from_d(const V4<double>& v) { return V4<T>((T)v
 // Observation pass: y = D'W(D x) and its relatives, one read of the codes.
 // ---------------------------------------------------------------------------
 
-enum ObsMode { OBS_GRAM = 0, OBS_RHS = 1, OBS_RESID = 2, OBS_DX = 3 };
+enum ObsMode { OBS_GRAM = 0, OBS_RHS = 1, OBS_RESID = 2, OBS_DX = 3, OBS_LSMR = 4 };
 
 // Work unit: observations [obs_begin, obs_end) (sorted by the primary factor) covering
 // primary levels [lvl_begin, lvl_end); a split chunk is a piece of one long level.
@@ -134,6 +134,10 @@ struct ObsParams {
     const uint32_t* hot_level[kMaxQ];  // hot slot -> level
     const ObsChunk* chunks;
     int64_t nchunks;
+    // OBS_LSMR: per-RHS scale of the old u, and per-warp partial sums of u^2
+    // ((block * warps + warp) * kp + rhs)
+    const double* lsmr_scale;
+    double* lsmr_part;
 };
 
 template <typename T> struct W4;
@@ -158,6 +162,9 @@ __device__ __forceinline__ uint32_t ucomp(const uint4& v, int b) { return b == 0
 // One pass over the observations computing, with one read of the codes,
 //   GRAM:  out = D'W D x          RHS:  out = D'W yin
 //   RESID: eout = yin - D x, out = D'W eout          DX: eout = D x
+//   LSMR:  eout = W D x + scale yin (w = the square roots of the weights; the LSMR
+//          bidiagonalization's u = A v + scale u with A = W^(1/2) D), out = D'W eout
+//          (A'u), and per-warp partial sums of eout^2 (||u||^2)
 // QT == Q, and the last NP factor slots are SINK_PRIVATE (both compile-time); QT = kMaxQ
 // is the generic kernel (any Q up to 16, sinks read at run time, no reuse of gathered
 // rows).  kp = 4 G.
@@ -224,6 +231,8 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
         else atomic_add4(out + ((size_t)P.off[q] + lv) * KP + c4, a);
     };
 
+    V4<double> lsc(0.0), usq(0.0);  // OBS_LSMR: this lane's scales and sum of u^2
+    if constexpr (MODE == OBS_LSMR) lsc = V4<double>(P.lsmr_scale[c4], P.lsmr_scale[c4 + 1], P.lsmr_scale[c4 + 2], P.lsmr_scale[c4 + 3]);
     for (int64_t ch = (int64_t)blockIdx.x * gpb + gl; ch < P.nchunks; ch += ngroups) {
         const ObsChunk C = P.chunks[ch];
         uint32_t lvl = C.lvl_begin;
@@ -265,8 +274,19 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
             }
             return s;
         };
-        auto scatter = [&](uint32_t i, const uint32_t (&c)[QT], T wi, const V4<T>& s) {
-            if constexpr (MODE == OBS_DX || MODE == OBS_RESID) st4(eout + (size_t)i * KP + c4, s);
+        auto scatter = [&](uint32_t i, const uint32_t (&c)[QT], T wi, const V4<T>& s0) {
+            V4<T> s = s0;
+            if constexpr (MODE == OBS_LSMR) {  // u = w (D x) + scale u_old
+                const V4<T> uo = ld4(yin + (size_t)i * KP + c4);
+                s = wi * s0;
+                if (lsc.a != 0.0) s.a += (T)lsc.a * uo.a;
+                if (lsc.b != 0.0) s.b += (T)lsc.b * uo.b;
+                if (lsc.c != 0.0) s.c += (T)lsc.c * uo.c;
+                if (lsc.d != 0.0) s.d += (T)lsc.d * uo.d;
+                usq.a += (double)s.a * s.a; usq.b += (double)s.b * s.b;
+                usq.c += (double)s.c * s.c; usq.d += (double)s.d * s.d;
+            }
+            if constexpr (MODE == OBS_DX || MODE == OBS_RESID || MODE == OBS_LSMR) st4(eout + (size_t)i * KP + c4, s);
             if constexpr (kScatter) {
                 const V4<T> t = wi * s;
                 const uint32_t p = c[0];
@@ -355,6 +375,19 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
                     acc = V4<T>(T(0));
                 }
             }
+        }
+    }
+    if constexpr (MODE == OBS_LSMR) {  // sum the warp's lane groups; lanes < G store
+#pragma unroll
+        for (int o = G; o < 32; o <<= 1) {
+            usq.a += __shfl_xor_sync(0xffffffffu, usq.a, o);
+            usq.b += __shfl_xor_sync(0xffffffffu, usq.b, o);
+            usq.c += __shfl_xor_sync(0xffffffffu, usq.c, o);
+            usq.d += __shfl_xor_sync(0xffffffffu, usq.d, o);
+        }
+        if ((threadIdx.x & 31) < G) {
+            double* pw = P.lsmr_part + ((size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * KP + c4;
+            pw[0] = usq.a; pw[1] = usq.b; pw[2] = usq.c; pw[3] = usq.d;
         }
     }
     if (kScatter && P.smem_elems > 0) {

@@ -1,4 +1,4 @@
-// FP64 observation-pass kernels (every mode).
+// FP64 observation-pass kernels (every mode; LSMR runs in FP64 only).
 #define WB_OBS_DEFINE
 #include "obs_launch.cuh"
 
@@ -11,4 +11,6 @@ template cudaError_t obs_dispatch<double, OBS_RESID>(const ObsParams&, int, int,
                                                      const double*, const double*, double*, double*);
 template cudaError_t obs_dispatch<double, OBS_DX>(const ObsParams&, int, int, int, size_t, cudaStream_t, const double*,
                                                   const double*, const double*, double*, double*);
+template cudaError_t obs_dispatch<double, OBS_LSMR>(const ObsParams&, int, int, int, size_t, cudaStream_t, const double*,
+                                                    const double*, const double*, double*, double*);
 }  // namespace wb

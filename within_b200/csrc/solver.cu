@@ -741,10 +741,14 @@ int obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
     return np;
 }
 
+// Returns the number of per-warp partial rows written (OBS_LSMR; grid x warps per block).
 template <typename T, int MODE>
-void launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* out, T* eout) {
+int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* out, T* eout,
+               const double* lsmr_scale = nullptr, double* lsmr_part = nullptr) {
     ObsParams P;
     const int np = obs_params_for(S, kp, sizeof(T), P);
+    P.lsmr_scale = lsmr_scale;
+    P.lsmr_part = lsmr_part;
     const int G = group_for(kp);
     if (MODE != OBS_DX && out) {
         // zero the outputs that are accumulated (every non-primary factor, split levels)
@@ -763,6 +767,7 @@ void launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* 
     const cudaError_t err = obs_dispatch<T, MODE>(P, np, G, grid, smem, S.stream, w, x, yin, out, eout);
     WB_CUDA(err);
     S.gpu_launches++;
+    return grid * (bt / 32);
 }
 
 // Dot partials over rows (at most 2 blocks per SM: few partials to reduce).
@@ -1732,8 +1737,10 @@ __global__ void lsmr_alpha1_kernel(LsmrState s, const double* __restrict__ red, 
     lsmr_count(s, kp);
 }
 
-// beta_{k+1} = ||u||: the breakdown flag, and the coefficients of the next vector update:
-// GK: u *= 1/beta (pa), v = A'u - beta v (pb = -beta);  MGK: p~ = (1/beta) A'u - (beta/alpha) p~.
+// beta_{k+1} = ||u||: the breakdown flag, and the coefficients of the next vector update.
+// u is kept unnormalized in both processes (its 1/beta goes into the coefficients):
+// GK: v = (1/beta) A'u - beta v;  MGK: p~ = (1/beta) A'u - (beta/alpha) p~.  The next
+// step's u-update scale is -alpha_{k+1} / beta_{k+1} (bpi = 1/beta).
 // Inactive or broken-down columns get zeros, which zero their v (and p~).
 __global__ void lsmr_beta_kernel(LsmrState s, const double* __restrict__ red, int kp) {
     const int c = threadIdx.x;
@@ -1744,10 +1751,10 @@ __global__ void lsmr_beta_kernel(LsmrState s, const double* __restrict__ red, in
         s.brk[c] = on && be == 0.0;
         const int go = on && be != 0.0;
         const double binv = be > 0.0 ? 1.0 / be : 0.0;
-        if (!s.precond) {
-            s.inv_alpha[c] = go ? binv : 0.0;  // scale of u
-            s.pa[c] = go ? 1.0 : 0.0;
+        if (!s.precond) {  // u stays unnormalized: A'u_{k+1} = A'u / beta
+            s.pa[c] = go ? binv : 0.0;
             s.pb[c] = go ? -be : 0.0;
+            s.bpi[c] = go ? binv : 0.0;
         } else {
             const double al = s.alpha[c];
             s.pa[c] = go ? binv : 0.0;
@@ -1810,7 +1817,7 @@ __global__ void lsmr_step_kernel(LsmrState s, const double* __restrict__ red, in
             } else if (itn >= s.maxiter) {
                 s.active[c] = 0;
             }
-            s.scale[c] = s.active[c] ? (s.precond ? -(sa * s.bpi[c]) : -sa) : 0.0;
+            s.scale[c] = s.active[c] ? -(sa * s.bpi[c]) : 0.0;
         } else {
             s.inv_alpha[c] = 0.0;
             s.scale[c] = 0.0;
@@ -1932,21 +1939,20 @@ void lsmr_device(SolverImpl& S, LsmrBufs& B, int kp, const double* yi, double* x
     WB_CUDA(cudaStreamSynchronize(S.stream));
     S.gpu_launches += 2;
     for (int itn = 1; itn <= S.params.maxiter && *S.h_active > 0; ++itn) {
-        // beta_{k+1} u_{k+1} = A v_k + scale u_k
-        launch_obs<double, OBS_DX>(S, kp, nullptr, B.v.p, nullptr, nullptr, B.av.p);
-        obs_axpy(B.av.p, B.scale.p);
+        // one pass over the observations: u_{k+1} = A v_k + scale u_k (into the other u
+        // buffer), its squared norm per warp, and A'u_{k+1}
+        const int nw = launch_obs<double, OBS_LSMR>(S, kp, sw, B.v.p, B.u.p, B.atu.p, B.av.p, B.scale.p, part);
+        launch_reduce(S, part, nw, kp, red);
+        std::swap(B.u, B.av);
         lsmr_beta_kernel<<<1, 32, 0, S.stream>>>(s, red, kp);
         S.gpu_launches++;
         if (!precond) {
-            scale_u();
-            adjoint(B.atu.p);
-            axpby(B.v.p, B.atu.p, B.pa.p, 1.0, B.pb.p, !cap);  // v = A'u - beta v, red = ||v||^2
+            axpby(B.v.p, B.atu.p, B.pa.p, 1.0, B.pb.p, !cap);  // v = A'u / beta - beta v, red = ||v||^2
             if (cap) {
                 ring_sweep();
                 dot(B.v.p, B.v.p);
             }
         } else {
-            adjoint(B.atu.p);
             axpby(B.pt.p, B.atu.p, B.pa.p, 1.0, B.pb.p, false);  // p~ = A'u / beta - (beta / alpha) p~
             int nbp = 0;
             apply_precond<double>(S, B.pt.p, B.v.p, kp, nullptr, nbp);
