@@ -546,15 +546,17 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
     std::iota(live.begin(), live.end(), 0);
     std::vector<int32_t> todo;
     std::vector<std::vector<Edge>> fills;
-    constexpr size_t kPerTask = 512;  // vertices per task of the parallel phases
+    // vertices per task of the parallel phases (small: the late rounds pick few vertices
+    // of high degree, whose lists and samples are the long ones)
+    constexpr size_t kCompactTask = 64, kSampleTask = 16;
     while (remaining > kAcCoreMax) {
         // compact the dirty lists (each list alone: independent across vertices)
         todo.clear();
         for (int32_t v : live)
             if (dirty[v]) todo.push_back(v);
-        parallel_tasks((todo.size() + kPerTask - 1) / kPerTask, [&](size_t t) {
+        parallel_tasks((todo.size() + kCompactTask - 1) / kCompactTask, [&](size_t t) {
             std::vector<Nbr> scr;
-            for (size_t a = t * kPerTask; a < std::min(todo.size(), (t + 1) * kPerTask); ++a) {
+            for (size_t a = t * kCompactTask; a < std::min(todo.size(), (t + 1) * kCompactTask); ++a) {
                 const int32_t v = todo[a];
                 sorted_len[v] = compact_adj_tail(g[v], sorted_len[v], dead, scr);
                 dirty[v] = 0;
@@ -585,9 +587,9 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
         // list, so every clique tree is sampled from the lists as they are now (in parallel,
         // each with its own seed) and the fill is then added in pick order
         fills.resize(picked.size());
-        parallel_tasks((picked.size() + kPerTask - 1) / kPerTask, [&](size_t t) {
+        parallel_tasks((picked.size() + kSampleTask - 1) / kSampleTask, [&](size_t t) {
             CliqueTreeSampler smp;
-            for (size_t a = t * kPerTask; a < std::min(picked.size(), (t + 1) * kPerTask); ++a) {
+            for (size_t a = t * kSampleTask; a < std::min(picked.size(), (t + 1) * kSampleTask); ++a) {
                 const int32_t v = picked[a];
                 const std::vector<Nbr>& L = g[v];
                 fills[a].clear();
@@ -609,11 +611,18 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
                 f.col_idx.push_back((int32_t)x.col);
                 f.col_coef.push_back(x.w / d);
             }
-            for (const Edge& e : fills[a]) {
-                g[e.lo].push_back(Nbr{e.hi, e.w});
-                g[e.hi].push_back(Nbr{e.lo, e.w});
-            }
         }
+        // the fill, appended in emission order: worker w of nw owns the target vertices
+        // u with u % nw == w and scans every edge, so each list receives its entries in
+        // the same order as one sequential pass (nw = 1) appends them
+        parallel_workers(8, [&](int w, int nw) {
+            const uint32_t uw = (uint32_t)w, un = (uint32_t)nw;
+            for (size_t a = 0; a < picked.size(); ++a)
+                for (const Edge& e : fills[a]) {
+                    if (e.lo % un == uw) g[e.lo].push_back(Nbr{e.hi, e.w});
+                    if (e.hi % un == uw) g[e.hi].push_back(Nbr{e.lo, e.w});
+                }
+        });
         for (int32_t v : picked)
             for (const Nbr& x : g[v]) dirty[x.col] = 1;
         for (int32_t v : picked) { dead[v] = 1; std::vector<Nbr>().swap(g[v]); }

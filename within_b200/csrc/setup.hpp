@@ -33,6 +33,19 @@ inline bool try_take_helper() {
 }
 inline void release_helper() { busy_threads().fetch_sub(1); }
 
+// Runs fn(w, nw) on nw workers (the calling thread and up to max_workers - 1 helpers,
+// as many as there are idle cores), w = 0..nw-1; with no idle core nw is 1.
+inline void parallel_workers(int max_workers, const std::function<void(int, int)>& fn) {
+    int got = 0;
+    while (got + 1 < max_workers && try_take_helper()) ++got;
+    const int nw = got + 1;
+    std::vector<std::thread> th;
+    for (int w = 1; w < nw; ++w) th.emplace_back([&, w] { fn(w, nw); });
+    fn(0, nw);
+    for (auto& x : th) x.join();
+    for (int w = 0; w < got; ++w) release_helper();
+}
+
 // Runs fn(t) for t in [0, ntasks) on the calling thread and as many helper threads as
 // there are idle cores (at most one per task).
 inline void parallel_tasks(size_t ntasks, const std::function<void(size_t)>& fn) {
