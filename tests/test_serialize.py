@@ -141,3 +141,31 @@ def test_reuse_across_precisions_and_errors():
         _apply_handle(q._h, "within_solver_apply_gramian", np.zeros(q.nrows), q.nrows)
     # no preconditioner, nothing to serialize
     assert wb.Solver(cats, preconditioner=wb.Preconditioner.Off).preconditioner() is None
+
+
+def test_reader_fuzz():
+    """Random mutations of a consistent blob, checksum re-signed so that the structural
+    checks are reached: every outcome is a ValueError (malformed bytes, or on a machine
+    without a GPU the device step) or, with a GPU, a handle; never a crash.  The dof
+    count is left alone: it is taken as given (it may exceed the subdomains' dofs when
+    levels are unobserved), and it sizes the handle's arrays."""
+    import torch
+    rng = np.random.default_rng(0)
+    good = bytearray(_blob()[:-8])
+    for trial in range(300):
+        b = bytearray(good)
+        for _ in range(int(rng.integers(1, 4))):
+            # every byte after the magic except the dof count (bytes 12-19): the reader
+            # bounds every index by it, and a bytes-only handle sizes host arrays by it
+            pos = int(rng.integers(8, len(b) - 8))
+            pos = pos + 8 if pos >= 12 else pos
+            b[pos] = int(rng.integers(0, 256))
+        if rng.random() < 0.2:  # also truncate or extend
+            cut = int(rng.integers(8, len(b)))
+            b = b[:cut] if rng.random() < 0.5 else b + bytes(int(rng.integers(1, 64)))
+        data = bytes(b) + struct.pack("<Q", _fnv(bytes(b)))
+        try:
+            p = wb.FePreconditioner(data)
+            assert torch.cuda.is_available() and p.nrows > 0
+        except ValueError:
+            pass
