@@ -556,7 +556,7 @@ int pad_kp(int k) {
 
 // Observation chunks over primary-sorted observations (level-aligned; long levels split).
 std::vector<ObsChunk> make_obs_chunks(const std::vector<int64_t>& lvl_ptr, int64_t nlev, bool& has_split) {
-    constexpr int64_t kObsPerChunk = 128;
+    constexpr int64_t kObsPerChunk = 32;
     std::vector<ObsChunk> out;
     has_split = false;
     int64_t l = 0;
@@ -2000,7 +2000,8 @@ std::vector<double> host_reduce(SolverImpl& S, int nb, int kp) {
 
 // Solve k <= 32 RHS with device inputs ycol (n x k RHS-major) into device outputs
 // x (n_dofs x k RHS-major) and dem (n x k RHS-major).  Solver::solve semantics
-// (solver.rs:209-238) batched over RHS, with the refinement residual b - G x.
+// (solver.rs:209-238) batched over RHS, with the refinement residual b - G x (computed
+// as D'W (y - D x) when that check may be the last).
 void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double* demcol, BatchOut& out) {
     const int kp = pad_kp(k);
     ensure_ws(S, kp);
@@ -2020,6 +2021,7 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
         abs_tol[c] = S.params.tol * rhs_norm[c];
     }
     std::vector<int32_t> conv(kp, 0), iters(kp, 0), part_of(kp, 0);
+    std::vector<double> final_rr;  // set when w.e and w.r already hold the final e and D'W e
     for (int c = 0; c < k; ++c) part_of[c] = 1;
     std::vector<double> tol(kp, S.params.tol);
     if (S.params.krylov == WITHIN_KRYLOV_LSMR) {
@@ -2077,7 +2079,15 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
             if (!S.mixed() && ref == n_corr) break;
             const bool first_mixed = S.mixed() && ref == 0;
             const double* rhs = w.b.p;
-            if (!first_mixed) {  // r = b - G x in FP64
+            // The residual b - G x equals D'W (y - D x).  A mixed-precision check after the
+            // first correction, likely the last, computes it that way, with e = y - D x, so
+            // that when it ends the loop it is also the final demeaning below.  (FP64 runs
+            // usually end with a correction after the last check, so theirs stay b - G x.)
+            const bool resid = S.mixed() && ref >= 2;
+            if (resid) {
+                launch_obs<double, OBS_RESID>(S, kp, S.w64.p, w.x.p, w.yi.p, w.r.p, w.e.p);
+                rhs = w.r.p;
+            } else if (!first_mixed) {  // r = b - G x in FP64
                 cudaEvent_t e0 = nullptr;
                 S.prof_begin(e0);
                 launch_gram<double>(S, kp, S.w64.p, w.x.p, w.gx.p);
@@ -2102,7 +2112,10 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
                 who[c] = 1;
                 ++nwho;
             }
-            if (nwho == 0 || ref == n_corr) break;
+            if (nwho == 0 || ref == n_corr) {
+                if (resid) final_rr = rr;  // x is unchanged since this check
+                break;
+            }
             run_inner(rhs, who, ctol, cv, it);
             for (int c = 0; c < k; ++c)
                 if (who[c]) { iters[c] += it[c]; conv[c] = cv[c]; }
@@ -2113,13 +2126,16 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
         }
     }
     // final demeaned e = y - D x and ||D'W e|| / ||b|| (solver.rs:222-227, 335-339)
-    launch_obs<double, OBS_RESID>(S, kp, S.w64.p, w.x.p, w.yi.p, w.r.p, w.e.p);
-    launch_dot<double, double>(S, w.r.p, w.r.p, m, kp, w.part.p, nb);
+    if (final_rr.empty()) {
+        launch_obs<double, OBS_RESID>(S, kp, S.w64.p, w.x.p, w.yi.p, w.r.p, w.e.p);
+        launch_dot<double, double>(S, w.r.p, w.r.p, m, kp, w.part.p, nb);
+    }
     scatter_deinterleave_kernel<double><<<xpose_blocks(n, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(w.e.p, n, k, kp, perm, demcol);
     scatter_deinterleave_kernel<double><<<xpose_blocks(m, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(w.x.p, m, k, kp, nullptr, xcol);
     WB_CUDA(cudaGetLastError());
     S.gpu_launches += 3;
-    std::vector<double> ee = host_reduce(S, nb, kp);
+    if (!final_rr.empty()) WB_CUDA(cudaStreamSynchronize(S.stream));  // as host_reduce would
+    const std::vector<double> ee = final_rr.empty() ? host_reduce(S, nb, kp) : final_rr;
     S.prof_harvest();
     out.conv.assign(conv.begin(), conv.begin() + k);
     out.iters.assign(iters.begin(), iters.begin() + k);
