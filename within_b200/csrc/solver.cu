@@ -19,6 +19,7 @@
 #include <string>
 #include <tuple>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/within_b200.h"
@@ -424,6 +425,22 @@ struct Workspace {
     DArr<int32_t> sweep_err;                 // set when a barrier wait ran out
 };
 
+// Resident blocks per SM of `kern` at kBlock threads without dynamic shared memory,
+// queried once per kernel (the instantiations of one template differ in registers, so
+// the count is kept per kernel, not per signature).
+inline int resident_per_sm(const void* kern) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    const auto it = cache.find(kern);
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    WB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kBlock, 0));
+    n = std::max(n, 1);
+    cache.emplace(kern, n);
+    return n;
+}
+
 struct SolverImpl {
     std::mutex mu;
     Design d;
@@ -497,6 +514,11 @@ struct SolverImpl {
     int nblk(int64_t rows, int G, int cap_per_sm = 8) const {
         const int64_t need = (rows * G + kBlock - 1) / kBlock;
         return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)n_sm * cap_per_sm));
+    }
+    // blocks for a grid-stride pass that needs `need` blocks, at most one resident wave
+    // of `kern` (a second, partial wave would leave SMs idle at the end)
+    int fit(int64_t need, const void* kern) const {
+        return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)n_sm * resident_per_sm(kern)));
     }
     cudaEvent_t take_event() {
         if (ev_pool.empty()) {
@@ -829,9 +851,12 @@ void launch_csr(SolverImpl& S, CsrDev<T>& c, int64_t ch0, int64_t ch1, const T* 
     const int64_t nch = ch1 - ch0;
     if (nch <= 0) return;
     const int G = group_for(kp);
-    const int grid = S.nblk(nch, 32);  // one warp per chunk
-    WB_DISPATCH_G(G, csr_rows_kernel<T, GV, EPI><<<grid, kBlock, 0, S.stream>>>(
-                         c.chunks.p + ch0, nch, c.row_slot.p, c.ptr.p, c.col.p, c.val.p, c.rscale.p, src, dst, kp));
+    const int64_t need = (nch * 32 + kBlock - 1) / kBlock;  // one warp per chunk
+    WB_DISPATCH_G(G, {
+        auto kern = csr_rows_kernel<T, GV, EPI>;
+        kern<<<S.fit(need, (const void*)kern), kBlock, 0, S.stream>>>(c.chunks.p + ch0, nch, c.row_slot.p, c.ptr.p,
+                                                                      c.col.p, c.val.p, c.rscale.p, src, dst, kp);
+    });
     WB_CUDA(cudaGetLastError());
     S.gpu_launches++;
 }
@@ -848,9 +873,12 @@ void launch_gram(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
     }
     WB_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * (size_t)S.d.ndofs * kp, S.stream));
     const int G = group_for(kp);
-    const int grid = S.nblk(S.g_nchunks, 32);  // one warp per chunk
-    WB_DISPATCH_G(G, csr_rows_kernel<T, GV, EPI_ACC><<<grid, kBlock, 0, S.stream>>>(
-                         S.g_chunks.p, S.g_nchunks, S.g_rows.p, S.g_ptr.p, S.g_idx.p, gram_val<T>(S), nullptr, x, y, kp));
+    const int64_t need = (S.g_nchunks * 32 + kBlock - 1) / kBlock;  // one warp per chunk
+    WB_DISPATCH_G(G, {
+        auto kern = csr_rows_kernel<T, GV, EPI_ACC>;
+        kern<<<S.fit(need, (const void*)kern), kBlock, 0, S.stream>>>(S.g_chunks.p, S.g_nchunks, S.g_rows.p, S.g_ptr.p,
+                                                                      S.g_idx.p, gram_val<T>(S), nullptr, x, y, kp);
+    });
     WB_CUDA(cudaGetLastError());
     S.gpu_launches++;
 }
@@ -874,9 +902,7 @@ void launch_sweep(SolverImpl& S, CsrDev<T>& c, const std::vector<int64_t>& lp, c
     int* err = S.ws.sweep_err.p;
     WB_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned), S.stream));
     auto go = [&](auto kern) {
-        static int per_sm = 0;  // resident blocks per SM of this instantiation
-        if (per_sm == 0) WB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0));
-        const int grid = std::max(1, per_sm) * S.n_sm;
+        const int grid = resident_per_sm((const void*)kern) * S.n_sm;  // every block resident
         const CsrChunk* ch = c.chunks.p;
         const uint32_t* rs = c.row_slot.p;
         const int64_t* pt = c.ptr.p;
