@@ -114,11 +114,14 @@ struct StageHost {
     std::vector<double> core_z;
     // additive prolongation gather: dof j <- slots gslot[gptr[j]..gptr[j+1]), with the
     // per-slot data and back-substitution rows stored in the same (gather) order, so the
-    // prolongation reads them without going through the slot index
+    // prolongation reads them without going through the slot index; each row starts at a
+    // multiple of 4 entries (16-byte loads of 4 columns and values) and holds gbs_cnt
+    // entries, padded to a multiple of 4 with the row's first column and value 0
     std::vector<int64_t> gptr;
     std::vector<uint32_t> gslot, gsub;
     std::vector<double> gspou, ginvd;
     std::vector<int64_t> gbs_ptr;
+    std::vector<uint32_t> gbs_cnt;
     std::vector<uint32_t> gbs_col;
     std::vector<double> gbs_val;
 };
@@ -151,6 +154,7 @@ struct StageDev {
     DArr<uint32_t> gslot, gsub;
     DArr<T> gspou, ginvd;
     DArr<int64_t> gbs_ptr;
+    DArr<uint32_t> gbs_cnt;
     DArr<uint32_t> gbs_col;
     DArr<T> gbs_val;
 };

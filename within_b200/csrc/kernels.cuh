@@ -1002,11 +1002,12 @@ static __global__ void sub_means_kernel(int32_t nsub, int kp, SubMeans M, double
 // dof's loads depend only on gptr[j].  Dofs in no subdomain get z = 0.  Optionally the
 // partial dot r.z for CG.
 template <typename T, int G>
-__global__ void __launch_bounds__(kBlock) prolong_kernel(int64_t m, const int64_t* __restrict__ gptr,
+__global__ void __launch_bounds__(kBlock, 4) prolong_kernel(int64_t m, const int64_t* __restrict__ gptr,
                                                          const uint32_t* __restrict__ gslot,
                                                          const uint32_t* __restrict__ gsub,
                                                          const T* __restrict__ gspou, const T* __restrict__ ginvd,
                                                          const int64_t* __restrict__ gbs_ptr,
+                                                         const uint32_t* __restrict__ gbs_cnt,
                                                          const uint32_t* __restrict__ gbs_col,
                                                          const T* __restrict__ gbs_val, const double* __restrict__ mm,
                                                          const T* __restrict__ v, const T* __restrict__ r,
@@ -1022,31 +1023,31 @@ __global__ void __launch_bounds__(kBlock) prolong_kernel(int64_t m, const int64_
             const uint32_t s = gsub[e];
             const double sp = (double)gspou[e];
             const T id = ginvd[e];
-            const V4<double> m0 = ld4(mm + (size_t)(2 * s) * kp + c4), m2 = ld4(mm + (size_t)(2 * s + 1) * kp + c4);
             V4<double> sol;
             if (id == T(0)) {
                 sol = to_d(ld4(v + (size_t)gslot[e] * kp + c4));
             } else {
                 V4<T> bs(T(0)), bs2(T(0));
-                const int64_t t0 = gbs_ptr[e], t1 = gbs_ptr[e + 1];
-                int64_t t = t0;
-                for (; t + 4 <= t1; t += 4) {  // four independent gathers in flight
-                    const uint32_t j0 = __ldg(gbs_col + t), j1 = __ldg(gbs_col + t + 1);
-                    const uint32_t j2 = __ldg(gbs_col + t + 2), j3 = __ldg(gbs_col + t + 3);
-                    const T v0 = __ldg(gbs_val + t), v1 = __ldg(gbs_val + t + 1);
-                    const T v2 = __ldg(gbs_val + t + 2), v3 = __ldg(gbs_val + t + 3);
-                    const V4<T> s0 = ld4(v + (size_t)j0 * kp + c4), s1 = ld4(v + (size_t)j1 * kp + c4);
-                    const V4<T> s2 = ld4(v + (size_t)j2 * kp + c4), s3 = ld4(v + (size_t)j3 * kp + c4);
-                    bs += v0 * s0;
-                    bs2 += v1 * s1;
-                    bs += v2 * s2;
-                    bs2 += v3 * s3;
+                // the row starts at a multiple of 4 entries and is padded to one (repeats of
+                // its first column with value 0): one 16-byte load of 4 columns and one of 4
+                // values, then four independent gathers in flight
+                const int64_t t0 = gbs_ptr[e], t1 = t0 + gbs_cnt[e];
+                for (int64_t t = t0; t < t1; t += 4) {
+                    const uint4 jj = __ldg(reinterpret_cast<const uint4*>(gbs_col + t));
+                    const V4<T> vv = ldg4(gbs_val + t);
+                    const V4<T> s0 = ld4(v + (size_t)jj.x * kp + c4), s1 = ld4(v + (size_t)jj.y * kp + c4);
+                    const V4<T> s2 = ld4(v + (size_t)jj.z * kp + c4), s3 = ld4(v + (size_t)jj.w * kp + c4);
+                    bs += vv.a * s0;
+                    bs2 += vv.b * s1;
+                    bs += vv.c * s2;
+                    bs2 += vv.d * s3;
                 }
-                for (; t < t1; ++t) bs += __ldg(gbs_val + t) * ld4(v + (size_t)__ldg(gbs_col + t) * kp + c4);
                 bs += bs2;
                 const double idd = (double)id;
+                const V4<double> m0 = ld4(mm + (size_t)(2 * s) * kp + c4);
                 sol = idd * (sp * rj - m0) + idd * to_d(bs);
             }
+            const V4<double> m2 = ld4(mm + (size_t)(2 * s + 1) * kp + c4);
             acc += sp * (sol - m2);
         }
         const V4<T> zt = from_d<T>(acc);

@@ -309,12 +309,15 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
         st.gspou.resize(ng);
         st.ginvd.resize(ng);
         st.gbs_ptr.assign(ng + 1, 0);
+        st.gbs_cnt.resize(ng);
         for (size_t e = 0; e < ng; ++e) {
             const uint32_t l = st.gslot[e];
-            st.gbs_ptr[e + 1] = st.gbs_ptr[e] + (st.bs_ptr[l + 1] - st.bs_ptr[l]);
+            const int64_t len = st.bs_ptr[l + 1] - st.bs_ptr[l];
+            st.gbs_cnt[e] = (uint32_t)len;
+            st.gbs_ptr[e + 1] = st.gbs_ptr[e] + ((len + 3) & ~int64_t(3));  // rows start at multiples of 4
         }
-        st.gbs_col.resize((size_t)st.gbs_ptr[ng]);
-        st.gbs_val.resize((size_t)st.gbs_ptr[ng]);
+        st.gbs_col.assign((size_t)st.gbs_ptr[ng], 0u);
+        st.gbs_val.assign((size_t)st.gbs_ptr[ng], 0.0);
         constexpr size_t kPer = 1 << 16;
         parallel_tasks((ng + kPer - 1) / kPer, [&](size_t t) {
             for (size_t e = t * kPer; e < std::min(ng, (t + 1) * kPer); ++e) {
@@ -324,6 +327,8 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
                 st.ginvd[e] = st.invd[l];
                 std::copy(st.bs_col.begin() + st.bs_ptr[l], st.bs_col.begin() + st.bs_ptr[l + 1],
                           st.gbs_col.begin() + st.gbs_ptr[e]);
+                for (int64_t q = st.gbs_ptr[e] + st.gbs_cnt[e]; q < st.gbs_ptr[e + 1]; ++q)  // padding
+                    st.gbs_col[q] = st.gbs_col[st.gbs_ptr[e]];
                 std::copy(st.bs_val.begin() + st.bs_ptr[l], st.bs_val.begin() + st.bs_ptr[l + 1],
                           st.gbs_val.begin() + st.gbs_ptr[e]);
             }
@@ -391,6 +396,7 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
     d.gspou.upload_cast(h.gspou);
     d.ginvd.upload_cast(h.ginvd);
     d.gbs_ptr.upload(h.gbs_ptr);
+    d.gbs_cnt.upload(h.gbs_cnt);
     d.gbs_col.upload(h.gbs_col);
     d.gbs_val.upload_cast(h.gbs_val);
 }
@@ -1011,10 +1017,14 @@ void apply_precond(SolverImpl& S, const T* r, T* z, int kp, double* part, int& n
         double* mm = S.ws.msum.p + (size_t)4 * S.max_nsub * kp;  // [nsub][2][kp]
         const int64_t nm = (int64_t)st.nsub * kp;
         sub_means_kernel<<<(unsigned)((nm + kBlock - 1) / kBlock), kBlock, 0, S.stream>>>(st.nsub, kp, M, mm);
-        nb_part = S.nblk(m, G, 4);  // latency-bound gathers: as many resident blocks as registers allow
-        WB_DISPATCH_G(G, prolong_kernel<T, GV><<<nb_part, kBlock, 0, S.stream>>>(
-                             m, st.gptr.p, st.gslot.p, st.gsub.p, st.gspou.p, st.ginvd.p, st.gbs_ptr.p, st.gbs_col.p,
-                             st.gbs_val.p, mm, v, r, z, kp, part));
+        // latency-bound gathers: as many resident blocks as registers allow, one wave
+        WB_DISPATCH_G(G, {
+            auto kern = prolong_kernel<T, GV>;
+            nb_part = S.fit(((int64_t)m * G + kBlock - 1) / kBlock, (const void*)kern);
+            kern<<<nb_part, kBlock, 0, S.stream>>>(m, st.gptr.p, st.gslot.p, st.gsub.p, st.gspou.p, st.ginvd.p,
+                                                   st.gbs_ptr.p, st.gbs_cnt.p, st.gbs_col.p, st.gbs_val.p, mm, v, r, z,
+                                                   kp, part);
+        });
         WB_CUDA(cudaGetLastError());
         S.gpu_launches += 2;
         if (!part) nb_part = 0;
