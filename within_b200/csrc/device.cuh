@@ -4,8 +4,11 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "kernels.cuh"
@@ -23,6 +26,31 @@ struct CudaError : std::runtime_error {
             throw ::wb::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " + \
                                   __FILE__ + ":" + std::to_string(__LINE__));                   \
     } while (0)
+
+// Allocator whose construct() without arguments default-initializes: resize() of a
+// vector of plain numbers then leaves the new elements unwritten, so that a large array
+// filled in parallel afterwards is not first zeroed page by page on one thread.
+template <typename T>
+struct DefaultInitAllocator : std::allocator<T> {
+    DefaultInitAllocator() = default;
+    template <typename U>
+    DefaultInitAllocator(const DefaultInitAllocator<U>&) noexcept {}
+    template <typename U>
+    struct rebind {
+        using other = DefaultInitAllocator<U>;
+    };
+    template <typename U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+// Host array of a stage layout that is written in full after it is sized.
+template <typename T>
+using HostVec = std::vector<T, DefaultInitAllocator<T>>;
 
 // Owning device array.
 template <typename T>
@@ -50,16 +78,22 @@ struct DArr {
         WB_CUDA(cudaMalloc(&p, count * sizeof(T)));
         n = count;
     }
-    void upload(const std::vector<T>& h) {
+    template <typename V>
+    void upload(const V& h) {
+        static_assert(std::is_same<typename V::value_type, T>::value, "upload: element type");
         release();
         if (h.empty()) return;
         alloc(h.size());
         WB_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
     }
-    template <typename S>
-    void upload_cast(const std::vector<S>& h) {
-        std::vector<T> t(h.begin(), h.end());
-        upload(t);
+    template <typename V>
+    void upload_cast(const V& h) {
+        if constexpr (std::is_same<typename V::value_type, T>::value) {
+            upload(h);
+        } else {
+            std::vector<T> t(h.begin(), h.end());
+            upload(t);
+        }
     }
 };
 
@@ -78,10 +112,10 @@ struct CsrDev {
 
 // Host form of a row-wise CSR over slots.
 struct CsrHost {
-    std::vector<uint32_t> row_slot;
+    HostVec<uint32_t> row_slot;
     std::vector<int64_t> ptr{0};
-    std::vector<uint32_t> col;
-    std::vector<double> val;
+    HostVec<uint32_t> col;
+    HostVec<double> val;
     std::vector<double> rscale;
     std::vector<CsrChunk> chunks;
     int64_t nrows() const { return (int64_t)row_slot.size(); }
@@ -92,14 +126,15 @@ struct CsrHost {
 struct StageHost {
     int32_t nsub = 0;
     int64_t nslots = 0;
-    std::vector<uint32_t> gidx, sub_of, keep_slots;
-    std::vector<double> spou, invd, rho;        // per slot, per slot (0 = kept), per keep entry
+    HostVec<uint32_t> gidx, sub_of, keep_slots;
+    HostVec<double> spou, rho;                  // per slot, per keep entry
+    std::vector<double> invd;                   // per slot (0 = kept)
     std::vector<int32_t> sub_nloc, sub_nkeep;
     std::vector<double> sub_I;                  // sum of invd over eliminated slots
     CsrHost keep;                               // rows: keep list; cols: global dofs
     std::vector<int64_t> bs_ptr{0};             // back substitution rows over all slots
-    std::vector<uint32_t> bs_col;               // keep slot
-    std::vector<double> bs_val;                 // C_ek
+    HostVec<uint32_t> bs_col;                   // keep slot
+    HostVec<double> bs_val;                     // C_ek
     // dense reduced solves
     std::vector<int64_t> dn_keep0, dn_loff;
     std::vector<int32_t> dn_n;
@@ -118,12 +153,12 @@ struct StageHost {
     // multiple of 4 entries (16-byte loads of 4 columns and values) and holds gbs_cnt
     // entries, padded to a multiple of 4 with the row's first column and value 0
     std::vector<int64_t> gptr;
-    std::vector<uint32_t> gslot, gsub;
-    std::vector<double> gspou, ginvd;
+    HostVec<uint32_t> gslot, gsub;
+    HostVec<double> gspou, ginvd;
     std::vector<int64_t> gbs_ptr;
     std::vector<uint32_t> gbs_cnt;
-    std::vector<uint32_t> gbs_col;
-    std::vector<double> gbs_val;
+    HostVec<uint32_t> gbs_col;
+    HostVec<double> gbs_val;
 };
 
 template <typename T>

@@ -316,8 +316,8 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
             st.gbs_cnt[e] = (uint32_t)len;
             st.gbs_ptr[e + 1] = st.gbs_ptr[e] + ((len + 3) & ~int64_t(3));  // rows start at multiples of 4
         }
-        st.gbs_col.assign((size_t)st.gbs_ptr[ng], 0u);
-        st.gbs_val.assign((size_t)st.gbs_ptr[ng], 0.0);
+        st.gbs_col.resize((size_t)st.gbs_ptr[ng]);  // every entry, padding included, written below
+        st.gbs_val.resize((size_t)st.gbs_ptr[ng]);
         constexpr size_t kPer = 1 << 16;
         parallel_tasks((ng + kPer - 1) / kPer, [&](size_t t) {
             for (size_t e = t * kPer; e < std::min(ng, (t + 1) * kPer); ++e) {
@@ -327,10 +327,12 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
                 st.ginvd[e] = st.invd[l];
                 std::copy(st.bs_col.begin() + st.bs_ptr[l], st.bs_col.begin() + st.bs_ptr[l + 1],
                           st.gbs_col.begin() + st.gbs_ptr[e]);
-                for (int64_t q = st.gbs_ptr[e] + st.gbs_cnt[e]; q < st.gbs_ptr[e + 1]; ++q)  // padding
-                    st.gbs_col[q] = st.gbs_col[st.gbs_ptr[e]];
                 std::copy(st.bs_val.begin() + st.bs_ptr[l], st.bs_val.begin() + st.bs_ptr[l + 1],
                           st.gbs_val.begin() + st.gbs_ptr[e]);
+                for (int64_t q = st.gbs_ptr[e] + st.gbs_cnt[e]; q < st.gbs_ptr[e + 1]; ++q) {  // padding
+                    st.gbs_col[q] = st.gbs_col[st.gbs_ptr[e]];
+                    st.gbs_val[q] = 0.0;
+                }
             }
         });
     }
