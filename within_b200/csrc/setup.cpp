@@ -719,23 +719,34 @@ Status build_design(const uint32_t* codes, int64_t n, int Q, int64_t row_stride,
     d.n = n;
     d.Q = Q;
     d.codes.resize((size_t)n * Q);
-    for (int q = 0; q < Q; ++q) {
-        uint32_t* dst = d.codes.data() + (size_t)q * n;
-        if (row_stride == 1) {
-            std::memcpy(dst, codes + q * col_stride, sizeof(uint32_t) * (size_t)n);
-        } else {
-            for (int64_t i = 0; i < n; ++i) dst[i] = codes[i * row_stride + q * col_stride];
+    if (weights) d.w.resize((size_t)n);
+    // copy and per-factor maxima over ranges of observations (a maximum does not depend
+    // on the order it is taken in)
+    constexpr int64_t kRange = 1 << 20;
+    const int64_t nr = (n + kRange - 1) / kRange;
+    std::vector<uint32_t> mx((size_t)nr * Q, 0);
+    parallel_tasks((size_t)nr, [&](size_t t) {
+        const int64_t i0 = (int64_t)t * kRange, i1 = std::min(n, i0 + kRange);
+        for (int q = 0; q < Q; ++q) {
+            uint32_t* dst = d.codes.data() + (size_t)q * n;
+            if (row_stride == 1) {
+                std::memcpy(dst + i0, codes + q * col_stride + i0, sizeof(uint32_t) * (size_t)(i1 - i0));
+            } else {
+                for (int64_t i = i0; i < i1; ++i) dst[i] = codes[i * row_stride + q * col_stride];
+            }
+            uint32_t m = 0;
+            for (int64_t i = i0; i < i1; ++i) m = std::max(m, dst[i]);
+            mx[t * Q + q] = m;
         }
-    }
-    if (weights) d.w.assign(weights, weights + n);
+        if (weights) std::memcpy(d.w.data() + i0, weights + i0, sizeof(double) * (size_t)(i1 - i0));
+    });
     d.nlev.resize(Q);
     d.off.resize(Q);
     int64_t off = 0;
     for (int q = 0; q < Q; ++q) {
-        const uint32_t* c = d.codes.data() + (size_t)q * n;
-        uint32_t mx = 0;
-        for (int64_t i = 0; i < n; ++i) mx = std::max(mx, c[i]);
-        d.nlev[q] = (int64_t)mx + 1;
+        uint32_t m = 0;
+        for (int64_t t = 0; t < nr; ++t) m = std::max(m, mx[(size_t)t * Q + q]);
+        d.nlev[q] = (int64_t)m + 1;
         d.off[q] = off;
         off += d.nlev[q];
     }
