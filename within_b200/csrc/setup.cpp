@@ -761,7 +761,25 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
     for (int q = 0; q < d.Q; ++q) {  // find_all_active_levels (cross_tab.rs:75-89)
         active[q].assign((size_t)d.nlev[q], 0);
         const uint32_t* c = d.codes.data() + (size_t)q * d.n;
-        for (int64_t i = 0; i < d.n; ++i) active[q][c[i]] = 1;
+        // observation ranges mark their own flags, which are then or-ed level by level
+        constexpr int64_t kRange = 1 << 21;
+        const int64_t nr = (d.n + kRange - 1) / kRange;
+        if (nr <= 1 || nr * d.nlev[q] > ((int64_t)1 << 26)) {  // one pass, or flags too large
+            for (int64_t i = 0; i < d.n; ++i) active[q][c[i]] = 1;
+            continue;
+        }
+        const int64_t L = d.nlev[q];
+        std::vector<uint8_t> part((size_t)nr * L, 0);
+        parallel_tasks((size_t)nr, [&](size_t t) {
+            uint8_t* a = part.data() + t * L;
+            for (int64_t i = (int64_t)t * kRange; i < std::min(d.n, ((int64_t)t + 1) * kRange); ++i) a[c[i]] = 1;
+        });
+        const int64_t nl = (L + kRange - 1) / kRange;
+        parallel_tasks((size_t)nl, [&](size_t b) {
+            for (int64_t j = (int64_t)b * kRange; j < std::min(L, ((int64_t)b + 1) * kRange); ++j)
+                for (int64_t t = 0; t < nr; ++t)
+                    if (part[(size_t)t * L + j]) { active[q][j] = 1; break; }
+        });
     }
     // Pairs (q < r) in lexicographic order (factor_pairs.rs:252-260); components in
     // order; indices q-levels then r-levels (:244-250).  The pairs are independent and
