@@ -30,6 +30,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "RHS solved/sec at tol 1e-8, 10M obs 3 FE; speedup vs plain FP64 GPU PCG"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the operator
+# apply on the headline workload, from ncu captures of one launch (the figure and its
+# command are in profiles/); these are not measured by the bench run itself
+TRAFFIC = {}
 
 
 def parse():
@@ -50,6 +54,10 @@ def parse():
                     help="panel: the 10M-obs weighted 3-FE panel (the headline); uneven: 256 independent "
                          "problems of 1e3-1e6 observations, 2-4 factors, 1-8 RHS each (solve_many)")
     ap.add_argument("--problems", type=int, default=256, help="number of problems of the uneven workload")
+    ap.add_argument("--shuffle", action="store_true",
+                    help="the headline workload with its rows in a random order (not worker-major)")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the secondary arms (configs 1 and 2, the GMRES cross-check, shuffled rows)")
     return ap.parse_args()
 
 
@@ -181,8 +189,10 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
-def cpu_baseline_run(cats, Y, w, n_rhs, threads):
-    """The oracle (CPU restatement of the reference path) on a bounded sample."""
+def cpu_baseline_run(cats, Y, w, n_rhs, threads, truth_rhs=0):
+    """The oracle (CPU restatement of the reference path) on a bounded sample: n_rhs of
+    the RHS at tol 1e-8 (timed), and, untimed, the first truth_rhs of them at tol 1e-13.
+    The solutions are returned for the accuracy report (the oracle is the checker)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     t0 = time.perf_counter()
@@ -191,10 +201,143 @@ def cpu_baseline_run(cats, Y, w, n_rhs, threads):
     t0 = time.perf_counter()
     r = s.solve_batch(Y[:, :n_rhs], threads=threads)
     dt = time.perf_counter() - t0
+    truth = None
+    if truth_rhs:
+        truth = oracle.OracleSolver(cats, w, tol=1e-13).solve_batch(Y[:, :truth_rhs], threads=threads)
     return {"value": n_rhs / dt, "unit": "RHS/s", "cores": threads, "kind": "port",
-            "sample": f"{n_rhs} of the 16 RHS on the same 10M-obs design, one RHS per thread (solve_batch), "
+            "sample": f"{n_rhs} of the {Y.shape[1]} RHS on the same design, one RHS per thread (solve_batch), "
                       f"setup {t_setup:.1f}s excluded",
-            "converged": all(r.converged), "max_residual": max(r.residual)}
+            "converged": all(r.converged), "max_residual": max(r.residual)}, r, truth
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def accuracy_vs_oracle(cats, X, D, o, truth):
+    """Relative errors of the GPU solutions (X, D: (m, j), (n, j)) against the oracle's at
+    the same tol (o) and against the oracle at tol 1e-13 (truth): demeaned residuals, and x
+    after removing the null-space shift (per component, tests/paritylib.normalize_x)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from paritylib import make_normalizer
+    normalize = make_normalizer(cats)
+    j = o.x.shape[1]
+    ed = [rel(D[:, c], o.demeaned[:, c]) for c in range(j)]
+    ex = [rel(normalize(X[:, c]), normalize(o.x[:, c])) for c in range(j)]
+    out = {"rhs_compared": j, "rel_err_demeaned_vs_oracle": max(ed), "rel_err_x_vs_oracle": max(ex)}
+    if truth is not None:
+        t = truth.x.shape[1]
+        out["truth_rhs"] = t
+        out["rel_err_demeaned_vs_truth"] = max(rel(D[:, c], truth.demeaned[:, c]) for c in range(t))
+        out["rel_err_x_vs_truth"] = max(rel(normalize(X[:, c]), normalize(truth.x[:, c]))
+                                        for c in range(t))
+        out["oracle_rel_err_demeaned_vs_truth"] = max(rel(o.demeaned[:, c], truth.demeaned[:, c]) for c in range(t))
+        out["oracle_rel_err_x_vs_truth"] = max(rel(normalize(o.x[:, c]), normalize(truth.x[:, c]))
+                                               for c in range(t))
+    return out
+
+
+def device_solve(L, h, dY, k, dX, dD, st, steps, warmup=1):
+    """Event-timed batched solves on device buffers; returns ms per solve."""
+    import torch
+    for _ in range(warmup):
+        _check_rc(L, L.within_solver_solve_batch_device(h, C.c_void_p(dY.data_ptr()), k, C.c_void_p(dX.data_ptr()),
+                                                        C.c_void_p(dD.data_ptr()), st, None))
+    torch.cuda.synchronize()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record()
+    for _ in range(steps):
+        _check_rc(L, L.within_solver_solve_batch_device(h, C.c_void_p(dY.data_ptr()), k, C.c_void_p(dX.data_ptr()),
+                                                        C.c_void_p(dD.data_ptr()), st, None))
+    a1.record()
+    torch.cuda.synchronize()
+    return a0.elapsed_time(a1) / steps
+
+
+def _check_rc(L, rc):
+    if rc != 0:
+        raise RuntimeError(L.within_last_error().decode(errors="replace"))
+
+
+def profile_step(L, solver, step):
+    """One untimed step with event timing of the operator and Schwarz applies: returns
+    {which: (launches, total ms)} for 0/1 operator FP64/FP32, 2/3 Schwarz FP64/FP32."""
+    import torch
+    L.within_solver_set_profiling(solver._h, 1)
+    step()
+    torch.cuda.synchronize()
+    kt = {}
+    for which in range(4):
+        cnt, ms = C.c_int64(), C.c_double()
+        L.within_solver_kernel_time(solver._h, which, C.byref(cnt), C.byref(ms))
+        kt[which] = (cnt.value, ms.value)
+    L.within_solver_set_profiling(solver._h, 0)
+    return kt
+
+
+def op_roofline(kt, which, op_bytes, peak, peak_src, kernel):
+    cnt, ms = kt[which]
+    achieved = op_bytes / (ms / cnt / 1000.0) / 1e9 if cnt else None
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
+            "algorithmic_bytes_per_launch": int(op_bytes), "launches": cnt,
+            "avg_launch_us": 1000.0 * ms / cnt if cnt else None}
+
+
+def secondary_arms(L, wb, torch, peak, peak_src):
+    """Configs 1 and 2 at their stated sizes, with the oracle's CPU time beside each (the
+    oracle on all host threads, one RHS per thread), and the GPU results' error against
+    the oracle at the same tol."""
+    from within_b200 import synthetic
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    threads = max(1, min(16, os.cpu_count() or 1))
+    out = {}
+
+    def arm(name, cats, Y, w, cfgs, ac_split=None):
+        n, k = Y.shape
+        pre = None
+        okw = {}
+        if ac_split is not None:
+            # SchurComplement(approx_chol=...) keeps the exact Schur complement, as the
+            # reference's Python class does by default (python/within/_within.pyi:490-513)
+            pre = wb.AdditiveSchwarz(local_solver=wb.SchurComplement(approx_chol=wb.ApproxCholConfig(seed=0, split=ac_split)))
+            okw = {"approx_chol_split": ac_split, "approx_schur": None}
+        t0 = time.perf_counter()
+        os_ = oracle.OracleSolver(cats, w, **okw)
+        t_set = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        o = os_.solve_batch(Y, threads=threads)
+        t_cpu = time.perf_counter() - t0
+        res = {"n_obs": n, "n_rhs": k,
+               "cpu_oracle": {"value": k / t_cpu, "unit": "RHS/s", "cores": threads, "kind": "port",
+                              "setup_s": t_set, "iterations": o.iterations}}
+        dY = torch.from_numpy(np.ascontiguousarray(Y.T)).cuda()
+        for prec in cfgs:
+            t0 = time.perf_counter()
+            s = wb.Solver(cats, wb.CG(precision=prec), weights=w, preconditioner=pre)
+            t_gset = time.perf_counter() - t0
+            m = s.n_dofs
+            dX = torch.empty((k, m), dtype=torch.float64, device="cuda")
+            dD = torch.empty((k, n), dtype=torch.float64, device="cuda")
+            st = (wb._lib.Stats * k)()
+            ms = device_solve(L, s._h, dY, k, dX, dD, st, steps=5, warmup=2)
+            X = dX.cpu().numpy().T
+            D = dD.cpu().numpy().T
+            acc = accuracy_vs_oracle(cats, X, D, o, None)
+            res[prec] = {"value": k / (ms / 1000.0), "unit": "RHS/s", "ms_per_step": ms, "setup_s": t_gset,
+                         "converged": all(bool(st[c].converged) for c in range(k)),
+                         "max_final_residual": max(float(st[c].final_residual) for c in range(k)),
+                         "iterations": [int(st[c].iterations) for c in range(k)], **acc}
+            del s
+        out[name] = res
+
+    c, Y, w = synthetic.config1()
+    arm("config1_split1", c, Y, w, ["fp64", "mixed"], ac_split=1)
+    arm("config1_split2_default", c, Y, w, ["fp64", "mixed"], ac_split=2)
+    c, Y, w = synthetic.config2()
+    arm("config2", c, np.asfortranarray(Y), w, ["fp64", "mixed"])
+    return out
 
 
 def reference_arm(args):
@@ -252,6 +395,24 @@ def uneven(args):
     clk = clocks.stop()
     conv = all(all(r.converged) for r in res)
     worst = max(max(r.residual) for r in res)
+    # CPU baseline: the oracle on a sample of the problems, one after another, setup
+    # included as in the GPU arm, the RHS of a problem in parallel over the host threads
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        threads = max(1, min(16, os.cpu_count() or 1))
+        idx = np.random.default_rng(1).choice(len(probs), size=min(24, len(probs)), replace=False)
+        t0 = time.perf_counter()
+        rhs = 0
+        for j in idx:
+            c, Yj = probs[j]
+            oracle.OracleSolver(c, None).solve_batch(Yj, threads=threads)
+            rhs += Yj.shape[1]
+        dt = time.perf_counter() - t0
+        cpu = {"value": rhs / dt, "unit": "RHS/s", "cores": threads, "kind": "port",
+               "sample": f"{len(idx)} of the {len(probs)} problems (seeded choice, {rhs} RHS), setup included, "
+                         f"one problem at a time"}
     line = {"metric": "RHS solved/sec at tol 1e-8, uneven batch of independent problems (setup included)",
             "value": args.steps * n_rhs / el, "unit": "RHS/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
@@ -264,6 +425,8 @@ def uneven(args):
                                    f"{os.cpu_count()} problems in flight (one per host core)",
                        "timing": "host wall clock, device synchronised"},
             "clocks": clk, "accuracy": {"converged": conv, "max_final_residual": worst}}
+    if cpu:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
 
 
@@ -283,6 +446,9 @@ def ours(args):
     L = _lib.load()
 
     cats, Y, w = workload(args.scale)
+    if args.shuffle:  # rows in arbitrary order: the device sort by the primary factor is not the identity
+        perm = np.random.default_rng(123).permutation(cats.shape[0])
+        cats, Y, w = np.asfortranarray(cats[perm]), np.asfortranarray(Y[perm]), (None if w is None else w[perm])
     n, k = Y.shape
     t0 = time.perf_counter()
     op = wb.OperatorRepr.Explicit if args.operator == "explicit" else wb.OperatorRepr.Implicit
@@ -296,10 +462,9 @@ def ours(args):
     st = (_lib.Stats * k)()
 
     def step():
-        rc = L.within_solver_solve_batch_device(solver._h, C.c_void_p(dY.data_ptr()), k, C.c_void_p(dX.data_ptr()),
-                                                C.c_void_p(dD.data_ptr()), st, None)
-        if rc != 0:
-            raise RuntimeError(_lib.last_error())
+        _check_rc(L, L.within_solver_solve_batch_device(solver._h, C.c_void_p(dY.data_ptr()), k,
+                                                        C.c_void_p(dX.data_ptr()), C.c_void_p(dD.data_ptr()), st,
+                                                        None))
 
     for _ in range(args.warmup):
         step()
@@ -321,18 +486,11 @@ def ours(args):
     conv = [bool(st[c].converged) for c in range(k)]
     res = [float(st[c].final_residual) for c in range(k)]
     iters = [int(st[c].iterations) for c in range(k)]
+    X_gpu, D_gpu = dX.cpu().numpy().T.copy(), dD.cpu().numpy().T.copy()  # the last timed step's solutions
     # one more (untimed) step with per-launch event timing of the operator and Schwarz
     # applies; event timing runs the CG iterations launch by launch instead of as the
     # captured graph, so it stays out of the timed region
-    L.within_solver_set_profiling(solver._h, 1)
-    step()
-    torch.cuda.synchronize()
-    kt = {}
-    for which in range(4):
-        cnt, ms = C.c_int64(), C.c_double()
-        L.within_solver_kernel_time(solver._h, which, C.byref(cnt), C.byref(ms))
-        kt[which] = (cnt.value, ms.value)
-    L.within_solver_set_profiling(solver._h, 0)
+    kt = profile_step(L, solver, step)
     if dist:
         elapsed_ms = max_over_ranks(dist, elapsed_ms)
     value = world * args.steps * k / (elapsed_ms / 1000.0)
@@ -344,10 +502,8 @@ def ours(args):
     e2e_steps = max(1, min(args.steps, 3))
 
     def host_step():
-        rc = L.within_solver_solve_batch(solver._h, C.c_void_p(hY.data_ptr()), k, C.c_void_p(hX.data_ptr()),
-                                         C.c_void_p(hD.data_ptr()), st)
-        if rc != 0:
-            raise RuntimeError(_lib.last_error())
+        _check_rc(L, L.within_solver_solve_batch(solver._h, C.c_void_p(hY.data_ptr()), k, C.c_void_p(hX.data_ptr()),
+                                                 C.c_void_p(hD.data_ptr()), st))
 
     host_step()
     torch.cuda.synchronize()
@@ -364,22 +520,31 @@ def ours(args):
         e2e_ms = max_over_ranks(dist, e2e_ms)
     e2e_value = world * e2e_steps * k / (e2e_ms / 1000.0)
 
-    # roofline of the dominant kernel: the operator apply G x = D'W(D x)
+    # roofline of the dominant kernel: the operator apply G x = D'W(D x), with algorithmic
+    # bytes n (4Q + s w) + 2 s m kp (codes, weights, x read and y written once)
     peaks = json.load(open(PEAKS)) if os.path.exists(PEAKS) else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
     Q = cats.shape[1]
-    which = 1 if args.precision == "mixed" else 0
+    kp = 4 if k <= 4 else 8 if k <= 8 else 16 if k <= 16 else 32
+    wt = 1 if w is not None else 0
+
+    def obs_bytes(s_b):
+        return n * (4 * Q + s_b * wt) + 2 * s_b * m * kp
+
+    which = 1 if (args.precision == "mixed" and args.krylov == "cg") else 0
     s_b = 4 if which == 1 else 8
-    op_bytes = n * (4 * Q + s_b * (1 if w is not None else 0)) + 2 * s_b * m * k
-    cnt, ms = kt[which]
-    achieved = op_bytes / (ms / cnt / 1000.0) / 1e9 if cnt else None
-    roofline = {"bound": "hbm", "kernel": "obs_pass_kernel (operator apply D'W(D x), %s)" % ("FP32" if which else "FP64"),
-                "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": op_bytes, "launches": cnt,
-                "avg_launch_us": 1000.0 * ms / cnt if cnt else None, "traffic": None,
-                "schwarz_apply_avg_us": 1000.0 * kt[which + 2][1] / kt[which + 2][0] if kt[which + 2][0] else None}
+    roofline = op_roofline(kt, which, obs_bytes(s_b), peak, peak_src,
+                           "obs_pass_kernel (operator apply D'W(D x), %s)" % ("FP32" if which else "FP64"))
+    roofline["traffic"] = None
+    sch_bytes = int(L.within_solver_schwarz_bytes(solver._h, kp, s_b))
+    scnt, sms = kt[which + 2]
+    roofline["schwarz_apply"] = {
+        "algorithmic_bytes_per_apply": sch_bytes, "avg_us": 1000.0 * sms / scnt if scnt else None,
+        "achieved": sch_bytes / (sms / scnt / 1000.0) / 1e9 if scnt else None, "unit": "GB/s",
+        "frac": sch_bytes / (sms / scnt / 1000.0) / 1e9 / peak if scnt else None,
+        "bytes_model": "per subdomain 2(4+s)nnz(C)+12 n_i+2 s n_i kp, + s(n_keep-1)^2 dense or "
+                       "2(4+s)nnz(L_AC)+s n_core^2 (within_solver_schwarz_bytes)"}
     if args.operator == "explicit":
         # CSR SpMV of G: row pointers, column indices and values once, x read and y
         # written once (nnz(G) = m + 2 x distinct level pairs of every factor pair)
@@ -387,61 +552,141 @@ def ours(args):
         for a in range(Q):
             for b in range(a + 1, Q):
                 nnz += 2 * int(np.unique(cats[:, a].astype(np.int64) * (int(cats[:, b].max()) + 1) + cats[:, b]).size)
-        op_bytes = (m + 1) * 8 + nnz * (4 + s_b) + 2 * s_b * m * k
-        achieved = op_bytes / (ms / cnt / 1000.0) / 1e9 if cnt else None
-        roofline.update({"kernel": "csr_rows_kernel (explicit Gramian SpMV, %s)" % ("FP32" if which else "FP64"),
-                         "achieved": achieved, "frac": (achieved / peak) if achieved else None,
-                         "algorithmic_bytes_per_launch": op_bytes, "gramian_nnz": nnz})
-    # DRAM bytes (dram__bytes_read.sum + write.sum) of one FP32 operator apply, from an ncu
-    # capture of the same panel at half size (5M observations), scaled by the observations
-    if which == 1 and abs(args.scale - 1.0) < 1e-9 and args.operator == "implicit":
-        roofline["traffic"] = int(2 * 111.6e6)
-        roofline["traffic_source"] = "ncu dram__bytes_read+write at 5M observations, x2 (scales with n)"
+        op_b = (m + 1) * 8 + nnz * (4 + s_b) + 2 * s_b * m * kp
+        rf = op_roofline(kt, which, op_b, peak, peak_src,
+                         "csr_rows_kernel (explicit Gramian SpMV, %s)" % ("FP32" if which else "FP64"))
+        rf["gramian_nnz"] = nnz
+        rf["schwarz_apply"] = roofline["schwarz_apply"]
+        roofline = rf
+        roofline["traffic"] = None
+    elif abs(args.scale - 1.0) < 1e-9 and not args.shuffle and args.krylov == "cg":
+        # DRAM bytes (dram__bytes_read.sum + write.sum) of one launch of this kernel on this
+        # workload, from an ncu capture (not measured by this run)
+        tr = TRAFFIC.get("fp32" if which == 1 else "fp64")
+        if tr:
+            roofline["traffic"] = tr[0]
+            roofline["traffic_source"] = tr[1]
 
     line = {"metric": METRIC, "value": value, "unit": "RHS/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 inner / f64 refinement" if args.precision == "mixed" else "f64",
+            "dtype": "f32 inner / f64 refinement" if which == 1 else "f64",
             "data": "synthetic (seeded generator with the reference benchmark's AKM shapes)",
-            "config": dict(config_dict(cats, k, args.scale, args.precision, args.operator), krylov=args.krylov),
+            "config": dict(config_dict(cats, k, args.scale, args.precision, args.operator), krylov=args.krylov,
+                           rows="shuffled" if args.shuffle else "worker-major"),
             "e2e": {"value": e2e_value, "unit": "RHS/s", "h2d_bytes_per_step": int(n * k * 8),
                     "d2h_bytes_per_step": int((m + n) * k * 8)},
             "gpu_launches": int(launches), "roofline": roofline, "clocks": clk,
             "accuracy": {"converged": all(conv), "max_final_residual": max(res), "iterations": iters},
             "setup_s": setup_s}
 
-    # the plain FP64 drop-in on the same inputs (the metric's denominator)
-    if args.precision == "mixed" and not args.no_dropin and args.krylov == "cg":
+    # the plain FP64 drop-in on the same inputs (the metric's denominator), with the
+    # roofline of its own operator apply (FP64) and Schwarz apply
+    X64 = D64 = None
+    if which == 1 and not args.no_dropin:
         d64 = wb.Solver(cats, wb.CG(precision="fp64"), weights=w)
-        for _ in range(max(1, args.warmup - 1)):
-            L.within_solver_solve_batch_device(d64._h, C.c_void_p(dY.data_ptr()), k, C.c_void_p(dX.data_ptr()),
-                                               C.c_void_p(dD.data_ptr()), st, None)
-        torch.cuda.synchronize()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record()
-        for _ in range(args.steps):
-            L.within_solver_solve_batch_device(d64._h, C.c_void_p(dY.data_ptr()), k, C.c_void_p(dX.data_ptr()),
-                                               C.c_void_p(dD.data_ptr()), st, None)
-        a1.record()
-        torch.cuda.synchronize()
-        d_ms = a0.elapsed_time(a1)
+        d_ms = device_solve(L, d64._h, dY, k, dX, dD, st, steps=args.steps, warmup=max(1, args.warmup - 1))
+        X64, D64 = dX.cpu().numpy().T.copy(), dD.cpu().numpy().T.copy()
         if dist:
             d_ms = max_over_ranks(dist, d_ms)
-        line["fp64_dropin"] = {"value": world * args.steps * k / (d_ms / 1000.0), "unit": "RHS/s",
-                               "ms_per_step": d_ms / args.steps,
+
+        def d64_step():
+            _check_rc(L, L.within_solver_solve_batch_device(d64._h, C.c_void_p(dY.data_ptr()), k,
+                                                            C.c_void_p(dX.data_ptr()), C.c_void_p(dD.data_ptr()),
+                                                            st, None))
+
+        kt64 = profile_step(L, d64, d64_step)
+        rf64 = op_roofline(kt64, 0, obs_bytes(8), peak, peak_src, "obs_pass_kernel (operator apply D'W(D x), FP64)")
+        s64 = int(L.within_solver_schwarz_bytes(d64._h, kp, 8))
+        c64, m64 = kt64[2]
+        rf64["schwarz_apply"] = {"algorithmic_bytes_per_apply": s64, "avg_us": 1000.0 * m64 / c64 if c64 else None,
+                                 "achieved": s64 / (m64 / c64 / 1000.0) / 1e9 if c64 else None, "unit": "GB/s",
+                                 "frac": s64 / (m64 / c64 / 1000.0) / 1e9 / peak if c64 else None}
+        if abs(args.scale - 1.0) < 1e-9 and not args.shuffle and "fp64" in TRAFFIC:
+            rf64["traffic"], rf64["traffic_source"] = TRAFFIC["fp64"]
+        line["fp64_dropin"] = {"value": world * k / (d_ms / 1000.0), "unit": "RHS/s", "ms_per_step": d_ms,
                                "converged": all(bool(st[c].converged) for c in range(k)),
-                               "max_final_residual": max(float(st[c].final_residual) for c in range(k))}
-        line["speedup_vs_fp64_dropin"] = line["fp64_dropin"]["ms_per_step"] / line["ms_per_step"]
+                               "max_final_residual": max(float(st[c].final_residual) for c in range(k)),
+                               "iterations": [int(st[c].iterations) for c in range(k)],
+                               "roofline": rf64}
+        line["speedup_vs_fp64_dropin"] = d_ms / line["ms_per_step"]
         del d64
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = max(1, min(4, os.cpu_count() or 1))
-        line["cpu_baseline"] = cpu_baseline_run(cats, Y, w, threads, threads)
+        threads = max(1, min(16, os.cpu_count() or 1))
+        cb, o, truth = cpu_baseline_run(cats, Y, w, min(k, threads), threads, truth_rhs=min(k, 4))
+        line["cpu_baseline"] = cb
+        line["accuracy"].update(accuracy_vs_oracle(cats, X_gpu[:, :o.x.shape[1]], D_gpu[:, :o.x.shape[1]], o, truth))
+        if X64 is not None:
+            line["fp64_dropin"]["accuracy"] = accuracy_vs_oracle(cats, X64[:, :o.x.shape[1]], D64[:, :o.x.shape[1]],
+                                                                 o, truth)
+    if rank == 0 and world == 1 and not args.no_secondary and args.scale == 1.0 and not args.shuffle:
+        del solver
+        line["secondary"] = secondary_arms(L, wb, torch, peak, peak_src)
+        line["secondary"]["gmres30_multiplicative_fp64"] = gmres_cross(L, wb, torch, cats, Y, w, D_gpu)
+        line["secondary"]["shuffled_rows"] = shuffled_arm(L, wb, torch, cats, Y, w, args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def gmres_cross(L, wb, torch, cats, Y, w, D_ref):
+    """The cross-check of the headline: GMRES(30) + multiplicative Schwarz, FP64, one RHS
+    (the first), against the headline's demeaned residuals of the same RHS."""
+    n = cats.shape[0]
+    t0 = time.perf_counter()
+    s = wb.Solver(cats, wb.GMRES(restart=30), weights=w, preconditioner=wb.MultiplicativeSchwarz())
+    t_set = time.perf_counter() - t0
+    m = s.n_dofs
+    dY = torch.from_numpy(np.ascontiguousarray(Y[:, :1].T)).cuda()
+    dX = torch.empty((1, m), dtype=torch.float64, device="cuda")
+    dD = torch.empty((1, n), dtype=torch.float64, device="cuda")
+    st = (wb._lib.Stats * 1)()
+    ms = device_solve(L, s._h, dY, 1, dX, dD, st, steps=2, warmup=1)
+    D = dD.cpu().numpy()[0]
+    return {"value": 1000.0 / ms, "unit": "RHS/s", "ms_per_rhs": ms, "setup_s": t_set,
+            "converged": bool(st[0].converged), "iterations": int(st[0].iterations),
+            "final_residual": float(st[0].final_residual),
+            "rel_diff_demeaned_vs_headline": rel(D, D_ref[:, 0])}
+
+
+def shuffled_arm(L, wb, torch, cats, Y, w, args):
+    """The headline workload with its rows in a random order (the primary-factor sort is
+    then a real permutation, and the transposes go through it): value and e2e."""
+    perm = np.random.default_rng(123).permutation(cats.shape[0])
+    c2, Y2 = np.asfortranarray(cats[perm]), np.asfortranarray(Y[perm])
+    w2 = None if w is None else w[perm]
+    n, k = Y2.shape
+    t0 = time.perf_counter()
+    s = wb.Solver(c2, wb.CG(precision=args.precision), weights=w2)
+    t_set = time.perf_counter() - t0
+    m = s.n_dofs
+    dY = torch.from_numpy(np.ascontiguousarray(Y2.T)).cuda()
+    dX = torch.empty((k, m), dtype=torch.float64, device="cuda")
+    dD = torch.empty((k, n), dtype=torch.float64, device="cuda")
+    st = (wb._lib.Stats * k)()
+    ms = device_solve(L, s._h, dY, k, dX, dD, st, steps=3, warmup=2)
+    del dY, dX, dD
+    hY = torch.from_numpy(np.ascontiguousarray(Y2.T)).pin_memory()
+    hX = torch.empty((k, m), dtype=torch.float64).pin_memory()
+    hD = torch.empty((k, n), dtype=torch.float64).pin_memory()
+    _check_rc(L, L.within_solver_solve_batch(s._h, C.c_void_p(hY.data_ptr()), k, C.c_void_p(hX.data_ptr()),
+                                             C.c_void_p(hD.data_ptr()), st))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(2):
+        _check_rc(L, L.within_solver_solve_batch(s._h, C.c_void_p(hY.data_ptr()), k, C.c_void_p(hX.data_ptr()),
+                                                 C.c_void_p(hD.data_ptr()), st))
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / 2
+    return {"value": k / (ms / 1000.0), "unit": "RHS/s", "ms_per_step": ms, "setup_s": t_set,
+            "e2e": {"value": k / (e2e_ms / 1000.0), "unit": "RHS/s"},
+            "converged": all(bool(st[c].converged) for c in range(k)),
+            "max_final_residual": max(float(st[c].final_residual) for c in range(k))}
 
 
 def main():

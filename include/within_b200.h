@@ -240,6 +240,49 @@ void within_solver_ac_arrays(const within_solver *solver, int32_t i, int32_t *le
                              int32_t *col_idx, double *col_coef, int32_t *core_vertex,
                              double *core_z);
 
+/* Coarse space for CG (no counterpart in the reference; it augments the additive Schwarz
+ * apply, schwarz-precond/src/schwarz/additive/executor.rs:59-147, inside CG,
+ * schwarz-precond/src/solve/cg.rs:45-133).  With a coarse basis Z (n_dofs x 32), CG's
+ * preconditioner becomes M^-1 r + Z E^+ Z' r with E = Z' G Z (FP64; E^+ drops the
+ * null-space directions of G), which is symmetric positive semi-definite, so CG stays
+ * valid and every solve still runs to the same tolerance.  GMRES, LSMR and
+ * apply_preconditioner do not use it.
+ *
+ * The learned basis comes from a message-passing network over the level graph (one node
+ * per level; edges weighted by the off-diagonal of G = D'WD): 16 input features per level
+ * (factor, log weighted count, log count, 10 hashed probe signs from `seed`), three
+ * layers H' = tanh([Ahat H, H] W + b) of 64 units with Ahat = D^-1/2 (G - diag G) D^-1/2,
+ * and Z = D^-1/2 H W_o.  Weights are used in BF16 (tensor cores, FP32 accumulation); the
+ * parameter vector is FP32 (W_0 32x64, b_0, W_1 128x64, b_1, W_2 128x64, b_2, W_o 64x32,
+ * row-major): within_coarse_net_params() values.
+ *
+ * set_coarse_net: evaluate the network on the solver's design and install its basis.
+ * set_coarse_basis: install a given basis (Z: n_dofs x k, RHS-major, k <= 32).
+ * clear_coarse: back to plain Schwarz.  coarse_basis: the installed basis (n_dofs x 32).
+ * set_coarse_targets / coarse_net_grad: training on this design: targets V (n_dofs x t,
+ * t <= 32, orthonormal columns in the D^1/2-scaled space), loss
+ * L = 1 - tr(B' A^-1 B)/t with A = Zt'Zt, B = Zt'V (Zt = D^1/2 Z: the fraction of the
+ * targets outside span(Z)), its gradient for every parameter (FP32, same layout), and
+ * optionally Zt (n_dofs x 32 RHS-major).  release_coarse_training frees the buffers. */
+int32_t within_coarse_net_params(void);
+int within_solver_set_coarse_net(within_solver *solver, const float *params, size_t n_params, uint64_t seed);
+int within_solver_set_coarse_basis(within_solver *solver, const double *z, size_t k);
+int within_solver_clear_coarse(within_solver *solver);
+int within_solver_coarse_basis(within_solver *solver, double *z);
+int within_solver_set_coarse_targets(within_solver *solver, const double *v, size_t t);
+int within_coarse_net_grad(within_solver *solver, const float *params, uint64_t seed, float *grad, double *loss,
+                           float *zt);
+int within_solver_release_coarse_training(within_solver *solver);
+
+/* Algorithmic bytes of one Schwarz apply over k RHS with elem_bytes (4 or 8) per vector
+ * element, counted from the built subdomains: per subdomain 2 (4+s) nnz(C_i) for the
+ * cross block read twice (reduced right-hand side and back substitution), 12 n_i for the
+ * slots' indices and weights, 2 s n_i k for the local vector, plus s (n_keep-1)^2 for a
+ * dense anchored factor or 2 (4+s) nnz(L_AC) + s n_core^2 for an approximate-Cholesky
+ * factor.  0 for a solver without subdomains.  A measurement hook with no counterpart in
+ * the reference (the per-subdomain sizes follow local_solver.rs:360-449). */
+int64_t within_solver_schwarz_bytes(const within_solver *solver, int32_t k, int32_t elem_bytes);
+
 /* Number of kernels this solver has launched so far, and its setup wall time (s).
  * Measurement hooks with no counterpart in the reference. */
 int64_t within_solver_gpu_launches(const within_solver *solver);

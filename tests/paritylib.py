@@ -1,12 +1,13 @@
-"""Helpers shared by the GPU parity tests."""
+"""Helpers shared by the GPU parity tests (and the accuracy report of bench.py)."""
 import numpy as np
 import scipy.sparse as sp
 from scipy.sparse.csgraph import connected_components
 
 
-def normalize_x(cats, x):
-    """x modulo the null space of G: in every connected component of the level graph,
-    each factor q >= 1 is centred and its mean moved onto factor 0 (D x is unchanged)."""
+def make_normalizer(cats):
+    """A function x -> x modulo the null space of G: in every connected component of the
+    level graph, each factor q >= 1 is centred and its mean moved onto factor 0 (D x is
+    unchanged).  The component structure is computed once per design."""
     cats = np.asarray(cats)
     n, Q = cats.shape
     nlev = cats.max(axis=0).astype(np.int64) + 1
@@ -19,18 +20,27 @@ def normalize_x(cats, x):
     active = np.zeros(m, bool)
     for q in range(Q):
         active[off[q] + np.unique(cats[:, q])] = True
-    x = np.asarray(x, dtype=np.float64).copy()
     fac = np.concatenate([np.full(nlev[q], q) for q in range(Q)])
-    for q in range(1, Q):
-        sel = (fac == q) & active
-        sums = np.bincount(lab[sel], weights=x[sel], minlength=ncomp)
-        cnt = np.bincount(lab[sel], minlength=ncomp)
-        mean = np.where(cnt > 0, sums / np.maximum(cnt, 1), 0.0)
-        x[sel] -= mean[lab[sel]]
-        s0 = (fac == 0) & active
-        x[s0] += mean[lab[s0]]
-    x[~active] = 0.0
-    return x
+    sel = [(fac == q) & active for q in range(Q)]
+    cnt = [np.bincount(lab[s], minlength=ncomp) for s in sel]
+
+    def normalize(x):
+        x = np.asarray(x, dtype=np.float64).copy()
+        for q in range(1, Q):
+            s = sel[q]
+            sums = np.bincount(lab[s], weights=x[s], minlength=ncomp)
+            mean = np.where(cnt[q] > 0, sums / np.maximum(cnt[q], 1), 0.0)
+            x[s] -= mean[lab[s]]
+            x[sel[0]] += mean[lab[sel[0]]]
+        x[~active] = 0.0
+        return x
+
+    return normalize
+
+
+def normalize_x(cats, x):
+    """x modulo the null space of G (see make_normalizer)."""
+    return make_normalizer(cats)(x)
 
 
 def rel(a, b):

@@ -1,0 +1,99 @@
+"""Coarse space for CG: the message-passing network's device forward and backward passes
+against the CPU oracle of the network (oracle/coarse_net.py), and CG with a coarse space
+against the CPU oracle's solution."""
+import os
+
+import numpy as np
+import pytest
+
+import coarse_net as cn
+import oracle
+import within_b200 as wb
+from within_b200 import coarse, synthetic
+from paritylib import make_normalizer, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _design(weighted, seed=1):
+    cats = synthetic.worker_firm_year(3000, 300, 5, 8, 0.2, seed=seed)
+    w = np.random.default_rng(seed + 1).lognormal(0, 1, cats.shape[0]) if weighted else None
+    return cats, w
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_network_forward_and_gradients_match_oracle(weighted):
+    cats, w = _design(weighted)
+    s = wb.Solver(cats, weights=w)
+    D = cn.Design(cats, w)
+    X = D.features(seed=0)
+    rng = np.random.default_rng(3)
+    P = cn.init_params(5)
+    for k in P:  # non-zero biases, so that every term of the gradient is exercised
+        if k.startswith("b"):
+            P[k] = (0.1 * rng.standard_normal(P[k].shape)).astype(np.float32)
+    flat = cn.flatten(P)
+    assert flat.size == coarse.n_params()
+    V, _ = np.linalg.qr(rng.standard_normal((D.m, 12)))
+    coarse.set_targets(s, V)
+    loss, g, zt = coarse.grad(s, flat, 0, want_z=True)
+    Z, cache = cn.forward(P, D, X)
+    L, dZ, _, _ = cn.loss_and_grad_z(Z, V)
+    go = cn.backward(P, D, cache, dZ)
+    # FP32 device arithmetic against FP64 with the same BF16 roundings: a rounding of the
+    # FP32 input to BF16 can land one BF16 step away from the FP64 one on a few entries
+    assert rel(zt, Z) < 2e-3
+    assert abs(loss - L) < 1e-4
+    gd = cn.unflatten(g.astype(np.float64))
+    for k in cn.PARAM_ORDER:
+        assert rel(gd[k], go[k]) < 1e-2, k
+    coarse.release_training(s)
+
+
+def test_cg_with_an_exact_ritz_basis_matches_the_oracle():
+    cats, w = _design(True, seed=4)
+    y = np.random.default_rng(9).standard_normal(cats.shape[0])
+    s = wb.Solver(cats, weights=w)
+    plain = s.solve(y)
+    d = coarse.level_diagonal(cats, w)
+    V, lam = coarse.ritz_targets(s, d, steps=60, nev=16)
+    Z = V / np.sqrt(np.where(d > 0, d, 1.0))[:, None]
+    s.set_coarse_space(Z)
+    r = s.solve(y)
+    o = oracle.OracleSolver(cats, w).solve(y)
+    truth = oracle.OracleSolver(cats, w, tol=1e-13).solve(y)
+    assert r.converged and r.residual <= 1e-8
+    # the same tolerance, a different Krylov space: held to the oracle's own error
+    # against the tol-1e-13 solution (at least as accurate as the reference's solve)
+    e_o = rel(o.demeaned, truth.demeaned)
+    assert rel(r.demeaned, truth.demeaned) <= max(2 * e_o, 1e-9)
+    NZ = make_normalizer(cats)
+    assert rel(NZ(r.x), NZ(truth.x)) <= max(2 * rel(NZ(o.x), NZ(truth.x)), 1e-8)
+    assert r.iterations <= plain.iterations
+    Zb = s.coarse_basis()
+    assert np.allclose(Zb[:, :Z.shape[1]], Z) and not Zb[:, Z.shape[1]:].any()
+    s.clear_coarse_space()
+    again = s.solve(y)
+    assert again.iterations == plain.iterations
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_learned_coarse_space_solves_to_the_same_tolerance(precision):
+    """The shipped network on a held-out design (switch probability 0.02, outside the
+    training draws' seeds): every RHS meets the same tolerance with at least the
+    reference's accuracy, and the iteration counts with and without it are reported."""
+    if not os.path.exists(coarse.WEIGHTS):
+        pytest.skip("no trained weights shipped")
+    cats = synthetic.worker_firm_year(20_000, 2_000, 10, 20, 0.02, seed=777)
+    Y = np.asfortranarray(np.random.default_rng(8).standard_normal((cats.shape[0], 8)))
+    s = wb.Solver(cats, wb.CG(precision=precision))
+    plain = s.solve_batch(Y)
+    s.set_coarse_space(coarse.CoarseNet.trained())
+    r = s.solve_batch(Y)
+    truth = oracle.OracleSolver(cats, None, tol=1e-13).solve_batch(Y[:, :2])
+    o = oracle.OracleSolver(cats, None).solve_batch(Y[:, :2])
+    assert all(r.converged) and max(r.residual) <= 1e-8
+    for c in range(2):
+        assert rel(r.demeaned[:, c], truth.demeaned[:, c]) <= max(2 * rel(o.demeaned[:, c], truth.demeaned[:, c]), 1e-9)
+    print(f"\n{precision}: iterations plain {plain.iterations} learned {r.iterations}")
+    assert sum(r.iterations) <= sum(plain.iterations) + len(r.iterations)

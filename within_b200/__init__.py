@@ -8,9 +8,11 @@ Mirrors ``within`` (python/within/__init__.py, within-py/src/lib.rs:62-1074):
 device through ``libwithin_b200.so``; invalid input raises ``ValueError``, a bad
 configuration type ``TypeError`` (as within-py does, lib.rs:480-483, 516, 590).
 
-One addition: ``CG``/``GMRES`` take ``precision="fp64"`` (the drop-in: every
+Additions: ``CG``/``GMRES`` take ``precision="fp64"`` (the drop-in: every
 step in FP64) or ``precision="mixed"`` (FP32 operator and Schwarz applies inside
-an FP64 iterative-refinement loop; same tolerance on the FP64 residual).
+an FP64 iterative-refinement loop; same tolerance on the FP64 residual);
+``Solver.set_coarse_space`` adds a coarse space to CG's preconditioner (a basis, or
+the message-passing network of ``within_b200.coarse``).
 """
 from __future__ import annotations
 
@@ -511,6 +513,32 @@ class Solver:
     @property
     def gpu_launches(self) -> int:
         return int(_lib.load().within_solver_gpu_launches(self._h))
+
+    # --- coarse space for CG (an addition: the reference has none) ---
+    def set_coarse_space(self, coarse) -> None:
+        """CG's preconditioner becomes M^-1 r + Z (Z'GZ)^+ Z' r.  ``coarse``: a
+        ``coarse.CoarseNet`` (its network is evaluated on this design on the GPU) or a
+        basis (n_dofs x k array, k <= 32).  GMRES and LSMR ignore it."""
+        from .coarse import CoarseNet
+        L = _lib.load()
+        if isinstance(coarse, CoarseNet):
+            rc = L.within_solver_set_coarse_net(self._h, coarse.params.ctypes.data_as(C.c_void_p), coarse.params.size,
+                                                coarse.seed)
+        else:
+            Z = np.asfortranarray(coarse, dtype=np.float64)
+            if Z.ndim != 2 or Z.shape[0] != self.n_dofs:
+                raise ValueError(f"a coarse basis has {self.n_dofs} rows")
+            rc = L.within_solver_set_coarse_basis(self._h, _lib.ptr(Z), Z.shape[1])
+        _check(rc)
+
+    def clear_coarse_space(self) -> None:
+        _check(_lib.load().within_solver_clear_coarse(self._h))
+
+    def coarse_basis(self) -> np.ndarray:
+        """The installed coarse basis (n_dofs x 32)."""
+        Z = np.empty((self.n_dofs, 32), order="F")
+        _check(_lib.load().within_solver_coarse_basis(self._h, _lib.ptr(Z)))
+        return Z
 
 
 def solve(categories, y, config=None, weights=None, preconditioner=None) -> SolveResult:

@@ -71,7 +71,10 @@ EXPORTED = [
     "within_solver_set_profiling", "within_solver_kernel_time", "within_solver_apply_gramian_noalloc",
     "within_solve_many", "within_solver_subdomain_inner_work", "within_solver_additive_diagnostics",
     "within_solver_preconditioner_bytes", "within_solver_new_with_preconditioner",
-    "within_preconditioner_from_bytes", "within_solver_preconditioner_kind",
+    "within_preconditioner_from_bytes", "within_solver_preconditioner_kind", "within_solver_schwarz_bytes",
+    "within_coarse_net_params", "within_solver_set_coarse_net", "within_solver_set_coarse_basis",
+    "within_solver_clear_coarse", "within_solver_coarse_basis", "within_solver_set_coarse_targets",
+    "within_coarse_net_grad", "within_solver_release_coarse_training",
 ]
 
 _lib = None
@@ -139,6 +142,20 @@ def load():
     L.within_solver_apply_gramian_noalloc.restype = C.c_int
     L.within_solver_set_profiling.argtypes = [vp, C.c_int32]
     L.within_solver_kernel_time.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+    L.within_solver_schwarz_bytes.argtypes = [vp, C.c_int32, C.c_int32]
+    L.within_solver_schwarz_bytes.restype = C.c_int64
+    L.within_coarse_net_params.restype = C.c_int32
+    L.within_solver_set_coarse_net.argtypes = [vp, vp, C.c_size_t, C.c_uint64]
+    L.within_solver_set_coarse_basis.argtypes = [vp, vp, C.c_size_t]
+    L.within_solver_clear_coarse.argtypes = [vp]
+    L.within_solver_coarse_basis.argtypes = [vp, vp]
+    L.within_solver_set_coarse_targets.argtypes = [vp, vp, C.c_size_t]
+    L.within_coarse_net_grad.argtypes = [vp, vp, C.c_uint64, vp, C.POINTER(C.c_double), vp]
+    L.within_solver_release_coarse_training.argtypes = [vp]
+    for f in ("within_solver_set_coarse_net", "within_solver_set_coarse_basis", "within_solver_clear_coarse",
+              "within_solver_coarse_basis", "within_solver_set_coarse_targets", "within_coarse_net_grad",
+              "within_solver_release_coarse_training"):
+        getattr(L, f).restype = C.c_int
     _lib = L
     return L
 

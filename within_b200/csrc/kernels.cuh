@@ -467,6 +467,24 @@ __global__ void __launch_bounds__(kXposeWarps * 32) scatter_deinterleave_kernel(
     }
 }
 
+// Row permutation of an interleaved n x kp FP64 array: out[i] = in[perm[i]] (gather) or
+// out[perm[i]] = in[i] (scatter), in 16-byte pieces.  With a non-identity order the
+// column-major <-> interleaved transposes run in user order (coalesced) and only this
+// pass moves whole rows (one random 16*kp/2-byte access per row instead of kp random
+// 8-byte ones).
+static __global__ void permute_rows_kernel(const double* __restrict__ in, int64_t n, int kp,
+                                    const uint32_t* __restrict__ perm, int scatter, double* __restrict__ out) {
+    const int per_row = kp / 2;
+    const int64_t total = n * per_row;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / per_row;
+        const int c = (int)(t % per_row);
+        const int64_t p = perm[i];
+        const int64_t src = scatter ? i : p, dst = scatter ? p : i;
+        reinterpret_cast<double2*>(out + (size_t)dst * kp)[c] = reinterpret_cast<const double2*>(in + (size_t)src * kp)[c];
+    }
+}
+
 // Blocks for a transpose over `rows` rows (grid-stride beyond 16 blocks per SM).
 inline unsigned xpose_blocks(int64_t rows, int n_sm) {
     const int64_t need = (rows + 32 * kXposeWarps - 1) / (32 * kXposeWarps);
@@ -1058,8 +1076,10 @@ __global__ void __launch_bounds__(kBlock, 4) prolong_kernel(int64_t m, const int
     if (part) block_reduce_store4<G>(dotp, kp, part);
 }
 
-// Multiplicative stage, part 1: c_l = spou_l (sol_l - m2) into cbuf, z[gidx_l] += c_l
-// (dofs are unique within one factor-pair stage).
+// Multiplicative stage, part 1: c_l = spou_l (sol_l - m2); z[gidx_l] += c_l and
+// cneg[gidx_l] = -c_l (dofs are unique within one factor-pair stage; cneg is zero
+// elsewhere).  Part 2 is r_work += G cneg, the assembled Gramian's rows as a CSR SpMV
+// (residual_update.rs:36-53 restricted to the touched columns, which cneg selects).
 template <typename T, int G>
 __global__ void __launch_bounds__(kBlock) mult_sol_kernel(int64_t nslots, const uint32_t* __restrict__ gidx,
                                                           const uint32_t* __restrict__ sub_of,
@@ -1068,7 +1088,7 @@ __global__ void __launch_bounds__(kBlock) mult_sol_kernel(int64_t nslots, const 
                                                           const uint32_t* __restrict__ bs_col,
                                                           const T* __restrict__ bs_val, SubMeans M,
                                                           const T* __restrict__ v, const T* __restrict__ rw,
-                                                          T* __restrict__ z, T* __restrict__ cbuf, int kp) {
+                                                          T* __restrict__ z, T* __restrict__ cneg, int kp) {
     const int c4 = (threadIdx.x & (G - 1)) * 4;
     const int64_t rpb = blockDim.x / G;
     for (int64_t l = (int64_t)blockIdx.x * rpb + threadIdx.x / G; l < nslots; l += (int64_t)gridDim.x * rpb) {
@@ -1080,26 +1100,9 @@ __global__ void __launch_bounds__(kBlock) mult_sol_kernel(int64_t nslots, const 
         const V4<double> u = sp * to_d(ld4(rw + (size_t)g * kp + c4));
         const V4<double> sol = slot_solution<T>((uint32_t)l, u, m0, invd[l], bs_ptr, bs_col, bs_val, v, kp, c4);
         const V4<T> cl = from_d<T>(sp * (sol - m2));
-        st4(cbuf + (size_t)l * kp + c4, cl);
+        st4(cneg + (size_t)g * kp + c4, V4<T>(-cl.a, -cl.b, -cl.c, -cl.d));
         T* zp = z + (size_t)g * kp + c4;
         st4(zp, ld4(zp) + cl);
-    }
-}
-// Multiplicative stage, part 2: r_work -= G[:, gidx_l] c_l (residual_update.rs:36-53).
-template <typename T, int G>
-__global__ void __launch_bounds__(kBlock) mult_resid_kernel(int64_t nslots, const uint32_t* __restrict__ gidx,
-                                                            const T* __restrict__ cbuf,
-                                                            const int64_t* __restrict__ gram_ptr,
-                                                            const uint32_t* __restrict__ gram_col,
-                                                            const T* __restrict__ gram_val, T* __restrict__ rw, int kp) {
-    const int c4 = (threadIdx.x & (G - 1)) * 4;
-    const int64_t rpb = blockDim.x / G;
-    for (int64_t l = (int64_t)blockIdx.x * rpb + threadIdx.x / G; l < nslots; l += (int64_t)gridDim.x * rpb) {
-        const V4<T> cl = ld4(cbuf + (size_t)l * kp + c4);
-        if (!cl.any()) continue;
-        const uint32_t g = gidx[l];
-        for (int64_t e = gram_ptr[g]; e < gram_ptr[g + 1]; ++e)
-            atomic_add4(rw + (size_t)gram_col[e] * kp + c4, (-__ldg(gram_val + e)) * cl);
     }
 }
 

@@ -26,6 +26,7 @@
 #include "device.cuh"
 #include "obs_launch.cuh"
 #include "kernels.cuh"
+#include "coarse.cuh"
 #include "setup.hpp"
 
 namespace wb {
@@ -416,8 +417,8 @@ struct Workspace {
     DArr<double> b, x, r, gx;                // m x kp FP64: rhs, solution, refinement residual, G x
     DArr<double> cx, cr, dz, dp, dap;        // FP64 inner CG vectors
     DArr<float> frhs, fx, fr, fz, fp, fap;   // FP32 inner CG vectors (mixed precision)
-    DArr<double> vloc, cbuf;                 // slots x kp (FP64)
-    DArr<float> floc, fcbuf;                 // slots x kp (FP32)
+    DArr<double> vloc, cbuf;                 // slots x kp; cbuf: m x kp, a multiplicative stage's -correction
+    DArr<float> floc, fcbuf;                 // the same in FP32
     DArr<double> core_tmp;
     DArr<float> fcore_tmp;
     DArr<double> rwork;                      // multiplicative residual
@@ -493,6 +494,7 @@ struct SolverImpl {
     DArr<double> host_y, host_x, host_dem;  // device side of the host-buffer entry points
     std::shared_ptr<void> gmres;  // GmresBufs, created on first GMRES solve
     std::shared_ptr<void> lsmr;   // LsmrBufs, created on first LSMR solve
+    std::shared_ptr<void> cn;     // CnState of the coarse-space network, kept while training
     bool precond_only = false;    // built from a serialized preconditioner: no design
     std::vector<uint8_t> pc_bytes;  // serialized preconditioner, made on first request
     int32_t* h_active = nullptr;  // pinned
@@ -509,6 +511,14 @@ struct SolverImpl {
     cudaGraphExec_t cg_exec = nullptr;
     std::array<uintptr_t, 9> cg_key{};
     int64_t cg_launches = 0;  // kernels in one captured iteration
+    // Coarse space (learned by the message-passing network, or given): CG adds
+    // Z E^+ Z' r to the Schwarz output.  Z is n_dofs x 32 row-major (unused columns zero).
+    int32_t coarse_k = 0;
+    DArr<double> coarse_z64, coarse_einv, coarse_part, coarse_u;
+    DArr<float> coarse_z32;
+    // training targets of the network on this design (n_dofs x t, scaled space)
+    DArr<float> cn_targets;
+    int32_t cn_t = 0;
 
     ~SolverImpl() {
         for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
@@ -874,12 +884,19 @@ void launch_csr(SolverImpl& S, CsrDev<T>& c, int64_t ch0, int64_t ch1, const T* 
 // assembled Gramian): y = 0, then the CSR rows of G, one warp per row, the pieces of
 // long rows added atomically.
 template <typename T>
+void launch_gram_acc(SolverImpl& S, int kp, const T* x, T* y);
+template <typename T>
 void launch_gram(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
     if (!S.explicit_op) {
         launch_obs<T, OBS_GRAM>(S, kp, w, x, nullptr, y, nullptr);
         return;
     }
     WB_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * (size_t)S.d.ndofs * kp, S.stream));
+    launch_gram_acc<T>(S, kp, x, y);
+}
+// y += G x with the assembled Gramian
+template <typename T>
+void launch_gram_acc(SolverImpl& S, int kp, const T* x, T* y) {
     const int G = group_for(kp);
     const int64_t need = (S.g_nchunks * 32 + kBlock - 1) / kBlock;  // one warp per chunk
     WB_DISPATCH_G(G, {
@@ -1034,21 +1051,45 @@ void apply_precond(SolverImpl& S, const T* r, T* z, int kp, double* part, int& n
     }
     // multiplicative: sequential stages (one per factor pair), residual updated after each
     T* rw = rwork_buf<T>(S);
-    T* cb = cbuf<T>(S);
+    T* cb = cbuf<T>(S);  // -(this stage's correction) on global dofs
     WB_CUDA(cudaMemcpyAsync(rw, r, sizeof(T) * m * kp, cudaMemcpyDeviceToDevice, S.stream));
     WB_CUDA(cudaMemsetAsync(z, 0, sizeof(T) * m * kp, S.stream));
     for (auto& st : sts) {
         const SubMeans M = stage_local_solve<T>(S, st, rw, v, kp);
         const int grid = S.nblk(st.nslots, G);
+        WB_CUDA(cudaMemsetAsync(cb, 0, sizeof(T) * m * kp, S.stream));
         WB_DISPATCH_G(G, mult_sol_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(
                              st.nslots, st.gidx.p, st.sub_of.p, st.spou.p, st.invd.p, st.bs_ptr.p, st.bs_col.p,
                              st.bs_val.p, M, v, rw, z, cb, kp));
-        WB_DISPATCH_G(G, mult_resid_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(st.nslots, st.gidx.p, cb, S.g_ptr.p,
-                                                                                S.g_idx.p, gram_val<T>(S), rw, kp));
         WB_CUDA(cudaGetLastError());
-        S.gpu_launches += 2;
+        S.gpu_launches++;
+        launch_gram_acc<T>(S, kp, cb, rw);  // r_work -= G c
     }
     if (part) launch_dot<T, T>(S, r, z, m, kp, part, nb_part);
+}
+
+template <typename T> const T* coarse_basis(SolverImpl& S);
+template <> const double* coarse_basis<double>(SolverImpl& S) { return S.coarse_z64.p; }
+template <> const float* coarse_basis<float>(SolverImpl& S) { return S.coarse_z32.p; }
+constexpr int kCoarseDotBlocksPerSm = 2;
+
+// The CG preconditioner: z = M^{-1} r and, with a coarse space, z += Z E^+ Z' r.  The
+// block partials of r.z (part, nb_part rows) then get one more row, c.u with c = Z' r and
+// u = E^+ c, so that the caller's reduction covers both terms.
+template <typename T>
+void apply_precond_cg(SolverImpl& S, const T* r, T* z, int kp, double* part, int& nb_part) {
+    apply_precond<T>(S, r, z, kp, part, nb_part);
+    if (S.coarse_k == 0) return;
+    const T* Z = coarse_basis<T>(S);
+    const int64_t m = S.d.ndofs;
+    const int nbc = S.n_sm * kCoarseDotBlocksPerSm;
+    coarse_dot_kernel<T><<<nbc, 256, 0, S.stream>>>(m, Z, r, kp, S.coarse_part.p);
+    coarse_solve_kernel<<<1, 256, 0, S.stream>>>(S.coarse_part.p, nbc, S.coarse_einv.p, kp, S.coarse_u.p, part,
+                                                 nb_part);
+    coarse_add_kernel<T><<<S.nblk(m * kp, 1), 256, 0, S.stream>>>(m, Z, S.coarse_u.p, kp, z);
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches += 3;
+    if (part) nb_part += 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -1185,11 +1226,11 @@ void ensure_ws(SolverImpl& S, int kp) {
         for (DArr<float>* a : {&w.frhs, &w.fx, &w.fr, &w.fz, &w.fp, &w.fap}) a->alloc(m * kp);
         w.floc.alloc(std::max<size_t>(1, S.max_slots * kp));
         w.fcore_tmp.alloc(std::max<size_t>(1, S.max_core_total * kp));
-        if (S.pc.kind == 2) { w.frwork.alloc(m * kp); w.fcbuf.alloc(std::max<size_t>(1, S.max_slots * kp)); }
+        if (S.pc.kind == 2) { w.frwork.alloc(m * kp); w.fcbuf.alloc(m * kp); }
     }
     w.vloc.alloc(std::max<size_t>(1, S.max_slots * kp));
     w.core_tmp.alloc(std::max<size_t>(1, S.max_core_total * kp));
-    if (S.pc.kind == 2) { w.rwork.alloc(m * kp); w.cbuf.alloc(std::max<size_t>(1, S.max_slots * kp)); }
+    if (S.pc.kind == 2) { w.rwork.alloc(m * kp); w.cbuf.alloc(m * kp); }
     w.msum.alloc(std::max<size_t>(1, 6 * (size_t)std::max(S.max_nsub, 1) * kp));  // S0, SB, M1, M2, means
     w.part.alloc((size_t)S.n_sm * 8 * kp + 64);
     w.red.alloc(32);
@@ -1221,7 +1262,7 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
     launch_dot<T, T>(S, b, b, m, kp, part, nb);
     launch_reduce(S, part, nb, kp, red);
     cg_init_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
-    apply_precond<T>(S, r, z, kp, part, nb);
+    apply_precond_cg<T>(S, r, z, kp, part, nb);
     launch_reduce(S, part, nb, kp, red);
     cg_rz0_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
     WB_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * m * kp, cudaMemcpyDeviceToDevice, S.stream));
@@ -1243,7 +1284,7 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
         cg_check_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
         cudaEvent_t e1 = nullptr;
         S.prof_begin(e1);
-        apply_precond<T>(S, r, z, kp, part, nb);
+        apply_precond_cg<T>(S, r, z, kp, part, nb);
         S.prof_end(kind + 2, e1);
         launch_reduce(S, part, nb, kp, red);
         cg_beta_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
@@ -2040,6 +2081,11 @@ std::vector<double> host_reduce(SolverImpl& S, int nb, int kp) {
 // x (n_dofs x k RHS-major) and dem (n x k RHS-major).  Solver::solve semantics
 // (solver.rs:209-238) batched over RHS, with the refinement residual b - G x (computed
 // as D'W (y - D x) when that check may be the last).
+#ifndef WB_MIXED_EXIT_MARGIN
+#define WB_MIXED_EXIT_MARGIN 0.3
+#endif
+constexpr double kMixedExitMargin = WB_MIXED_EXIT_MARGIN;
+
 void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double* demcol, BatchOut& out) {
     const int kp = pad_kp(k);
     ensure_ws(S, kp);
@@ -2047,16 +2093,28 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
     const int64_t n = S.d.n, m = S.d.ndofs;
     const uint32_t* perm = S.perm_identity ? nullptr : S.perm.p;
     // y -> interleaved, primary-sorted, padded to kp columns
-    gather_interleave_kernel<double><<<xpose_blocks(n, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(ycol, n, k, kp, perm, w.yi.p);
+    if (perm) {  // user order interleaved (coalesced), then the rows into primary order
+        gather_interleave_kernel<double><<<xpose_blocks(n, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(ycol, n, k, kp, nullptr, w.e.p);
+        permute_rows_kernel<<<S.nblk(n * kp / 2, 1), kBlock, 0, S.stream>>>(w.e.p, n, kp, perm, 0, w.yi.p);
+        S.gpu_launches++;
+    } else {
+        gather_interleave_kernel<double><<<xpose_blocks(n, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(ycol, n, k, kp, nullptr, w.yi.p);
+    }
     // b = D'W y (rmatvec_wdt, solver.rs:210-211)
     launch_obs<double, OBS_RHS>(S, kp, S.w64.p, nullptr, w.yi.p, w.b.p, nullptr);
     int nb = 0;
     launch_dot<double, double>(S, w.b.p, w.b.p, m, kp, w.part.p, nb);
     std::vector<double> bb = host_reduce(S, nb, kp);
     std::vector<double> rhs_norm(kp), abs_tol(kp);
+    // Mixed precision refines until the FP64 residual is kMixedExitMargin x the tolerance:
+    // its last correction is a short FP32 solve, whose error at a given residual is larger
+    // than that of a CG that ran the whole way, so the margin keeps its result at least
+    // as accurate as the FP64 solve's at the same tolerance.  `converged` is still judged
+    // on tol (final FP64 residual).
+    const double exit_margin = S.mixed() ? kMixedExitMargin : 1.0;
     for (int c = 0; c < kp; ++c) {
         rhs_norm[c] = std::max(std::sqrt(bb[c]), 1e-15);  // solver.rs:212
-        abs_tol[c] = S.params.tol * rhs_norm[c];
+        abs_tol[c] = exit_margin * S.params.tol * rhs_norm[c];
     }
     std::vector<int32_t> conv(kp, 0), iters(kp, 0), part_of(kp, 0);
     std::vector<double> final_rr;  // set when w.e and w.r already hold the final e and D'W e
@@ -2168,7 +2226,13 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
         launch_obs<double, OBS_RESID>(S, kp, S.w64.p, w.x.p, w.yi.p, w.r.p, w.e.p);
         launch_dot<double, double>(S, w.r.p, w.r.p, m, kp, w.part.p, nb);
     }
-    scatter_deinterleave_kernel<double><<<xpose_blocks(n, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(w.e.p, n, k, kp, perm, demcol);
+    if (perm) {  // the rows back into user order (yi is free now), then column-major
+        permute_rows_kernel<<<S.nblk(n * kp / 2, 1), kBlock, 0, S.stream>>>(w.e.p, n, kp, perm, 1, w.yi.p);
+        scatter_deinterleave_kernel<double><<<xpose_blocks(n, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(w.yi.p, n, k, kp, nullptr, demcol);
+        S.gpu_launches++;
+    } else {
+        scatter_deinterleave_kernel<double><<<xpose_blocks(n, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(w.e.p, n, k, kp, nullptr, demcol);
+    }
     scatter_deinterleave_kernel<double><<<xpose_blocks(m, S.n_sm), kXposeWarps * 32, xpose_smem(kp), S.stream>>>(w.x.p, m, k, kp, nullptr, xcol);
     WB_CUDA(cudaGetLastError());
     S.gpu_launches += 3;
@@ -2179,6 +2243,346 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
     out.iters.assign(iters.begin(), iters.begin() + k);
     out.fres.resize(k);
     for (int c = 0; c < k; ++c) out.fres[c] = std::sqrt(ee[c]) / rhs_norm[c];
+    if (S.mixed())
+        for (int c = 0; c < k; ++c) out.conv[c] = out.fres[c] <= S.params.tol ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Learned coarse space: the network's forward and backward passes on this solver's
+// design, and the coarse correction it feeds (see coarse.cuh)
+// ---------------------------------------------------------------------------
+
+// Offsets of the parameter vector (FP32 masters; the forward pass reads BF16 copies).
+struct CnLayout {
+    int64_t W[kCnLayers], b[kCnLayers], Wo;
+    CnLayout() {
+        int64_t o = 0;
+        int fin = kCnIn;
+        for (int l = 0; l < kCnLayers; ++l) {
+            W[l] = o; o += (int64_t)2 * fin * kCnHidden;
+            b[l] = o; o += kCnHidden;
+            fin = kCnHidden;
+        }
+        Wo = o;
+    }
+};
+
+// Device buffers of one network evaluation on a design of m levels.
+struct CnState {
+    int64_t m = 0;
+    DArr<double> d, cnt, isq;
+    DArr<float> X, H[kCnLayers], P[kCnLayers], T, GT, Zt, w32;
+    DArr<float> params;
+    DArr<__nv_bfloat16> pb;
+    // backward
+    DArr<float> dZ, dH, dpre, dS, ones, grad, fpart;
+    DArr<double> dpart, small;
+};
+
+int cn_blocks(int64_t n) { return (int)std::max<int64_t>(1, (n + 255) / 256); }
+
+// diag(G), level counts and D^-1/2 of the design, on the device
+void cn_design_stats(SolverImpl& S, CnState& C) {
+    const Design& d = S.d;
+    const int64_t m = d.ndofs;
+    std::vector<double> dg((size_t)m, 0.0), cnt((size_t)m, 0.0), isq((size_t)m, 0.0);
+    for (int q = 0; q < d.Q; ++q) {
+        const uint32_t* c = d.codes.data() + (size_t)q * d.n;
+        const int64_t o = d.off[q];
+        for (int64_t i = 0; i < d.n; ++i) {
+            dg[(size_t)(o + c[i])] += d.weight(i);
+            cnt[(size_t)(o + c[i])] += 1.0;
+        }
+    }
+    for (int64_t l = 0; l < m; ++l) isq[(size_t)l] = dg[(size_t)l] > 0.0 ? 1.0 / std::sqrt(dg[(size_t)l]) : 0.0;
+    C.m = m;
+    C.d.upload(dg);
+    C.cnt.upload(cnt);
+    C.isq.upload(isq);
+}
+
+// P[:, pc0:pc0+ncols] (+)= Ahat H[:, 0:ncols] (H has row stride F >= ncols, P row stride
+// PF >= pc0 + ncols) via passes of the FP32 observation pass over column blocks of 16 or
+// 32 (ncols a multiple of 16).
+void cn_ahat(SolverImpl& S, CnState& C, const float* H, int F, int ncols, float* P, int PF, int pc0, bool accumulate) {
+    const int64_t m = C.m;
+    const float* w = S.w32.p ? S.w32.p : C.w32.p;  // null: unit weights
+    for (int c0 = 0; c0 < ncols; c0 += 32) {
+        const int kt = std::min(32, ncols - c0);
+        cn_scale_cols_kernel<<<cn_blocks(m * kt), 256, 0, S.stream>>>(m, F, c0, kt, H, C.isq.p, C.T.p);
+        launch_obs<float, OBS_GRAM>(S, kt, w, C.T.p, nullptr, C.GT.p, nullptr);
+        cn_combine_kernel<<<cn_blocks(m * kt), 256, 0, S.stream>>>(m, F, c0, kt, C.GT.p, C.isq.p, H, P, PF, pc0 + c0,
+                                                                   accumulate ? 1 : 0);
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches += 2;
+    }
+}
+
+template <int N, int ACT>
+void cn_dense(SolverImpl& S, int64_t m, const float* A0, int K0, const float* A1, int K1, const __nv_bfloat16* W,
+              const float* bias, float* out) {
+    const size_t smem = sizeof(__nv_bfloat16) * (size_t)(K0 + K1) * N;
+    const int64_t warps = (m + 15) / 16;
+    const int grid = (int)std::max<int64_t>(1, (warps + 3) / 4);
+    cn_dense_fwd_kernel<N, ACT><<<grid, 128, smem, S.stream>>>(m, A0, K0, A1, K1, W, bias, out);
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches++;
+}
+
+// Buffers for a design (features once per seed) and the parameters (FP32 + BF16).
+void cn_prepare(SolverImpl& S, CnState& C, const float* params, uint64_t seed) {
+    if (C.m == 0) cn_design_stats(S, C);
+    const int64_t m = C.m;
+    if (S.w64.p && !S.w32.p && !C.w32.p) {  // FP32 weights for the FP32 observation pass
+        C.w32.alloc((size_t)S.obs.ns);
+        convert_kernel<double, float><<<S.nblk(S.obs.ns, 1), kBlock, 0, S.stream>>>(S.w64.p, C.w32.p, S.obs.ns);
+        WB_CUDA(cudaGetLastError());
+    }
+    C.X.alloc((size_t)m * kCnIn);
+    for (int l = 0; l < kCnLayers; ++l) {
+        C.H[l].alloc((size_t)m * kCnHidden);
+        C.P[l].alloc((size_t)m * (l == 0 ? kCnIn : kCnHidden));
+    }
+    C.T.alloc((size_t)m * 32);
+    C.GT.alloc((size_t)m * 32);
+    C.Zt.alloc((size_t)m * kCnOut);
+    CnOffsets fo{};
+    fo.Q = S.d.Q;
+    for (int q = 0; q < S.d.Q; ++q) fo.off[q] = S.d.off[q];
+    fo.off[S.d.Q] = m;
+    cn_features_kernel<<<cn_blocks(m), 256, 0, S.stream>>>(m, fo, C.d.p, C.cnt.p, seed, C.X.p);
+    C.params.alloc(kCnParams);
+    C.pb.alloc(kCnParams);
+    WB_CUDA(cudaMemcpyAsync(C.params.p, params, sizeof(float) * kCnParams, cudaMemcpyHostToDevice, S.stream));
+    cn_to_bf16_kernel<<<cn_blocks(kCnParams), 256, 0, S.stream>>>(kCnParams, C.params.p, C.pb.p);
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches += 2;
+}
+
+// Zt = network(X): H_0 = X, H_{l+1} = tanh(bf16([Ahat H_l, H_l]) W_l + b_l), Zt = bf16(H_3) W_o
+void cn_forward(SolverImpl& S, CnState& C) {
+    static const CnLayout L;
+    const int64_t m = C.m;
+    const float* Hin = C.X.p;
+    int F = kCnIn;
+    for (int l = 0; l < kCnLayers; ++l) {
+        cn_ahat(S, C, Hin, F, F, C.P[l].p, F, 0, false);
+        cn_dense<kCnHidden, 1>(S, m, C.P[l].p, F, Hin, F, C.pb.p + L.W[l], C.params.p + L.b[l], C.H[l].p);
+        Hin = C.H[l].p;
+        F = kCnHidden;
+    }
+    cn_dense<kCnOut, 0>(S, m, C.H[kCnLayers - 1].p, kCnHidden, nullptr, 0, C.pb.p + L.Wo, nullptr, C.Zt.p);
+}
+
+// sum_rows a' b into out (K x N) with the block partials of cn_tn_partial_kernel
+template <typename TACC, typename TOUT>
+void cn_tn(SolverImpl& S, CnState& C, int64_t m, const float* A0, int K0, const float* A1, int K1, bool round_a,
+           const float* B, int N, TOUT* out) {
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((m + 255) / 256, (int64_t)S.n_sm * 2));
+    const int64_t KN = (int64_t)(K0 + K1) * N;
+    TACC* part;
+    if (std::is_same<TACC, double>::value) {
+        C.dpart.alloc((size_t)nb * KN);
+        part = reinterpret_cast<TACC*>(C.dpart.p);
+    } else {
+        C.fpart.alloc((size_t)nb * KN);
+        part = reinterpret_cast<TACC*>(C.fpart.p);
+    }
+    cn_tn_partial_kernel<TACC><<<nb, 256, 0, S.stream>>>(m, A0, K0, A1, K1, round_a ? 1 : 0, B, N, part);
+    cn_reduce_partials_kernel<TACC, TOUT><<<cn_blocks(KN), 256, 0, S.stream>>>(part, nb, KN, out);
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches += 2;
+}
+
+// Loss L = 1 - tr(B'A^-1 B)/t (A = Zt'Zt + eps I, B = Zt'V) and the gradient of every
+// parameter into grad (kCnParams, FP32).  V: the design's targets (m x t).
+double cn_backward(SolverImpl& S, CnState& C, float* grad_host) {
+    static const CnLayout L;
+    const int64_t m = C.m;
+    const int t = S.cn_t;
+    const float* V = S.cn_targets.p;
+    C.small.alloc((size_t)32 * 32 * 2 + 32 * 32 * 2);
+    double* dA = C.small.p;              // 32 x 32
+    double* dB = C.small.p + 32 * 32;    // 32 x t
+    cn_tn<double, double>(S, C, m, C.Zt.p, kCnOut, nullptr, 0, false, C.Zt.p, kCnOut, dA);
+    cn_tn<double, double>(S, C, m, C.Zt.p, kCnOut, nullptr, 0, false, V, t, dB);
+    std::vector<double> A(32 * 32), B((size_t)32 * t);
+    WB_CUDA(cudaMemcpyAsync(A.data(), dA, sizeof(double) * 32 * 32, cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaMemcpyAsync(B.data(), dB, sizeof(double) * 32 * t, cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    // A += eps I, A^-1 by Gauss-Jordan (32 x 32, SPD)
+    double tr = 0.0;
+    for (int i = 0; i < 32; ++i) tr += A[i * 32 + i];
+    for (int i = 0; i < 32; ++i) A[i * 32 + i] += 1e-6 * tr / 32.0 + 1e-300;
+    std::vector<double> Ai(32 * 32, 0.0);
+    {
+        std::vector<double> M(A);
+        for (int i = 0; i < 32; ++i) Ai[i * 32 + i] = 1.0;
+        for (int c = 0; c < 32; ++c) {
+            int piv = c;
+            for (int r = c + 1; r < 32; ++r)
+                if (std::fabs(M[r * 32 + c]) > std::fabs(M[piv * 32 + c])) piv = r;
+            if (piv != c)
+                for (int j = 0; j < 32; ++j) { std::swap(M[c * 32 + j], M[piv * 32 + j]); std::swap(Ai[c * 32 + j], Ai[piv * 32 + j]); }
+            const double inv = 1.0 / M[c * 32 + c];
+            for (int j = 0; j < 32; ++j) { M[c * 32 + j] *= inv; Ai[c * 32 + j] *= inv; }
+            for (int r = 0; r < 32; ++r) {
+                if (r == c) continue;
+                const double f = M[r * 32 + c];
+                if (f == 0.0) continue;
+                for (int j = 0; j < 32; ++j) { M[r * 32 + j] -= f * M[c * 32 + j]; Ai[r * 32 + j] -= f * Ai[c * 32 + j]; }
+            }
+        }
+    }
+    std::vector<double> AiB((size_t)32 * t, 0.0);  // 32 x t
+    for (int i = 0; i < 32; ++i)
+        for (int a = 0; a < 32; ++a)
+            for (int j = 0; j < t; ++j) AiB[(size_t)i * t + j] += Ai[i * 32 + a] * B[(size_t)a * t + j];
+    double trv = 0.0;
+    for (int i = 0; i < 32; ++i)
+        for (int j = 0; j < t; ++j) trv += B[(size_t)i * t + j] * AiB[(size_t)i * t + j];
+    const double loss = 1.0 - trv / t;
+    // dZ = V C1 + Z C2: C1 = -2/t (A^-1 B)' (t x 32), C2 = 2/t (A^-1 B)(A^-1 B)' (32 x 32)
+    std::vector<double> C1((size_t)t * 32), C2(32 * 32, 0.0);
+    for (int j = 0; j < t; ++j)
+        for (int i = 0; i < 32; ++i) C1[(size_t)j * 32 + i] = -2.0 / t * AiB[(size_t)i * t + j];
+    for (int i = 0; i < 32; ++i)
+        for (int k = 0; k < 32; ++k) {
+            double v = 0.0;
+            for (int j = 0; j < t; ++j) v += AiB[(size_t)i * t + j] * AiB[(size_t)k * t + j];
+            C2[i * 32 + k] = 2.0 / t * v;
+        }
+    WB_CUDA(cudaMemcpyAsync(dA, C1.data(), sizeof(double) * t * 32, cudaMemcpyHostToDevice, S.stream));
+    WB_CUDA(cudaMemcpyAsync(dB, C2.data(), sizeof(double) * 32 * 32, cudaMemcpyHostToDevice, S.stream));
+    C.dZ.alloc((size_t)m * kCnOut);
+    C.dH.alloc((size_t)m * kCnHidden);
+    C.dpre.alloc((size_t)m * kCnHidden);
+    C.dS.alloc((size_t)m * 2 * kCnHidden);
+    C.grad.alloc(kCnParams);
+    if (C.ones.n < (size_t)m) {
+        std::vector<float> one((size_t)m, 1.0f);
+        C.ones.upload(one);
+    }
+    cn_dz_kernel<<<cn_blocks(m * 32), 256, 0, S.stream>>>(m, V, t, dA, C.Zt.p, dB, C.dZ.p);
+    // W_o: H_3' dZ (H_3 rounded as the forward pass read it); dH_3 = dZ W_o'
+    cn_tn<float, float>(S, C, m, C.H[kCnLayers - 1].p, kCnHidden, nullptr, 0, true, C.dZ.p, kCnOut, C.grad.p + L.Wo);
+    {
+        const size_t smem = sizeof(float) * kCnHidden * kCnOut;
+        cn_matmul_nt_kernel<<<S.nblk(m * kCnHidden, 1), 256, smem, S.stream>>>(m, C.dZ.p, kCnOut, C.pb.p + L.Wo,
+                                                                              kCnHidden, C.dH.p);
+    }
+    for (int l = kCnLayers - 1; l >= 0; --l) {
+        const int F = l == 0 ? kCnIn : kCnHidden;
+        const float* Hl = l == 0 ? C.X.p : C.H[l - 1].p;
+        cn_dtanh_kernel<<<cn_blocks(m * kCnHidden), 256, 0, S.stream>>>(m * kCnHidden, C.dH.p, C.H[l].p, C.dpre.p);
+        cn_tn<float, float>(S, C, m, C.P[l].p, F, Hl, F, true, C.dpre.p, kCnHidden, C.grad.p + L.W[l]);
+        cn_tn<float, float>(S, C, m, C.ones.p, 1, nullptr, 0, false, C.dpre.p, kCnHidden, C.grad.p + L.b[l]);
+        if (l == 0) break;
+        // dS = dpre W_l' (m x 2F); dH_l = dS[:, F:] + Ahat dS[:, :F]
+        const size_t smem = sizeof(float) * 2 * F * kCnHidden;
+        if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(cn_matmul_nt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cn_matmul_nt_kernel<<<S.nblk(m * 2 * F, 1), 256, smem, S.stream>>>(m, C.dpre.p, kCnHidden, C.pb.p + L.W[l],
+                                                                           2 * F, C.dS.p);
+        cn_copy_cols_kernel<<<cn_blocks(m * F), 256, 0, S.stream>>>(m, 2 * F, F, F, C.dS.p, C.dH.p, F, 0);
+        cn_ahat(S, C, C.dS.p, 2 * F, F, C.dH.p, F, 0, true);
+    }
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches += 8;
+    WB_CUDA(cudaMemcpyAsync(grad_host, C.grad.p, sizeof(float) * kCnParams, cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    return loss;
+}
+
+// Eigen-decomposition of a symmetric n x n matrix by cyclic Jacobi rotations (n <= 32):
+// A is destroyed, eigenvalues into lam, eigenvectors into the columns of V.
+void jacobi_eigen(std::vector<double>& A, int n, std::vector<double>& lam, std::vector<double>& V) {
+    V.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0, tot = 0.0;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                tot += A[(size_t)i * n + j] * A[(size_t)i * n + j];
+                if (i != j) off += A[(size_t)i * n + j] * A[(size_t)i * n + j];
+            }
+        if (off <= 1e-30 * std::max(tot, 1e-300)) break;
+        for (int p = 0; p < n; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = A[(size_t)p * n + q];
+                if (std::fabs(apq) < 1e-300) continue;
+                const double app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double tt = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(tt * tt + 1.0), s = tt * c;
+                for (int k = 0; k < n; ++k) {
+                    const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+                    A[(size_t)k * n + p] = c * akp - s * akq;
+                    A[(size_t)k * n + q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                    A[(size_t)p * n + k] = c * apk - s * aqk;
+                    A[(size_t)q * n + k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+                    V[(size_t)k * n + p] = c * vkp - s * vkq;
+                    V[(size_t)k * n + q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    lam.resize(n);
+    for (int i = 0; i < n; ++i) lam[i] = A[(size_t)i * n + i];
+}
+
+// Installs the coarse space spanned by the columns of Z64 (m x 32 row-major, FP64, on the
+// device): E = Z'GZ in FP64, its pseudo-inverse (eigenvalues below 1e-10 of the largest
+// dropped: null-space directions of G), and an FP32 copy of Z for mixed precision.
+void install_coarse(SolverImpl& S) {
+    const int64_t m = S.d.ndofs;
+    DArr<double> gz;
+    gz.alloc((size_t)m * 32);
+    launch_gram<double>(S, 32, S.w64.p, S.coarse_z64.p, gz.p);
+    const int nbc = S.n_sm * kCoarseDotBlocksPerSm;
+    S.coarse_part.alloc((size_t)nbc * 32 * 32);
+    S.coarse_u.alloc(32 * 32);
+    S.coarse_einv.alloc(32 * 32);
+    coarse_dot_kernel<double><<<nbc, 256, 0, S.stream>>>(m, S.coarse_z64.p, gz.p, 32, S.coarse_part.p);
+    // E = sum of the partials: coarse_solve with the identity as "E^+" gives u = c = E
+    std::vector<double> I(32 * 32, 0.0);
+    for (int i = 0; i < 32; ++i) I[i * 32 + i] = 1.0;
+    WB_CUDA(cudaMemcpyAsync(S.coarse_einv.p, I.data(), sizeof(double) * 32 * 32, cudaMemcpyHostToDevice, S.stream));
+    coarse_solve_kernel<<<1, 256, 0, S.stream>>>(S.coarse_part.p, nbc, S.coarse_einv.p, 32, S.coarse_u.p, nullptr, 0);
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches += 2;
+    std::vector<double> E(32 * 32);
+    WB_CUDA(cudaMemcpyAsync(E.data(), S.coarse_u.p, sizeof(double) * 32 * 32, cudaMemcpyDeviceToHost, S.stream));
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    for (int i = 0; i < 32; ++i)
+        for (int j = i + 1; j < 32; ++j) E[i * 32 + j] = E[j * 32 + i] = 0.5 * (E[i * 32 + j] + E[j * 32 + i]);
+    std::vector<double> lam, V;
+    jacobi_eigen(E, 32, lam, V);
+    double lmax = 0.0;
+    for (double v : lam) lmax = std::max(lmax, v);
+    std::vector<double> Ei(32 * 32, 0.0);
+    for (int k = 0; k < 32; ++k) {
+        if (!(lam[k] > 1e-10 * lmax)) continue;
+        const double inv = 1.0 / lam[k];
+        for (int i = 0; i < 32; ++i)
+            for (int j = 0; j < 32; ++j) Ei[i * 32 + j] += V[(size_t)i * 32 + k] * inv * V[(size_t)j * 32 + k];
+    }
+    WB_CUDA(cudaMemcpyAsync(S.coarse_einv.p, Ei.data(), sizeof(double) * 32 * 32, cudaMemcpyHostToDevice, S.stream));
+    if (S.mixed()) {
+        S.coarse_z32.alloc((size_t)m * 32);
+        convert_kernel<double, float><<<S.nblk(m * 32, 1), kBlock, 0, S.stream>>>(S.coarse_z64.p, S.coarse_z32.p, m * 32);
+        WB_CUDA(cudaGetLastError());
+    }
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    S.coarse_k = 32;
+    if (S.cg_exec) {  // the captured CG iteration changes
+        WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
+        S.cg_exec = nullptr;
+    }
 }
 
 }  // namespace
@@ -2723,6 +3127,137 @@ void within_solver_ac_arrays(const within_solver* s, int32_t i, int32_t* level_p
     std::copy(f.core_z.begin(), f.core_z.end(), core_z);
 }
 
+// --- learned coarse space ---
+
+int32_t within_coarse_net_params(void) { return (int32_t)wb::kCnParams; }
+
+static int coarse_common(within_solver* s, const std::function<int(SolverImpl&)>& f) {
+    if (!s) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "solver is null");
+    SolverImpl& S = *s->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    return guard([&]() -> int {
+        if (S.precond_only) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "this handle holds only a preconditioner");
+        return f(S);
+    });
+}
+
+int within_solver_set_coarse_net(within_solver* s, const float* params, size_t n_params, uint64_t seed) {
+    return coarse_common(s, [&](SolverImpl& S) -> int {
+        if (!params || n_params != (size_t)wb::kCnParams)
+            return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the coarse-space network has " +
+                                                             std::to_string(wb::kCnParams) + " parameters");
+        wb::CnState C;
+        wb::cn_prepare(S, C, params, seed);
+        wb::cn_forward(S, C);
+        const int64_t m = S.d.ndofs;
+        S.coarse_z64.alloc((size_t)m * 32);
+        wb::cn_unscale_kernel<<<wb::cn_blocks(m * 32), 256, 0, S.stream>>>(m, C.Zt.p, C.isq.p, S.coarse_z64.p, nullptr);
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+        wb::install_coarse(S);
+        return WITHIN_OK;
+    });
+}
+
+int within_solver_set_coarse_basis(within_solver* s, const double* Z, size_t k) {
+    return coarse_common(s, [&](SolverImpl& S) -> int {
+        if (!Z || k == 0 || k > 32) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "a coarse basis has 1 to 32 columns");
+        const size_t m = (size_t)S.d.ndofs;
+        std::vector<double> zr(m * 32, 0.0);  // row-major, 32 columns
+        for (size_t j = 0; j < k; ++j)
+            for (size_t i = 0; i < m; ++i) zr[i * 32 + j] = Z[j * m + i];
+        S.coarse_z64.upload(zr);
+        wb::install_coarse(S);
+        return WITHIN_OK;
+    });
+}
+
+int within_solver_clear_coarse(within_solver* s) {
+    return coarse_common(s, [&](SolverImpl& S) -> int {
+        S.coarse_k = 0;
+        if (S.cg_exec) {
+            WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
+            S.cg_exec = nullptr;
+        }
+        return WITHIN_OK;
+    });
+}
+
+int within_solver_coarse_basis(within_solver* s, double* Z) {
+    return coarse_common(s, [&](SolverImpl& S) -> int {
+        if (S.coarse_k == 0) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the solver has no coarse space");
+        const size_t m = (size_t)S.d.ndofs;
+        std::vector<double> zr(m * 32);
+        WB_CUDA(cudaMemcpy(zr.data(), S.coarse_z64.p, sizeof(double) * m * 32, cudaMemcpyDeviceToHost));
+        for (size_t j = 0; j < 32; ++j)
+            for (size_t i = 0; i < m; ++i) Z[j * m + i] = zr[i * 32 + j];
+        return WITHIN_OK;
+    });
+}
+
+int within_solver_set_coarse_targets(within_solver* s, const double* V, size_t t) {
+    return coarse_common(s, [&](SolverImpl& S) -> int {
+        if (!V || t == 0 || t > 32) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "targets have 1 to 32 columns");
+        const size_t m = (size_t)S.d.ndofs;
+        std::vector<float> vr(m * t);
+        for (size_t j = 0; j < t; ++j)
+            for (size_t i = 0; i < m; ++i) vr[i * t + j] = (float)V[j * m + i];
+        S.cn_targets.upload(vr);
+        S.cn_t = (int32_t)t;
+        return WITHIN_OK;
+    });
+}
+
+int within_coarse_net_grad(within_solver* s, const float* params, uint64_t seed, float* grad, double* loss,
+                           float* zt) {
+    return coarse_common(s, [&](SolverImpl& S) -> int {
+        if (!params || !grad || !loss) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "null buffer");
+        if (S.cn_t == 0) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "no training targets on this solver");
+        if (!S.cn) S.cn = std::make_shared<wb::CnState>();
+        wb::CnState& C = *std::static_pointer_cast<wb::CnState>(S.cn);
+        wb::cn_prepare(S, C, params, seed);
+        wb::cn_forward(S, C);
+        *loss = wb::cn_backward(S, C, grad);
+        if (zt) {
+            const size_t m = (size_t)S.d.ndofs;
+            std::vector<float> zr(m * 32);
+            WB_CUDA(cudaMemcpy(zr.data(), C.Zt.p, sizeof(float) * m * 32, cudaMemcpyDeviceToHost));
+            for (size_t j = 0; j < 32; ++j)
+                for (size_t i = 0; i < m; ++i) zt[j * m + i] = zr[i * 32 + j];
+        }
+        return WITHIN_OK;
+    });
+}
+
+int within_solver_release_coarse_training(within_solver* s) {
+    return coarse_common(s, [&](SolverImpl& S) -> int {
+        S.cn.reset();
+        S.cn_targets.release();
+        S.cn_t = 0;
+        return WITHIN_OK;
+    });
+}
+
+int64_t within_solver_schwarz_bytes(const within_solver* s, int32_t k, int32_t elem_bytes) {
+    if (!s || k <= 0 || (elem_bytes != 4 && elem_bytes != 8)) return 0;
+    const int64_t e = elem_bytes;
+    int64_t b = 0;
+    for (const wb::Subdomain& sd : s->impl->subs) {
+        const int64_t nl = sd.n_local();
+        b += 2 * (4 + e) * sd.ct.c.nnz();  // the cross block: reduced rhs and back substitution
+        b += (4 + 8) * nl;                 // global index and partition-of-unity weight per slot
+        b += 2 * e * nl * k;               // the local vector, gathered and scattered
+        if (sd.kind == 0) {
+            const int64_t r = std::max<int64_t>(sd.n_red - 1, 0);
+            b += e * r * r;                // the anchored dense factor
+        } else {
+            b += 2 * (4 + e) * (int64_t)sd.ac.col_idx.size();  // AC forward and backward sweeps
+            b += e * (int64_t)sd.ac.ncore * sd.ac.ncore;        // the dense core's inverse
+        }
+    }
+    return b;
+}
+
 const char* within_last_error(void) { return wb::g_last_error.c_str(); }
 
 int within_solve_many(within_problem* problems, size_t n_problems, const within_params* params,
@@ -2825,6 +3360,25 @@ int noalloc_scratch(double** out) {
     *out = g_noalloc_addr[dev];
     return WITHIN_OK;
 }
+
+// The error mapping of guard() for a callable passed by template parameter (no
+// std::function, so no host allocation on the success path).  No exception crosses the
+// C ABI: anything other than a CUDA error or host memory exhaustion maps to
+// WITHIN_ERR_CUDA, as only the device calls above can raise on this path.
+template <typename F>
+int noalloc_guard(F&& f) {
+    try {
+        const int rc = f();
+        if (rc == WITHIN_OK) wb::g_last_error.clear();
+        return rc;
+    } catch (const wb::CudaError& e) {
+        return wb::fail(WITHIN_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return wb::fail(WITHIN_ERR_OVERFLOW, "out of host memory");
+    } catch (...) {
+        return wb::fail(WITHIN_ERR_CUDA, "unexpected error in the no-allocation apply");
+    }
+}
 }  // namespace
 
 extern "C" int within_solver_apply_gramian_noalloc(within_solver* s, const double* d_x, size_t k, double* d_y,
@@ -2834,6 +3388,9 @@ extern "C" int within_solver_apply_gramian_noalloc(within_solver* s, const doubl
     if (k == 0) return WITHIN_OK;
     if (k > 32) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "at most 32 vectors per call");
     SolverImpl& S = *s->impl;
+    // a handle rebuilt from preconditioner bytes has no design to apply
+    if (S.precond_only)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "this handle holds only a preconditioner");
     const int kk = (int)k, kp = wb::pad_kp(kk);
     const size_t m = (size_t)S.d.ndofs;
     const size_t need = 2 * m * (size_t)kp;
@@ -2843,25 +3400,28 @@ extern "C" int within_solver_apply_gramian_noalloc(within_solver* s, const doubl
                             " doubles of scratch (2 x n_dofs x k rounded up to 4, 8, 16 or 32), the limit is " +
                             std::to_string(kNoAllocScratchDoubles));
     std::lock_guard<std::mutex> lk(S.mu);
-    double* scratch = nullptr;
-    const int rc = noalloc_scratch(&scratch);
-    if (rc != WITHIN_OK) return rc;
-    double* xi = scratch;               // x, RHS-interleaved (m x kp)
-    double* yi = scratch + m * kp;      // G x, RHS-interleaved (m x kp)
-    cudaStream_t saved = S.stream;
-    S.stream = stream ? (cudaStream_t)stream : saved;
-    int status = WITHIN_OK;
-    try {  // no std::function wrapper here: nothing on this path allocates
-        wb::gather_interleave_kernel<double><<<wb::xpose_blocks((int64_t)m, S.n_sm), wb::kXposeWarps * 32, wb::xpose_smem(kp), S.stream>>>(d_x, (int64_t)m, kk, kp,
-                                                                                             nullptr, xi);
+    // the solver's own stream comes back however this call leaves
+    struct StreamRestore {
+        SolverImpl& S;
+        cudaStream_t saved;
+        ~StreamRestore() { S.stream = saved; }
+    } restore{S, S.stream};
+    // guard() takes a std::function; this lambda is called directly so that nothing here
+    // allocates on the host either
+    return noalloc_guard([&]() -> int {
+        double* scratch = nullptr;
+        const int rc = noalloc_scratch(&scratch);
+        if (rc != WITHIN_OK) return rc;
+        double* xi = scratch;           // x, RHS-interleaved (m x kp)
+        double* yi = scratch + m * kp;  // G x, RHS-interleaved (m x kp)
+        if (stream) S.stream = (cudaStream_t)stream;
+        wb::gather_interleave_kernel<double><<<wb::xpose_blocks((int64_t)m, S.n_sm), wb::kXposeWarps * 32, wb::xpose_smem(kp), S.stream>>>(
+            d_x, (int64_t)m, kk, kp, nullptr, xi);
         wb::launch_obs<double, wb::OBS_GRAM>(S, kp, S.w64.p, xi, nullptr, yi, nullptr);
-        wb::scatter_deinterleave_kernel<double><<<wb::xpose_blocks((int64_t)m, S.n_sm), wb::kXposeWarps * 32, wb::xpose_smem(kp), S.stream>>>(yi, (int64_t)m, kk, kp,
-                                                                                                nullptr, d_y);
+        wb::scatter_deinterleave_kernel<double><<<wb::xpose_blocks((int64_t)m, S.n_sm), wb::kXposeWarps * 32, wb::xpose_smem(kp), S.stream>>>(
+            yi, (int64_t)m, kk, kp, nullptr, d_y);
         WB_CUDA(cudaGetLastError());
         S.gpu_launches += 2;
-    } catch (const wb::CudaError& e) {
-        status = wb::fail(WITHIN_ERR_CUDA, e.what());
-    }
-    S.stream = saved;
-    return status;
+        return WITHIN_OK;
+    });
 }
