@@ -33,7 +33,10 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the operator
 # apply on the headline workload, from ncu captures of one launch (the figure and its
 # command are in profiles/); these are not measured by the bench run itself
-TRAFFIC = {}
+TRAFFIC = {"fp32": (230_120_000, "ncu dram__bytes_read+write of one launch at 5M observations (115.06 MB), x2 for "
+                                  "10M (profiles/obs_pass_dram_traffic_5Mobs_16rhs.md); not measured by this run"),
+           "fp64": (342_480_000, "ncu dram__bytes_read+write of one launch at 5M observations (171.24 MB), x2 for "
+                                  "10M (profiles/obs_pass_dram_traffic_5Mobs_16rhs.md); not measured by this run")}
 
 
 def parse():

@@ -240,6 +240,17 @@ void within_solver_ac_arrays(const within_solver *solver, int32_t i, int32_t *le
                              int32_t *col_idx, double *col_coef, int32_t *core_vertex,
                              double *core_z);
 
+/* Test hook for the failure path of a local solve (no counterpart in the reference, whose
+ * tests use a failing LocalSolver stub: schwarz-precond/tests/schwarz.rs:947-1001).  With
+ * `on`, the approximate-Cholesky sweeps' grid barriers wait for one block more than the
+ * grid has, with a short limit (about a millisecond per wait): the waits run out, the
+ * device error flag is set and the launches end; no GPU fault is involved.  Such a local
+ * solve did not complete, and, as in the reference, within_solver_apply_preconditioner
+ * returns z filled with NaN (Preconditioner::apply, additive/preconditioner.rs:197-201)
+ * while a solve returns WITHIN_ERR_ITERATIVE_SOLVE (CG's try_apply, cg.rs:69, 104).
+ * WITHIN_ERR_INVALID_ARGUMENT when the preconditioner has no such sweeps. */
+int within_solver_inject_sweep_timeout(within_solver *solver, int32_t on);
+
 /* Coarse space for CG (no counterpart in the reference; it augments the additive Schwarz
  * apply, schwarz-precond/src/schwarz/additive/executor.rs:59-147, inside CG,
  * schwarz-precond/src/solve/cg.rs:45-133).  With a coarse basis Z (n_dofs x 32), CG's
@@ -273,6 +284,15 @@ int within_solver_set_coarse_targets(within_solver *solver, const double *v, siz
 int within_coarse_net_grad(within_solver *solver, const float *params, uint64_t seed, float *grad, double *loss,
                            float *zt);
 int within_solver_release_coarse_training(within_solver *solver);
+
+/* Block shape of the observation pass for k RHS in elem_bytes (4 FP32, 8 FP64)
+ * precision: observations per work chunk (16, 32 or 64) and resident blocks per SM (1
+ * or 2).  The solver's autotuner picks them the first time it needs the pass (each
+ * candidate timed on the solver's own design; cached per shape class for the process).
+ * Returns 0 when tuned, 1 when not tuned yet (the defaults, 32 and 2, are reported).
+ * A measurement hook with no counterpart in the reference. */
+int within_solver_obs_config(const within_solver *solver, int32_t k, int32_t elem_bytes, int32_t *obs_per_chunk,
+                             int32_t *blocks_per_sm);
 
 /* Algorithmic bytes of one Schwarz apply over k RHS with elem_bytes (4 or 8) per vector
  * element, counted from the built subdomains: per subdomain 2 (4+s) nnz(C_i) for the

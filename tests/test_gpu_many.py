@@ -6,7 +6,7 @@ import pytest
 import oracle
 import within_b200 as wb
 from within_b200 import synthetic
-from paritylib import normalize_x, rel
+from paritylib import make_normalizer, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -19,12 +19,16 @@ def test_solve_many_matches_oracle(precision):
     for (cats, Y), r in zip(probs, res):
         assert r.x.shape == (sum(int(cats[:, j].max()) + 1 for j in range(cats.shape[1])), Y.shape[1])
         o = oracle.OracleSolver(cats, None).solve_batch(Y, threads=4)
+        t = oracle.OracleSolver(cats, None, tol=1e-13).solve_batch(Y, threads=4)
+        NZ = make_normalizer(cats)
         for c in range(Y.shape[1]):
             assert r.converged[c] and r.residual[c] <= 1e-8
-            # tolerance 1e-8 relative (demeaned) against the oracle at the same tol; mixed
-            # precision is held to 1e-7 (its inner solves stop at a different point)
-            assert rel(r.demeaned[:, c], o.demeaned[:, c]) < (1e-8 if precision == "fp64" else 1e-7)
-            assert rel(normalize_x(cats, r.x[:, c]), normalize_x(cats, o.x[:, c])) < 1e-6
+            if precision == "fp64":  # the reference's iterates: within 1e-8 of the oracle
+                assert rel(r.demeaned[:, c], o.demeaned[:, c]) < 1e-8
+                assert rel(NZ(r.x[:, c]), NZ(o.x[:, c])) < 1e-8
+            # within twice the reference's own error at the same tolerance
+            assert rel(r.demeaned[:, c], t.demeaned[:, c]) <= 2 * rel(o.demeaned[:, c], t.demeaned[:, c]) + 1e-9
+            assert rel(NZ(r.x[:, c]), NZ(t.x[:, c])) <= 2 * rel(NZ(o.x[:, c]), NZ(t.x[:, c])) + 1e-9
 
 
 def test_solve_many_equals_single_solves_and_weights():

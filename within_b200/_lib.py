@@ -74,7 +74,8 @@ EXPORTED = [
     "within_preconditioner_from_bytes", "within_solver_preconditioner_kind", "within_solver_schwarz_bytes",
     "within_coarse_net_params", "within_solver_set_coarse_net", "within_solver_set_coarse_basis",
     "within_solver_clear_coarse", "within_solver_coarse_basis", "within_solver_set_coarse_targets",
-    "within_coarse_net_grad", "within_solver_release_coarse_training",
+    "within_coarse_net_grad", "within_solver_release_coarse_training", "within_solver_inject_sweep_timeout",
+    "within_solver_obs_config",
 ]
 
 _lib = None
@@ -152,6 +153,10 @@ def load():
     L.within_solver_set_coarse_targets.argtypes = [vp, vp, C.c_size_t]
     L.within_coarse_net_grad.argtypes = [vp, vp, C.c_uint64, vp, C.POINTER(C.c_double), vp]
     L.within_solver_release_coarse_training.argtypes = [vp]
+    L.within_solver_inject_sweep_timeout.argtypes = [vp, C.c_int32]
+    L.within_solver_inject_sweep_timeout.restype = C.c_int
+    L.within_solver_obs_config.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.within_solver_obs_config.restype = C.c_int
     for f in ("within_solver_set_coarse_net", "within_solver_set_coarse_basis", "within_solver_clear_coarse",
               "within_solver_coarse_basis", "within_solver_set_coarse_targets", "within_coarse_net_grad",
               "within_solver_release_coarse_training"):

@@ -198,12 +198,38 @@ def train(designs, epochs: int = 20, lr: float = 2e-3, seed: int = 0, params=Non
     return p, hist
 
 
-def train_default(out: str = WEIGHTS, n_designs: int = 96, epochs: int = 24, log=print):
+def install_judged(solver, coarse, n_probe: int = 2, seed: int = 0) -> dict:
+    """Installs `coarse` (a CoarseNet or a basis) on the solver only if CG with it solves
+    probe right-hand sides (seeded N(0,1), n_probe columns) in less time than with plain
+    additive Schwarz; otherwise the solver keeps plain Schwarz.  Plain Schwarz is both
+    the fallback and the judge: every solve runs to the same tolerance either way.
+    Returns the probe measurements and whether the coarse space was kept."""
+    import time
+    y = np.asfortranarray(np.random.default_rng(seed).standard_normal((solver.n_obs, n_probe)))
+
+    def timed():
+        solver.solve_batch(y)  # the first solve captures the CG iteration
+        t0 = time.perf_counter()
+        r = solver.solve_batch(y)
+        return time.perf_counter() - t0, r.iterations
+
+    solver.clear_coarse_space()
+    t_plain, it_plain = timed()
+    solver.set_coarse_space(coarse)
+    t_coarse, it_coarse = timed()
+    kept = t_coarse < t_plain
+    if not kept:
+        solver.clear_coarse_space()
+    return {"kept": kept, "plain_s": t_plain, "coarse_s": t_coarse, "plain_iterations": it_plain,
+            "coarse_iterations": it_coarse}
+
+
+def train_default(out: str = WEIGHTS, n_designs: int = 96, epochs: int = 40, log=print):
     """Trains the shipped network: 96 generated worker-firm-year designs (1e5 to 5e5
-    observations, switch probability 0.01 to 0.3, seed 2024), 32 Ritz targets each, 24
-    epochs of Adam; saves the parameters to `out`."""
+    observations, switch probability 0.01 to 0.3, seed 2024), 32 Ritz targets each, 40
+    epochs of Adam (learning rate 3e-3); saves the parameters to `out`."""
     designs = training_designs(n_designs, seed=2024)
-    p, hist = train(designs, epochs=epochs, log=log)
+    p, hist = train(designs, epochs=epochs, lr=3e-3, log=log)
     np.save(out, p)
     return p, hist
 

@@ -300,44 +300,86 @@ __global__ void cn_to_bf16_kernel(int64_t n, const float* __restrict__ p, __nv_b
 }
 
 // ---------------------------------------------------------------------------
-// Coarse correction inside CG: c = Z' r, u = E^+ c, z += Z u, and r.z += c.u
+// Coarse correction inside CG, balancing form (Mandel 1993, BNN):
+//   z = P' M^-1 P r + Q r,  Q = Z E^+ Z',  P = I - G Q,  E = Z' G Z
+// With GZ = G Z kept on the device: u1 = E^+ Z' r;  y = M^-1 (r - GZ u1);
+// u2 = E^+ (GZ)' y;  z = y + Z (u1 - u2).  Symmetric, and on span(Z) the preconditioned
+// operator is the identity while its other eigenvalues stay within the Schwarz bounds.
 // ---------------------------------------------------------------------------
 
-// Block partials of c[j][col] = sum_rows Z[row][j] r[row][col] (Z: m x 32, r: m x kp
-// interleaved, FP64 accumulation); lane j of each warp owns column j of Z.
+constexpr int kCoarseTileRows = 64;
+
+// Block partials of C (32 x kp) = A' B, A: m x 32 (Z or GZ), B: m x kp interleaved, in
+// FP64; tiles of 64 rows staged in shared memory, each thread owning 32*kp/256 outputs.
 template <typename T>
-__global__ void __launch_bounds__(256) coarse_dot_kernel(int64_t m, const T* __restrict__ Z, const T* __restrict__ r,
-                                                         int kp, double* __restrict__ part) {
-    __shared__ double sm[32 * 32];
-    for (int i = threadIdx.x; i < 32 * kp; i += blockDim.x) sm[i] = 0.0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
-    double acc[32];
+__global__ void __launch_bounds__(256) coarse_tn_kernel(int64_t m, const T* __restrict__ A, const T* __restrict__ B,
+                                                        int kp, double* __restrict__ part) {
+    constexpr int R = kCoarseTileRows;
+    __shared__ T As[R][32];
+    __shared__ T Bs[R][32];
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const int nout = 32 * kp;
+    const int64_t ntiles = (m + R - 1) / R;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t r0 = tile * R;
+        const int nr = (int)min((int64_t)R, m - r0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < R * 32; i += blockDim.x) {
+            const int r = i >> 5, j = i & 31;
+            As[r][j] = r < nr ? A[(size_t)(r0 + r) * 32 + j] : T(0);
+        }
+        for (int i = threadIdx.x; i < R * kp; i += blockDim.x) {
+            const int r = i / kp, c = i % kp;
+            Bs[r][c] = r < nr ? B[(size_t)(r0 + r) * kp + c] : T(0);
+        }
+        __syncthreads();
 #pragma unroll
-    for (int c = 0; c < 32; ++c) acc[c] = 0.0;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < m; row += nw) {
-        const double zj = (double)Z[(size_t)row * 32 + lane];
-        const T* rr = r + (size_t)row * kp;
-#pragma unroll
-        for (int c = 0; c < 32; ++c)
-            if (c < kp) acc[c] += zj * (double)rr[c];
+        for (int q = 0; q < 4; ++q) {
+            const int o = threadIdx.x + q * 256;
+            if (o < nout) {
+                const int j = o / kp, c = o % kp;
+                double s = 0.0;
+#pragma unroll 8
+                for (int r = 0; r < R; ++r) s += (double)As[r][j] * (double)Bs[r][c];
+                acc[q] += s;
+            }
+        }
     }
 #pragma unroll
-    for (int c = 0; c < 32; ++c)
-        if (c < kp) atomicAdd(&sm[lane * kp + c], acc[c]);
-    __syncthreads();
-    for (int i = threadIdx.x; i < 32 * kp; i += blockDim.x) part[(size_t)blockIdx.x * 32 * kp + i] = sm[i];
+    for (int q = 0; q < 4; ++q) {
+        const int o = threadIdx.x + q * 256;
+        if (o < nout) part[(size_t)blockIdx.x * nout + o] = acc[q];
+    }
 }
 
-// One block: c = sum of the partials; u = E^+ c (masked to the RHS in `active`, null:
-// every RHS); and the term c.u of r.z appended as row `rz_row` of the CG partials.
-__global__ void coarse_solve_kernel(const double* __restrict__ part, int nb, const double* __restrict__ Einv, int kp,
-                                    double* __restrict__ u, double* __restrict__ rz_part, int rz_row) {
+// One block of 1024 threads: c = the sum of the partials (each output summed by
+// 1024/(32 kp) threads over strided subsets, eight loads in flight, then combined in a
+// fixed order: deterministic); u = E^+ c (32 x kp).
+constexpr int kCoarseSolveThreads = 1024;
+__global__ void __launch_bounds__(kCoarseSolveThreads) coarse_solve_kernel(const double* __restrict__ part, int nb,
+                                                                           const double* __restrict__ Einv, int kp,
+                                                                           double* __restrict__ u) {
     __shared__ double c[32 * 32];
-    for (int i = threadIdx.x; i < 32 * kp; i += blockDim.x) {
+    __shared__ double sub[kCoarseSolveThreads];
+    const int nout = 32 * kp;
+    const int J = blockDim.x / nout;  // threads per output (>= 1)
+    {
+        const int i = threadIdx.x % nout, j = threadIdx.x / nout;
+        double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (j < J) {
+            int b = j;
+            for (; b + 7 * J < nb; b += 8 * J) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) a[q] += part[(size_t)(b + q * J) * nout + i];
+            }
+            for (; b < nb; b += J) a[0] += part[(size_t)b * nout + i];
+        }
+        sub[threadIdx.x] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nout; i += blockDim.x) {
         double s = 0.0;
-        for (int b = 0; b < nb; ++b) s += part[(size_t)b * 32 * kp + i];
+        for (int j = 0; j < J; ++j) s += sub[j * nout + i];
         c[i] = s;
     }
     __syncthreads();
@@ -347,30 +389,39 @@ __global__ void coarse_solve_kernel(const double* __restrict__ part, int nb, con
         for (int a = 0; a < 32; ++a) s += Einv[j * 32 + a] * c[a * kp + col];
         u[i] = s;
     }
-    __syncthreads();
-    if (rz_part && threadIdx.x < kp) {
-        double s = 0.0;
-        for (int j = 0; j < 32; ++j) s += c[j * kp + threadIdx.x] * u[j * kp + threadIdx.x];
-        rz_part[(size_t)rz_row * kp + threadIdx.x] = s;
-    }
 }
 
-// z[row][col] += sum_j Z[row][j] u[j][col]
+// out = x + alpha * A (ua - ub), A: m x 32, ua/ub: 32 x kp (ub may be null); one thread
+// per (row, 4 RHS), the row of A shared through L1 by the row's kp/4 threads.
 template <typename T>
-__global__ void __launch_bounds__(256) coarse_add_kernel(int64_t m, const T* __restrict__ Z, const double* __restrict__ u,
-                                                         int kp, T* __restrict__ z) {
-    __shared__ double us[32 * 32];
-    for (int i = threadIdx.x; i < 32 * kp; i += blockDim.x) us[i] = u[i];
+__global__ void __launch_bounds__(256) coarse_axpy_kernel(int64_t m, const T* __restrict__ A,
+                                                          const double* __restrict__ ua,
+                                                          const double* __restrict__ ub, double alpha, int kp,
+                                                          const T* __restrict__ x, T* __restrict__ out) {
+    __shared__ float us[32 * 32];
+    for (int i = threadIdx.x; i < 32 * kp; i += blockDim.x) us[i] = (float)(alpha * (ua[i] - (ub ? ub[i] : 0.0)));
+    __shared__ double ud[32 * 32];
+    for (int i = threadIdx.x; i < 32 * kp; i += blockDim.x) ud[i] = alpha * (ua[i] - (ub ? ub[i] : 0.0));
     __syncthreads();
-    const int64_t total = m * kp;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t row = i / kp;
-        const int col = (int)(i % kp);
-        const T* zr = Z + (size_t)row * 32;
-        double s = 0.0;
+    const int g = kp / 4;
+    const int64_t total = m * g;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / g;
+        const int c4 = (int)(t % g) * 4;
+        const T* ar = A + (size_t)row * 32;
+        V4<T> s(T(0));
 #pragma unroll 8
-        for (int j = 0; j < 32; ++j) s += (double)zr[j] * us[j * kp + col];
-        z[i] = (T)((double)z[i] + s);
+        for (int j = 0; j < 32; ++j) {
+            const T a = ar[j];
+            if (sizeof(T) == 4) {
+                const float* uj = us + j * kp + c4;
+                s.a += a * (T)uj[0]; s.b += a * (T)uj[1]; s.c += a * (T)uj[2]; s.d += a * (T)uj[3];
+            } else {
+                const double* uj = ud + j * kp + c4;
+                s.a += a * (T)uj[0]; s.b += a * (T)uj[1]; s.c += a * (T)uj[2]; s.d += a * (T)uj[3];
+            }
+        }
+        st4(out + (size_t)row * kp + c4, ld4(x + (size_t)row * kp + c4) + s);
     }
 }
 

@@ -159,7 +159,19 @@ struct StageHost {
     std::vector<uint32_t> gbs_cnt;
     HostVec<uint32_t> gbs_col;
     HostVec<double> gbs_val;
+    // reduced right-hand sides of the dense subdomains, from their eliminated side (when
+    // their kept rows, over the stage, number at most kDenseKeepMax): rows = eliminated
+    // slots (dk_slot: the slot, its global dof and scale invd * spou), entries = (position
+    // of the kept row among the stage's dense kept rows, C_ek); dk_keep[p] = kept slot
+    std::vector<int64_t> dk_ptr{0};
+    HostVec<uint32_t> dk_gidx, dk_col;
+    HostVec<double> dk_scale, dk_val;
+    std::vector<uint32_t> dk_keep;
 };
+
+// The dense subdomains' kept rows of a stage that the transposed reduced-rhs pass holds
+// in shared memory (per warp, kp columns): beyond this they stay in the keep CSR.
+constexpr int32_t kDenseKeepMax = 48;
 
 template <typename T>
 struct StageDev {
@@ -192,6 +204,11 @@ struct StageDev {
     DArr<uint32_t> gbs_cnt;
     DArr<uint32_t> gbs_col;
     DArr<T> gbs_val;
+    int64_t dk_rows = 0;
+    int32_t dk_nkeep = 0;
+    DArr<int64_t> dk_ptr;
+    DArr<uint32_t> dk_gidx, dk_col, dk_keep;
+    DArr<T> dk_scale, dk_val;
 };
 
 constexpr int kCoreRowsPerBlock = 2;  // output rows per block of core_gemv_kernel (4 warps each)

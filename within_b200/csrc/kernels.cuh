@@ -83,6 +83,9 @@ template <typename T>
 __device__ __forceinline__ void red_shared4(T* p, const V4<T>& v) {
     red_shared(p, v.a); red_shared(p + 1, v.b); red_shared(p + 2, v.c); red_shared(p + 3, v.d);
 }
+template <typename T> __device__ __forceinline__ T quiet_nan();
+template <> __device__ __forceinline__ float quiet_nan<float>() { return __int_as_float(0x7fc00000); }
+template <> __device__ __forceinline__ double quiet_nan<double>() { return __longlong_as_double(0x7ff8000000000000LL); }
 template <typename T>
 __device__ __forceinline__ V4<double> to_d(const V4<T>& v) { return V4<double>(v.a, v.b, v.c, v.d); }
 template <typename T>
@@ -485,6 +488,15 @@ static __global__ void permute_rows_kernel(const double* __restrict__ in, int64_
     }
 }
 
+// z = NaN everywhere when *failed is set (a multiplicative apply whose local solve did
+// not complete).
+template <typename T>
+__global__ void nan_on_failure_kernel(T* __restrict__ z, int64_t n, const int32_t* __restrict__ failed) {
+    if (*failed == 0) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        z[i] = quiet_nan<T>();
+}
+
 // Blocks for a transpose over `rows` rows (grid-stride beyond 16 blocks per SM).
 inline unsigned xpose_blocks(int64_t rows, int n_sm) {
     const int64_t need = (rows + 32 * kXposeWarps - 1) / (32 * kXposeWarps);
@@ -682,7 +694,7 @@ __device__ __forceinline__ void stcg4(double* p, const V4<double>& v) {
 // runs out, *err is set and the block goes on (the results are then invalid and the
 // host reports the error).
 constexpr unsigned kBarrierSpins = 1u << 22;
-__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned target, int* err) {
+__device__ __forceinline__ void grid_barrier(unsigned* count, unsigned target, int* err, unsigned max_spins) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -691,7 +703,7 @@ __device__ __forceinline__ void grid_barrier(unsigned* count, unsigned target, i
             unsigned c;
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(count) : "memory");
             if (c >= target) break;
-            if (spins >= kBarrierSpins) {
+            if (spins >= max_spins) {
                 atomicExch(err, 1);
                 break;
             }
@@ -713,7 +725,8 @@ __global__ void __launch_bounds__(kBlock) csr_levels_kernel(const CsrChunk* __re
                                                             const int64_t* __restrict__ ptr,
                                                             const uint32_t* __restrict__ col,
                                                             const T* __restrict__ val, const T* __restrict__ rscale,
-                                                            T* v, int kp, unsigned* bar, int* err) {
+                                                            T* v, int kp, unsigned* bar, int* err,
+                                                            unsigned target_extra, unsigned max_spins) {
     constexpr int NG = 32 / G;
     const int lane = threadIdx.x & 31;
     const int grp = lane / G;
@@ -760,7 +773,7 @@ __global__ void __launch_bounds__(kBlock) csr_levels_kernel(const CsrChunk* __re
                 }
             }
         }
-        if (li + 1 < nlev) grid_barrier(bar, (unsigned)(li + 1) * gridDim.x, err);
+        if (li + 1 < nlev) grid_barrier(bar, (unsigned)(li + 1) * gridDim.x + target_extra, err, max_spins);
     }
 }
 
@@ -911,6 +924,51 @@ __global__ void __launch_bounds__(kBlock) keep_init_kernel(int64_t nkeep, const 
     }
 }
 
+// Reduced right-hand sides of the stage's dense subdomains, from their eliminated side:
+// for every eliminated slot e (row of the dk arrays) and each entry (p, C_ek) of its row,
+// v[dk_keep[p]] += C_ek * scale_e * r[gidx_e] with scale_e = invd_e * spou_e.  This is the
+// keep CSR's product for those kept rows, read by eliminated slot: each slot's r row is
+// loaded once.  Each warp adds into its own table of the nkeep kept rows in shared memory
+// (red.shared), the lane groups of a warp starting their rows at spread-out entries so
+// that they hit different kept rows at a time; the block then adds its tables into v.
+template <typename T, int G>
+__global__ void __launch_bounds__(kBlock) dense_keep_kernel(int64_t nrows, const int64_t* __restrict__ ptr,
+                                                            const uint32_t* __restrict__ gidx,
+                                                            const T* __restrict__ scale,
+                                                            const uint32_t* __restrict__ col,
+                                                            const T* __restrict__ val, int nkeep,
+                                                            const uint32_t* __restrict__ keep_slot,
+                                                            const T* __restrict__ r, T* __restrict__ v, int kp) {
+    constexpr int NG = 32 / G;
+    extern __shared__ __align__(16) unsigned char dk_smem[];
+    T* tab = reinterpret_cast<T*>(dk_smem);
+    const int nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < nw * nkeep * kp; i += blockDim.x) tab[i] = T(0);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane / G;
+    const int c4 = (lane & (G - 1)) * 4;
+    T* mytab = tab + (size_t)warp * nkeep * kp + c4;
+    const int64_t rpb = blockDim.x / G;
+    for (int64_t i = (int64_t)blockIdx.x * rpb + threadIdx.x / G; i < nrows; i += (int64_t)gridDim.x * rpb) {
+        const V4<T> t = scale[i] * ld4(r + (size_t)gidx[i] * kp + c4);
+        const int64_t e0 = ptr[i];
+        const int len = (int)(ptr[i + 1] - e0);
+        int j = (grp * len) / NG;  // this group's starting entry
+        for (int a = 0; a < len; ++a) {
+            const int64_t e = e0 + j;
+            red_shared4(mytab + (size_t)col[e] * kp, val[e] * t);
+            if (++j == len) j = 0;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nkeep * kp; i += blockDim.x) {
+        T sum = T(0);
+        for (int w = 0; w < nw; ++w) sum += tab[(size_t)w * nkeep * kp + i];
+        if (sum != T(0)) atomicAdd(v + (size_t)keep_slot[i / kp] * kp + i % kp, sum);
+    }
+}
+
 // Keep-list segmented sums: M[s] += v[k] * (1 + rho_k if with_rho), block-reduced.
 template <typename T, int G>
 __global__ void __launch_bounds__(kBlock) keep_sum_kernel(int64_t nkeep, int spb, const uint32_t* __restrict__ keep_slots,
@@ -1029,9 +1087,14 @@ __global__ void __launch_bounds__(kBlock, 4) prolong_kernel(int64_t m, const int
                                                          const uint32_t* __restrict__ gbs_col,
                                                          const T* __restrict__ gbs_val, const double* __restrict__ mm,
                                                          const T* __restrict__ v, const T* __restrict__ r,
-                                                         T* __restrict__ z, int kp, double* __restrict__ part) {
+                                                         T* __restrict__ z, int kp, double* __restrict__ part,
+                                                         const int32_t* __restrict__ failed) {
     const int c4 = (threadIdx.x & (G - 1)) * 4;
     V4<double> dotp(0.0);
+    // a local solve that did not complete (an AC sweep's barrier wait ran out): z is NaN
+    // everywhere, as the reference's apply fills it (schwarz-precond additive/
+    // preconditioner.rs:197-201)
+    const bool nan_out = failed != nullptr && *failed != 0;
     const int64_t rpb = blockDim.x / G;
     for (int64_t j = (int64_t)blockIdx.x * rpb + threadIdx.x / G; j < m; j += (int64_t)gridDim.x * rpb) {
         const V4<double> rj = to_d(ld4(r + (size_t)j * kp + c4));
@@ -1068,7 +1131,7 @@ __global__ void __launch_bounds__(kBlock, 4) prolong_kernel(int64_t m, const int
             const V4<double> m2 = ld4(mm + (size_t)(2 * s + 1) * kp + c4);
             acc += sp * (sol - m2);
         }
-        const V4<T> zt = from_d<T>(acc);
+        const V4<T> zt = nan_out ? V4<T>(quiet_nan<T>()) : from_d<T>(acc);
         st4(z + (size_t)j * kp + c4, zt);
         const V4<double> zd = to_d(zt);
         dotp.a += rj.a * zd.a; dotp.b += rj.b * zd.b; dotp.c += rj.c * zd.c; dotp.d += rj.d * zd.d;

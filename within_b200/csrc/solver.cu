@@ -11,6 +11,7 @@
 #include <cstring>
 #include <functional>
 #include <future>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -296,8 +297,74 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
         st.bwd.chunks.insert(st.bwd.chunks.end(), bc.begin(), bc.end());
         st.bwd_lp.push_back((int64_t)st.bwd.chunks.size());
     }
-    // one warp per chunk (csr_rows_kernel): single rows, long rows in pieces of 256
-    st.keep.chunks = make_chunks(st.keep.ptr, 0, st.keep.nrows(), 256, 1, true);
+    // Dense subdomains (anchored dense solve, at most dense_threshold kept rows) get their
+    // reduced right-hand sides from their eliminated side when all of them together keep
+    // at most kDenseKeepMax rows: each eliminated slot reads its r row once and adds into
+    // a small shared table, instead of every kept row gathering all eliminated rows (the
+    // 20 year rows of a worker-year subdomain hold one entry per observation).
+    // The dense subdomains with the most keep-row entries are taken first (a pair's
+    // small components are dense subdomains too, with few entries each).
+    std::vector<char> keep_by_dense(ns, 0);
+    {
+        std::vector<int32_t> cand;
+        for (int32_t si = 0; si < ns; ++si)
+            if (subs[ids[si]].kind == 0 && kno[si + 1] > kno[si]) cand.push_back(si);
+        std::stable_sort(cand.begin(), cand.end(), [&](int32_t a, int32_t b) {
+            return kno[a + 1] - kno[a] > kno[b + 1] - kno[b];
+        });
+        int64_t nd = 0;
+        for (int32_t si : cand) {
+            const int64_t rows = kro[si + 1] - kro[si];
+            if (nd + rows > kDenseKeepMax) continue;
+            keep_by_dense[si] = 1;
+            nd += rows;
+        }
+        if (nd > 0) {
+            // rows: (slot, keep0, first table position) of every eliminated slot of a chosen
+            // dense subdomain, in slot order; sized first, then filled in parallel
+            struct DkRow { int64_t slot, keep0; uint32_t pos0; };
+            std::vector<DkRow> rows;
+            for (int32_t si = 0; si < ns; ++si) {
+                const Subdomain& sd = subs[ids[si]];
+                if (!keep_by_dense[si]) continue;
+                const int32_t nq = sd.n_q();
+                const int64_t o = so[si];
+                const int64_t keep0 = o + (sd.elim_q ? nq : 0), elim0 = o + (sd.elim_q ? 0 : nq);
+                const int32_t n_elim = sd.elim_q ? nq : sd.n_r(), n_keep = sd.elim_q ? sd.n_r() : nq;
+                const uint32_t pos0 = (uint32_t)st.dk_keep.size();
+                for (int32_t k = 0; k < n_keep; ++k) st.dk_keep.push_back((uint32_t)(keep0 + k));
+                for (int32_t e = 0; e < n_elim; ++e) rows.push_back(DkRow{elim0 + e, keep0, pos0});
+            }
+            const size_t nr = rows.size();
+            st.dk_ptr.assign(nr + 1, 0);
+            for (size_t i = 0; i < nr; ++i)
+                st.dk_ptr[i + 1] = st.dk_ptr[i] + (st.bs_ptr[rows[i].slot + 1] - st.bs_ptr[rows[i].slot]);
+            st.dk_gidx.resize(nr);
+            st.dk_scale.resize(nr);
+            st.dk_col.resize((size_t)st.dk_ptr[nr]);
+            st.dk_val.resize((size_t)st.dk_ptr[nr]);
+            constexpr size_t kRowsPerTask = 1 << 16;
+            parallel_tasks((nr + kRowsPerTask - 1) / kRowsPerTask, [&](size_t t) {
+                for (size_t i = t * kRowsPerTask; i < std::min(nr, (t + 1) * kRowsPerTask); ++i) {
+                    const int64_t l = rows[i].slot;
+                    st.dk_gidx[i] = st.gidx[l];
+                    st.dk_scale[i] = st.invd[l] * st.spou[l];
+                    int64_t d = st.dk_ptr[i];
+                    for (int64_t x = st.bs_ptr[l]; x < st.bs_ptr[l + 1]; ++x, ++d) {
+                        st.dk_col[d] = rows[i].pos0 + (uint32_t)(st.bs_col[x] - rows[i].keep0);
+                        st.dk_val[d] = st.bs_val[x];
+                    }
+                }
+            });
+        }
+    }
+    // one warp per chunk (csr_rows_kernel): single rows, long rows in pieces of 256; the
+    // kept rows of subdomains handled above are left out
+    for (int32_t si = 0; si < ns; ++si) {
+        if (keep_by_dense[si]) continue;
+        auto kc = make_chunks(st.keep.ptr, kro[si], kro[si + 1], 256, 1, true);
+        st.keep.chunks.insert(st.keep.chunks.end(), kc.begin(), kc.end());
+    }
     if (with_gather) {
         st.gptr.assign((size_t)ndofs + 1, 0);
         for (uint32_t g : st.gidx) st.gptr[g + 1]++;
@@ -402,6 +469,16 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
     d.gbs_cnt.upload(h.gbs_cnt);
     d.gbs_col.upload(h.gbs_col);
     d.gbs_val.upload_cast(h.gbs_val);
+    d.dk_rows = (int64_t)h.dk_gidx.size();
+    d.dk_nkeep = (int32_t)h.dk_keep.size();
+    if (d.dk_rows > 0) {
+        d.dk_ptr.upload(h.dk_ptr);
+        d.dk_gidx.upload(h.dk_gidx);
+        d.dk_col.upload(h.dk_col);
+        d.dk_keep.upload(h.dk_keep);
+        d.dk_scale.upload_cast(h.dk_scale);
+        d.dk_val.upload_cast(h.dk_val);
+    }
 }
 
 }  // namespace
@@ -469,6 +546,13 @@ struct SolverImpl {
     DArr<ObsChunk> chunks;
     ObsParams obs{};
     bool has_split = false;
+    // observation-pass block shapes the autotuner picks from: chunk tables of 16, 32 and
+    // 64 observations per work unit, and 1 or 2 resident blocks per SM; choice per
+    // (kp class, element size), -1 = not tuned (32 observations, 2 blocks per SM)
+    DArr<ObsChunk> chunk_tab[3];
+    int64_t nchunk_tab[3] = {0, 0, 0};
+    bool split_tab[3] = {false, false, false};
+    int32_t obs_choice[4][2] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}};
     // hottest levels of every non-primary factor, for the observation pass
     std::vector<DArr<uint32_t>> hot_level;
     std::vector<int32_t> hot_count;
@@ -496,6 +580,7 @@ struct SolverImpl {
     std::shared_ptr<void> lsmr;   // LsmrBufs, created on first LSMR solve
     std::shared_ptr<void> cn;     // CnState of the coarse-space network, kept while training
     bool precond_only = false;    // built from a serialized preconditioner: no design
+    bool inject_sweep_timeout = false;  // test hook: AC sweep barriers that cannot be met
     std::vector<uint8_t> pc_bytes;  // serialized preconditioner, made on first request
     int32_t* h_active = nullptr;  // pinned
     double setup_time = 0.0;
@@ -514,8 +599,8 @@ struct SolverImpl {
     // Coarse space (learned by the message-passing network, or given): CG adds
     // Z E^+ Z' r to the Schwarz output.  Z is n_dofs x 32 row-major (unused columns zero).
     int32_t coarse_k = 0;
-    DArr<double> coarse_z64, coarse_einv, coarse_part, coarse_u;
-    DArr<float> coarse_z32;
+    DArr<double> coarse_z64, coarse_gz64, coarse_einv, coarse_part, coarse_u, coarse_tmp64;
+    DArr<float> coarse_z32, coarse_gz32, coarse_tmp32;
     // training targets of the network on this design (n_dofs x t, scaled space)
     DArr<float> cn_targets;
     int32_t cn_t = 0;
@@ -595,8 +680,8 @@ int pad_kp(int k) {
 }
 
 // Observation chunks over primary-sorted observations (level-aligned; long levels split).
-std::vector<ObsChunk> make_obs_chunks(const std::vector<int64_t>& lvl_ptr, int64_t nlev, bool& has_split) {
-    constexpr int64_t kObsPerChunk = 32;
+std::vector<ObsChunk> make_obs_chunks(const std::vector<int64_t>& lvl_ptr, int64_t nlev, bool& has_split,
+                                      int64_t kObsPerChunk = 32) {
     std::vector<ObsChunk> out;
     has_split = false;
     int64_t l = 0;
@@ -631,14 +716,6 @@ void upload_design(SolverImpl& S) {
     std::vector<int64_t> lvl_ptr((size_t)np + 1, 0);
     for (int64_t i = 0; i < d.n; ++i) lvl_ptr[cp[i] + 1]++;
     for (int64_t l = 0; l < np; ++l) lvl_ptr[l + 1] += lvl_ptr[l];
-    std::vector<uint32_t> perm((size_t)d.n);
-    {
-        std::vector<int64_t> cur(lvl_ptr.begin(), lvl_ptr.end() - 1);
-        for (int64_t i = 0; i < d.n; ++i) perm[cur[cp[i]]++] = (uint32_t)i;
-    }
-    S.perm_identity = true;
-    for (int64_t i = 0; i < d.n; ++i)
-        if (perm[i] != (uint32_t)i) { S.perm_identity = false; break; }
     // device factor order: the primary factor first, then the others by level count,
     // largest first (the observation pass's private-table factors are a suffix)
     S.dev_factor.clear();
@@ -647,6 +724,35 @@ void upload_design(SolverImpl& S) {
         if (q != S.primary) S.dev_factor.push_back(q);
     std::stable_sort(S.dev_factor.begin() + 1, S.dev_factor.end(),
                      [&](int a, int b) { return d.nlev[a] > d.nlev[b]; });
+    std::vector<uint32_t> perm((size_t)d.n);
+    {
+        std::vector<int64_t> cur(lvl_ptr.begin(), lvl_ptr.end() - 1);
+        for (int64_t i = 0; i < d.n; ++i) perm[cur[cp[i]]++] = (uint32_t)i;
+    }
+    // Within a primary level the observation pass keeps a running sum of the slot-1
+    // factor while its level repeats.  When the rows come in an order where that factor
+    // alternates (short runs: a worker's years shuffled between its firms), the
+    // observations of each primary level are also sorted by it (G does not depend on the
+    // order): a stable counting sort by the slot-1 level, then by the primary level.
+    if (d.Q >= 2) {
+        const uint32_t* c1 = d.codes.data() + (size_t)S.dev_factor[1] * d.n;
+        int64_t runs = 0;
+        for (int64_t i = 0; i < d.n; ++i)
+            if (i == 0 || cp[perm[i]] != cp[perm[i - 1]] || c1[perm[i]] != c1[perm[i - 1]]) ++runs;
+        if (runs > d.n * 3 / 10) {
+            const int64_t L1 = d.nlev[S.dev_factor[1]];
+            std::vector<int64_t> c1ptr((size_t)L1 + 1, 0);
+            for (int64_t i = 0; i < d.n; ++i) c1ptr[c1[i] + 1]++;
+            for (int64_t l = 0; l < L1; ++l) c1ptr[l + 1] += c1ptr[l];
+            std::vector<uint32_t> by1((size_t)d.n);
+            for (int64_t i = 0; i < d.n; ++i) by1[c1ptr[c1[i]]++] = (uint32_t)i;
+            std::vector<int64_t> cur(lvl_ptr.begin(), lvl_ptr.end() - 1);
+            for (int64_t a = 0; a < d.n; ++a) perm[cur[cp[by1[a]]]++] = by1[a];
+        }
+    }
+    S.perm_identity = true;
+    for (int64_t i = 0; i < d.n; ++i)
+        if (perm[i] != (uint32_t)i) { S.perm_identity = false; break; }
     // hot levels: the 255 most frequent levels (hit >= 64 times) of each non-primary
     // factor with more than 256 levels and fewer than 2^24; their codes on the device
     // carry the hot slot + 1 in bits 24-31 (kObsLevelBits) next to the level
@@ -706,6 +812,12 @@ void upload_design(SolverImpl& S) {
     }
     auto ch = make_obs_chunks(lvl_ptr, np, S.has_split);
     S.chunks.upload(ch);
+    for (int ci = 0; ci < 3; ++ci) {
+        const int64_t per = (int64_t)16 << ci;
+        auto t = make_obs_chunks(lvl_ptr, np, S.split_tab[ci], per);
+        S.nchunk_tab[ci] = (int64_t)t.size();
+        S.chunk_tab[ci].upload(t);
+    }
     P.n = d.n;
     P.ns = ns;
     P.Q = d.Q;
@@ -781,6 +893,8 @@ int obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
     return np;
 }
 
+int kp_class(int kp) { return kp <= 4 ? 0 : kp <= 8 ? 1 : kp <= 16 ? 2 : 3; }
+
 // Returns the number of per-warp partial rows written (OBS_LSMR; grid x warps per block).
 template <typename T, int MODE>
 int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* out, T* eout,
@@ -790,10 +904,21 @@ int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* o
     P.lsmr_scale = lsmr_scale;
     P.lsmr_part = lsmr_part;
     const int G = group_for(kp);
+    // the autotuned block shape (obs_autotune), else 32 observations per chunk, 2 blocks/SM
+    const int choice = S.obs_choice[kp_class(kp)][sizeof(T) == 8 ? 1 : 0];
+    bool split = S.has_split;
+    int blocks_per_sm = 2;
+    if (choice >= 0) {
+        const int ci = choice / 2;
+        P.chunks = S.chunk_tab[ci].p;
+        P.nchunks = S.nchunk_tab[ci];
+        split = S.split_tab[ci];
+        blocks_per_sm = 1 + choice % 2;
+    }
     if (MODE != OBS_DX && out) {
         // zero the outputs that are accumulated (every non-primary factor, split levels)
         const size_t m = (size_t)S.d.ndofs;
-        if (S.has_split) {
+        if (split) {
             WB_CUDA(cudaMemsetAsync(out, 0, m * kp * sizeof(T), S.stream));
         } else {
             const size_t a = (size_t)S.d.off[S.primary] * kp, b = (size_t)(S.d.off[S.primary] + S.d.nlev[S.primary]) * kp;
@@ -803,11 +928,63 @@ int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* o
     }
     const size_t smem = (size_t)P.smem_elems * sizeof(T);
     const int bt = obs_block<T>();  // two resident blocks per SM (registers and shared memory)
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P.nchunks * G + bt - 1) / bt, (int64_t)S.n_sm * 2));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P.nchunks * G + bt - 1) / bt, (int64_t)S.n_sm * blocks_per_sm));
     const cudaError_t err = obs_dispatch<T, MODE>(P, np, G, grid, smem, S.stream, w, x, yin, out, eout);
     WB_CUDA(err);
     S.gpu_launches++;
     return grid * (bt / 32);
+}
+
+// Autotuner of the observation pass's block shape (the dominant kernel): the first time a
+// solver needs the pass for kp RHS in a precision, each candidate (16, 32 or 64
+// observations per chunk; 1 or 2 resident blocks per SM) runs twice on the solver's own
+// design, timed with events on its stream after a warm-up launch, and the fastest is
+// kept.  The choice is cached for the process per shape class (log2 of the observation
+// count, factor count, kp, element size), so that solvers of the same class (the
+// problems of an uneven batch) reuse it without timing.  Runs outside any stream
+// capture; x is read and y overwritten.
+std::mutex g_obs_tune_mu;
+std::map<std::array<int64_t, 4>, int32_t> g_obs_tune;
+
+template <typename T>
+void obs_autotune(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
+    int32_t& choice = S.obs_choice[kp_class(kp)][sizeof(T) == 8 ? 1 : 0];
+    if (choice >= 0 || S.d.n == 0) return;
+    int64_t lg = 0;
+    for (int64_t v = S.d.n; v > 1; v >>= 1) ++lg;
+    const std::array<int64_t, 4> key{lg, (int64_t)S.d.Q, (int64_t)kp, (int64_t)sizeof(T)};
+    {
+        std::lock_guard<std::mutex> lk(g_obs_tune_mu);
+        const auto it = g_obs_tune.find(key);
+        if (it != g_obs_tune.end()) {
+            choice = it->second;
+            return;
+        }
+    }
+    cudaEvent_t e0, e1;
+    WB_CUDA(cudaEventCreate(&e0));
+    WB_CUDA(cudaEventCreate(&e1));
+    float best = 0.f;
+    int32_t best_c = 3;  // 32 observations per chunk, 2 blocks per SM
+    for (int32_t c = 0; c < 6; ++c) {
+        choice = c;
+        launch_obs<T, OBS_GRAM>(S, kp, w, x, nullptr, y, nullptr);
+        WB_CUDA(cudaEventRecord(e0, S.stream));
+        for (int rep = 0; rep < 2; ++rep) launch_obs<T, OBS_GRAM>(S, kp, w, x, nullptr, y, nullptr);
+        WB_CUDA(cudaEventRecord(e1, S.stream));
+        WB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        WB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (c == 0 || ms < best) {
+            best = ms;
+            best_c = c;
+        }
+    }
+    WB_CUDA(cudaEventDestroy(e0));
+    WB_CUDA(cudaEventDestroy(e1));
+    choice = best_c;
+    std::lock_guard<std::mutex> lk(g_obs_tune_mu);
+    g_obs_tune.emplace(key, best_c);
 }
 
 // Dot partials over rows (at most 2 blocks per SM: few partials to reduce).
@@ -820,7 +997,9 @@ void launch_dot(SolverImpl& S, const TA* a, const TB* b, int64_t rows, int kp, d
     S.gpu_launches++;
 }
 
-// red[c] = sum_b part[b*kp + c] (fixed order per c; deterministic).
+// red[c] = sum_b part[b*kp + c] (fixed order per c; deterministic).  Each thread sums a
+// strided subset of the partials with eight independent accumulators, so that eight
+// loads are in flight at a time, and combines them in a fixed order.
 __global__ void reduce_parts_kernel(const double* __restrict__ part, int nb, int kp, double* __restrict__ red) {
     __shared__ double sm[kBlock];
     const int t = threadIdx.x;
@@ -828,7 +1007,14 @@ __global__ void reduce_parts_kernel(const double* __restrict__ part, int nb, int
     double s = 0.0;
     if (t < J * kp) {
         const int c = t % kp, j = t / kp;
-        for (int b = j; b < nb; b += J) s += part[(size_t)b * kp + c];
+        double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int b = j;
+        for (; b + 7 * J < nb; b += 8 * J) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) a[u] += part[(size_t)(b + u * J) * kp + c];
+        }
+        for (; b < nb; b += J) a[0] += part[(size_t)b * kp + c];
+        s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
     }
     sm[t] = s;
     __syncthreads();
@@ -908,6 +1094,9 @@ void launch_gram_acc(SolverImpl& S, int kp, const T* x, T* y) {
     S.gpu_launches++;
 }
 
+// Spin limit of the barrier waits under the test hook (about a millisecond per wait).
+constexpr unsigned kInjectedBarrierSpins = 1u << 12;
+
 // All levels of one AC sweep direction of a stage as one cooperative launch (grid
 // barriers between levels), when the device supports it; otherwise one launch per level.
 template <typename T, int EPI>
@@ -935,23 +1124,28 @@ void launch_sweep(SolverImpl& S, CsrDev<T>& c, const std::vector<int64_t>& lp, c
         const T* vl = c.val.p;
         const T* sc = c.rscale.p;
         int nl = nlev, bw = backward ? 1 : 0, k = kp;
+        // a test can make every barrier wait for one block more than the grid has, with a
+        // short limit: the waits run out, the error flag is set, the launch ends
+        unsigned extra = S.inject_sweep_timeout ? 1u : 0u;
+        unsigned spins = S.inject_sweep_timeout ? kInjectedBarrierSpins : kBarrierSpins;
         void* args[] = {(void*)&ch, (void*)&lp_d, (void*)&nl, (void*)&bw, (void*)&rs, (void*)&pt, (void*)&cl,
-                        (void*)&vl, (void*)&sc, (void*)&v, (void*)&k, (void*)&bar, (void*)&err};
+                        (void*)&vl, (void*)&sc, (void*)&v, (void*)&k, (void*)&bar, (void*)&err, (void*)&extra,
+                        (void*)&spins};
         WB_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kBlock), args, 0, S.stream));
         S.gpu_launches++;
     };
     WB_DISPATCH_G(G, go(csr_levels_kernel<T, GV, EPI>));
 }
 
-// The host learns of a grid-barrier timeout here (after the work that set it is done).
-void check_sweeps(SolverImpl& S) {
-    if (!S.coop || !S.ws.sweep_err.p) return;
+// The host learns of a grid-barrier timeout here (after the work that set it is done):
+// true when a local solve did not complete since the last check (the flag is cleared).
+bool sweeps_failed(SolverImpl& S) {
+    if (!S.coop || !S.ws.sweep_err.p) return false;
     int32_t e = 0;
+    WB_CUDA(cudaStreamSynchronize(S.stream));
     WB_CUDA(cudaMemcpy(&e, S.ws.sweep_err.p, sizeof(int32_t), cudaMemcpyDeviceToHost));
-    if (e) {
-        WB_CUDA(cudaMemset(S.ws.sweep_err.p, 0, sizeof(int32_t)));
-        throw CudaError("an AC sweep grid barrier wait exceeded its limit; the result is invalid");
-    }
+    if (e) WB_CUDA(cudaMemset(S.ws.sweep_err.p, 0, sizeof(int32_t)));
+    return e != 0;
 }
 
 // The local solves of one stage from the restriction input r up to the kept solution
@@ -976,6 +1170,17 @@ SubMeans stage_local_solve(SolverImpl& S, StageDev<T>& st, const T* r, T* v, int
                              st.nkeep, st.keep_slots.p, st.gidx.p, st.spou.p, st.rho.p, st.sub_of.p, st.sub_nloc.p, S0, r,
                              v, kp));
         launch_csr<T, EPI_ACC>(S, st.keep, 0, st.keep.nchunks, r, v, kp);
+        if (st.dk_rows > 0) {  // the dense subdomains' kept rows, from their eliminated side
+            const size_t smem = sizeof(T) * (size_t)(kBlock / 32) * st.dk_nkeep * kp;
+            WB_DISPATCH_G(G, {
+                auto kern = dense_keep_kernel<T, GV>;
+                if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                kern<<<S.n_sm * 2, kBlock, smem, S.stream>>>(st.dk_rows, st.dk_ptr.p, st.dk_gidx.p, st.dk_scale.p,
+                                                             st.dk_col.p, st.dk_val.p, st.dk_nkeep, st.dk_keep.p, r, v, kp);
+            });
+            WB_CUDA(cudaGetLastError());
+            S.gpu_launches++;
+        }
         const int gs = (int)std::max<int64_t>(1, (st.nkeep + kSpb - 1) / kSpb);
         WB_DISPATCH_G(G, keep_sum_kernel<T, GV><<<gs, kBlock, 0, S.stream>>>(st.nkeep, kSpb, st.keep_slots.p, st.rho.p, 0,
                                                                               st.sub_of.p, v, kp, M1));
@@ -1042,7 +1247,7 @@ void apply_precond(SolverImpl& S, const T* r, T* z, int kp, double* part, int& n
             nb_part = S.fit(((int64_t)m * G + kBlock - 1) / kBlock, (const void*)kern);
             kern<<<nb_part, kBlock, 0, S.stream>>>(m, st.gptr.p, st.gslot.p, st.gsub.p, st.gspou.p, st.ginvd.p,
                                                    st.gbs_ptr.p, st.gbs_cnt.p, st.gbs_col.p, st.gbs_val.p, mm, v, r, z,
-                                                   kp, part);
+                                                   kp, part, S.ws.sweep_err.p);
         });
         WB_CUDA(cudaGetLastError());
         S.gpu_launches += 2;
@@ -1065,31 +1270,58 @@ void apply_precond(SolverImpl& S, const T* r, T* z, int kp, double* part, int& n
         S.gpu_launches++;
         launch_gram_acc<T>(S, kp, cb, rw);  // r_work -= G c
     }
+    if (S.coop && S.ws.sweep_err.p) {  // a local solve that did not complete: z = NaN
+        nan_on_failure_kernel<T><<<S.nblk(m * kp, 1), kBlock, 0, S.stream>>>(z, m * kp, S.ws.sweep_err.p);
+        WB_CUDA(cudaGetLastError());
+        S.gpu_launches++;
+    }
     if (part) launch_dot<T, T>(S, r, z, m, kp, part, nb_part);
 }
 
 template <typename T> const T* coarse_basis(SolverImpl& S);
 template <> const double* coarse_basis<double>(SolverImpl& S) { return S.coarse_z64.p; }
 template <> const float* coarse_basis<float>(SolverImpl& S) { return S.coarse_z32.p; }
-constexpr int kCoarseDotBlocksPerSm = 2;
+template <typename T> const T* coarse_gbasis(SolverImpl& S);
+template <> const double* coarse_gbasis<double>(SolverImpl& S) { return S.coarse_gz64.p; }
+template <> const float* coarse_gbasis<float>(SolverImpl& S) { return S.coarse_gz32.p; }
+template <typename T> DArr<T>& coarse_tmp(SolverImpl& S);
+template <> DArr<double>& coarse_tmp<double>(SolverImpl& S) { return S.coarse_tmp64; }
+template <> DArr<float>& coarse_tmp<float>(SolverImpl& S) { return S.coarse_tmp32; }
+int coarse_blocks(const SolverImpl& S) {
+    const int64_t tiles = (S.d.ndofs + kCoarseTileRows - 1) / kCoarseTileRows;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)S.n_sm * 2));
+}
 
-// The CG preconditioner: z = M^{-1} r and, with a coarse space, z += Z E^+ Z' r.  The
-// block partials of r.z (part, nb_part rows) then get one more row, c.u with c = Z' r and
-// u = E^+ c, so that the caller's reduction covers both terms.
+// The CG preconditioner: z = M^{-1} r, or with a coarse space the balancing form
+// z = P' M^-1 P r + Z E^+ Z' r (coarse.cuh), whose r.z partials come from a dot of their
+// own (nb_part rows in part).
 template <typename T>
 void apply_precond_cg(SolverImpl& S, const T* r, T* z, int kp, double* part, int& nb_part) {
-    apply_precond<T>(S, r, z, kp, part, nb_part);
-    if (S.coarse_k == 0) return;
+    if (S.coarse_k == 0) {
+        apply_precond<T>(S, r, z, kp, part, nb_part);
+        return;
+    }
     const T* Z = coarse_basis<T>(S);
+    const T* GZ = coarse_gbasis<T>(S);
+    T* rp = coarse_tmp<T>(S).p;
     const int64_t m = S.d.ndofs;
-    const int nbc = S.n_sm * kCoarseDotBlocksPerSm;
-    coarse_dot_kernel<T><<<nbc, 256, 0, S.stream>>>(m, Z, r, kp, S.coarse_part.p);
-    coarse_solve_kernel<<<1, 256, 0, S.stream>>>(S.coarse_part.p, nbc, S.coarse_einv.p, kp, S.coarse_u.p, part,
-                                                 nb_part);
-    coarse_add_kernel<T><<<S.nblk(m * kp, 1), 256, 0, S.stream>>>(m, Z, S.coarse_u.p, kp, z);
+    const int nbc = coarse_blocks(S);
+    double* u1 = S.coarse_u.p;
+    double* u2 = S.coarse_u.p + 32 * 32;
+    const int ga = S.nblk(m * kp / 4, 1);
+    coarse_tn_kernel<T><<<nbc, 256, 0, S.stream>>>(m, Z, r, kp, S.coarse_part.p);
+    coarse_solve_kernel<<<1, kCoarseSolveThreads, 0, S.stream>>>(S.coarse_part.p, nbc, S.coarse_einv.p, kp, u1);
+    coarse_axpy_kernel<T><<<ga, 256, 0, S.stream>>>(m, GZ, u1, nullptr, -1.0, kp, r, rp);  // P r
     WB_CUDA(cudaGetLastError());
-    S.gpu_launches += 3;
-    if (part) nb_part += 1;
+    int nb = 0;
+    apply_precond<T>(S, rp, z, kp, nullptr, nb);  // y = M^-1 P r
+    coarse_tn_kernel<T><<<nbc, 256, 0, S.stream>>>(m, GZ, z, kp, S.coarse_part.p);
+    coarse_solve_kernel<<<1, kCoarseSolveThreads, 0, S.stream>>>(S.coarse_part.p, nbc, S.coarse_einv.p, kp, u2);
+    coarse_axpy_kernel<T><<<ga, 256, 0, S.stream>>>(m, Z, u1, u2, 1.0, kp, z, z);  // z = y + Z (u1 - u2)
+    WB_CUDA(cudaGetLastError());
+    S.gpu_launches += 6;
+    nb_part = 0;
+    if (part) launch_dot<T, T>(S, r, z, m, kp, part, nb_part);
 }
 
 // ---------------------------------------------------------------------------
@@ -1150,7 +1382,7 @@ __global__ void cg_alpha_kernel(KState s, const double* red, int kp) {
         if (s.active[c]) {
             const double pap = red[c];
             s.iters[c] += 1;
-            if (pap <= 0.0) {
+            if (!(pap > 0.0)) {  // pAp <= 0 (cg.rs:79-84), or not finite (a failed local solve)
                 s.active[c] = 0;
                 s.conv[c] = 0;
             } else {
@@ -1257,6 +1489,7 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
     double* part = w.part.p;
     double* red = w.red.p;
     int nb = 0;
+    if (S.coarse_k) coarse_tmp<T>(S).alloc((size_t)m * kp);  // before any capture
     WB_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * m * kp, S.stream));
     WB_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * m * kp, cudaMemcpyDeviceToDevice, S.stream));
     launch_dot<T, T>(S, b, b, m, kp, part, nb);
@@ -1268,6 +1501,7 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
     WB_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * m * kp, cudaMemcpyDeviceToDevice, S.stream));
     S.gpu_launches += 2;
     const T* w_t = std::is_same<T, double>::value ? (const T*)S.w64.p : (const T*)S.w32.p;
+    if (!S.explicit_op) obs_autotune<T>(S, kp, w_t, p, ap);  // before the iteration is captured
     const int kind = std::is_same<T, double>::value ? 0 : 1;
     // one iteration: q = G p, alpha, x/r update, convergence check, z = M r, beta, p update
     auto body = [&]() {
@@ -2102,6 +2336,7 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
     }
     // b = D'W y (rmatvec_wdt, solver.rs:210-211)
     launch_obs<double, OBS_RHS>(S, kp, S.w64.p, nullptr, w.yi.p, w.b.p, nullptr);
+    obs_autotune<double>(S, kp, S.w64.p, w.b.p, w.gx.p);  // FP64 passes: refinement and demeaning
     int nb = 0;
     launch_dot<double, double>(S, w.b.p, w.b.p, m, kp, w.part.p, nb);
     std::vector<double> bb = host_reduce(S, nb, kp);
@@ -2536,23 +2771,23 @@ void jacobi_eigen(std::vector<double>& A, int n, std::vector<double>& lam, std::
 }
 
 // Installs the coarse space spanned by the columns of Z64 (m x 32 row-major, FP64, on the
-// device): E = Z'GZ in FP64, its pseudo-inverse (eigenvalues below 1e-10 of the largest
-// dropped: null-space directions of G), and an FP32 copy of Z for mixed precision.
+// device): GZ = G Z and E = Z'GZ in FP64, E's pseudo-inverse (eigenvalues below 1e-10 of
+// the largest dropped: null-space directions of G), and FP32 copies of Z and GZ for
+// mixed precision.
 void install_coarse(SolverImpl& S) {
     const int64_t m = S.d.ndofs;
-    DArr<double> gz;
-    gz.alloc((size_t)m * 32);
-    launch_gram<double>(S, 32, S.w64.p, S.coarse_z64.p, gz.p);
-    const int nbc = S.n_sm * kCoarseDotBlocksPerSm;
+    S.coarse_gz64.alloc((size_t)m * 32);
+    launch_gram<double>(S, 32, S.w64.p, S.coarse_z64.p, S.coarse_gz64.p);
+    const int nbc = coarse_blocks(S);
     S.coarse_part.alloc((size_t)nbc * 32 * 32);
-    S.coarse_u.alloc(32 * 32);
+    S.coarse_u.alloc(2 * 32 * 32);
     S.coarse_einv.alloc(32 * 32);
-    coarse_dot_kernel<double><<<nbc, 256, 0, S.stream>>>(m, S.coarse_z64.p, gz.p, 32, S.coarse_part.p);
-    // E = sum of the partials: coarse_solve with the identity as "E^+" gives u = c = E
+    coarse_tn_kernel<double><<<nbc, 256, 0, S.stream>>>(m, S.coarse_z64.p, S.coarse_gz64.p, 32, S.coarse_part.p);
+    // E = the sum of the partials: coarse_solve with the identity as "E^+" gives u = E
     std::vector<double> I(32 * 32, 0.0);
     for (int i = 0; i < 32; ++i) I[i * 32 + i] = 1.0;
     WB_CUDA(cudaMemcpyAsync(S.coarse_einv.p, I.data(), sizeof(double) * 32 * 32, cudaMemcpyHostToDevice, S.stream));
-    coarse_solve_kernel<<<1, 256, 0, S.stream>>>(S.coarse_part.p, nbc, S.coarse_einv.p, 32, S.coarse_u.p, nullptr, 0);
+    coarse_solve_kernel<<<1, kCoarseSolveThreads, 0, S.stream>>>(S.coarse_part.p, nbc, S.coarse_einv.p, 32, S.coarse_u.p);
     WB_CUDA(cudaGetLastError());
     S.gpu_launches += 2;
     std::vector<double> E(32 * 32);
@@ -2574,7 +2809,9 @@ void install_coarse(SolverImpl& S) {
     WB_CUDA(cudaMemcpyAsync(S.coarse_einv.p, Ei.data(), sizeof(double) * 32 * 32, cudaMemcpyHostToDevice, S.stream));
     if (S.mixed()) {
         S.coarse_z32.alloc((size_t)m * 32);
+        S.coarse_gz32.alloc((size_t)m * 32);
         convert_kernel<double, float><<<S.nblk(m * 32, 1), kBlock, 0, S.stream>>>(S.coarse_z64.p, S.coarse_z32.p, m * 32);
+        convert_kernel<double, float><<<S.nblk(m * 32, 1), kBlock, 0, S.stream>>>(S.coarse_gz64.p, S.coarse_gz32.p, m * 32);
         WB_CUDA(cudaGetLastError());
     }
     WB_CUDA(cudaStreamSynchronize(S.stream));
@@ -2800,7 +3037,11 @@ int solve_device(SolverImpl& S, const double* d_ys, size_t k, double* d_x, doubl
                 s.time_total = dt;
             }
     }
-    wb::check_sweeps(S);
+    // LocalSolveFailed inside CG's try_apply (schwarz-precond solve/cg.rs:69, 104) ends the
+    // solve with an error (IterativeSolve)
+    if (wb::sweeps_failed(S))
+        return wb::fail(WITHIN_ERR_ITERATIVE_SOLVE,
+                        "local solve failed: an approximate-Cholesky sweep's grid barrier wait ran out");
     return WITHIN_OK;
 }
 
@@ -3059,7 +3300,9 @@ static int apply_common(within_solver* s, const double* in, size_t k, double* ou
         WB_CUDA(cudaGetLastError());
         WB_CUDA(cudaMemcpyAsync(out, dout.p, sizeof(double) * out_rows * k, cudaMemcpyDeviceToHost, S.stream));
         WB_CUDA(cudaStreamSynchronize(S.stream));
-        if (which == 1) wb::check_sweeps(S);
+        // a local solve that did not complete left z all NaN, as the reference's apply
+        // does (schwarz-precond additive/preconditioner.rs:197-201); the flag is cleared
+        if (which == 1) wb::sweeps_failed(S);
         return WITHIN_OK;
     });
 }
@@ -3125,6 +3368,24 @@ void within_solver_ac_arrays(const within_solver* s, int32_t i, int32_t* level_p
     std::copy(f.col_coef.begin(), f.col_coef.end(), col_coef);
     std::copy(f.core_vertex.begin(), f.core_vertex.end(), core_vertex);
     std::copy(f.core_z.begin(), f.core_z.end(), core_z);
+}
+
+int within_solver_inject_sweep_timeout(within_solver* s, int32_t on) {
+    if (!s) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "solver is null");
+    SolverImpl& S = *s->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    return guard([&]() -> int {
+        bool sweeps = false;
+        for (const auto& st : S.stages64) sweeps = sweeps || st.fwd_lp.size() > 2 || st.bwd_lp.size() > 2;
+        if (!S.coop || !sweeps)
+            return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the preconditioner has no fused approximate-Cholesky sweeps");
+        S.inject_sweep_timeout = on != 0;
+        if (S.cg_exec) {  // the captured CG iteration holds the sweep parameters
+            WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
+            S.cg_exec = nullptr;
+        }
+        return WITHIN_OK;
+    });
 }
 
 // --- learned coarse space ---
@@ -3236,6 +3497,16 @@ int within_solver_release_coarse_training(within_solver* s) {
         S.cn_t = 0;
         return WITHIN_OK;
     });
+}
+
+int within_solver_obs_config(const within_solver* s, int32_t k, int32_t elem_bytes, int32_t* obs_per_chunk,
+                             int32_t* blocks_per_sm) {
+    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) || !obs_per_chunk || !blocks_per_sm)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
+    const int32_t c = s->impl->obs_choice[wb::kp_class(wb::pad_kp(k))][elem_bytes == 8 ? 1 : 0];
+    *obs_per_chunk = c < 0 ? 32 : 16 << (c / 2);
+    *blocks_per_sm = c < 0 ? 2 : 1 + c % 2;
+    return c < 0 ? 1 : 0;
 }
 
 int64_t within_solver_schwarz_bytes(const within_solver* s, int32_t k, int32_t elem_bytes) {
