@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwithin_b200.so")
 # translation units, compiled in parallel (the observation-pass instantiations are split
 # out because ptxas spends most of the build on them)
-SOURCES = ["solver.cu", "obs_f64.cu", "obs_f32.cu", "setup.cpp"]
+SOURCES = ["solver.cu", "obs_f64.cu", "obs_f32.cu", "setup.cpp", "crosstab.cu"]
 DEPS = SOURCES + ["kernels.cuh", "device.cuh", "obs_launch.cuh", "coarse.cuh", "setup.hpp",
                   os.path.join("..", "..", "include", "within_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -97,6 +97,19 @@ struct DArr {
     }
 };
 
+// A dense subdomain whose reduced right-hand side is read from its eliminated side:
+// dk rows [r0, r1), kept rows at table positions [pos0, pos0 + nk).  Chosen when it has
+// at most kDenseKeepMaxRows kept rows and at least kDenseKeepMinEntries cross entries
+// (the worker-year subdomain of a panel: 20 kept rows, one entry per observation), at
+// most kDenseKeepMaxSubs per stage, the heaviest first.
+struct DkSub {
+    int64_t r0, r1;
+    int32_t pos0, nk;
+};
+constexpr int32_t kDenseKeepMaxRows = 32;
+constexpr int64_t kDenseKeepMinEntries = 1 << 16;
+constexpr int kDenseKeepMaxSubs = 8;
+
 // Row-wise CSR over local slots with its balanced work chunks.
 template <typename T>
 struct CsrDev {
@@ -159,19 +172,16 @@ struct StageHost {
     std::vector<uint32_t> gbs_cnt;
     HostVec<uint32_t> gbs_col;
     HostVec<double> gbs_val;
-    // reduced right-hand sides of the dense subdomains, from their eliminated side (when
-    // their kept rows, over the stage, number at most kDenseKeepMax): rows = eliminated
-    // slots (dk_slot: the slot, its global dof and scale invd * spou), entries = (position
-    // of the kept row among the stage's dense kept rows, C_ek); dk_keep[p] = kept slot
+    // reduced right-hand sides of the heaviest dense subdomains, from their eliminated
+    // side: rows = eliminated slots (their global dof and scale invd * spou), entries =
+    // (position of the kept row among the chosen subdomains' kept rows, C_ek);
+    // dk_keep[p] = kept slot; dk_subs: each chosen subdomain's rows and positions
     std::vector<int64_t> dk_ptr{0};
     HostVec<uint32_t> dk_gidx, dk_col;
     HostVec<double> dk_scale, dk_val;
     std::vector<uint32_t> dk_keep;
+    std::vector<DkSub> dk_subs;
 };
-
-// The dense subdomains' kept rows of a stage that the transposed reduced-rhs pass holds
-// in shared memory (per warp, kp columns): beyond this they stay in the keep CSR.
-constexpr int32_t kDenseKeepMax = 48;
 
 template <typename T>
 struct StageDev {
@@ -205,7 +215,7 @@ struct StageDev {
     DArr<uint32_t> gbs_col;
     DArr<T> gbs_val;
     int64_t dk_rows = 0;
-    int32_t dk_nkeep = 0;
+    std::vector<DkSub> dk_subs;
     DArr<int64_t> dk_ptr;
     DArr<uint32_t> dk_gidx, dk_col, dk_keep;
     DArr<T> dk_scale, dk_val;

@@ -56,7 +56,7 @@ Csr transpose(const Csr& a) {
 // gramian/cross_tab.rs:246-265; bucket accumulation :568-664).  Returns false when a
 // factor of the pair has no active level.
 bool pair_crosstab(const Design& d, int q, int r, const std::vector<std::vector<uint8_t>>& active,
-                   CrossTab& out, std::vector<uint32_t>& l2g, int32_t& nq_out) {
+                   CrossTab& out, std::vector<uint32_t>& l2g, int32_t& nq_out, int device) {
     const int64_t Lq = d.nlev[q], Lr = d.nlev[r];
     std::vector<uint32_t> qmap((size_t)Lq, UINT32_MAX), rmap((size_t)Lr, UINT32_MAX);
     int32_t nq = 0, nr = 0;
@@ -70,6 +70,39 @@ bool pair_crosstab(const Design& d, int q, int r, const std::vector<std::vector<
 
     const uint32_t* cq = d.codes.data() + (size_t)q * d.n;
     const uint32_t* cr = d.codes.data() + (size_t)r * d.n;
+    std::vector<uint64_t> seg_key;
+    std::vector<double> seg_sum;
+    if (device >= 0 && d.n >= kDeviceCrosstabMinObs &&
+        device_pair_sums(device, d.n, cq, cr, d.w.empty() ? nullptr : d.w.data(), qmap, rmap, (uint32_t)nq,
+                         (uint32_t)nr, seg_key, seg_sum)) {
+        // the device's distinct (row, column) keys in ascending order with their sums
+        std::vector<double> dq((size_t)nq, 0.0), dr((size_t)nr, 0.0);
+        for (int64_t i = 0; i < d.n; ++i) {
+            const double w = d.weight(i);
+            dq[qmap[cq[i]]] += w;
+            dr[rmap[cr[i]]] += w;
+        }
+        Csr c;
+        c.nrows = nq;
+        c.ncols = nr;
+        c.ptr.assign((size_t)nq + 1, 0);
+        c.idx.reserve(seg_key.size());
+        c.val.reserve(seg_key.size());
+        for (size_t s = 0; s < seg_key.size(); ++s) {
+            if (seg_sum[s] == 0.0) continue;  // as the host build drops exact zeros
+            const uint64_t row = seg_key[s] / (uint64_t)nr;
+            c.idx.push_back((uint32_t)(seg_key[s] % (uint64_t)nr));
+            c.val.push_back(seg_sum[s]);
+            c.ptr[row + 1]++;
+        }
+        for (int32_t j = 0; j < nq; ++j) c.ptr[j + 1] += c.ptr[j];
+        out.ct = transpose(c);
+        out.c = std::move(c);
+        out.dq = std::move(dq);
+        out.dr = std::move(dr);
+        nq_out = nq;
+        return true;
+    }
     std::vector<double> dq((size_t)nq, 0.0), dr((size_t)nr, 0.0);
     std::vector<uint32_t> bptr((size_t)nq + 1, 0);
     for (int64_t i = 0; i < d.n; ++i) {
@@ -755,7 +788,7 @@ Status build_design(const uint32_t* codes, int64_t n, int Q, int64_t row_stride,
     return st;
 }
 
-Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<Subdomain>& subs) {
+Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<Subdomain>& subs, int device) {
     subs.clear();
     std::vector<std::vector<uint8_t>> active((size_t)d.Q);
     for (int q = 0; q < d.Q; ++q) {  // find_all_active_levels (cross_tab.rs:75-89)
@@ -815,7 +848,7 @@ Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<S
         CrossTab full;
         std::vector<uint32_t> l2g;
         int32_t nqf = 0;
-        if (!pair_crosstab(d, q, r, active, full, l2g, nqf)) return;
+        if (!pair_crosstab(d, q, r, active, full, l2g, nqf, device)) return;
         std::vector<Component> comps = components(full);
         for (size_t c = 0; c < comps.size(); ++c) {
             Subdomain sd;

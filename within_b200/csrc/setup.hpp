@@ -163,7 +163,21 @@ struct Setup {
 Status build_design(const uint32_t* codes, int64_t n, int Q, int64_t row_stride, int64_t col_stride,
                     const double* weights, Design& d);
 // Builds subdomains and their local factors (build_local_domains + build_additive).
-Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<Subdomain>& subs);
+// device >= 0: the factor pairs' cross-tabulations of designs with at least
+// kDeviceCrosstabMinObs observations are summed on that CUDA device (device_pair_sums);
+// the result is identical to the host build, which is used otherwise or on any failure.
+Status build_subdomains(const Design& d, const PrecondConfig& cfg, std::vector<Subdomain>& subs, int device = -1);
+#ifndef WB_DEVICE_CROSSTAB_MIN_OBS
+#define WB_DEVICE_CROSSTAB_MIN_OBS (1 << 15)
+#endif
+constexpr int64_t kDeviceCrosstabMinObs = WB_DEVICE_CROSSTAB_MIN_OBS;
+// For the observations of a factor pair (q codes cq, r codes cr, weights w or null): the
+// distinct keys qmap[cq] * nr + rmap[cr] in ascending order, with the sum of the weights of
+// each key's observations taken in observation order (crosstab.cu).  False when the device
+// path is unavailable or failed.
+bool device_pair_sums(int device, int64_t n, const uint32_t* cq, const uint32_t* cr, const double* w,
+                      const std::vector<uint32_t>& qmap, const std::vector<uint32_t>& rmap, uint32_t nq, uint32_t nr,
+                      std::vector<uint64_t>& seg_key, std::vector<double>& seg_sum);
 // Explicit Gramian for the multiplicative residual updater.
 void build_explicit_gramian(const Design& d, std::vector<int64_t>& ptr, std::vector<uint32_t>& idx,
                             std::vector<double>& val);

@@ -297,43 +297,41 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
         st.bwd.chunks.insert(st.bwd.chunks.end(), bc.begin(), bc.end());
         st.bwd_lp.push_back((int64_t)st.bwd.chunks.size());
     }
-    // Dense subdomains (anchored dense solve, at most dense_threshold kept rows) get their
-    // reduced right-hand sides from their eliminated side when all of them together keep
-    // at most kDenseKeepMax rows: each eliminated slot reads its r row once and adds into
-    // a small shared table, instead of every kept row gathering all eliminated rows (the
-    // 20 year rows of a worker-year subdomain hold one entry per observation).
-    // The dense subdomains with the most keep-row entries are taken first (a pair's
-    // small components are dense subdomains too, with few entries each).
+    // The heaviest dense subdomains (anchored dense solve, few kept rows, many cross
+    // entries) get their reduced right-hand sides from their eliminated side: each
+    // eliminated slot reads its r row once and adds into a small table of the kept rows,
+    // instead of every kept row gathering all eliminated rows (the 20 year rows of a
+    // worker-year subdomain hold one entry per observation).
     std::vector<char> keep_by_dense(ns, 0);
     {
         std::vector<int32_t> cand;
         for (int32_t si = 0; si < ns; ++si)
-            if (subs[ids[si]].kind == 0 && kno[si + 1] > kno[si]) cand.push_back(si);
+            if (subs[ids[si]].kind == 0 && kno[si + 1] - kno[si] >= kDenseKeepMinEntries &&
+                kro[si + 1] - kro[si] <= kDenseKeepMaxRows)
+                cand.push_back(si);
         std::stable_sort(cand.begin(), cand.end(), [&](int32_t a, int32_t b) {
             return kno[a + 1] - kno[a] > kno[b + 1] - kno[b];
         });
-        int64_t nd = 0;
-        for (int32_t si : cand) {
-            const int64_t rows = kro[si + 1] - kro[si];
-            if (nd + rows > kDenseKeepMax) continue;
-            keep_by_dense[si] = 1;
-            nd += rows;
-        }
-        if (nd > 0) {
+        if ((int)cand.size() > kDenseKeepMaxSubs) cand.resize(kDenseKeepMaxSubs);
+        std::sort(cand.begin(), cand.end());
+        if (!cand.empty()) {
             // rows: (slot, keep0, first table position) of every eliminated slot of a chosen
-            // dense subdomain, in slot order; sized first, then filled in parallel
+            // subdomain, subdomain by subdomain in slot order; sized first, then filled in
+            // parallel
             struct DkRow { int64_t slot, keep0; uint32_t pos0; };
             std::vector<DkRow> rows;
-            for (int32_t si = 0; si < ns; ++si) {
+            for (int32_t si : cand) {
                 const Subdomain& sd = subs[ids[si]];
-                if (!keep_by_dense[si]) continue;
+                keep_by_dense[si] = 1;
                 const int32_t nq = sd.n_q();
                 const int64_t o = so[si];
                 const int64_t keep0 = o + (sd.elim_q ? nq : 0), elim0 = o + (sd.elim_q ? 0 : nq);
                 const int32_t n_elim = sd.elim_q ? nq : sd.n_r(), n_keep = sd.elim_q ? sd.n_r() : nq;
                 const uint32_t pos0 = (uint32_t)st.dk_keep.size();
                 for (int32_t k = 0; k < n_keep; ++k) st.dk_keep.push_back((uint32_t)(keep0 + k));
+                const int64_t r0 = (int64_t)rows.size();
                 for (int32_t e = 0; e < n_elim; ++e) rows.push_back(DkRow{elim0 + e, keep0, pos0});
+                st.dk_subs.push_back(DkSub{r0, (int64_t)rows.size(), (int32_t)pos0, n_keep});
             }
             const size_t nr = rows.size();
             st.dk_ptr.assign(nr + 1, 0);
@@ -470,7 +468,7 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
     d.gbs_col.upload(h.gbs_col);
     d.gbs_val.upload_cast(h.gbs_val);
     d.dk_rows = (int64_t)h.dk_gidx.size();
-    d.dk_nkeep = (int32_t)h.dk_keep.size();
+    d.dk_subs = h.dk_subs;
     if (d.dk_rows > 0) {
         d.dk_ptr.upload(h.dk_ptr);
         d.dk_gidx.upload(h.dk_gidx);
@@ -1000,7 +998,8 @@ void launch_dot(SolverImpl& S, const TA* a, const TB* b, int64_t rows, int kp, d
 // red[c] = sum_b part[b*kp + c] (fixed order per c; deterministic).  Each thread sums a
 // strided subset of the partials with eight independent accumulators, so that eight
 // loads are in flight at a time, and combines them in a fixed order.
-__global__ void reduce_parts_kernel(const double* __restrict__ part, int nb, int kp, double* __restrict__ red) {
+__device__ __forceinline__ void reduce_parts_body(const double* __restrict__ part, int nb, int kp,
+                                                  double* __restrict__ red) {
     __shared__ double sm[kBlock];
     const int t = threadIdx.x;
     const int J = blockDim.x / kp;
@@ -1023,6 +1022,10 @@ __global__ void reduce_parts_kernel(const double* __restrict__ part, int nb, int
         for (int j = 0; j < J; ++j) a += sm[j * kp + t];
         red[t] = a;
     }
+}
+
+__global__ void reduce_parts_kernel(const double* __restrict__ part, int nb, int kp, double* __restrict__ red) {
+    reduce_parts_body(part, nb, kp, red);
 }
 
 void launch_reduce(SolverImpl& S, const double* part, int nb, int kp, double* red) {
@@ -1170,13 +1173,21 @@ SubMeans stage_local_solve(SolverImpl& S, StageDev<T>& st, const T* r, T* v, int
                              st.nkeep, st.keep_slots.p, st.gidx.p, st.spou.p, st.rho.p, st.sub_of.p, st.sub_nloc.p, S0, r,
                              v, kp));
         launch_csr<T, EPI_ACC>(S, st.keep, 0, st.keep.nchunks, r, v, kp);
-        if (st.dk_rows > 0) {  // the dense subdomains' kept rows, from their eliminated side
-            const size_t smem = sizeof(T) * (size_t)(kBlock / 32) * st.dk_nkeep * kp;
+        for (const DkSub& ds : st.dk_subs) {  // heavy dense subdomains, from their eliminated side
+            // a table per lane group of threads x nk x 4 elements: 128 threads while that
+            // fits in 96 KB, else fewer
+            int threads = 128;
+            while (threads > 32 && dense_keep_smem<T>(threads, ds.nk, kp) > 96 * 1024) threads /= 2;
+            const size_t smem = dense_keep_smem<T>(threads, ds.nk, kp);
+            const int64_t rows = ds.r1 - ds.r0;
             WB_DISPATCH_G(G, {
                 auto kern = dense_keep_kernel<T, GV>;
                 if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                kern<<<S.n_sm * 2, kBlock, smem, S.stream>>>(st.dk_rows, st.dk_ptr.p, st.dk_gidx.p, st.dk_scale.p,
-                                                             st.dk_col.p, st.dk_val.p, st.dk_nkeep, st.dk_keep.p, r, v, kp);
+                const int64_t need = (rows * GV + threads - 1) / threads;
+                const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)S.n_sm * 4));
+                kern<<<grid, threads, smem, S.stream>>>(ds.r0, ds.r1, st.dk_ptr.p, st.dk_gidx.p, st.dk_scale.p,
+                                                        st.dk_col.p, st.dk_val.p, ds.pos0, ds.nk, st.dk_keep.p, r, v,
+                                                        kp);
             });
             WB_CUDA(cudaGetLastError());
             S.gpu_launches++;
@@ -1375,7 +1386,7 @@ __global__ void cg_rz0_kernel(KState s, const double* red, int kp) {
 // cg.rs:76-86
 // An RHS is active from the first iteration until it stops, so counting its alpha steps
 // gives the iteration number without passing it in (the iteration is graph-captured).
-__global__ void cg_alpha_kernel(KState s, const double* red, int kp) {
+__device__ void cg_alpha_step(KState s, const double* red, int kp) {
     const int c = threadIdx.x;
     if (c < kp) {
         s.alpha[c] = 0.0;
@@ -1393,7 +1404,7 @@ __global__ void cg_alpha_kernel(KState s, const double* red, int kp) {
     count_active(s, kp);
 }
 // cg.rs:94-103
-__global__ void cg_check_kernel(KState s, const double* red, int kp) {
+__device__ void cg_check_step(KState s, const double* red, int kp) {
     const int c = threadIdx.x;
     if (c < kp && s.active[c]) {
         const double rn = sqrt(red[c]);
@@ -1403,7 +1414,7 @@ __global__ void cg_check_kernel(KState s, const double* red, int kp) {
     count_active(s, kp);
 }
 // cg.rs:105-125 (EPS^2 stagnation guard)
-__global__ void cg_beta_kernel(KState s, const double* red, int kp) {
+__device__ void cg_beta_step(KState s, const double* red, int kp) {
     const int c = threadIdx.x;
     if (c < kp && s.active[c]) {
         const double rzn = red[c];
@@ -1419,6 +1430,20 @@ __global__ void cg_beta_kernel(KState s, const double* red, int kp) {
     }
     count_active(s, kp);
 }
+// The partial-sum reduction of reduce_parts_kernel followed, in the same launch, by one
+// CG scalar step on the reduced values (threads < kp of warp 0; the reduction's thread t
+// wrote red[t] itself).  Saves a launch per step.
+enum CgStep { CG_STEP_ALPHA = 0, CG_STEP_CHECK = 1, CG_STEP_BETA = 2 };
+template <int STEP>
+__global__ void reduce_step_kernel(const double* __restrict__ part, int nb, int kp, double* __restrict__ red,
+                                   KState ks) {
+    reduce_parts_body(part, nb, kp, red);
+    if (threadIdx.x >= 32) return;
+    if (STEP == CG_STEP_ALPHA) cg_alpha_step(ks, red, kp);
+    else if (STEP == CG_STEP_CHECK) cg_check_step(ks, red, kp);
+    else cg_beta_step(ks, red, kp);
+}
+
 __global__ void cg_final_kernel(KState s, int kp, int maxiter) {
     const int c = threadIdx.x;
     if (c < kp && s.active[c]) { s.active[c] = 0; s.conv[c] = 0; s.iters[c] = maxiter; }
@@ -1510,18 +1535,15 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
         launch_gram<T>(S, kp, w_t, p, ap);
         S.prof_end(kind, e0);
         launch_dot<T, T>(S, p, ap, m, kp, part, nb);
-        launch_reduce(S, part, nb, kp, red);
-        cg_alpha_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
+        reduce_step_kernel<CG_STEP_ALPHA><<<1, kBlock, 0, S.stream>>>(part, nb, kp, red, ks);
         const int grid = S.nblk(m, G, 2);
         WB_DISPATCH_G(G, cg_xr_kernel<T, GV><<<grid, kBlock, 0, S.stream>>>(x, r, p, ap, w.st_alpha.p, m, kp, part));
-        launch_reduce(S, part, grid, kp, red);
-        cg_check_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
+        reduce_step_kernel<CG_STEP_CHECK><<<1, kBlock, 0, S.stream>>>(part, grid, kp, red, ks);
         cudaEvent_t e1 = nullptr;
         S.prof_begin(e1);
         apply_precond_cg<T>(S, r, z, kp, part, nb);
         S.prof_end(kind + 2, e1);
-        launch_reduce(S, part, nb, kp, red);
-        cg_beta_kernel<<<1, 32, 0, S.stream>>>(ks, red, kp);
+        reduce_step_kernel<CG_STEP_BETA><<<1, kBlock, 0, S.stream>>>(part, nb, kp, red, ks);
         const int gridp = S.nblk(m, G);
         WB_DISPATCH_G(G, cg_p_kernel<T, GV><<<gridp, kBlock, 0, S.stream>>>(p, z, w.st_beta.p, w.st_active.p, m, kp));
         WB_CUDA(cudaGetLastError());
@@ -2966,8 +2988,10 @@ int build_solver(const uint32_t* codes, size_t n_obs, size_t n_factors, int64_t 
         return wb::fail(WITHIN_ERR_CUDA, "no CUDA device is available (the solve phase has no CPU path)");
     // the subdomains and their factors (host) are built while the design goes to the device
     std::future<wb::Status> subs_job;
+    int dev = 0;
+    WB_CUDA(cudaGetDevice(&dev));
     if (S->pc.kind != 0 && !img)
-        subs_job = std::async(std::launch::async, [&S]() { return wb::build_subdomains(S->d, S->pc, S->subs); });
+        subs_job = std::async(std::launch::async, [&S, dev]() { return wb::build_subdomains(S->d, S->pc, S->subs, dev); });
     init_device(*S);
     wb::upload_design(*S);
     if (subs_job.valid()) {
