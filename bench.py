@@ -628,6 +628,7 @@ def ours(args):
         line["secondary"] = secondary_arms(L, wb, torch, peak, peak_src)
         line["secondary"]["gmres30_multiplicative_fp64"] = gmres_cross(L, wb, torch, cats, Y, w, D_gpu)
         line["secondary"]["shuffled_rows"] = shuffled_arm(L, wb, torch, cats, Y, w, args)
+        line["secondary"]["config5_coarse_space"] = coarse_arm(L, wb, torch)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -653,6 +654,48 @@ def gmres_cross(L, wb, torch, cats, Y, w, D_ref):
             "converged": bool(st[0].converged), "iterations": int(st[0].iterations),
             "final_residual": float(st[0].final_residual),
             "rel_diff_demeaned_vs_headline": rel(D, D_ref[:, 0])}
+
+
+def coarse_arm(L, wb, torch):
+    """Config 5's evaluation: a held-out 5M-observation worker-firm panel (500k workers x 10
+    years, 50k firms, switch probability 0.02), 8 N(0,1) RHS, mixed precision, tol 1e-8:
+    plain additive Schwarz, the shipped network's coarse space (and what the judge keeps),
+    and an exact basis of 32 Ritz vectors of the same design (40 Lanczos steps), with
+    iterations and device time per solve."""
+    from within_b200 import coarse, synthetic
+    cats = synthetic.worker_firm_year(500_000, 50_000, 10, 20, 0.02, seed=4242)
+    n, k = cats.shape[0], 8
+    Y = np.asfortranarray(np.random.default_rng(7).standard_normal((n, k)))
+    s = wb.Solver(cats, wb.CG(precision="mixed"))
+    m = s.n_dofs
+    dY = torch.from_numpy(np.ascontiguousarray(Y.T)).cuda()
+    dX = torch.empty((k, m), dtype=torch.float64, device="cuda")
+    dD = torch.empty((k, n), dtype=torch.float64, device="cuda")
+    st = (wb._lib.Stats * k)()
+
+    def measure():
+        ms = device_solve(L, s._h, dY, k, dX, dD, st, steps=3, warmup=2)
+        return {"ms_per_step": ms, "value": k / (ms / 1000.0), "unit": "RHS/s",
+                "iterations": [int(st[c].iterations) for c in range(k)],
+                "max_final_residual": max(float(st[c].final_residual) for c in range(k)),
+                "converged": all(bool(st[c].converged) for c in range(k))}
+
+    out = {"n_obs": n, "n_rhs": k, "plain": measure()}
+    if os.path.exists(coarse.WEIGHTS):
+        net = coarse.CoarseNet.trained()
+        t0 = time.perf_counter()
+        s.set_coarse_space(net)
+        out["learned"] = dict(measure(), setup_s=time.perf_counter() - t0)
+        verdict = coarse.install_judged(s, net)
+        out["learned"]["judge_kept"] = verdict["kept"]
+        s.clear_coarse_space()
+    d = coarse.level_diagonal(cats, None)
+    t0 = time.perf_counter()
+    V, lam = coarse.ritz_targets(s, d, steps=40, nev=32)
+    s.set_coarse_space(V / np.sqrt(np.where(d > 0, d, 1.0))[:, None])
+    out["exact_ritz"] = dict(measure(), setup_s=time.perf_counter() - t0,
+                             lowest_ritz_values=[float(v) for v in lam[:4]])
+    return out
 
 
 def shuffled_arm(L, wb, torch, cats, Y, w, args):

@@ -152,26 +152,35 @@ __global__ void seg_start_kernel(const uint64_t* __restrict__ keys, int64_t n, c
     if (i < n && (i == 0 || keys[i] != keys[i - 1])) start[pos[i]] = (uint32_t)i;
 }
 
+// ws[e] = w[idx[e]]: the weights in sorted order, contiguous.
+__global__ void gather_weights_kernel(int64_t n, const uint32_t* __restrict__ idx, const double* __restrict__ w,
+                                      double* __restrict__ ws) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) ws[e] = w[idx[e]];
+}
+
 // One thread per segment: the key and the sum of its weights in sorted (= observation)
-// order; w null = unit weights.
-__global__ void seg_sum_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ idx,
-                               const double* __restrict__ w, const uint32_t* __restrict__ start, int64_t nseg,
-                               int64_t n, uint64_t* __restrict__ skey, double* __restrict__ ssum) {
+// order; ws null = unit weights.
+__global__ void seg_sum_kernel(const uint64_t* __restrict__ keys, const double* __restrict__ ws,
+                               const uint32_t* __restrict__ start, int64_t nseg, int64_t n,
+                               uint64_t* __restrict__ skey, double* __restrict__ ssum) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nseg) return;
     const int64_t a = start[s], b = s + 1 < nseg ? (int64_t)start[s + 1] : n;
     double sum = 0.0;
     int64_t e = a;
-    if (w) {  // eight loads in flight, the additions still one after another in order
-        for (; e + 8 <= b; e += 8) {
-            double v[8];
+    if (ws) {  // sixteen loads in flight, the additions still one after another in order
+        for (; e + 16 <= b; e += 16) {
+            double v[16];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = w[idx[e + u]];
+            for (int u = 0; u < 16; ++u) v[u] = ws[e + u];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) sum += v[u];
+            for (int u = 0; u < 16; ++u) sum += v[u];
         }
+        for (; e < b; ++e) sum += ws[e];
+    } else {
+        sum = (double)(b - a);  // unit weights: an exact count
     }
-    for (; e < b; ++e) sum += w ? w[idx[e]] : 1.0;
     skey[s] = keys[a];
     ssum[s] = sum;
 }
@@ -187,13 +196,19 @@ bool scan_u32(uint32_t* a, int64_t n, uint32_t* tot, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess;
 }
 
+// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync): no device-wide
+// synchronisation with the other setup threads' work.
 template <typename T>
 struct Buf {
     T* p = nullptr;
+    cudaStream_t st = nullptr;
     ~Buf() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, st);
     }
-    bool alloc(size_t n) { return cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) == cudaSuccess; }
+    bool alloc(size_t n, cudaStream_t s) {
+        st = s;
+        return cudaMallocAsync((void**)&p, std::max<size_t>(n, 1) * sizeof(T), s) == cudaSuccess;
+    }
 };
 
 }  // namespace
@@ -209,11 +224,13 @@ bool device_pair_sums(int device, int64_t n, const uint32_t* cq, const uint32_t*
     {
         Buf<uint32_t> dcq, dcr, dqm, drm, i0, i1, hist, flag, start, tot;
         Buf<uint64_t> k0, k1, skey;
-        Buf<double> dw, ssum;
+        Buf<double> dw, dws, ssum;
         const int nb = blocks_for(n, kSortTile);
-        ok = dcq.alloc(n) && dcr.alloc(n) && dqm.alloc(qmap.size()) && drm.alloc(rmap.size()) && i0.alloc(n) &&
-             i1.alloc(n) && k0.alloc(n) && k1.alloc(n) && hist.alloc((size_t)256 * nb) && flag.alloc(n) &&
-             start.alloc(n) && tot.alloc(blocks_for(n, kSortTile) + 1) && (!w || dw.alloc(n));
+        ok = dcq.alloc(n, st) && dcr.alloc(n, st) && dqm.alloc(qmap.size(), st) && drm.alloc(rmap.size(), st) &&
+             i0.alloc(n, st) && i1.alloc(n, st) && k0.alloc(n, st) && k1.alloc(n, st) &&
+             hist.alloc((size_t)256 * nb, st) && flag.alloc(n, st) && start.alloc(n, st) &&
+             tot.alloc(blocks_for(std::max<int64_t>(n, (int64_t)256 * nb), kSortTile) + 1, st) &&
+             (!w || (dw.alloc(n, st) && dws.alloc(n, st)));
         ok = ok && cudaMemcpyAsync(dcq.p, cq, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st) == cudaSuccess &&
              cudaMemcpyAsync(dcr.p, cr, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st) == cudaSuccess &&
              cudaMemcpyAsync(dqm.p, qmap.data(), sizeof(uint32_t) * qmap.size(), cudaMemcpyHostToDevice, st) ==
@@ -231,7 +248,7 @@ bool device_pair_sums(int device, int64_t n, const uint32_t* cq, const uint32_t*
             uint32_t *iin = i0.p, *iout = i1.p;
             for (int shift = 0; shift < bits && ok; shift += 8) {
                 radix_hist_kernel<<<nb, kSortThreads, 0, st>>>(kin, n, shift, hist.p, nb);
-                scan_block_kernel<<<1, kScanThreads, 0, st>>>(hist.p, (int64_t)256 * nb);
+                ok = scan_u32(hist.p, (int64_t)256 * nb, tot.p, st);
                 radix_scatter_kernel<<<nb, kSortThreads, 0, st>>>(kin, iin, n, shift, hist.p, nb, kout, iout);
                 ok = cudaGetLastError() == cudaSuccess;
                 std::swap(kin, kout);
@@ -247,10 +264,11 @@ bool device_pair_sums(int device, int64_t n, const uint32_t* cq, const uint32_t*
                            cudaSuccess;
             ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
             const int64_t nseg = ok ? (int64_t)last_pos + last_flag : 0;
-            ok = ok && nseg > 0 && skey.alloc(nseg) && ssum.alloc(nseg);
+            ok = ok && nseg > 0 && skey.alloc(nseg, st) && ssum.alloc(nseg, st);
             if (ok) {
                 seg_start_kernel<<<blocks_for(n, 256), 256, 0, st>>>(kin, n, flag.p, start.p);
-                seg_sum_kernel<<<blocks_for(nseg, 256), 256, 0, st>>>(kin, iin, w ? dw.p : nullptr, start.p, nseg, n,
+                if (w) gather_weights_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, iin, dw.p, dws.p);
+                seg_sum_kernel<<<blocks_for(nseg, 256), 256, 0, st>>>(kin, w ? dws.p : nullptr, start.p, nseg, n,
                                                                       skey.p, ssum.p);
                 seg_key.resize((size_t)nseg);
                 seg_sum.resize((size_t)nseg);
@@ -263,6 +281,7 @@ bool device_pair_sums(int device, int64_t n, const uint32_t* cq, const uint32_t*
             }
         }
     }
+    cudaStreamSynchronize(st);  // the buffers' stream-ordered frees
     cudaStreamDestroy(st);
     if (!ok) cudaGetLastError();  // clear a non-sticky error; the host path takes over
     return ok;

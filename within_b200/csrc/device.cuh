@@ -97,19 +97,6 @@ struct DArr {
     }
 };
 
-// A dense subdomain whose reduced right-hand side is read from its eliminated side:
-// dk rows [r0, r1), kept rows at table positions [pos0, pos0 + nk).  Chosen when it has
-// at most kDenseKeepMaxRows kept rows and at least kDenseKeepMinEntries cross entries
-// (the worker-year subdomain of a panel: 20 kept rows, one entry per observation), at
-// most kDenseKeepMaxSubs per stage, the heaviest first.
-struct DkSub {
-    int64_t r0, r1;
-    int32_t pos0, nk;
-};
-constexpr int32_t kDenseKeepMaxRows = 32;
-constexpr int64_t kDenseKeepMinEntries = 1 << 16;
-constexpr int kDenseKeepMaxSubs = 8;
-
 // Row-wise CSR over local slots with its balanced work chunks.
 template <typename T>
 struct CsrDev {
@@ -172,15 +159,6 @@ struct StageHost {
     std::vector<uint32_t> gbs_cnt;
     HostVec<uint32_t> gbs_col;
     HostVec<double> gbs_val;
-    // reduced right-hand sides of the heaviest dense subdomains, from their eliminated
-    // side: rows = eliminated slots (their global dof and scale invd * spou), entries =
-    // (position of the kept row among the chosen subdomains' kept rows, C_ek);
-    // dk_keep[p] = kept slot; dk_subs: each chosen subdomain's rows and positions
-    std::vector<int64_t> dk_ptr{0};
-    HostVec<uint32_t> dk_gidx, dk_col;
-    HostVec<double> dk_scale, dk_val;
-    std::vector<uint32_t> dk_keep;
-    std::vector<DkSub> dk_subs;
 };
 
 template <typename T>
@@ -214,11 +192,6 @@ struct StageDev {
     DArr<uint32_t> gbs_cnt;
     DArr<uint32_t> gbs_col;
     DArr<T> gbs_val;
-    int64_t dk_rows = 0;
-    std::vector<DkSub> dk_subs;
-    DArr<int64_t> dk_ptr;
-    DArr<uint32_t> dk_gidx, dk_col, dk_keep;
-    DArr<T> dk_scale, dk_val;
 };
 
 constexpr int kCoreRowsPerBlock = 2;  // output rows per block of core_gemv_kernel (4 warps each)

@@ -30,34 +30,8 @@ struct V4 {
     __device__ __forceinline__ V4& operator*=(T s) { a *= s; b *= s; c *= s; d *= s; return *this; }
     __device__ __forceinline__ bool any() const { return a != T(0) || b != T(0) || c != T(0) || d != T(0); }
 };
-#ifdef WB_PACKED_F32
-// FP32 pairs on sm_100's packed FP32x2 add and multiply (two lanes per instruction;
-// each lane rounds as the scalar operation does)
-template <>
-__device__ __forceinline__ V4<float>& V4<float>::operator+=(const V4<float>& o) {
-    const float2 x = __fadd2_rn(make_float2(a, b), make_float2(o.a, o.b));
-    const float2 y = __fadd2_rn(make_float2(c, d), make_float2(o.c, o.d));
-    a = x.x; b = x.y; c = y.x; d = y.y;
-    return *this;
-}
-template <>
-__device__ __forceinline__ V4<float>& V4<float>::operator-=(const V4<float>& o) {
-    const float2 x = __fadd2_rn(make_float2(a, b), make_float2(-o.a, -o.b));
-    const float2 y = __fadd2_rn(make_float2(c, d), make_float2(-o.c, -o.d));
-    a = x.x; b = x.y; c = y.x; d = y.y;
-    return *this;
-}
-#endif
 template <typename T>
 __device__ __forceinline__ V4<T> operator*(T s, const V4<T>& v) { return V4<T>(s * v.a, s * v.b, s * v.c, s * v.d); }
-#ifdef WB_PACKED_F32
-template <>
-__device__ __forceinline__ V4<float> operator*(float s, const V4<float>& v) {
-    const float2 x = __fmul2_rn(make_float2(s, s), make_float2(v.a, v.b));
-    const float2 y = __fmul2_rn(make_float2(s, s), make_float2(v.c, v.d));
-    return V4<float>(x.x, x.y, y.x, y.y);
-}
-#endif
 template <typename T>
 __device__ __forceinline__ V4<T> operator+(V4<T> x, const V4<T>& y) { x += y; return x; }
 template <typename T>
@@ -947,65 +921,6 @@ __global__ void __launch_bounds__(kBlock) keep_init_kernel(int64_t nkeep, const 
         const V4<double> m0 = inv_n * V4<double>(S0[o], S0[o + 1], S0[o + 2], S0[o + 3]);
         const V4<double> u = (double)spou[l] * to_d(ld4(r + (size_t)gidx[l] * kp + c4));
         st4(v + (size_t)l * kp + c4, from_d<T>(u - m0 - (double)rho[a] * m0));
-    }
-}
-
-// Reduced right-hand sides of one heavy dense subdomain, from its eliminated side: for
-// every eliminated slot e (dk rows [r0, r1)) and each entry (p, C_ek) of its row,
-// v[keep_slot[p]] += C_ek * scale_e * r[gidx_e] with scale_e = invd_e * spou_e.  This is
-// the keep CSR's product for the subdomain's nk kept rows, read by eliminated slot, so
-// each slot's r row is loaded once.  Each lane group adds into a table of its own in
-// shared memory (plain loads and stores, no atomics; the groups' tables are padded apart
-// so that the groups of a warp fall in different banks); the block then sums its
-// groups' tables and adds the result into v.
-inline int dense_keep_stride(int nk, int kp) { return nk * kp + 4; }
-template <typename T>
-inline size_t dense_keep_smem(int threads, int nk, int kp) {
-    return sizeof(T) * (size_t)(threads / (kp / 4)) * dense_keep_stride(nk, kp);
-}
-template <typename T, int G>
-__global__ void dense_keep_kernel(int64_t r0, int64_t r1, const int64_t* __restrict__ ptr,
-                                  const uint32_t* __restrict__ gidx, const T* __restrict__ scale,
-                                  const uint32_t* __restrict__ col, const T* __restrict__ val, int pos0, int nk,
-                                  const uint32_t* __restrict__ keep_slot, const T* __restrict__ r, T* __restrict__ v,
-                                  int kp) {
-    extern __shared__ __align__(16) unsigned char dk_smem[];
-    T* tab = reinterpret_cast<T*>(dk_smem);
-    const int stride = nk * kp + 4;
-    const int gpb = blockDim.x / G;
-    for (int i = threadIdx.x; i < gpb * stride; i += blockDim.x) tab[i] = T(0);
-    __syncthreads();
-    const int g = threadIdx.x / G;
-    const int c4 = (threadIdx.x & (G - 1)) * 4;
-    T* mytab = tab + (size_t)g * stride + c4;
-    for (int64_t i = r0 + (int64_t)blockIdx.x * gpb + g; i < r1; i += (int64_t)gridDim.x * gpb) {
-        const V4<T> t = scale[i] * ld4(r + (size_t)gidx[i] * kp + c4);
-        const int64_t e1 = ptr[i + 1];
-        int64_t e = ptr[i];
-        // the entries' columns and values come four at a time, so that their loads are in
-        // flight together ahead of the table updates (col in [pos0, pos0 + nk))
-        for (; e + 4 <= e1; e += 4) {
-            const uint32_t j0 = __ldg(col + e), j1 = __ldg(col + e + 1), j2 = __ldg(col + e + 2), j3 = __ldg(col + e + 3);
-            const T v0 = __ldg(val + e), v1 = __ldg(val + e + 1), v2 = __ldg(val + e + 2), v3 = __ldg(val + e + 3);
-            T* q0 = mytab + (size_t)(j0 - (uint32_t)pos0) * kp;
-            st4(q0, ld4(q0) + v0 * t);
-            T* q1 = mytab + (size_t)(j1 - (uint32_t)pos0) * kp;
-            st4(q1, ld4(q1) + v1 * t);
-            T* q2 = mytab + (size_t)(j2 - (uint32_t)pos0) * kp;
-            st4(q2, ld4(q2) + v2 * t);
-            T* q3 = mytab + (size_t)(j3 - (uint32_t)pos0) * kp;
-            st4(q3, ld4(q3) + v3 * t);
-        }
-        for (; e < e1; ++e) {
-            T* q = mytab + (size_t)(__ldg(col + e) - (uint32_t)pos0) * kp;
-            st4(q, ld4(q) + __ldg(val + e) * t);
-        }
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nk * kp; i += blockDim.x) {
-        T sum = T(0);
-        for (int h = 0; h < gpb; ++h) sum += tab[(size_t)h * stride + i];
-        if (sum != T(0)) atomicAdd(v + (size_t)keep_slot[pos0 + i / kp] * kp + i % kp, sum);
     }
 }
 

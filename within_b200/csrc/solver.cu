@@ -297,72 +297,8 @@ StageHost build_stage(const std::vector<Subdomain>& subs, const std::vector<int3
         st.bwd.chunks.insert(st.bwd.chunks.end(), bc.begin(), bc.end());
         st.bwd_lp.push_back((int64_t)st.bwd.chunks.size());
     }
-    // The heaviest dense subdomains (anchored dense solve, few kept rows, many cross
-    // entries) get their reduced right-hand sides from their eliminated side: each
-    // eliminated slot reads its r row once and adds into a small table of the kept rows,
-    // instead of every kept row gathering all eliminated rows (the 20 year rows of a
-    // worker-year subdomain hold one entry per observation).
-    std::vector<char> keep_by_dense(ns, 0);
-    {
-        std::vector<int32_t> cand;
-        for (int32_t si = 0; si < ns; ++si)
-            if (subs[ids[si]].kind == 0 && kno[si + 1] - kno[si] >= kDenseKeepMinEntries &&
-                kro[si + 1] - kro[si] <= kDenseKeepMaxRows)
-                cand.push_back(si);
-        std::stable_sort(cand.begin(), cand.end(), [&](int32_t a, int32_t b) {
-            return kno[a + 1] - kno[a] > kno[b + 1] - kno[b];
-        });
-        if ((int)cand.size() > kDenseKeepMaxSubs) cand.resize(kDenseKeepMaxSubs);
-        std::sort(cand.begin(), cand.end());
-        if (!cand.empty()) {
-            // rows: (slot, keep0, first table position) of every eliminated slot of a chosen
-            // subdomain, subdomain by subdomain in slot order; sized first, then filled in
-            // parallel
-            struct DkRow { int64_t slot, keep0; uint32_t pos0; };
-            std::vector<DkRow> rows;
-            for (int32_t si : cand) {
-                const Subdomain& sd = subs[ids[si]];
-                keep_by_dense[si] = 1;
-                const int32_t nq = sd.n_q();
-                const int64_t o = so[si];
-                const int64_t keep0 = o + (sd.elim_q ? nq : 0), elim0 = o + (sd.elim_q ? 0 : nq);
-                const int32_t n_elim = sd.elim_q ? nq : sd.n_r(), n_keep = sd.elim_q ? sd.n_r() : nq;
-                const uint32_t pos0 = (uint32_t)st.dk_keep.size();
-                for (int32_t k = 0; k < n_keep; ++k) st.dk_keep.push_back((uint32_t)(keep0 + k));
-                const int64_t r0 = (int64_t)rows.size();
-                for (int32_t e = 0; e < n_elim; ++e) rows.push_back(DkRow{elim0 + e, keep0, pos0});
-                st.dk_subs.push_back(DkSub{r0, (int64_t)rows.size(), (int32_t)pos0, n_keep});
-            }
-            const size_t nr = rows.size();
-            st.dk_ptr.assign(nr + 1, 0);
-            for (size_t i = 0; i < nr; ++i)
-                st.dk_ptr[i + 1] = st.dk_ptr[i] + (st.bs_ptr[rows[i].slot + 1] - st.bs_ptr[rows[i].slot]);
-            st.dk_gidx.resize(nr);
-            st.dk_scale.resize(nr);
-            st.dk_col.resize((size_t)st.dk_ptr[nr]);
-            st.dk_val.resize((size_t)st.dk_ptr[nr]);
-            constexpr size_t kRowsPerTask = 1 << 16;
-            parallel_tasks((nr + kRowsPerTask - 1) / kRowsPerTask, [&](size_t t) {
-                for (size_t i = t * kRowsPerTask; i < std::min(nr, (t + 1) * kRowsPerTask); ++i) {
-                    const int64_t l = rows[i].slot;
-                    st.dk_gidx[i] = st.gidx[l];
-                    st.dk_scale[i] = st.invd[l] * st.spou[l];
-                    int64_t d = st.dk_ptr[i];
-                    for (int64_t x = st.bs_ptr[l]; x < st.bs_ptr[l + 1]; ++x, ++d) {
-                        st.dk_col[d] = rows[i].pos0 + (uint32_t)(st.bs_col[x] - rows[i].keep0);
-                        st.dk_val[d] = st.bs_val[x];
-                    }
-                }
-            });
-        }
-    }
-    // one warp per chunk (csr_rows_kernel): single rows, long rows in pieces of 256; the
-    // kept rows of subdomains handled above are left out
-    for (int32_t si = 0; si < ns; ++si) {
-        if (keep_by_dense[si]) continue;
-        auto kc = make_chunks(st.keep.ptr, kro[si], kro[si + 1], 256, 1, true);
-        st.keep.chunks.insert(st.keep.chunks.end(), kc.begin(), kc.end());
-    }
+    // one warp per chunk (csr_rows_kernel): single rows, long rows in pieces of 256
+    st.keep.chunks = make_chunks(st.keep.ptr, 0, st.keep.nrows(), 256, 1, true);
     if (with_gather) {
         st.gptr.assign((size_t)ndofs + 1, 0);
         for (uint32_t g : st.gidx) st.gptr[g + 1]++;
@@ -467,16 +403,6 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
     d.gbs_cnt.upload(h.gbs_cnt);
     d.gbs_col.upload(h.gbs_col);
     d.gbs_val.upload_cast(h.gbs_val);
-    d.dk_rows = (int64_t)h.dk_gidx.size();
-    d.dk_subs = h.dk_subs;
-    if (d.dk_rows > 0) {
-        d.dk_ptr.upload(h.dk_ptr);
-        d.dk_gidx.upload(h.dk_gidx);
-        d.dk_col.upload(h.dk_col);
-        d.dk_keep.upload(h.dk_keep);
-        d.dk_scale.upload_cast(h.dk_scale);
-        d.dk_val.upload_cast(h.dk_val);
-    }
 }
 
 }  // namespace
@@ -484,6 +410,8 @@ void upload_stage(StageDev<T>& d, const StageHost& h) {
 // ---------------------------------------------------------------------------
 // Solver
 // ---------------------------------------------------------------------------
+
+
 
 struct Workspace {
     int kp = 0;
@@ -1173,25 +1101,6 @@ SubMeans stage_local_solve(SolverImpl& S, StageDev<T>& st, const T* r, T* v, int
                              st.nkeep, st.keep_slots.p, st.gidx.p, st.spou.p, st.rho.p, st.sub_of.p, st.sub_nloc.p, S0, r,
                              v, kp));
         launch_csr<T, EPI_ACC>(S, st.keep, 0, st.keep.nchunks, r, v, kp);
-        for (const DkSub& ds : st.dk_subs) {  // heavy dense subdomains, from their eliminated side
-            // a table per lane group of threads x nk x 4 elements: 128 threads while that
-            // fits in 96 KB, else fewer
-            int threads = 128;
-            while (threads > 32 && dense_keep_smem<T>(threads, ds.nk, kp) > 96 * 1024) threads /= 2;
-            const size_t smem = dense_keep_smem<T>(threads, ds.nk, kp);
-            const int64_t rows = ds.r1 - ds.r0;
-            WB_DISPATCH_G(G, {
-                auto kern = dense_keep_kernel<T, GV>;
-                if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                const int64_t need = (rows * GV + threads - 1) / threads;
-                const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)S.n_sm * 4));
-                kern<<<grid, threads, smem, S.stream>>>(ds.r0, ds.r1, st.dk_ptr.p, st.dk_gidx.p, st.dk_scale.p,
-                                                        st.dk_col.p, st.dk_val.p, ds.pos0, ds.nk, st.dk_keep.p, r, v,
-                                                        kp);
-            });
-            WB_CUDA(cudaGetLastError());
-            S.gpu_launches++;
-        }
         const int gs = (int)std::max<int64_t>(1, (st.nkeep + kSpb - 1) / kSpb);
         WB_DISPATCH_G(G, keep_sum_kernel<T, GV><<<gs, kBlock, 0, S.stream>>>(st.nkeep, kSpb, st.keep_slots.p, st.rho.p, 0,
                                                                               st.sub_of.p, v, kp, M1));
