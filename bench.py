@@ -32,11 +32,16 @@ METRIC = "RHS solved/sec at tol 1e-8, 10M obs 3 FE; speedup vs plain FP64 GPU PC
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the operator
 # apply on the headline workload, from ncu captures of one launch (the figure and its
-# command are in profiles/); these are not measured by the bench run itself
-TRAFFIC = {"fp32": (230_120_000, "ncu dram__bytes_read+write of one launch at 5M observations (115.06 MB), x2 for "
+# command are in profiles/), per precision and hot-table variant (within_solver_obs_hot_global);
+# these are not measured by the bench run itself
+TRAFFIC = {("fp32", 0): (230_120_000, "ncu dram__bytes_read+write of one launch at 5M observations (115.06 MB), x2 for "
                                   "10M (profiles/obs_pass_dram_traffic_5Mobs_16rhs.md); not measured by this run"),
-           "fp64": (342_480_000, "ncu dram__bytes_read+write of one launch at 5M observations (171.24 MB), x2 for "
-                                  "10M (profiles/obs_pass_dram_traffic_5Mobs_16rhs.md); not measured by this run")}
+           ("fp64", 0): (342_480_000, "ncu dram__bytes_read+write of one launch at 5M observations (171.24 MB), x2 for "
+                                  "10M (profiles/obs_pass_dram_traffic_5Mobs_16rhs.md); not measured by this run"),
+           ("fp32", 1): (230_400_000, "ncu dram__bytes_read+write of one launch at 5M observations (115.2 MB), x2 for "
+                                       "10M (profiles/obs_pass_dram_traffic_5Mobs_16rhs.md); not measured by this run"),
+           ("fp64", 1): (369_000_000, "ncu dram__bytes_read+write of one launch at 5M observations (184.5 MB), x2 for "
+                                       "10M (profiles/obs_pass_dram_traffic_5Mobs_16rhs.md); not measured by this run")}
 
 
 def parse():
@@ -276,6 +281,16 @@ def profile_step(L, solver, step):
         kt[which] = (cnt.value, ms.value)
     L.within_solver_set_profiling(solver._h, 0)
     return kt
+
+
+def obs_kernel_name(L, solver, k, elem):
+    """The operator-apply kernel with the shape the solver's autotuner chose for k RHS."""
+    per, bps = C.c_int32(), C.c_int32()
+    L.within_solver_obs_config(solver._h, k, elem, C.byref(per), C.byref(bps))
+    hot = L.within_solver_obs_hot_global(solver._h, k, elem)
+    return "obs_pass_kernel (operator apply D'W(D x), %s; %d observations per chunk, %d blocks per SM, " \
+           "hot-level tables in %s)" % ("FP32" if elem == 4 else "FP64", per.value, bps.value,
+                                       "per-block global copies" if hot == 1 else "shared memory")
 
 
 def op_roofline(kt, which, op_bytes, peak, peak_src, kernel):
@@ -537,8 +552,7 @@ def ours(args):
 
     which = 1 if (args.precision == "mixed" and args.krylov == "cg") else 0
     s_b = 4 if which == 1 else 8
-    roofline = op_roofline(kt, which, obs_bytes(s_b), peak, peak_src,
-                           "obs_pass_kernel (operator apply D'W(D x), %s)" % ("FP32" if which else "FP64"))
+    roofline = op_roofline(kt, which, obs_bytes(s_b), peak, peak_src, obs_kernel_name(L, solver, k, s_b))
     roofline["traffic"] = None
     sch_bytes = int(L.within_solver_schwarz_bytes(solver._h, kp, s_b))
     scnt, sms = kt[which + 2]
@@ -565,7 +579,7 @@ def ours(args):
     elif abs(args.scale - 1.0) < 1e-9 and not args.shuffle and args.krylov == "cg":
         # DRAM bytes (dram__bytes_read.sum + write.sum) of one launch of this kernel on this
         # workload, from an ncu capture (not measured by this run)
-        tr = TRAFFIC.get("fp32" if which == 1 else "fp64")
+        tr = TRAFFIC.get(("fp32" if which == 1 else "fp64", L.within_solver_obs_hot_global(solver._h, k, s_b)))
         if tr:
             roofline["traffic"] = tr[0]
             roofline["traffic_source"] = tr[1]
@@ -599,14 +613,15 @@ def ours(args):
                                                             st, None))
 
         kt64 = profile_step(L, d64, d64_step)
-        rf64 = op_roofline(kt64, 0, obs_bytes(8), peak, peak_src, "obs_pass_kernel (operator apply D'W(D x), FP64)")
+        rf64 = op_roofline(kt64, 0, obs_bytes(8), peak, peak_src, obs_kernel_name(L, d64, k, 8))
         s64 = int(L.within_solver_schwarz_bytes(d64._h, kp, 8))
         c64, m64 = kt64[2]
         rf64["schwarz_apply"] = {"algorithmic_bytes_per_apply": s64, "avg_us": 1000.0 * m64 / c64 if c64 else None,
                                  "achieved": s64 / (m64 / c64 / 1000.0) / 1e9 if c64 else None, "unit": "GB/s",
                                  "frac": s64 / (m64 / c64 / 1000.0) / 1e9 / peak if c64 else None}
-        if abs(args.scale - 1.0) < 1e-9 and not args.shuffle and "fp64" in TRAFFIC:
-            rf64["traffic"], rf64["traffic_source"] = TRAFFIC["fp64"]
+        tr64 = TRAFFIC.get(("fp64", L.within_solver_obs_hot_global(d64._h, k, 8)))
+        if abs(args.scale - 1.0) < 1e-9 and not args.shuffle and tr64:
+            rf64["traffic"], rf64["traffic_source"] = tr64
         line["fp64_dropin"] = {"value": world * k / (d_ms / 1000.0), "unit": "RHS/s", "ms_per_step": d_ms,
                                "converged": all(bool(st[c].converged) for c in range(k)),
                                "max_final_residual": max(float(st[c].final_residual) for c in range(k)),

@@ -294,6 +294,27 @@ int within_solver_release_coarse_training(within_solver *solver);
 int within_solver_obs_config(const within_solver *solver, int32_t k, int32_t elem_bytes, int32_t *obs_per_chunk,
                              int32_t *blocks_per_sm);
 
+/* Where the observation pass for k RHS in elem_bytes precision adds the run sums of a
+ * factor's most frequent levels: 0 in a table in each block's shared memory, 1 in a
+ * per-block copy in global memory (16-byte vector reductions in L2), -1 not tuned yet.
+ * The autotuner tries both for designs that have such levels.  No counterpart in the
+ * reference. */
+int32_t within_solver_obs_hot_global(const within_solver *solver, int32_t k, int32_t elem_bytes);
+
+/* The autotuner's measured time (milliseconds per operator apply, the best of two
+ * sweeps over the candidates) of each candidate shape for k RHS in elem_bytes precision:
+ * ms[c] for c < n and c < 12, where c = hot_global * 6 + 2 * log2(obs_per_chunk / 16) +
+ * blocks_per_sm - 1; 0 for candidates not timed (a shape class tuned earlier in the
+ * process, or no hot levels).  A measurement hook with no counterpart in the reference. */
+int within_solver_obs_tune_times(const within_solver *solver, int32_t k, int32_t elem_bytes, float *ms, int32_t n);
+
+/* Fixes the observation pass's shape for k RHS in elem_bytes precision instead of
+ * autotuning it: obs_per_chunk 16, 32 or 64, blocks_per_sm 1 or 2, hot_global 0 or 1 (see
+ * within_solver_obs_hot_global; 1 allocates the per-block copies here).  For
+ * reproducible timing and for testing each variant.  No counterpart in the reference. */
+int within_solver_set_obs_config(within_solver *solver, int32_t k, int32_t elem_bytes, int32_t obs_per_chunk,
+                                 int32_t blocks_per_sm, int32_t hot_global);
+
 /* Algorithmic bytes of one Schwarz apply over k RHS with elem_bytes (4 or 8) per vector
  * element, counted from the built subdomains: per subdomain 2 (4+s) nnz(C_i) for the
  * cross block read twice (reduced right-hand side and back substitution), 12 n_i for the

@@ -35,6 +35,16 @@ def test_autotuned_shape_is_a_candidate_and_shared(precision):
     s2 = wb.Solver(cats2, wb.CG(precision=precision), weights=w2)
     s2.solve_batch(np.asfortranarray(Y2))
     assert _config(s2, 9, elem) == (0, per, bps)
+    # the same variant of the hot tables runs in both (the second allocates its own copies)
+    L = _lib.load()
+    assert L.within_solver_obs_hot_global(s._h, 9, elem) in (0, 1)
+    assert L.within_solver_obs_hot_global(s2._h, 9, elem) == L.within_solver_obs_hot_global(s._h, 9, elem)
+    # the tuner's table: every shared-memory candidate timed by the first solver, none by
+    # the second (it reused the choice)
+    t1, t2 = (C.c_float * 12)(), (C.c_float * 12)()
+    assert L.within_solver_obs_tune_times(s._h, 9, elem, t1, 12) == 0
+    assert L.within_solver_obs_tune_times(s2._h, 9, elem, t2, 12) == 0
+    assert all(t1[c] > 0 for c in range(6)) and all(t2[c] == 0 for c in range(12))
     # the operator apply under the tuned shape (FP64 solvers tune their FP64 pass)
     if precision == "fp64":
         o = oracle.OracleSolver(cats, w)

@@ -141,6 +141,13 @@ struct ObsParams {
     // ((block * warps + warp) * kp + rhs)
     const double* lsmr_scale;
     double* lsmr_part;
+    // SINK_HOT tables in global memory instead of shared memory when non-null: block b's
+    // copy starts at hot_glob + b * hot_glob_stride elements, factor q's table at
+    // hot_goff[q] within it (hot_cap[q] x kp); the block zeroes its copy first and adds it
+    // into `out` at the end
+    void* hot_glob;
+    int64_t hot_glob_stride;
+    int32_t hot_goff[kMaxQ];
 };
 
 template <typename T> struct W4;
@@ -202,8 +209,12 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
     static_assert(kGeneric || NP < QT, "the primary slot is never private");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sm = reinterpret_cast<T*>(smem_raw);
+    T* const hotg = (kScatter && P.hot_glob) ? reinterpret_cast<T*>(P.hot_glob) + (size_t)blockIdx.x * P.hot_glob_stride
+                                             : nullptr;
     if (kScatter) {
         for (int i = threadIdx.x; i < P.smem_elems; i += blockDim.x) sm[i] = T(0);
+        if (hotg)
+            for (int i = threadIdx.x; i < (int)P.hot_glob_stride; i += blockDim.x) hotg[i] = T(0);
         __syncthreads();
     }
     const int c4 = (threadIdx.x & (G - 1)) * 4;
@@ -229,9 +240,10 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
         const int32_t sink = P.sink[q];
         const uint32_t lv = lev(q, c), hot = P.packed[q] ? (c >> kObsLevelBits) : 0u;
         if (sink == SINK_BLOCK) red_shared4(sm + P.smem_base[q] + c4 + (size_t)lv * KP, a);
-        else if (sink == SINK_HOT && hot && (int32_t)hot <= P.hot_cap[q])
-            red_shared4(sm + P.smem_base[q] + c4 + (size_t)(hot - 1) * KP, a);
-        else atomic_add4(out + ((size_t)P.off[q] + lv) * KP + c4, a);
+        else if (sink == SINK_HOT && hot && (int32_t)hot <= P.hot_cap[q]) {
+            if (hotg) atomic_add4(hotg + P.hot_goff[q] + c4 + (size_t)(hot - 1) * KP, a);
+            else red_shared4(sm + P.smem_base[q] + c4 + (size_t)(hot - 1) * KP, a);
+        } else atomic_add4(out + ((size_t)P.off[q] + lv) * KP + c4, a);
     };
 
     V4<double> lsc(0.0), usq(0.0);  // OBS_LSMR: this lane's scales and sum of u^2
@@ -393,9 +405,10 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
             pw[0] = usq.a; pw[1] = usq.b; pw[2] = usq.c; pw[3] = usq.d;
         }
     }
-    if (kScatter && P.smem_elems > 0) {
+    if (kScatter && (P.smem_elems > 0 || hotg)) {
         __syncthreads();
-        // the block's shared tables into `out`: one atomic per nonzero entry
+        // the block's tables into `out`: one atomic per nonzero entry (the global hot
+        // tables read from L2, where the reductions went)
         for (int q = 1; q < Q; ++q) {
             const int32_t sink = P.sink[q];
             if (sink == SINK_GLOBAL) continue;
@@ -406,7 +419,7 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
                     for (int g = 0; g < (int)gpb; ++g) v += sm[(size_t)g * P.priv_stride + P.smem_base[q] + e];
                     lv = (uint32_t)(e / KP);
                 } else {
-                    v = sm[P.smem_base[q] + e];
+                    v = (sink == SINK_HOT && hotg) ? __ldcg(hotg + P.hot_goff[q] + e) : sm[P.smem_base[q] + e];
                     lv = (sink == SINK_BLOCK) ? (uint32_t)(e / KP) : P.hot_level[q][e / KP];
                 }
                 if (v != T(0)) atomicAdd(out + (size_t)(P.off[q] + lv) * KP + e % KP, v);

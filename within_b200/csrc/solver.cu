@@ -479,6 +479,8 @@ struct SolverImpl {
     int64_t nchunk_tab[3] = {0, 0, 0};
     bool split_tab[3] = {false, false, false};
     int32_t obs_choice[4][2] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}};
+    DArr<unsigned char> obs_hot;  // per-block global hot tables of the observation pass
+    float obs_tune_ms[4][2][12] = {};  // the autotuner's time per candidate (0: not timed)
     // hottest levels of every non-primary factor, for the observation pass
     std::vector<DArr<uint32_t>> hot_level;
     std::vector<int32_t> hot_count;
@@ -760,9 +762,13 @@ void upload_design(SolverImpl& S) {
 // and the others their hottest levels, within kObsSmemBytes per block (two blocks/SM).
 constexpr int64_t kObsPrivBytes = 96 * 1024, kObsSmemBytes = 110 * 1024;
 
-int obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
+// `hot_global`: the hot tables go to per-block copies in S.obs_hot (sized by
+// obs_hot_bytes) instead of shared memory, all of each factor's hot levels.
+int obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P, bool hot_global = false) {
     P = S.obs;
     P.kp = kp;
+    P.hot_glob = nullptr;
+    P.hot_glob_stride = 0;
     const int G = group_for(kp);
     const int64_t gpb = (elem == 8 ? obs_block<double>() : obs_block<float>()) / G;
     const int Q = S.d.Q;
@@ -804,9 +810,19 @@ int obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
             used += nl * kp;
         }
     }
+    int64_t goff = 0;
     for (int sl = 1; sl < Q; ++sl) {  // hot levels, the hottest first, as many as fit
         P.hot_cap[sl] = 0;
+        P.hot_goff[sl] = 0;
         if (P.sink[sl] != SINK_GLOBAL || S.hot_count[sl] == 0) continue;
+        if (hot_global) {
+            P.sink[sl] = SINK_HOT;
+            P.hot_cap[sl] = S.hot_count[sl];
+            P.hot_goff[sl] = (int32_t)goff;
+            P.smem_len[sl] = (int32_t)(S.hot_count[sl] * kp);
+            goff += (int64_t)S.hot_count[sl] * kp;
+            continue;
+        }
         const int64_t cap = std::min<int64_t>(S.hot_count[sl], (budget - used) / kp);
         if (cap < 16) continue;
         P.sink[sl] = SINK_HOT;
@@ -816,22 +832,54 @@ int obs_params_for(SolverImpl& S, int kp, size_t elem, ObsParams& P) {
         used += cap * kp;
     }
     P.smem_elems = (int32_t)used;
+    if (goff > 0) {
+        // 16-byte aligned per-block copies; the pass runs at most 2 blocks per SM
+        P.hot_glob_stride = (goff + 1) / 2 * 2;
+        const size_t need = (size_t)S.n_sm * 2 * (size_t)P.hot_glob_stride * elem;
+        P.hot_glob = S.obs_hot.n >= need ? (void*)S.obs_hot.p : nullptr;
+    }
     return np;
+}
+
+// Grows S.obs_hot to `bytes`; a captured CG iteration holds the old address, so it is
+// dropped (recaptured on its next use).  Outside any stream capture.
+void grow_obs_hot(SolverImpl& S, size_t bytes) {
+    if (bytes <= S.obs_hot.n) return;
+    if (S.cg_exec) {
+        WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
+        S.cg_exec = nullptr;
+    }
+    S.obs_hot.alloc(bytes);
+}
+
+// Bytes of S.obs_hot that the global hot tables need for kp RHS of `elem` bytes (0: the
+// design has no hot levels outside shared memory's other tables).
+size_t obs_hot_bytes(SolverImpl& S, int kp, size_t elem) {
+    ObsParams P;
+    obs_params_for(S, kp, elem, P, true);
+    return (size_t)S.n_sm * 2 * (size_t)P.hot_glob_stride * elem;
 }
 
 int kp_class(int kp) { return kp <= 4 ? 0 : kp <= 8 ? 1 : kp <= 16 ? 2 : 3; }
 
 // Returns the number of per-warp partial rows written (OBS_LSMR; grid x warps per block).
+// Shapes of the observation pass: choice c < kObsShapes runs 16 << (c / 2) observations
+// per chunk and 1 + c % 2 blocks per SM with the hot tables in shared memory; choice
+// kObsShapes + c the same shape with them in per-block global copies (S.obs_hot).
+constexpr int kObsShapes = 6;
+
 template <typename T, int MODE>
 int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* out, T* eout,
                const double* lsmr_scale = nullptr, double* lsmr_part = nullptr) {
     ObsParams P;
-    const int np = obs_params_for(S, kp, sizeof(T), P);
+    // the autotuned block shape (obs_autotune), else 32 observations per chunk, 2 blocks/SM
+    int choice = S.obs_choice[kp_class(kp)][sizeof(T) == 8 ? 1 : 0];
+    int np = obs_params_for(S, kp, sizeof(T), P, choice >= kObsShapes);
+    if (choice >= kObsShapes && !P.hot_glob) np = obs_params_for(S, kp, sizeof(T), P);  // no global copies
+    choice = choice < 0 ? -1 : choice % kObsShapes;
     P.lsmr_scale = lsmr_scale;
     P.lsmr_part = lsmr_part;
     const int G = group_for(kp);
-    // the autotuned block shape (obs_autotune), else 32 observations per chunk, 2 blocks/SM
-    const int choice = S.obs_choice[kp_class(kp)][sizeof(T) == 8 ? 1 : 0];
     bool split = S.has_split;
     int blocks_per_sm = 2;
     if (choice >= 0) {
@@ -882,17 +930,27 @@ void obs_autotune(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
     {
         std::lock_guard<std::mutex> lk(g_obs_tune_mu);
         const auto it = g_obs_tune.find(key);
-        if (it != g_obs_tune.end()) {
-            choice = it->second;
-            return;
-        }
+        if (it != g_obs_tune.end()) choice = it->second;
+    }
+    if (choice >= 0) {  // tuned by a solver of the same class: this one's global copies
+        if (choice >= kObsShapes) grow_obs_hot(S, obs_hot_bytes(S, kp, sizeof(T)));
+        return;
     }
     cudaEvent_t e0, e1;
     WB_CUDA(cudaEventCreate(&e0));
     WB_CUDA(cudaEventCreate(&e1));
     float best = 0.f;
     int32_t best_c = 3;  // 32 observations per chunk, 2 blocks per SM
-    for (int32_t c = 0; c < 6; ++c) {
+    // candidates with global hot tables when the design has hot levels (their copies are
+    // allocated here, outside any stream capture)
+    const size_t hot = obs_hot_bytes(S, kp, sizeof(T));
+    grow_obs_hot(S, hot);
+    const int32_t nc = hot ? 2 * kObsShapes : kObsShapes;
+    // two sweeps over the candidates, the second in reverse order; each keeps its best
+    float* tms = S.obs_tune_ms[kp_class(kp)][sizeof(T) == 8 ? 1 : 0];
+    for (int32_t c = 0; c < 2 * kObsShapes; ++c) tms[c] = 0.f;
+    for (int32_t it = 0; it < 2 * nc; ++it) {
+        const int32_t c = it < nc ? it : 2 * nc - 1 - it;
         choice = c;
         launch_obs<T, OBS_GRAM>(S, kp, w, x, nullptr, y, nullptr);
         WB_CUDA(cudaEventRecord(e0, S.stream));
@@ -901,11 +959,14 @@ void obs_autotune(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
         WB_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         WB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (c == 0 || ms < best) {
-            best = ms;
+        ms *= 0.5f;
+        if (tms[c] == 0.f || ms < tms[c]) tms[c] = ms;
+    }
+    for (int32_t c = 0; c < nc; ++c)
+        if (c == 0 || tms[c] < best) {
+            best = tms[c];
             best_c = c;
         }
-    }
     WB_CUDA(cudaEventDestroy(e0));
     WB_CUDA(cudaEventDestroy(e1));
     choice = best_c;
@@ -3437,9 +3498,50 @@ int within_solver_obs_config(const within_solver* s, int32_t k, int32_t elem_byt
     if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) || !obs_per_chunk || !blocks_per_sm)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
     const int32_t c = s->impl->obs_choice[wb::kp_class(wb::pad_kp(k))][elem_bytes == 8 ? 1 : 0];
-    *obs_per_chunk = c < 0 ? 32 : 16 << (c / 2);
+    *obs_per_chunk = c < 0 ? 32 : 16 << ((c % wb::kObsShapes) / 2);
     *blocks_per_sm = c < 0 ? 2 : 1 + c % 2;
     return c < 0 ? 1 : 0;
+}
+
+int32_t within_solver_obs_hot_global(const within_solver* s, int32_t k, int32_t elem_bytes) {
+    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8)) return -1;
+    const int kp = wb::pad_kp(k);
+    const int32_t c = s->impl->obs_choice[wb::kp_class(kp)][elem_bytes == 8 ? 1 : 0];
+    if (c < 0) return -1;
+    if (c < wb::kObsShapes) return 0;
+    wb::ObsParams P;
+    wb::obs_params_for(*s->impl, kp, (size_t)elem_bytes, P, true);
+    return P.hot_glob ? 1 : 0;
+}
+
+int within_solver_obs_tune_times(const within_solver* s, int32_t k, int32_t elem_bytes, float* ms, int32_t n) {
+    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) || !ms || n < 0)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
+    const float* t = s->impl->obs_tune_ms[wb::kp_class(wb::pad_kp(k))][elem_bytes == 8 ? 1 : 0];
+    for (int32_t c = 0; c < n && c < 2 * wb::kObsShapes; ++c) ms[c] = t[c];
+    return 0;
+}
+
+int within_solver_set_obs_config(within_solver* s, int32_t k, int32_t elem_bytes, int32_t obs_per_chunk,
+                                 int32_t blocks_per_sm, int32_t hot_global) {
+    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) ||
+        (obs_per_chunk != 16 && obs_per_chunk != 32 && obs_per_chunk != 64) || blocks_per_sm < 1 ||
+        blocks_per_sm > 2 || hot_global < 0 || hot_global > 1)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
+    wb::SolverImpl& S = *s->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    return guard([&]() -> int {
+        const int kp = wb::pad_kp(k);
+        if (hot_global) wb::grow_obs_hot(S, wb::obs_hot_bytes(S, kp, (size_t)elem_bytes));
+        if (S.cg_exec) {  // the captured CG iteration holds the pass's old shape
+            WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
+            S.cg_exec = nullptr;
+        }
+        const int32_t ci = obs_per_chunk == 16 ? 0 : obs_per_chunk == 32 ? 1 : 2;
+        S.obs_choice[wb::kp_class(kp)][elem_bytes == 8 ? 1 : 0] =
+            (hot_global ? wb::kObsShapes : 0) + 2 * ci + (blocks_per_sm - 1);
+        return 0;
+    });
 }
 
 int64_t within_solver_schwarz_bytes(const within_solver* s, int32_t k, int32_t elem_bytes) {
