@@ -251,6 +251,15 @@ void within_solver_ac_arrays(const within_solver *solver, int32_t i, int32_t *le
  * WITHIN_ERR_INVALID_ARGUMENT when the preconditioner has no such sweeps. */
 int within_solver_inject_sweep_timeout(within_solver *solver, int32_t on);
 
+/* Tuning knob (no counterpart in the reference, whose approximate-Cholesky solve,
+ * approx_chol::Factor::solve_in_place, is sequential).  The longest run of consecutive
+ * levels of an approximate-Cholesky sweep direction with at most `max_chunks` row pieces
+ * each (default 512; at least two levels) runs in one thread-block cluster, separated by
+ * the cluster's hardware barrier; the other levels run in cooperative grid launches with
+ * grid barriers.  0 puts every level on the grid.  Same arithmetic in the same order
+ * either way.  WITHIN_ERR_INVALID_ARGUMENT for a negative value. */
+int within_solver_set_sweep_cluster(within_solver *solver, int64_t max_chunks);
+
 /* Coarse space for CG (no counterpart in the reference; it augments the additive Schwarz
  * apply, schwarz-precond/src/schwarz/additive/executor.rs:59-147, inside CG,
  * schwarz-precond/src/solve/cg.rs:45-133).  With a coarse basis Z (n_dofs x 32), CG's

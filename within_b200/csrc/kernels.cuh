@@ -727,66 +727,103 @@ __device__ __forceinline__ void grid_barrier(unsigned* count, unsigned target, i
     __syncthreads();
 }
 
-// Every level of one AC sweep direction in one cooperative launch: level l's chunks are
-// [lp[l], lp[l+1]); levels run in order (backward: from the last), separated by grid
-// barriers; within a level the work is that of csr_rows_kernel (one warp per chunk) on
-// the vector v, read and written through L2.
+// One chunk of an AC level (csr_rows_kernel's work for one warp) on the vector v, read
+// and written through L2: the warp's lane groups take the chunk's entries in turn, four
+// gathers in flight each, and combine with shuffles; lane group 0 writes the row.
+template <typename T, int G, int EPI>
+__device__ __forceinline__ void level_chunk(const CsrChunk& C, const uint32_t* __restrict__ row_slot,
+                                            const int64_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                                            const T* __restrict__ val, const T* __restrict__ rscale, T* v, int kp,
+                                            int grp, int c4) {
+    constexpr int NG = 32 / G;
+    for (uint32_t row = C.row_begin; row < C.row_end; ++row) {
+        const bool one = C.whole != 0;  // one complete row: its range is the chunk's
+        const int64_t rb = one ? C.nz_begin : ptr[row], re = one ? C.nz_end : ptr[row + 1];
+        const int64_t e0 = max(rb, C.nz_begin), e1 = min(re, C.nz_end);
+        V4<T> acc(T(0));
+        int64_t e = e0 + grp;
+        for (; e + 3 * NG < e1; e += 4 * NG) {
+            const uint32_t j0 = __ldg(col + e), j1 = __ldg(col + e + NG);
+            const uint32_t j2 = __ldg(col + e + 2 * NG), j3 = __ldg(col + e + 3 * NG);
+            const T v0 = __ldg(val + e), v1 = __ldg(val + e + NG), v2 = __ldg(val + e + 2 * NG), v3 = __ldg(val + e + 3 * NG);
+            const V4<T> s0 = ldcg4(v + (size_t)j0 * kp + c4), s1 = ldcg4(v + (size_t)j1 * kp + c4);
+            const V4<T> s2 = ldcg4(v + (size_t)j2 * kp + c4), s3 = ldcg4(v + (size_t)j3 * kp + c4);
+            acc += v0 * s0;
+            acc += v1 * s1;
+            acc += v2 * s2;
+            acc += v3 * s3;
+        }
+        for (; e < e1; e += NG) acc += __ldg(val + e) * ldcg4(v + (size_t)__ldg(col + e) * kp + c4);
+#pragma unroll
+        for (int off = G; off < 32; off <<= 1) {
+            acc.a += __shfl_xor_sync(0xffffffffu, acc.a, off);
+            acc.b += __shfl_xor_sync(0xffffffffu, acc.b, off);
+            acc.c += __shfl_xor_sync(0xffffffffu, acc.c, off);
+            acc.d += __shfl_xor_sync(0xffffffffu, acc.d, off);
+        }
+        if (grp == 0) {
+            T* d = v + (size_t)row_slot[row] * kp + c4;
+            if (EPI == EPI_ACC) {
+                if (e0 != rb || e1 != re) atomic_add4(d, acc);
+                else stcg4(d, ldcg4(d) + acc);
+            } else {
+                stcg4(d, rscale[row] * ldcg4(d) + acc);
+            }
+        }
+    }
+}
+
+// Levels lev0 .. lev0 + nlev - 1 of one AC sweep direction in one cooperative launch:
+// level l's chunks are [lp[l], lp[l+1]); levels run in order (backward: from the last),
+// separated by grid barriers.
 template <typename T, int G, int EPI>
 __global__ void __launch_bounds__(kBlock) csr_levels_kernel(const CsrChunk* __restrict__ chunks,
-                                                            const int64_t* __restrict__ lp, int nlev, int backward,
-                                                            const uint32_t* __restrict__ row_slot,
+                                                            const int64_t* __restrict__ lp, int lev0, int nlev,
+                                                            int backward, const uint32_t* __restrict__ row_slot,
                                                             const int64_t* __restrict__ ptr,
                                                             const uint32_t* __restrict__ col,
                                                             const T* __restrict__ val, const T* __restrict__ rscale,
                                                             T* v, int kp, unsigned* bar, int* err,
                                                             unsigned target_extra, unsigned max_spins) {
-    constexpr int NG = 32 / G;
     const int lane = threadIdx.x & 31;
     const int grp = lane / G;
     const int c4 = (lane & (G - 1)) * 4;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     for (int li = 0; li < nlev; ++li) {
-        const int l = backward ? nlev - 1 - li : li;
-        for (int64_t ch = lp[l] + wid; ch < lp[l + 1]; ch += nw) {
-            const CsrChunk C = chunks[ch];
-            for (uint32_t row = C.row_begin; row < C.row_end; ++row) {
-                const bool one = C.whole != 0;  // one complete row: its range is the chunk's
-                const int64_t rb = one ? C.nz_begin : ptr[row], re = one ? C.nz_end : ptr[row + 1];
-                const int64_t e0 = max(rb, C.nz_begin), e1 = min(re, C.nz_end);
-                V4<T> acc(T(0));
-                int64_t e = e0 + grp;
-                for (; e + 3 * NG < e1; e += 4 * NG) {
-                    const uint32_t j0 = __ldg(col + e), j1 = __ldg(col + e + NG);
-                    const uint32_t j2 = __ldg(col + e + 2 * NG), j3 = __ldg(col + e + 3 * NG);
-                    const T v0 = __ldg(val + e), v1 = __ldg(val + e + NG), v2 = __ldg(val + e + 2 * NG), v3 = __ldg(val + e + 3 * NG);
-                    const V4<T> s0 = ldcg4(v + (size_t)j0 * kp + c4), s1 = ldcg4(v + (size_t)j1 * kp + c4);
-                    const V4<T> s2 = ldcg4(v + (size_t)j2 * kp + c4), s3 = ldcg4(v + (size_t)j3 * kp + c4);
-                    acc += v0 * s0;
-                    acc += v1 * s1;
-                    acc += v2 * s2;
-                    acc += v3 * s3;
-                }
-                for (; e < e1; e += NG) acc += __ldg(val + e) * ldcg4(v + (size_t)__ldg(col + e) * kp + c4);
-#pragma unroll
-                for (int off = G; off < 32; off <<= 1) {
-                    acc.a += __shfl_xor_sync(0xffffffffu, acc.a, off);
-                    acc.b += __shfl_xor_sync(0xffffffffu, acc.b, off);
-                    acc.c += __shfl_xor_sync(0xffffffffu, acc.c, off);
-                    acc.d += __shfl_xor_sync(0xffffffffu, acc.d, off);
-                }
-                if (grp == 0) {
-                    T* d = v + (size_t)row_slot[row] * kp + c4;
-                    if (EPI == EPI_ACC) {
-                        if (e0 != rb || e1 != re) atomic_add4(d, acc);
-                        else stcg4(d, ldcg4(d) + acc);
-                    } else {
-                        stcg4(d, rscale[row] * ldcg4(d) + acc);
-                    }
-                }
-            }
-        }
+        const int l = lev0 + (backward ? nlev - 1 - li : li);
+        for (int64_t ch = lp[l] + wid; ch < lp[l + 1]; ch += nw)
+            level_chunk<T, G, EPI>(chunks[ch], row_slot, ptr, col, val, rscale, v, kp, grp, c4);
         if (li + 1 < nlev) grid_barrier(bar, (unsigned)(li + 1) * gridDim.x + target_extra, err, max_spins);
+    }
+}
+
+// The small levels lev0 .. lev0 + nlev - 1 of a sweep direction (a few thousand rows or
+// fewer each: the last levels of an AC factor) in one thread-block cluster, separated by
+// the cluster's hardware barrier (release/acquire at cluster scope; v is read and written
+// through L2) instead of a barrier across the whole grid.  Launched as exactly one
+// cluster of gridDim.x blocks.
+constexpr int kLevelClusterBlock = 1024;
+
+template <typename T, int G, int EPI>
+__global__ void __launch_bounds__(kLevelClusterBlock, 1)
+    csr_levels_cluster_kernel(const CsrChunk* __restrict__ chunks, const int64_t* __restrict__ lp, int lev0,
+                              int nlev, int backward, const uint32_t* __restrict__ row_slot,
+                              const int64_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                              const T* __restrict__ val, const T* __restrict__ rscale, T* v, int kp) {
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / G;
+    const int c4 = (lane & (G - 1)) * 4;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    for (int li = 0; li < nlev; ++li) {
+        const int l = lev0 + (backward ? nlev - 1 - li : li);
+        for (int64_t ch = lp[l] + wid; ch < lp[l + 1]; ch += nw)
+            level_chunk<T, G, EPI>(chunks[ch], row_slot, ptr, col, val, rscale, v, kp, grp, c4);
+        if (li + 1 < nlev) {
+            asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+            asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+        }
     }
 }
 

@@ -509,6 +509,7 @@ struct SolverImpl {
     std::shared_ptr<void> cn;     // CnState of the coarse-space network, kept while training
     bool precond_only = false;    // built from a serialized preconditioner: no design
     bool inject_sweep_timeout = false;  // test hook: AC sweep barriers that cannot be met
+    int64_t sweep_cluster_chunks = 512;  // AC levels of at most this many chunks go to one cluster (0: none)
     std::vector<uint8_t> pc_bytes;  // serialized preconditioner, made on first request
     int32_t* h_active = nullptr;  // pinned
     double setup_time = 0.0;
@@ -1089,8 +1090,48 @@ void launch_gram_acc(SolverImpl& S, int kp, const T* x, T* y) {
 // Spin limit of the barrier waits under the test hook (about a millisecond per wait).
 constexpr unsigned kInjectedBarrierSpins = 1u << 12;
 
-// All levels of one AC sweep direction of a stage as one cooperative launch (grid
-// barriers between levels), when the device supports it; otherwise one launch per level.
+// Blocks of the thread-block cluster that runs the small last levels of an AC sweep
+// (csr_levels_cluster_kernel), per kernel: 16 (non-portable size) or 8 when the device
+// can hold such a cluster of 1024-thread blocks, else 0 (no cluster path).
+inline int level_cluster_blocks(const void* kern) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    const auto it = cache.find(kern);
+    if (it != cache.end()) return it->second;
+    int best = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) cudaGetLastError();
+    for (int cb : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)cb;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(cb);
+        cfg.blockDim = dim3(kLevelClusterBlock);
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int nc = 0;
+        if (cudaOccupancyMaxActiveClusters(&nc, kern, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            nc = 0;
+        }
+        if (nc >= 1) {
+            best = cb;
+            break;
+        }
+    }
+    cache.emplace(kern, best);
+    return best;
+}
+
+// All levels of one AC sweep direction of a stage: the large levels as one cooperative
+// launch (grid barriers between levels), the trailing run of small levels (the last
+// rounds of the factor: a few hundred rows each) as one launch of a single thread-block
+// cluster, whose hardware barrier separates them.  The forward direction runs the large
+// levels first, the backward one the small levels first.  Without cooperative launches,
+// one launch per level.
 template <typename T, int EPI>
 void launch_sweep(SolverImpl& S, CsrDev<T>& c, const std::vector<int64_t>& lp, const int64_t* lp_d, bool backward,
                   T* v, int kp, int which) {
@@ -1106,27 +1147,81 @@ void launch_sweep(SolverImpl& S, CsrDev<T>& c, const std::vector<int64_t>& lp, c
     const int G = group_for(kp);
     unsigned* bar = S.ws.sweep_bar.p + which;
     int* err = S.ws.sweep_err.p;
-    WB_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned), S.stream));
-    auto go = [&](auto kern) {
+    const CsrChunk* ch = c.chunks.p;
+    const uint32_t* rs = c.row_slot.p;
+    const int64_t* pt = c.ptr.p;
+    const uint32_t* cl = c.col.p;
+    const T* vl = c.val.p;
+    const T* sc = c.rscale.p;
+    int bw = backward ? 1 : 0, k = kp;
+    // the longest run [a, b) of consecutive small levels (at least two, so that a barrier
+    // is saved); the levels before and after it run on the grid
+    int a = 0, b = 0;
+    const int64_t max_chunks = S.sweep_cluster_chunks;
+    if (max_chunks > 0 && !S.inject_sweep_timeout) {
+        for (int l = 0; l < nlev;) {
+            if (lp[l + 1] - lp[l] > max_chunks) {
+                ++l;
+                continue;
+            }
+            int e = l;
+            while (e < nlev && lp[e + 1] - lp[e] <= max_chunks) ++e;
+            if (e - l > b - a) a = l, b = e;
+            l = e;
+        }
+        if (b - a < 2) a = b = 0;
+    }
+    auto grid_part = [&](auto kern, int l0, int nl) {  // levels [l0, l0 + nl)
+        if (nl <= 0) return;
+        if (nl == 1) {
+            launch_csr<T, EPI>(S, c, lp[l0], lp[l0 + 1], v, v, kp);
+            return;
+        }
+        WB_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned), S.stream));
         const int grid = resident_per_sm((const void*)kern) * S.n_sm;  // every block resident
-        const CsrChunk* ch = c.chunks.p;
-        const uint32_t* rs = c.row_slot.p;
-        const int64_t* pt = c.ptr.p;
-        const uint32_t* cl = c.col.p;
-        const T* vl = c.val.p;
-        const T* sc = c.rscale.p;
-        int nl = nlev, bw = backward ? 1 : 0, k = kp;
         // a test can make every barrier wait for one block more than the grid has, with a
         // short limit: the waits run out, the error flag is set, the launch ends
         unsigned extra = S.inject_sweep_timeout ? 1u : 0u;
         unsigned spins = S.inject_sweep_timeout ? kInjectedBarrierSpins : kBarrierSpins;
-        void* args[] = {(void*)&ch, (void*)&lp_d, (void*)&nl, (void*)&bw, (void*)&rs, (void*)&pt, (void*)&cl,
-                        (void*)&vl, (void*)&sc, (void*)&v, (void*)&k, (void*)&bar, (void*)&err, (void*)&extra,
-                        (void*)&spins};
+        void* args[] = {(void*)&ch, (void*)&lp_d, (void*)&l0, (void*)&nl, (void*)&bw, (void*)&rs, (void*)&pt,
+                        (void*)&cl, (void*)&vl, (void*)&sc, (void*)&v, (void*)&k, (void*)&bar, (void*)&err,
+                        (void*)&extra, (void*)&spins};
         WB_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(kBlock), args, 0, S.stream));
         S.gpu_launches++;
     };
-    WB_DISPATCH_G(G, go(csr_levels_kernel<T, GV, EPI>));
+    auto cluster_part = [&](auto kern) {  // levels [a, b)
+        if (b == a) return;
+        const int cb = level_cluster_blocks((const void*)kern);
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)cb;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(cb);
+        cfg.blockDim = dim3(kLevelClusterBlock);
+        cfg.stream = S.stream;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        WB_CUDA(cudaLaunchKernelEx(&cfg, kern, ch, lp_d, a, b - a, bw, rs, pt, cl, vl, sc, v, k));
+        S.gpu_launches++;
+    };
+    WB_DISPATCH_G(G, {
+        auto gk = csr_levels_kernel<T, GV, EPI>;
+        auto ck = csr_levels_cluster_kernel<T, GV, EPI>;
+        if (b > a && level_cluster_blocks((const void*)ck) == 0) a = b = 0;  // no cluster: all levels on the grid
+        if (b == a) {
+            grid_part(gk, 0, nlev);
+        } else if (!backward) {
+            grid_part(gk, 0, a);
+            cluster_part(ck);
+            grid_part(gk, b, nlev - b);
+        } else {
+            grid_part(gk, b, nlev - b);
+            cluster_part(ck);
+            grid_part(gk, 0, a);
+        }
+    });
 }
 
 // The host learns of a grid-barrier timeout here (after the work that set it is done):
@@ -3375,6 +3470,20 @@ int within_solver_inject_sweep_timeout(within_solver* s, int32_t on) {
             return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the preconditioner has no fused approximate-Cholesky sweeps");
         S.inject_sweep_timeout = on != 0;
         if (S.cg_exec) {  // the captured CG iteration holds the sweep parameters
+            WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
+            S.cg_exec = nullptr;
+        }
+        return WITHIN_OK;
+    });
+}
+
+int within_solver_set_sweep_cluster(within_solver* s, int64_t max_chunks) {
+    if (!s || max_chunks < 0) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
+    SolverImpl& S = *s->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    return guard([&]() -> int {
+        S.sweep_cluster_chunks = max_chunks;
+        if (S.cg_exec) {  // the captured CG iteration holds the sweep launches
             WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
             S.cg_exec = nullptr;
         }
