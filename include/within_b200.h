@@ -310,19 +310,30 @@ int within_solver_obs_config(const within_solver *solver, int32_t k, int32_t ele
  * reference. */
 int32_t within_solver_obs_hot_global(const within_solver *solver, int32_t k, int32_t elem_bytes);
 
+/* Right-hand sides per lane of the observation pass for k RHS in elem_bytes precision:
+ * 4, or 8 for wide lanes (FP32 operator apply with k > 4: the per-observation control is
+ * shared by 8 RHS, with half the threads per block); -1 not tuned yet.  The autotuner
+ * tries both where wide lanes apply.  No counterpart in the reference. */
+int32_t within_solver_obs_rhs_per_lane(const within_solver *solver, int32_t k, int32_t elem_bytes);
+
 /* The autotuner's measured time (milliseconds per operator apply, the best of two
  * sweeps over the candidates) of each candidate shape for k RHS in elem_bytes precision:
- * ms[c] for c < n and c < 12, where c = hot_global * 6 + 2 * log2(obs_per_chunk / 16) +
- * blocks_per_sm - 1; 0 for candidates not timed (a shape class tuned earlier in the
- * process, or no hot levels).  A measurement hook with no counterpart in the reference. */
+ * ms[c] for c < n and c < 24, where c = wide * 12 + hot_global * 6 +
+ * 2 * log2(obs_per_chunk / 16) + blocks_per_sm - 1 (wide: 8 RHS per lane); 0 for
+ * candidates not timed (a shape class tuned earlier in the process, no hot levels, or
+ * no wide lanes for this precision and k).  A measurement hook with no counterpart in the reference. */
 int within_solver_obs_tune_times(const within_solver *solver, int32_t k, int32_t elem_bytes, float *ms, int32_t n);
 
 /* Fixes the observation pass's shape for k RHS in elem_bytes precision instead of
- * autotuning it: obs_per_chunk 16, 32 or 64, blocks_per_sm 1 or 2, hot_global 0 or 1 (see
- * within_solver_obs_hot_global; 1 allocates the per-block copies here).  For
- * reproducible timing and for testing each variant.  No counterpart in the reference. */
+ * autotuning it: obs_per_chunk 16, 32 or 64, blocks_per_sm 1 or 2, and `variant` the sum
+ * of 1 for the hot tables in per-block global copies (see within_solver_obs_hot_global;
+ * the copies are allocated here) and 2 for wide lanes (see
+ * within_solver_obs_rhs_per_lane; FP32, k > 4 and the exact kernels only: at most 3
+ * factors, or 4 with at most one small factor in lane-group tables; otherwise
+ * WITHIN_ERR_INVALID_ARGUMENT).  For reproducible timing and for testing each variant.
+ * No counterpart in the reference. */
 int within_solver_set_obs_config(within_solver *solver, int32_t k, int32_t elem_bytes, int32_t obs_per_chunk,
-                                 int32_t blocks_per_sm, int32_t hot_global);
+                                 int32_t blocks_per_sm, int32_t variant);
 
 /* Algorithmic bytes of one Schwarz apply over k RHS with elem_bytes (4 or 8) per vector
  * element, counted from the built subdomains: per subdomain 2 (4+s) nnz(C_i) for the

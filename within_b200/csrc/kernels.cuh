@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace wb {
 
 constexpr int kMaxQ = 16;
@@ -90,6 +92,78 @@ template <typename T>
 __device__ __forceinline__ V4<double> to_d(const V4<T>& v) { return V4<double>(v.a, v.b, v.c, v.d); }
 template <typename T>
 __device__ __forceinline__ V4<T> from_d(const V4<double>& v) { return V4<T>((T)v.a, (T)v.b, (T)v.c, (T)v.d); }
+
+// RV consecutive 4-wide RHS vectors of one lane (4 RV right-hand sides), for the
+// observation pass's wide lanes; VecR<T, 1> is V4<T> itself.
+template <typename T, int RV>
+struct VR {
+    V4<T> v[RV];
+    __device__ __forceinline__ VR() {}
+    __device__ __forceinline__ VR(T s) {
+#pragma unroll
+        for (int j = 0; j < RV; ++j) v[j] = V4<T>(s);
+    }
+    __device__ __forceinline__ VR& operator+=(const VR& o) {
+#pragma unroll
+        for (int j = 0; j < RV; ++j) v[j] += o.v[j];
+        return *this;
+    }
+    __device__ __forceinline__ VR& operator-=(const VR& o) {
+#pragma unroll
+        for (int j = 0; j < RV; ++j) v[j] -= o.v[j];
+        return *this;
+    }
+};
+template <typename T, int RV>
+__device__ __forceinline__ VR<T, RV> operator*(T s, const VR<T, RV>& a) {
+    VR<T, RV> r;
+#pragma unroll
+    for (int j = 0; j < RV; ++j) r.v[j] = s * a.v[j];
+    return r;
+}
+template <typename T, int RV>
+__device__ __forceinline__ VR<T, RV> operator+(VR<T, RV> x, const VR<T, RV>& y) { x += y; return x; }
+template <typename T, int RV>
+__device__ __forceinline__ VR<T, RV> operator-(VR<T, RV> x, const VR<T, RV>& y) { x -= y; return x; }
+template <typename T, int RV>
+using VecR = typename std::conditional<RV == 1, V4<T>, VR<T, RV>>::type;
+template <int RV, typename T>
+__device__ __forceinline__ VecR<T, RV> ldv(const T* p) {
+    if constexpr (RV == 1) {
+        return ld4(p);
+    } else {
+        VR<T, RV> r;
+#pragma unroll
+        for (int j = 0; j < RV; ++j) r.v[j] = ld4(p + 4 * j);
+        return r;
+    }
+}
+template <int RV, typename T>
+__device__ __forceinline__ VecR<T, RV> ldgv(const T* p) {
+    if constexpr (RV == 1) {
+        return ldg4(p);
+    } else {
+        VR<T, RV> r;
+#pragma unroll
+        for (int j = 0; j < RV; ++j) r.v[j] = ldg4(p + 4 * j);
+        return r;
+    }
+}
+template <typename T, int RV>
+__device__ __forceinline__ void st4(T* p, const VR<T, RV>& a) {
+#pragma unroll
+    for (int j = 0; j < RV; ++j) st4(p + 4 * j, a.v[j]);
+}
+template <typename T, int RV>
+__device__ __forceinline__ void atomic_add4(T* p, const VR<T, RV>& a) {
+#pragma unroll
+    for (int j = 0; j < RV; ++j) atomic_add4(p + 4 * j, a.v[j]);
+}
+template <typename T, int RV>
+__device__ __forceinline__ void red_shared4(T* p, const VR<T, RV>& a) {
+#pragma unroll
+    for (int j = 0; j < RV; ++j) red_shared4(p + 4 * j, a.v[j]);
+}
 
 // ---------------------------------------------------------------------------
 // Observation pass: y = D'W(D x) and its relatives, one read of the codes.
@@ -189,16 +263,23 @@ __device__ __forceinline__ uint32_t ucomp(const uint4& v, int b) { return b == 0
 // every observation of the generic kernel) go one at a time.  Addresses come from
 // per-factor base pointers with the row stride a compile-time constant.  The block adds
 // its shared tables into `out` at the end.
+// Wide lanes (RV = 2, the FP32 operator apply only): a lane owns 8 RHS and a group of
+// G = kp/8 lanes a row, so the per-observation control (level tests, code and weight
+// loads, addresses) is shared by twice the RHS; the group-private tables are as large
+// as with 4 RHS per lane, so the block has half the threads (same tables per block).
 // Threads per block of the observation pass: 256, or 128 for FP64, whose group-private
-// tables are twice as large (the tables of a block are its lane groups' copies).
-template <typename T>
-constexpr int obs_block() { return sizeof(T) == 8 ? 128 : 256; }
+// tables are twice as large (the tables of a block are its lane groups' copies), and for
+// wide lanes.
+template <typename T, int RV = 1>
+constexpr int obs_block() { return (sizeof(T) == 8 || RV > 1) ? 128 : 256; }
 
-template <typename T, int G, int MODE, int QT, int NP>
-__global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P, const T* __restrict__ w,
+template <typename T, int G, int MODE, int QT, int NP, int RV = 1>
+__global__ void __launch_bounds__(obs_block<T, RV>(), 2) obs_pass_kernel(ObsParams P, const T* __restrict__ w,
                                                              const T* __restrict__ x, const T* __restrict__ yin,
                                                              T* __restrict__ out, T* __restrict__ eout) {
-    constexpr int KP = 4 * G;
+    static_assert(RV == 1 || MODE == OBS_GRAM, "wide lanes: operator apply only");
+    using Vec = VecR<T, RV>;
+    constexpr int KP = 4 * G * RV;
     constexpr bool kScatter = MODE != OBS_DX;
     constexpr bool kGather = MODE != OBS_RHS;
     constexpr bool kGeneric = QT == kMaxQ;
@@ -217,7 +298,7 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
             for (int i = threadIdx.x; i < (int)P.hot_glob_stride; i += blockDim.x) hotg[i] = T(0);
         __syncthreads();
     }
-    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const int c4 = (threadIdx.x & (G - 1)) * 4 * RV;
     const int gl = threadIdx.x / G;
     const int64_t gpb = blockDim.x / G;
     const int64_t ngroups = (int64_t)gridDim.x * gpb;
@@ -236,7 +317,7 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
         return x + ((size_t)P.off[q] + (q == 0 || is_priv(q) ? c : lev(q, c))) * KP + c4;
     };
     // run sum of non-private slot q at device code c into its sink
-    auto flush = [&](int q, uint32_t c, const V4<T>& a) {
+    auto flush = [&](int q, uint32_t c, const Vec& a) {
         const int32_t sink = P.sink[q];
         const uint32_t lv = lev(q, c), hot = P.packed[q] ? (c >> kObsLevelBits) : 0u;
         if (sink == SINK_BLOCK) red_shared4(sm + P.smem_base[q] + c4 + (size_t)lv * KP, a);
@@ -251,48 +332,48 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
     for (int64_t ch = (int64_t)blockIdx.x * gpb + gl; ch < P.nchunks; ch += ngroups) {
         const ObsChunk C = P.chunks[ch];
         uint32_t lvl = C.lvl_begin;
-        V4<T> acc(T(0));
+        Vec acc(T(0));
         uint32_t run_l[QT], cl[NS];
-        V4<T> run_a[QT], cv[NS];
+        Vec run_a[QT], cv[NS];
 #pragma unroll
         for (int q = 0; q < QT; ++q) {
             run_l[q] = kNone;
-            run_a[q] = V4<T>(T(0));
+            run_a[q] = Vec(T(0));
         }
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
             cl[q] = kNone;
-            cv[q] = V4<T>(T(0));
+            cv[q] = Vec(T(0));
         }
         // one observation: codes c[0..Q), weight wi
         // one observation in two phases: its row sum (loads) and its scatter; a batch
         // runs the first phase for all its observations before the second, so their
         // loads are in flight together (the scatter's reductions order memory)
-        auto gather = [&](uint32_t i, const uint32_t (&c)[QT]) -> V4<T> {
-            V4<T> s(T(0));
+        auto gather = [&](uint32_t i, const uint32_t (&c)[QT]) -> Vec {
+            Vec s(T(0));
             if constexpr (kGather) {
 #pragma unroll
                 for (int q = 0; q < QT; ++q) {
                     if (q >= Q) continue;
                     if (kGeneric || is_priv(q)) {
-                        s += ldg4(xrow(q, c[q]));  // generic kernel, or a level that changes every time
+                        s += ldgv<RV>(xrow(q, c[q]));  // generic kernel, or a level that changes every time
                     } else {
-                        if (c[q] != cl[q]) cv[q] = ldg4(xrow(q, c[q]));
+                        if (c[q] != cl[q]) cv[q] = ldgv<RV>(xrow(q, c[q]));
                         cl[q] = c[q];
                         s += cv[q];
                     }
                 }
             }
             if constexpr (MODE == OBS_RHS || MODE == OBS_RESID) {
-                const V4<T> yv = ld4(yin + (size_t)i * KP + c4);
+                const Vec yv = ldv<RV>(yin + (size_t)i * KP + c4);
                 s = (MODE == OBS_RHS) ? yv : yv - s;
             }
             return s;
         };
-        auto scatter = [&](uint32_t i, const uint32_t (&c)[QT], T wi, const V4<T>& s0) {
-            V4<T> s = s0;
+        auto scatter = [&](uint32_t i, const uint32_t (&c)[QT], T wi, const Vec& s0) {
+            Vec s = s0;
             if constexpr (MODE == OBS_LSMR) {  // u = w (D x) + scale u_old
-                const V4<T> uo = ld4(yin + (size_t)i * KP + c4);
+                const Vec uo = ldv<RV>(yin + (size_t)i * KP + c4);
                 s = wi * s0;
                 if (lsc.a != 0.0) s.a += (T)lsc.a * uo.a;
                 if (lsc.b != 0.0) s.b += (T)lsc.b * uo.b;
@@ -303,12 +384,12 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
             }
             if constexpr (MODE == OBS_DX || MODE == OBS_RESID || MODE == OBS_LSMR) st4(eout + (size_t)i * KP + c4, s);
             if constexpr (kScatter) {
-                const V4<T> t = wi * s;
+                const Vec t = wi * s;
                 const uint32_t p = c[0];
                 if (p != lvl) {  // primary level complete: plain store
                     st4(out0 + (size_t)lvl * KP, acc);
-                    for (uint32_t l = lvl + 1; l < p; ++l) st4(out0 + (size_t)l * KP, V4<T>(T(0)));  // empty levels
-                    acc = V4<T>(T(0));
+                    for (uint32_t l = lvl + 1; l < p; ++l) st4(out0 + (size_t)l * KP, Vec(T(0)));  // empty levels
+                    acc = Vec(T(0));
                     lvl = p;
                 }
                 acc += t;
@@ -317,7 +398,7 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
                     if (q >= Q) continue;
                     if (is_priv(q)) {
                         T* pt = priv + P.smem_base[q] + (size_t)c[q] * KP;
-                        st4(pt, ld4(pt) + t);
+                        st4(pt, ldv<RV>(pt) + t);
                     } else if (c[q] != run_l[q]) {
                         if (run_l[q] != kNone) flush(q, run_l[q], run_a[q]);
                         run_l[q] = c[q];
@@ -355,7 +436,7 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
                         if (weighted && more) nw = load_w4v(w, i + 4);
                     }
                     uint32_t c[4][QT];
-                    V4<T> s[4];
+                    Vec s[4];
 #pragma unroll
                     for (int b = 0; b < 4; ++b) {
 #pragma unroll
@@ -387,7 +468,7 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) obs_pass_kernel(ObsParams P
             } else {
                 for (; lvl < C.lvl_end; ++lvl) {
                     st4(out0 + (size_t)lvl * KP, acc);
-                    acc = V4<T>(T(0));
+                    acc = Vec(T(0));
                 }
             }
         }

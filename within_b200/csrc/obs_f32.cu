@@ -3,6 +3,6 @@
 #include "obs_launch.cuh"
 
 namespace wb {
-template cudaError_t obs_dispatch<float, OBS_GRAM>(const ObsParams&, int, int, int, size_t, cudaStream_t, const float*,
+template cudaError_t obs_dispatch<float, OBS_GRAM>(const ObsParams&, int, int, int, int, size_t, cudaStream_t, const float*,
                                                    const float*, const float*, float*, float*);
 }  // namespace wb

@@ -12,25 +12,54 @@
 namespace wb {
 
 // Picks the exact kernel for P.Q <= 4 with the trailing np private slots (Q = 4: np <= 1),
-// else the generic one, for G = kp/4 lanes per row, and launches `grid` blocks of
-// obs_block<T>() threads on `stream`.
+// else the generic one, for G lanes per row of rv 4-wide RHS vectors each (rv = 2: wide
+// lanes, FP32 operator apply, exact kernels only), and launches `grid` blocks of
+// obs_block<T, rv>() threads on `stream`.
 template <typename T, int MODE>
-cudaError_t obs_dispatch(const ObsParams& P, int np, int G, int grid, size_t smem, cudaStream_t stream, const T* w,
-                         const T* x, const T* yin, T* out, T* eout);
+cudaError_t obs_dispatch(const ObsParams& P, int np, int G, int rv, int grid, size_t smem, cudaStream_t stream,
+                         const T* w, const T* x, const T* yin, T* out, T* eout);
 
 #ifdef WB_OBS_DEFINE
 template <typename T, int MODE>
-cudaError_t obs_dispatch(const ObsParams& P, int np, int G, int grid, size_t smem, cudaStream_t stream, const T* w,
-                         const T* x, const T* yin, T* out, T* eout) {
+cudaError_t obs_dispatch(const ObsParams& P, int np, int G, int rv, int grid, size_t smem, cudaStream_t stream,
+                         const T* w, const T* x, const T* yin, T* out, T* eout) {
     cudaError_t err = cudaSuccess;
+    int bt = obs_block<T>();
     auto go = [&](auto kern) {
         if (smem > 48 * 1024) {
             err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (err != cudaSuccess) return;
         }
-        kern<<<grid, obs_block<T>(), smem, stream>>>(P, w, x, yin, out, eout);
+        kern<<<grid, bt, smem, stream>>>(P, w, x, yin, out, eout);
         err = cudaGetLastError();
     };
+    if constexpr (std::is_same<T, float>::value && MODE == OBS_GRAM) {
+        if (rv == 2) {
+            bt = obs_block<T, 2>();
+            auto wide = [&](auto gtag) {
+                constexpr int GV = decltype(gtag)::value;
+                switch (P.Q * 8 + (np < 2 ? np : 2)) {
+                    case 1 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 1, 0, 2>); break;
+                    case 2 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 2, 0, 2>); break;
+                    case 2 * 8 + 1: go(obs_pass_kernel<T, GV, MODE, 2, 1, 2>); break;
+                    case 3 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 3, 0, 2>); break;
+                    case 3 * 8 + 1: go(obs_pass_kernel<T, GV, MODE, 3, 1, 2>); break;
+                    case 3 * 8 + 2: go(obs_pass_kernel<T, GV, MODE, 3, 2, 2>); break;
+                    case 4 * 8 + 0: go(obs_pass_kernel<T, GV, MODE, 4, 0, 2>); break;
+                    case 4 * 8 + 1: go(obs_pass_kernel<T, GV, MODE, 4, 1, 2>); break;
+                    default: err = cudaErrorInvalidValue; break;  // no generic wide kernel
+                }
+            };
+            switch (G) {
+                case 1: wide(std::integral_constant<int, 1>{}); break;
+                case 2: wide(std::integral_constant<int, 2>{}); break;
+                case 4: wide(std::integral_constant<int, 4>{}); break;
+                default: err = cudaErrorInvalidValue; break;
+            }
+            return err;
+        }
+    }
+    if (rv != 1) return cudaErrorInvalidValue;
     auto by_q = [&](auto gtag) {
         constexpr int GV = decltype(gtag)::value;
         switch (P.Q * 8 + (np < 2 ? np : 2)) {

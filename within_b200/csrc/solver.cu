@@ -480,7 +480,7 @@ struct SolverImpl {
     bool split_tab[3] = {false, false, false};
     int32_t obs_choice[4][2] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}};
     DArr<unsigned char> obs_hot;  // per-block global hot tables of the observation pass
-    float obs_tune_ms[4][2][12] = {};  // the autotuner's time per candidate (0: not timed)
+    float obs_tune_ms[4][2][24] = {};  // the autotuner's time per candidate (0: not timed)
     // hottest levels of every non-primary factor, for the observation pass
     std::vector<DArr<uint32_t>> hot_level;
     std::vector<int32_t> hot_count;
@@ -866,8 +866,18 @@ int kp_class(int kp) { return kp <= 4 ? 0 : kp <= 8 ? 1 : kp <= 16 ? 2 : 3; }
 // Returns the number of per-warp partial rows written (OBS_LSMR; grid x warps per block).
 // Shapes of the observation pass: choice c < kObsShapes runs 16 << (c / 2) observations
 // per chunk and 1 + c % 2 blocks per SM with the hot tables in shared memory; choice
-// kObsShapes + c the same shape with them in per-block global copies (S.obs_hot).
+// kObsShapes + c the same shape with them in per-block global copies (S.obs_hot); choice
+// 2 kObsShapes + c the shape of c with wide lanes (8 RHS per lane; FP32, kp >= 8).
 constexpr int kObsShapes = 6;
+inline bool obs_wide_ok(int kp, size_t elem) { return elem == 4 && kp >= 8; }
+// Wide lanes exist for the exact kernels only (Q <= 3, or Q = 4 with at most one private
+// factor).
+inline bool obs_wide_exact(int Q, int np) { return Q <= 3 || (Q == 4 && np <= 1); }
+bool obs_wide_for(SolverImpl& S, int kp, size_t elem) {
+    if (!obs_wide_ok(kp, elem)) return false;
+    ObsParams P;
+    return obs_wide_exact(S.d.Q, obs_params_for(S, kp, elem, P));
+}
 
 template <typename T, int MODE>
 int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* out, T* eout,
@@ -875,12 +885,15 @@ int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* o
     ObsParams P;
     // the autotuned block shape (obs_autotune), else 32 observations per chunk, 2 blocks/SM
     int choice = S.obs_choice[kp_class(kp)][sizeof(T) == 8 ? 1 : 0];
+    int rv = (MODE == OBS_GRAM && choice >= 2 * kObsShapes && obs_wide_ok(kp, sizeof(T))) ? 2 : 1;
+    if (choice >= 0) choice %= 2 * kObsShapes;
     int np = obs_params_for(S, kp, sizeof(T), P, choice >= kObsShapes);
     if (choice >= kObsShapes && !P.hot_glob) np = obs_params_for(S, kp, sizeof(T), P);  // no global copies
+    if (!obs_wide_exact(S.d.Q, np)) rv = 1;
     choice = choice < 0 ? -1 : choice % kObsShapes;
     P.lsmr_scale = lsmr_scale;
     P.lsmr_part = lsmr_part;
-    const int G = group_for(kp);
+    const int G = group_for(kp) / rv;
     bool split = S.has_split;
     int blocks_per_sm = 2;
     if (choice >= 0) {
@@ -902,9 +915,10 @@ int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* o
         }
     }
     const size_t smem = (size_t)P.smem_elems * sizeof(T);
-    const int bt = obs_block<T>();  // two resident blocks per SM (registers and shared memory)
+    // two resident blocks per SM (registers and shared memory)
+    const int bt = rv == 2 ? obs_block<T, 2>() : obs_block<T>();
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P.nchunks * G + bt - 1) / bt, (int64_t)S.n_sm * blocks_per_sm));
-    const cudaError_t err = obs_dispatch<T, MODE>(P, np, G, grid, smem, S.stream, w, x, yin, out, eout);
+    const cudaError_t err = obs_dispatch<T, MODE>(P, np, G, rv, grid, smem, S.stream, w, x, yin, out, eout);
     WB_CUDA(err);
     S.gpu_launches++;
     return grid * (bt / 32);
@@ -934,7 +948,7 @@ void obs_autotune(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
         if (it != g_obs_tune.end()) choice = it->second;
     }
     if (choice >= 0) {  // tuned by a solver of the same class: this one's global copies
-        if (choice >= kObsShapes) grow_obs_hot(S, obs_hot_bytes(S, kp, sizeof(T)));
+        if (choice % (2 * kObsShapes) >= kObsShapes) grow_obs_hot(S, obs_hot_bytes(S, kp, sizeof(T)));
         return;
     }
     cudaEvent_t e0, e1;
@@ -946,12 +960,18 @@ void obs_autotune(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
     // allocated here, outside any stream capture)
     const size_t hot = obs_hot_bytes(S, kp, sizeof(T));
     grow_obs_hot(S, hot);
-    const int32_t nc = hot ? 2 * kObsShapes : kObsShapes;
+    std::vector<int32_t> cands;
+    const bool wide = obs_wide_for(S, kp, sizeof(T));
+    for (int32_t c = 0; c < (hot ? 2 * kObsShapes : kObsShapes); ++c) {
+        cands.push_back(c);
+        if (wide) cands.push_back(2 * kObsShapes + c);
+    }
+    const int32_t nc = (int32_t)cands.size();
     // two sweeps over the candidates, the second in reverse order; each keeps its best
     float* tms = S.obs_tune_ms[kp_class(kp)][sizeof(T) == 8 ? 1 : 0];
-    for (int32_t c = 0; c < 2 * kObsShapes; ++c) tms[c] = 0.f;
+    for (int32_t c = 0; c < 4 * kObsShapes; ++c) tms[c] = 0.f;
     for (int32_t it = 0; it < 2 * nc; ++it) {
-        const int32_t c = it < nc ? it : 2 * nc - 1 - it;
+        const int32_t c = cands[it < nc ? it : 2 * nc - 1 - it];
         choice = c;
         launch_obs<T, OBS_GRAM>(S, kp, w, x, nullptr, y, nullptr);
         WB_CUDA(cudaEventRecord(e0, S.stream));
@@ -963,10 +983,10 @@ void obs_autotune(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
         ms *= 0.5f;
         if (tms[c] == 0.f || ms < tms[c]) tms[c] = ms;
     }
-    for (int32_t c = 0; c < nc; ++c)
-        if (c == 0 || tms[c] < best) {
-            best = tms[c];
-            best_c = c;
+    for (int32_t i = 0; i < nc; ++i)
+        if (i == 0 || tms[cands[i]] < best) {
+            best = tms[cands[i]];
+            best_c = cands[i];
         }
     WB_CUDA(cudaEventDestroy(e0));
     WB_CUDA(cudaEventDestroy(e1));
@@ -3617,26 +3637,37 @@ int32_t within_solver_obs_hot_global(const within_solver* s, int32_t k, int32_t 
     const int kp = wb::pad_kp(k);
     const int32_t c = s->impl->obs_choice[wb::kp_class(kp)][elem_bytes == 8 ? 1 : 0];
     if (c < 0) return -1;
-    if (c < wb::kObsShapes) return 0;
+    if (c % (2 * wb::kObsShapes) < wb::kObsShapes) return 0;
     wb::ObsParams P;
     wb::obs_params_for(*s->impl, kp, (size_t)elem_bytes, P, true);
     return P.hot_glob ? 1 : 0;
+}
+
+int32_t within_solver_obs_rhs_per_lane(const within_solver* s, int32_t k, int32_t elem_bytes) {
+    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8)) return -1;
+    const int kp = wb::pad_kp(k);
+    const int32_t c = s->impl->obs_choice[wb::kp_class(kp)][elem_bytes == 8 ? 1 : 0];
+    if (c < 0) return -1;
+    return (c >= 2 * wb::kObsShapes && wb::obs_wide_for(*s->impl, kp, (size_t)elem_bytes)) ? 8 : 4;
 }
 
 int within_solver_obs_tune_times(const within_solver* s, int32_t k, int32_t elem_bytes, float* ms, int32_t n) {
     if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) || !ms || n < 0)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
     const float* t = s->impl->obs_tune_ms[wb::kp_class(wb::pad_kp(k))][elem_bytes == 8 ? 1 : 0];
-    for (int32_t c = 0; c < n && c < 2 * wb::kObsShapes; ++c) ms[c] = t[c];
+    for (int32_t c = 0; c < n && c < 4 * wb::kObsShapes; ++c) ms[c] = t[c];
     return 0;
 }
 
 int within_solver_set_obs_config(within_solver* s, int32_t k, int32_t elem_bytes, int32_t obs_per_chunk,
-                                 int32_t blocks_per_sm, int32_t hot_global) {
+                                 int32_t blocks_per_sm, int32_t variant) {
     if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) ||
         (obs_per_chunk != 16 && obs_per_chunk != 32 && obs_per_chunk != 64) || blocks_per_sm < 1 ||
-        blocks_per_sm > 2 || hot_global < 0 || hot_global > 1)
+        blocks_per_sm > 2 || variant < 0 || variant > 3)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
+    if ((variant & 2) && !wb::obs_wide_for(*s->impl, wb::pad_kp(k), (size_t)elem_bytes))
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "no wide lanes for this precision, RHS count and design");
+    const int32_t hot_global = variant & 1;
     wb::SolverImpl& S = *s->impl;
     std::lock_guard<std::mutex> lk(S.mu);
     return guard([&]() -> int {
@@ -3648,7 +3679,7 @@ int within_solver_set_obs_config(within_solver* s, int32_t k, int32_t elem_bytes
         }
         const int32_t ci = obs_per_chunk == 16 ? 0 : obs_per_chunk == 32 ? 1 : 2;
         S.obs_choice[wb::kp_class(kp)][elem_bytes == 8 ? 1 : 0] =
-            (hot_global ? wb::kObsShapes : 0) + 2 * ci + (blocks_per_sm - 1);
+            ((variant & 2) ? 2 * wb::kObsShapes : 0) + (hot_global ? wb::kObsShapes : 0) + 2 * ci + (blocks_per_sm - 1);
         return 0;
     });
 }
