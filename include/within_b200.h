@@ -316,6 +316,21 @@ int32_t within_solver_obs_hot_global(const within_solver *solver, int32_t k, int
  * tries both where wide lanes apply.  No counterpart in the reference. */
 int32_t within_solver_obs_rhs_per_lane(const within_solver *solver, int32_t k, int32_t elem_bytes);
 
+/* Hybrid operator apply (no counterpart in the reference; it computes the same
+ * GramianOperator::apply, operator/gramian.rs:84-89).  The blocks of G = D'WD between the
+ * factor with the most levels (primary) and the small factors held in the observation
+ * pass's lane-group tables stay implicit: one pass over the observations, with no code of
+ * any other factor read.  Every other block is a factor-pair cross-tabulation of the
+ * additive Schwarz setup, applied as CSR rows.  The autotuner times it against the
+ * observation pass once per shape class and keeps the faster.  within_solver_set_hybrid
+ * fixes the choice for k RHS in elem_bytes precision (1 builds its arrays here; outside
+ * any stream capture): WITHIN_ERR_INVALID_ARGUMENT when the solver has no additive
+ * Schwarz preconditioner, uses the assembled Gramian, or has no (or more than two) small
+ * factors.  within_solver_hybrid returns 1 (on), 0 (off) or -1 (not decided yet), with
+ * the autotuner's time per apply in *ms (0 when not timed; ms may be null). */
+int within_solver_set_hybrid(within_solver *solver, int32_t k, int32_t elem_bytes, int32_t on);
+int32_t within_solver_hybrid(const within_solver *solver, int32_t k, int32_t elem_bytes, float *ms);
+
 /* The autotuner's measured time (milliseconds per operator apply, the best of two
  * sweeps over the candidates) of each candidate shape for k RHS in elem_bytes precision:
  * ms[c] for c < n and c < 24, where c = wide * 12 + hot_global * 6 +

@@ -509,6 +509,206 @@ __global__ void __launch_bounds__(obs_block<T, RV>(), 2) obs_pass_kernel(ObsPara
     }
 }
 
+// ---------------------------------------------------------------------------
+// Hybrid operator apply, primary-major part.  G x splits into the blocks between the
+// primary factor P and the small factors S (their cross-tabulations hold one entry per
+// observation, so they stay implicit: one pass over the observations), and every block
+// that involves another factor O (small cross-tabulations, applied as CSR rows of the
+// assembled Gramian: csr_rows_kernel).  This kernel computes, per primary level p,
+//   y_P[p] = (sum_i w_i) x_P[p] + sum_i w_i sum_j x_Sj[s_j,i] + sum_e C_PO[p,e] x_O[o_e]
+// over its observations i and its C_PO entries, stored once (pieces of split levels add
+// atomically), and adds w_i x_P[p] into group-private tables of the S factors, summed
+// into y_S at the end (the S rows' other terms, D_S x_S, C_SO x_O and C_SS' x_S', come
+// from the CSR rows).  Each lane group (G lanes x 4 RHS) walks whole level-aligned chunks
+// of primary-sorted observations in aligned batches of 4 (16-byte loads of 4 codes and
+// 4 weights), with a level change the only per-observation test; no code of the primary
+// or of an O factor is read.
+// ---------------------------------------------------------------------------
+constexpr int kPrimMaxS = 2;
+
+struct PrimParams {
+    int64_t ns;                    // stride of one factor's codes
+    int32_t nsmall;                // S factors (1 or 2)
+    int32_t smem_elems;            // dynamic shared memory, elements
+    int32_t priv_stride;           // elements between consecutive lane groups' private tables
+    int64_t off_p;                 // first dof of the primary factor
+    const uint32_t* codes_s[kPrimMaxS];  // the S factors' device codes (primary-sorted)
+    int64_t off_s[kPrimMaxS];      // first dof of each S factor
+    int32_t nlev_s[kPrimMaxS];
+    int32_t priv_base[kPrimMaxS];  // offset of the factor's table inside a group's area
+    int32_t xs_base[kPrimMaxS];    // offset of the factor's staged x rows (after the private areas)
+    const ObsChunk* chunks;
+    int64_t nchunks;
+    const uint32_t* lvl_ptr;       // first observation of each primary level (+ n)
+    const int64_t* pptr;           // C_PO rows of the primary levels
+    const uint32_t* pcol;          // global dof of each entry
+};
+
+template <typename T, int G, int NS>
+__global__ void __launch_bounds__(obs_block<T>(), 2) prim_rows_kernel(PrimParams P, const T* __restrict__ w,
+                                                              const T* __restrict__ pval, const T* __restrict__ x,
+                                                              T* __restrict__ out) {
+    constexpr int KP = 4 * G;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);
+    const int gpb0 = blockDim.x / G;
+    for (int i = threadIdx.x; i < P.smem_elems; i += blockDim.x) sm[i] = T(0);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NS; ++j)  // stage the S factors' rows of x
+        for (int e = threadIdx.x; e < P.nlev_s[j] * KP; e += blockDim.x)
+            sm[P.xs_base[j] + e] = x[(size_t)P.off_s[j] * KP + e];
+    __syncthreads();
+    const int c4 = (threadIdx.x & (G - 1)) * 4;
+    const int gl = threadIdx.x / G;
+    const int64_t ngroups = (int64_t)gridDim.x * gpb0;
+    const bool weighted = w != nullptr;
+    T* const priv = sm + (size_t)gl * P.priv_stride + c4;
+    T* const out0 = out + (size_t)P.off_p * KP + c4;
+    const T* const x0 = x + (size_t)P.off_p * KP + c4;
+    // The next chunk's descriptor, first primary row, first kPrimPre C_PO gathers and
+    // first batch of codes and weights are loaded while the current chunk runs (a chunk
+    // is often one primary level of a few dozen observations: its loads would otherwise
+    // stand exposed at its start and end).
+    constexpr int kPrimPre = 4;
+    struct Pre {
+        ObsChunk C;
+        uint32_t nb;
+        bool first;
+        V4<T> xp, g[kPrimPre];
+        T v[kPrimPre];
+        int64_t e1;
+        uint4 cb[NS];
+        typename W4<T>::type wb;
+    };
+    auto prefetch = [&](int64_t c, Pre& q) {
+        q.C = P.chunks[c];
+        const uint32_t p = q.C.lvl_begin;
+        q.first = __ldg(P.lvl_ptr + p) >= q.C.obs_begin;
+        q.nb = __ldg(P.lvl_ptr + p + 1);
+        q.xp = ldg4(x0 + (size_t)p * KP);
+        const int64_t e0 = __ldg(P.pptr + p);
+        q.e1 = __ldg(P.pptr + p + 1);
+#pragma unroll
+        for (int k = 0; k < kPrimPre; ++k) {
+            const bool ok = q.first && e0 + k < q.e1;
+            const uint32_t col = ok ? __ldg(P.pcol + e0 + k) : (uint32_t)P.off_p;
+            q.v[k] = ok ? __ldg(pval + e0 + k) : T(0);
+            q.g[k] = ldg4(x + (size_t)col * KP + c4);
+        }
+        const uint32_t i0 = q.C.obs_begin;
+        const bool full = (i0 & 3u) == 0 && i0 + 4 <= q.C.obs_end;
+#pragma unroll
+        for (int j = 0; j < NS; ++j)
+            q.cb[j] = full ? __ldg(reinterpret_cast<const uint4*>(P.codes_s[j] + i0)) : make_uint4(0, 0, 0, 0);
+        q.wb = typename W4<T>::type{};
+        if (weighted && full) q.wb = load_w4v(w, i0);
+    };
+    int64_t ch = (int64_t)blockIdx.x * gpb0 + gl;
+    Pre nx;
+    if (ch < P.nchunks) prefetch(ch, nx);
+    for (; ch < P.nchunks; ch += ngroups) {
+        const Pre cu = nx;
+        if (ch + ngroups < P.nchunks) prefetch(ch + ngroups, nx);
+        const ObsChunk C = cu.C;
+        uint32_t p = C.lvl_begin;
+        uint32_t nb = cu.nb;
+        bool first = cu.first, lead = true;  // lead: the chunk's first level (prefetched C_PO)
+        V4<T> xp = cu.xp, acc(T(0));
+        T ws = T(0);
+        // level p complete (or the chunk's piece of it): its sums into y_P
+        auto finish = [&]() {
+            acc += ws * xp;
+            if (first) {
+                int64_t e = __ldg(P.pptr + p);
+                const int64_t e1 = lead ? cu.e1 : __ldg(P.pptr + p + 1);
+                if (lead) {
+#pragma unroll
+                    for (int k = 0; k < kPrimPre; ++k) acc += cu.v[k] * cu.g[k];
+                    e += kPrimPre;
+                }
+                for (; e < e1; ++e) acc += __ldg(pval + e) * ldg4(x + (size_t)__ldg(P.pcol + e) * KP + c4);
+            }
+            if (C.split) atomic_add4(out0 + (size_t)p * KP, acc);
+            else st4(out0 + (size_t)p * KP, acc);
+        };
+        // observation i with S codes s[] and weight wi; advances the level first
+        auto body = [&](uint32_t i, const uint32_t (&s)[NS], T wi) {
+            if (i == nb) {
+                finish();
+                lead = false;
+                for (++p; __ldg(P.lvl_ptr + p + 1) == i; ++p) st4(out0 + (size_t)p * KP, V4<T>(T(0)));  // empty levels
+                nb = __ldg(P.lvl_ptr + p + 1);
+                first = true;
+                xp = ldg4(x0 + (size_t)p * KP);
+                acc = V4<T>(T(0));
+                ws = T(0);
+            }
+            V4<T> xs = ld4(sm + P.xs_base[0] + (size_t)s[0] * KP + c4);
+            if (NS > 1) xs += ld4(sm + P.xs_base[NS - 1] + (size_t)s[NS - 1] * KP + c4);
+            ws += wi;
+            acc += wi * xs;
+            const V4<T> t = wi * xp;
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                T* pt = priv + P.priv_base[j] + (size_t)s[j] * KP;
+                st4(pt, ld4(pt) + t);
+            }
+        };
+        auto single = [&](uint32_t i) {
+            uint32_t s[NS];
+#pragma unroll
+            for (int j = 0; j < NS; ++j) s[j] = __ldg(P.codes_s[j] + i);
+            body(i, s, weighted ? __ldg(w + i) : T(1));
+        };
+        uint32_t i = C.obs_begin;
+        for (; i < C.obs_end && (i & 3u); ++i) single(i);
+        if (i + 4 <= C.obs_end) {
+            uint4 cb[NS];
+            typename W4<T>::type wb = cu.wb;
+#pragma unroll
+            for (int j = 0; j < NS; ++j) cb[j] = cu.cb[j];
+            if (i != C.obs_begin) {  // unaligned start: the first batch was not prefetched
+#pragma unroll
+                for (int j = 0; j < NS; ++j) cb[j] = __ldg(reinterpret_cast<const uint4*>(P.codes_s[j] + i));
+                if (weighted) wb = load_w4v(w, i);
+            }
+            for (; i + 4 <= C.obs_end; i += 4) {
+                uint4 nbk[NS];
+                typename W4<T>::type nw = wb;
+                const bool more = i + 8 <= C.obs_end;
+#pragma unroll
+                for (int j = 0; j < NS; ++j)
+                    nbk[j] = more ? __ldg(reinterpret_cast<const uint4*>(P.codes_s[j] + i + 4)) : cb[j];
+                if (weighted && more) nw = load_w4v(w, i + 4);
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    uint32_t s[NS];
+#pragma unroll
+                    for (int j = 0; j < NS; ++j) s[j] = ucomp(cb[j], b);
+                    body(i + b, s, weighted ? (T)wcomp(wb, b) : T(1));
+                }
+#pragma unroll
+                for (int j = 0; j < NS; ++j) cb[j] = nbk[j];
+                wb = nw;
+            }
+        }
+        for (; i < C.obs_end; ++i) single(i);
+        finish();
+        if (!C.split)
+            for (++p; p < C.lvl_end; ++p) st4(out0 + (size_t)p * KP, V4<T>(T(0)));  // trailing empty levels
+    }
+    __syncthreads();
+    // the lane groups' tables into y_S: one atomic per nonzero entry
+#pragma unroll
+    for (int j = 0; j < NS; ++j)
+        for (int e = threadIdx.x; e < P.nlev_s[j] * KP; e += blockDim.x) {
+            T v = T(0);
+            for (int g = 0; g < gpb0; ++g) v += sm[(size_t)g * P.priv_stride + P.priv_base[j] + e];
+            if (v != T(0)) atomicAdd(out + (size_t)P.off_s[j] * KP + e, v);
+        }
+}
+
 // Column-major (RHS-major) user order <-> interleaved primary-sorted order with kp
 // columns (padding columns are zero).  perm[i] = user index of sorted row i (or identity).
 // Each warp transposes tiles of 32 rows through its own shared-memory tile (32 x kp+1):

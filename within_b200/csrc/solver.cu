@@ -453,6 +453,26 @@ inline int resident_per_sm(const void* kern) {
     return n;
 }
 
+// Device arrays of the hybrid operator apply (prim_rows_kernel + CSR rows; see
+// build_hybrid): the C_PO entries of every primary level, and the Gramian rows of the
+// other factors' dofs.  Built for one set of small factors (smask: bits of design
+// factors).
+struct HybridDev {
+    uint32_t smask = 0;
+    DArr<uint32_t> lvl_ptr;  // primary level -> first observation in device order (+ n)
+    DArr<int64_t> pptr;      // C_PO rows of the primary levels
+    DArr<uint32_t> pcol;
+    DArr<double> pval64;
+    DArr<float> pval32;
+    DArr<uint32_t> rows;     // dofs of the other rows
+    DArr<int64_t> optr;
+    DArr<uint32_t> ocol;
+    DArr<double> oval64;
+    DArr<float> oval32;
+    DArr<CsrChunk> ochunks;
+    int64_t nochunks = 0, nnz = 0;
+};
+
 struct SolverImpl {
     std::mutex mu;
     Design d;
@@ -481,6 +501,12 @@ struct SolverImpl {
     int32_t obs_choice[4][2] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}};
     DArr<unsigned char> obs_hot;  // per-block global hot tables of the observation pass
     float obs_tune_ms[4][2][24] = {};  // the autotuner's time per candidate (0: not timed)
+    // hybrid operator apply: per (kp class, precision) -1 not decided, 0 off, 1 on (the
+    // autotuner's choice), its timed apply (ms; 0 not timed), and its arrays
+    int32_t hyb_on[4][2] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}};
+    float hyb_ms[4][2] = {};
+    std::unique_ptr<HybridDev> hyb;
+    std::vector<int64_t> lvl_ptr_h;  // primary level -> first observation (device order)
     // hottest levels of every non-primary factor, for the observation pass
     std::vector<DArr<uint32_t>> hot_level;
     std::vector<int32_t> hot_count;
@@ -741,6 +767,7 @@ void upload_design(SolverImpl& S) {
     }
     auto ch = make_obs_chunks(lvl_ptr, np, S.has_split);
     S.chunks.upload(ch);
+    S.lvl_ptr_h = lvl_ptr;
     for (int ci = 0; ci < 3; ++ci) {
         const int64_t per = (int64_t)16 << ci;
         auto t = make_obs_chunks(lvl_ptr, np, S.split_tab[ci], per);
@@ -924,6 +951,221 @@ int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* o
     return grid * (bt / 32);
 }
 
+// ---- hybrid operator apply ----
+// G x = D'W D x splits by blocks of factor pairs.  The blocks between the primary factor
+// P and the small factors S (those whose lane-group tables fit the observation pass's
+// shared memory; their cross-tabulations have one entry per observation) stay implicit:
+// prim_rows_kernel walks the observations.  Every other block is a cross-tabulation
+// that the Schwarz setup already built (factor_pairs.rs:63-304, cross_tab.rs:514-664),
+// much smaller than the observations, and is applied as CSR rows: the C_PO entries of
+// each primary level inside prim_rows_kernel, and the rows of the other factors' dofs
+// (their diagonal, C_OP, C_OO', C_OS, and for the S dofs D_S, C_SO, C_SS') by
+// csr_rows_kernel.  Same sums as D'W D x up to the order of the additions.
+
+// Design factors in the private tables of the pass for kp RHS of `elem` bytes, as a
+// bit mask (0: none, or more than kPrimMaxS); np = their count.
+uint32_t hybrid_smask(SolverImpl& S, int kp, size_t elem, int& np) {
+    ObsParams P;
+    np = obs_params_for(S, kp, elem, P);
+    uint32_t m = 0;
+    for (int sl = 1; sl < S.d.Q; ++sl)
+        if (P.sink[sl] == SINK_PRIVATE) m |= 1u << S.dev_factor[sl];
+    return (np >= 1 && np <= kPrimMaxS) ? m : 0u;
+}
+
+// The hybrid apply needs the factor-pair cross-tabulations of an additive Schwarz
+// preconditioner (every pair of factors is a subdomain set) and the implicit operator.
+bool hybrid_possible(const SolverImpl& S) {
+    return !S.explicit_op && !S.precond_only && S.pc.kind == 1 && !S.subs.empty() && S.d.n > 0 && S.d.Q >= 2 &&
+           S.d.n < ((int64_t)1 << 32);
+}
+
+void build_hybrid(SolverImpl& S, uint32_t smask) {
+    const Design& d = S.d;
+    const int P = S.primary;
+    const int64_t nP = d.nlev[P], offP = d.off[P], m = d.ndofs;
+    auto small = [&](int f) { return ((smask >> f) & 1u) != 0; };
+    // each non-primary factor's diagonal comes from the first pair (in subdomain order)
+    // that holds it: its levels are spread over that pair's components
+    std::vector<int64_t> dsrc((size_t)d.Q, -1);
+    for (const Subdomain& sd : S.subs)
+        for (int f : {sd.q, sd.r})
+            if (f != P && dsrc[f] < 0) dsrc[f] = (int64_t)sd.q * d.Q + sd.r;
+    std::vector<int64_t> pcnt((size_t)nP + 1, 0), ocnt((size_t)m + 1, 0);
+    std::vector<uint32_t> pcol, ocol;
+    std::vector<double> pval, oval;
+    // two passes: count the entries of every row, then place them
+    for (int pass = 0; pass < 2; ++pass) {
+        auto emit = [&](uint32_t row, uint32_t col, double v) {
+            if ((int64_t)row >= offP && (int64_t)row < offP + nP) {
+                const int64_t l = (int64_t)row - offP;
+                if (pass == 0) { pcnt[l + 1]++; return; }
+                const int64_t at = pcnt[l]++;
+                pcol[at] = col;
+                pval[at] = v;
+            } else {
+                if (pass == 0) { ocnt[row + 1]++; return; }
+                const int64_t at = ocnt[row]++;
+                ocol[at] = col;
+                oval[at] = v;
+            }
+        };
+        for (const Subdomain& sd : S.subs) {
+            const int nq = sd.n_q();
+            const bool implicit = (sd.q == P && small(sd.r)) || (sd.r == P && small(sd.q));
+            if (!implicit) {
+                const Csr& c = sd.ct.c;
+                for (int32_t a = 0; a < c.nrows; ++a)
+                    for (uint32_t e = c.ptr[a]; e < c.ptr[a + 1]; ++e) {
+                        const uint32_t gq = sd.gidx[a], gr = sd.gidx[nq + c.idx[e]];
+                        emit(gq, gr, c.val[e]);
+                        emit(gr, gq, c.val[e]);
+                    }
+            }
+            const int64_t pair = (int64_t)sd.q * d.Q + sd.r;
+            if (sd.q != P && dsrc[sd.q] == pair)
+                for (int32_t a = 0; a < nq; ++a) emit(sd.gidx[a], sd.gidx[a], sd.ct.dq[a]);
+            if (sd.r != P && dsrc[sd.r] == pair)
+                for (int32_t b = 0; b < sd.n_r(); ++b) emit(sd.gidx[nq + b], sd.gidx[nq + b], sd.ct.dr[b]);
+        }
+        if (pass == 0) {
+            for (int64_t l = 0; l < nP; ++l) pcnt[l + 1] += pcnt[l];
+            for (int64_t r = 0; r < m; ++r) ocnt[r + 1] += ocnt[r];
+            pcol.resize((size_t)pcnt[nP]);
+            pval.resize((size_t)pcnt[nP]);
+            ocol.resize((size_t)ocnt[m]);
+            oval.resize((size_t)ocnt[m]);
+        } else {  // the cursors ended at the next row's start: shift back
+            for (int64_t l = nP; l > 0; --l) pcnt[l] = pcnt[l - 1];
+            pcnt[0] = 0;
+            for (int64_t r = m; r > 0; --r) ocnt[r] = ocnt[r - 1];
+            ocnt[0] = 0;
+        }
+    }
+    // columns ascending within each row (fixed summation order)
+    auto sort_rows = [&](const std::vector<int64_t>& ptr, std::vector<uint32_t>& col, std::vector<double>& val,
+                         int64_t nrows) {
+        const int64_t tasks = std::min<int64_t>(64, std::max<int64_t>(1, nrows / 4096));
+        parallel_tasks((size_t)tasks, [&](size_t t) {
+            std::vector<std::pair<uint32_t, double>> tmp;
+            for (int64_t r = nrows * (int64_t)t / tasks; r < nrows * ((int64_t)t + 1) / tasks; ++r) {
+                const int64_t a = ptr[r], b = ptr[r + 1];
+                if (b - a < 2) continue;
+                tmp.clear();
+                for (int64_t e = a; e < b; ++e) tmp.emplace_back(col[e], val[e]);
+                std::sort(tmp.begin(), tmp.end());
+                for (int64_t e = a; e < b; ++e) col[e] = tmp[e - a].first, val[e] = tmp[e - a].second;
+            }
+        });
+    };
+    sort_rows(pcnt, pcol, pval, nP);
+    sort_rows(ocnt, ocol, oval, m);
+    // the non-empty other rows, compacted
+    std::vector<uint32_t> rows;
+    std::vector<int64_t> optr(1, 0);
+    for (int64_t r = 0; r < m; ++r)
+        if (ocnt[r + 1] > ocnt[r]) {
+            rows.push_back((uint32_t)r);
+            optr.push_back(ocnt[r + 1]);
+        }
+    auto H = std::make_unique<HybridDev>();
+    H->smask = smask;
+    std::vector<uint32_t> lp(S.lvl_ptr_h.begin(), S.lvl_ptr_h.end());
+    H->lvl_ptr.upload(lp);
+    H->pptr.upload(pcnt);
+    H->pcol.upload(pcol);
+    H->pval64.upload(pval);
+    if (S.mixed()) H->pval32.upload_cast(pval);
+    H->rows.upload(rows);
+    H->optr.upload(optr);
+    H->ocol.upload(ocol);
+    H->oval64.upload(oval);
+    if (S.mixed()) H->oval32.upload_cast(oval);
+    const std::vector<CsrChunk> ch = make_chunks(optr, 0, (int64_t)rows.size(), 256, 1, true);
+    H->ochunks.upload(ch);
+    H->nochunks = (int64_t)ch.size();
+    H->nnz = (int64_t)pcol.size() + (int64_t)ocol.size();
+    if (S.cg_exec) {  // a captured CG iteration may hold the old arrays
+        WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
+        S.cg_exec = nullptr;
+    }
+    S.hyb = std::move(H);
+}
+
+template <typename T> const T* hyb_pval(const HybridDev& H);
+template <> const double* hyb_pval<double>(const HybridDev& H) { return H.pval64.p; }
+template <> const float* hyb_pval<float>(const HybridDev& H) { return H.pval32.p; }
+template <typename T> const T* hyb_oval(const HybridDev& H);
+template <> const double* hyb_oval<double>(const HybridDev& H) { return H.oval64.p; }
+template <> const float* hyb_oval<float>(const HybridDev& H) { return H.oval32.p; }
+
+// y = G x by the hybrid apply (S.hyb built for the pass's small factors at this kp and
+// precision): zero the accumulated outputs, the primary-major pass, then the other rows.
+template <typename T>
+void launch_hybrid(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
+    const HybridDev& H = *S.hyb;
+    ObsParams O;
+    const int np = obs_params_for(S, kp, sizeof(T), O);
+    const int G = group_for(kp);
+    const int ci = 1;  // 32 observations per chunk
+    PrimParams P{};
+    P.ns = O.ns;
+    P.nsmall = np;
+    P.priv_stride = O.priv_stride;
+    P.off_p = S.d.off[S.primary];
+    const int64_t gpb = obs_block<T>() / G;
+    int64_t used = gpb * O.priv_stride;
+    int j = 0;
+    for (int sl = 1; sl < S.d.Q; ++sl) {
+        if (O.sink[sl] != SINK_PRIVATE) continue;
+        P.codes_s[j] = S.codes.p + (size_t)sl * O.ns;
+        P.off_s[j] = O.off[sl];
+        P.nlev_s[j] = (int32_t)S.d.nlev[S.dev_factor[sl]];
+        P.priv_base[j] = O.smem_base[sl];
+        used = (used + 3) / 4 * 4;
+        P.xs_base[j] = (int32_t)used;
+        used += (int64_t)P.nlev_s[j] * kp;
+        ++j;
+    }
+    P.smem_elems = (int32_t)used;
+    P.chunks = S.chunk_tab[ci].p;
+    P.nchunks = S.nchunk_tab[ci];
+    P.lvl_ptr = H.lvl_ptr.p;
+    P.pptr = H.pptr.p;
+    P.pcol = H.pcol.p;
+    const bool split = S.split_tab[ci];
+    const size_t mrow = (size_t)S.d.ndofs;
+    if (split) {
+        WB_CUDA(cudaMemsetAsync(y, 0, mrow * kp * sizeof(T), S.stream));
+    } else {  // every row but the primary factor's is accumulated
+        const size_t a = (size_t)P.off_p * kp, b = (size_t)(P.off_p + S.d.nlev[S.primary]) * kp;
+        if (a > 0) WB_CUDA(cudaMemsetAsync(y, 0, a * sizeof(T), S.stream));
+        if (mrow * kp > b) WB_CUDA(cudaMemsetAsync(y + b, 0, (mrow * kp - b) * sizeof(T), S.stream));
+    }
+    const size_t smem = (size_t)used * sizeof(T);
+    const int bt = obs_block<T>();
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((P.nchunks * G + bt - 1) / bt, (int64_t)S.n_sm * 2));
+    auto go = [&](auto kern) {
+        if (smem > 48 * 1024) WB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, bt, smem, S.stream>>>(P, w, hyb_pval<T>(H), x, y);
+    };
+    WB_DISPATCH_G(G, {
+        if (np == 1) go(prim_rows_kernel<T, GV, 1>);
+        else go(prim_rows_kernel<T, GV, 2>);
+    });
+    WB_CUDA(cudaGetLastError());
+    if (H.nochunks > 0) {
+        const int64_t need = (H.nochunks * 32 + kBlock - 1) / kBlock;  // one warp per chunk
+        WB_DISPATCH_G(G, {
+            auto kern = csr_rows_kernel<T, GV, EPI_ACC>;
+            kern<<<S.fit(need, (const void*)kern), kBlock, 0, S.stream>>>(H.ochunks.p, H.nochunks, H.rows.p, H.optr.p,
+                                                                          H.ocol.p, hyb_oval<T>(H), nullptr, x, y, kp);
+        });
+        WB_CUDA(cudaGetLastError());
+    }
+    S.gpu_launches += 2;
+}
+
 // Autotuner of the observation pass's block shape (the dominant kernel): the first time a
 // solver needs the pass for kp RHS in a precision, each candidate (16, 32 or 64
 // observations per chunk; 1 or 2 resident blocks per SM) runs twice on the solver's own
@@ -934,6 +1176,63 @@ int launch_obs(SolverImpl& S, int kp, const T* w, const T* x, const T* yin, T* o
 // capture; x is read and y overwritten.
 std::mutex g_obs_tune_mu;
 std::map<std::array<int64_t, 4>, int32_t> g_obs_tune;
+std::map<std::array<int64_t, 4>, int32_t> g_hyb_tune;  // same classes: hybrid apply on (1) or off (0)
+
+bool hybrid_in_use(const SolverImpl& S) {
+    for (const auto& c : S.hyb_on)
+        for (int32_t v : c)
+            if (v == 1) return true;
+    return false;
+}
+
+// Whether the operator apply for kp RHS in T runs as the hybrid apply: decided once per
+// shape class by timing it against the tuned observation pass (`best_ms`; < 0: take the
+// class's cached decision).  x is read and y overwritten.
+template <typename T>
+void hybrid_decide(SolverImpl& S, int kp, const T* w, const T* x, T* y, float best_ms,
+                   const std::array<int64_t, 4>& key) {
+    int32_t& on = S.hyb_on[kp_class(kp)][sizeof(T) == 8 ? 1 : 0];
+    if (on >= 0) return;
+    on = 0;
+    int np = 0;
+    const uint32_t smask = hybrid_possible(S) ? hybrid_smask(S, kp, sizeof(T), np) : 0u;
+    if (smask == 0) return;
+    int32_t cached = -1;
+    {
+        std::lock_guard<std::mutex> lk(g_obs_tune_mu);
+        const auto it = g_hyb_tune.find(key);
+        if (it != g_hyb_tune.end()) cached = it->second;
+    }
+    if (best_ms < 0.f && cached == 0) return;
+    if (S.hyb && S.hyb->smask != smask && hybrid_in_use(S)) return;  // one set of arrays per solver
+    if (!S.hyb || S.hyb->smask != smask) build_hybrid(S, smask);
+    if (best_ms < 0.f && cached == 1) {
+        on = 1;
+        return;
+    }
+    cudaEvent_t e0, e1;
+    WB_CUDA(cudaEventCreate(&e0));
+    WB_CUDA(cudaEventCreate(&e1));
+    float ms_best = 0.f;
+    for (int sweep = 0; sweep < 2; ++sweep) {
+        launch_hybrid<T>(S, kp, w, x, y);
+        WB_CUDA(cudaEventRecord(e0, S.stream));
+        for (int rep = 0; rep < 2; ++rep) launch_hybrid<T>(S, kp, w, x, y);
+        WB_CUDA(cudaEventRecord(e1, S.stream));
+        WB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        WB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        ms *= 0.5f;
+        if (sweep == 0 || ms < ms_best) ms_best = ms;
+    }
+    WB_CUDA(cudaEventDestroy(e0));
+    WB_CUDA(cudaEventDestroy(e1));
+    S.hyb_ms[kp_class(kp)][sizeof(T) == 8 ? 1 : 0] = ms_best;
+    on = (best_ms < 0.f || ms_best < best_ms) ? 1 : 0;
+    if (!on && !hybrid_in_use(S)) S.hyb.reset();
+    std::lock_guard<std::mutex> lk(g_obs_tune_mu);
+    g_hyb_tune.emplace(key, on);
+}
 
 template <typename T>
 void obs_autotune(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
@@ -949,6 +1248,7 @@ void obs_autotune(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
     }
     if (choice >= 0) {  // tuned by a solver of the same class: this one's global copies
         if (choice % (2 * kObsShapes) >= kObsShapes) grow_obs_hot(S, obs_hot_bytes(S, kp, sizeof(T)));
+        hybrid_decide<T>(S, kp, w, x, y, -1.f, key);
         return;
     }
     cudaEvent_t e0, e1;
@@ -991,8 +1291,11 @@ void obs_autotune(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
     WB_CUDA(cudaEventDestroy(e0));
     WB_CUDA(cudaEventDestroy(e1));
     choice = best_c;
-    std::lock_guard<std::mutex> lk(g_obs_tune_mu);
-    g_obs_tune.emplace(key, best_c);
+    {
+        std::lock_guard<std::mutex> lk(g_obs_tune_mu);
+        g_obs_tune.emplace(key, best_c);
+    }
+    hybrid_decide<T>(S, kp, w, x, y, best, key);
 }
 
 // Dot partials over rows (at most 2 blocks per SM: few partials to reduce).
@@ -1087,6 +1390,10 @@ void launch_gram_acc(SolverImpl& S, int kp, const T* x, T* y);
 template <typename T>
 void launch_gram(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
     if (!S.explicit_op) {
+        if (S.hyb_on[kp_class(kp)][sizeof(T) == 8 ? 1 : 0] == 1 && S.hyb) {
+            launch_hybrid<T>(S, kp, w, x, y);
+            return;
+        }
         launch_obs<T, OBS_GRAM>(S, kp, w, x, nullptr, y, nullptr);
         return;
     }
@@ -3649,6 +3956,46 @@ int32_t within_solver_obs_rhs_per_lane(const within_solver* s, int32_t k, int32_
     const int32_t c = s->impl->obs_choice[wb::kp_class(kp)][elem_bytes == 8 ? 1 : 0];
     if (c < 0) return -1;
     return (c >= 2 * wb::kObsShapes && wb::obs_wide_for(*s->impl, kp, (size_t)elem_bytes)) ? 8 : 4;
+}
+
+int within_solver_set_hybrid(within_solver* s, int32_t k, int32_t elem_bytes, int32_t on) {
+    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) || on < 0 || on > 1)
+        return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
+    wb::SolverImpl& S = *s->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    return guard([&]() -> int {
+        const int kp = wb::pad_kp(k);
+        if (elem_bytes == 4 && !S.mixed())
+            return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the solver has no FP32 operator");
+        int np = 0;
+        const uint32_t smask = (on && wb::hybrid_possible(S)) ? wb::hybrid_smask(S, kp, (size_t)elem_bytes, np) : 0u;
+        if (on && smask == 0)
+            return wb::fail(WITHIN_ERR_INVALID_ARGUMENT,
+                            "no hybrid operator apply for this solver (it needs an additive Schwarz preconditioner, "
+                            "the implicit operator, and one or two factors in lane-group tables)");
+        int32_t& cur = S.hyb_on[wb::kp_class(kp)][elem_bytes == 8 ? 1 : 0];
+        if (on) {
+            if (S.hyb && S.hyb->smask != smask) {
+                cur = 0;
+                if (wb::hybrid_in_use(S))
+                    return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the hybrid apply is in use with other small factors");
+            }
+            if (!S.hyb || S.hyb->smask != smask) wb::build_hybrid(S, smask);
+        }
+        cur = on;
+        if (S.cg_exec) {  // the captured CG iteration holds the old operator
+            WB_CUDA(cudaGraphExecDestroy(S.cg_exec));
+            S.cg_exec = nullptr;
+        }
+        return 0;
+    });
+}
+
+int32_t within_solver_hybrid(const within_solver* s, int32_t k, int32_t elem_bytes, float* ms) {
+    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8)) return -1;
+    const int c = wb::kp_class(wb::pad_kp(k)), e = elem_bytes == 8 ? 1 : 0;
+    if (ms) *ms = s->impl->hyb_ms[c][e];
+    return s->impl->hyb_on[c][e];
 }
 
 int within_solver_obs_tune_times(const within_solver* s, int32_t k, int32_t elem_bytes, float* ms, int32_t n) {
