@@ -44,6 +44,17 @@ TRAFFIC = {("fp32", 0): (230_120_000, "ncu dram__bytes_read+write of one launch 
                                        "10M (profiles/obs_pass_dram_traffic_5Mobs_16rhs.md); not measured by this run")}
 
 
+# The same for the hybrid operator apply (both of its kernels, one apply), per precision:
+# captures at 5M observations (prim_rows_kernel + the csr_rows_kernel launch that follows
+# it), x2 for 10M (observations, levels and cross-tabulation entries all double)
+TRAFFIC_HYB = {"fp32": (221_400_000, "ncu dram__bytes_read+write of one hybrid apply at 5M observations "
+                                     "(prim_rows_kernel 73.6 MB + csr_rows_kernel 37.1 MB), x2 for 10M "
+                                     "(profiles/hybrid_apply_dram_traffic_5Mobs_16rhs.md); not measured by this run"),
+               "fp64": (382_300_000, "ncu dram__bytes_read+write of one hybrid apply at 5M observations "
+                                     "(prim_rows_kernel 127.1 MB + csr_rows_kernel 64.0 MB), x2 for 10M "
+                                     "(profiles/hybrid_apply_dram_traffic_5Mobs_16rhs.md); not measured by this run")}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -291,6 +302,33 @@ def obs_kernel_name(L, solver, k, elem):
     return "obs_pass_kernel (operator apply D'W(D x), %s; %d observations per chunk, %d blocks per SM, " \
            "hot-level tables in %s)" % ("FP32" if elem == 4 else "FP64", per.value, bps.value,
                                        "per-block global copies" if hot == 1 else "shared memory")
+
+
+def operator_roofline(L, solver, kt, which, k, s_b, implicit_bytes, peak, peak_src, full_size):
+    """Roofline of the operator apply the solver's autotuner chose for k RHS in s_b-byte
+    precision: the hybrid apply (its own algorithmic bytes, with the observation pass's
+    byte count over the same time beside it) or the observation pass."""
+    prec = "fp32" if s_b == 4 else "fp64"
+    if L.within_solver_hybrid(solver._h, k, s_b, None) == 1:
+        hb = int(L.within_solver_hybrid_bytes(solver._h, k, s_b))
+        rf = op_roofline(kt, which, hb, peak, peak_src,
+                         "hybrid operator apply (%s): prim_rows_kernel (primary x small-factor blocks over the "
+                         "observations) + csr_rows_kernel (rows of the other blocks)" % prec.upper())
+        cnt, ms = kt[which]
+        if cnt:
+            ach = implicit_bytes / (ms / cnt / 1000.0) / 1e9
+            rf["observation_pass_bytes"] = {"algorithmic_bytes_per_launch": int(implicit_bytes), "achieved": ach,
+                                            "frac": ach / peak,
+                                            "note": "the observation pass's byte count n(4Q+s w)+2 s m kp over the "
+                                                    "same time (the work both compute)"}
+        tr = TRAFFIC_HYB.get(prec) if full_size else None
+    else:
+        rf = op_roofline(kt, which, implicit_bytes, peak, peak_src, obs_kernel_name(L, solver, k, s_b))
+        tr = TRAFFIC.get((prec, L.within_solver_obs_hot_global(solver._h, k, s_b))) if full_size else None
+    rf["traffic"] = tr[0] if tr else None
+    if tr:
+        rf["traffic_source"] = tr[1]
+    return rf
 
 
 def op_roofline(kt, which, op_bytes, peak, peak_src, kernel):
@@ -552,8 +590,8 @@ def ours(args):
 
     which = 1 if (args.precision == "mixed" and args.krylov == "cg") else 0
     s_b = 4 if which == 1 else 8
-    roofline = op_roofline(kt, which, obs_bytes(s_b), peak, peak_src, obs_kernel_name(L, solver, k, s_b))
-    roofline["traffic"] = None
+    full_size = abs(args.scale - 1.0) < 1e-9 and not args.shuffle and args.krylov == "cg"
+    roofline = operator_roofline(L, solver, kt, which, k, s_b, obs_bytes(s_b), peak, peak_src, full_size)
     sch_bytes = int(L.within_solver_schwarz_bytes(solver._h, kp, s_b))
     scnt, sms = kt[which + 2]
     roofline["schwarz_apply"] = {
@@ -576,13 +614,6 @@ def ours(args):
         rf["schwarz_apply"] = roofline["schwarz_apply"]
         roofline = rf
         roofline["traffic"] = None
-    elif abs(args.scale - 1.0) < 1e-9 and not args.shuffle and args.krylov == "cg":
-        # DRAM bytes (dram__bytes_read.sum + write.sum) of one launch of this kernel on this
-        # workload, from an ncu capture (not measured by this run)
-        tr = TRAFFIC.get(("fp32" if which == 1 else "fp64", L.within_solver_obs_hot_global(solver._h, k, s_b)))
-        if tr:
-            roofline["traffic"] = tr[0]
-            roofline["traffic_source"] = tr[1]
 
     line = {"metric": METRIC, "value": value, "unit": "RHS/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
@@ -613,15 +644,13 @@ def ours(args):
                                                             st, None))
 
         kt64 = profile_step(L, d64, d64_step)
-        rf64 = op_roofline(kt64, 0, obs_bytes(8), peak, peak_src, obs_kernel_name(L, d64, k, 8))
+        rf64 = operator_roofline(L, d64, kt64, 0, k, 8, obs_bytes(8), peak, peak_src,
+                                 abs(args.scale - 1.0) < 1e-9 and not args.shuffle)
         s64 = int(L.within_solver_schwarz_bytes(d64._h, kp, 8))
         c64, m64 = kt64[2]
         rf64["schwarz_apply"] = {"algorithmic_bytes_per_apply": s64, "avg_us": 1000.0 * m64 / c64 if c64 else None,
                                  "achieved": s64 / (m64 / c64 / 1000.0) / 1e9 if c64 else None, "unit": "GB/s",
                                  "frac": s64 / (m64 / c64 / 1000.0) / 1e9 / peak if c64 else None}
-        tr64 = TRAFFIC.get(("fp64", L.within_solver_obs_hot_global(d64._h, k, 8)))
-        if abs(args.scale - 1.0) < 1e-9 and not args.shuffle and tr64:
-            rf64["traffic"], rf64["traffic_source"] = tr64
         line["fp64_dropin"] = {"value": world * k / (d_ms / 1000.0), "unit": "RHS/s", "ms_per_step": d_ms,
                                "converged": all(bool(st[c].converged) for c in range(k)),
                                "max_final_residual": max(float(st[c].final_residual) for c in range(k)),

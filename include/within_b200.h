@@ -330,6 +330,12 @@ int32_t within_solver_obs_rhs_per_lane(const within_solver *solver, int32_t k, i
  * the autotuner's time per apply in *ms (0 when not timed; ms may be null). */
 int within_solver_set_hybrid(within_solver *solver, int32_t k, int32_t elem_bytes, int32_t on);
 int32_t within_solver_hybrid(const within_solver *solver, int32_t k, int32_t elem_bytes, float *ms);
+/* Algorithmic bytes of one hybrid apply for k RHS of elem_bytes per element (0 when the
+ * solver holds no hybrid arrays): the small factors' codes and the weights once per
+ * observation, the CSR entries (column 4 bytes, value elem_bytes) of the primary levels'
+ * C_PO rows and of the other rows, their row pointers, and x read and y written once
+ * (2 elem_bytes n_dofs kp). */
+int64_t within_solver_hybrid_bytes(const within_solver *solver, int32_t k, int32_t elem_bytes);
 
 /* The autotuner's measured time (milliseconds per operator apply, the best of two
  * sweeps over the candidates) of each candidate shape for k RHS in elem_bytes precision:

@@ -75,7 +75,7 @@ EXPORTED = [
     "within_coarse_net_params", "within_solver_set_coarse_net", "within_solver_set_coarse_basis",
     "within_solver_clear_coarse", "within_solver_coarse_basis", "within_solver_set_coarse_targets",
     "within_coarse_net_grad", "within_solver_release_coarse_training", "within_solver_inject_sweep_timeout", "within_solver_set_sweep_cluster",
-    "within_solver_obs_config", "within_solver_obs_hot_global", "within_solver_obs_rhs_per_lane", "within_solver_set_hybrid", "within_solver_hybrid", "within_solver_set_obs_config",
+    "within_solver_obs_config", "within_solver_obs_hot_global", "within_solver_obs_rhs_per_lane", "within_solver_set_hybrid", "within_solver_hybrid", "within_solver_hybrid_bytes", "within_solver_set_obs_config",
     "within_solver_obs_tune_times",
 ]
 
@@ -168,6 +168,8 @@ def load():
     L.within_solver_set_hybrid.restype = C.c_int
     L.within_solver_hybrid.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_float)]
     L.within_solver_hybrid.restype = C.c_int32
+    L.within_solver_hybrid_bytes.argtypes = [vp, C.c_int32, C.c_int32]
+    L.within_solver_hybrid_bytes.restype = C.c_int64
     L.within_solver_set_obs_config.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.within_solver_set_obs_config.restype = C.c_int
     L.within_solver_obs_tune_times.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_float), C.c_int32]

@@ -3998,6 +3998,16 @@ int32_t within_solver_hybrid(const within_solver* s, int32_t k, int32_t elem_byt
     return s->impl->hyb_on[c][e];
 }
 
+int64_t within_solver_hybrid_bytes(const within_solver* s, int32_t k, int32_t elem_bytes) {
+    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) || !s->impl->hyb) return 0;
+    const wb::SolverImpl& S = *s->impl;
+    const wb::HybridDev& H = *S.hyb;
+    const int64_t e = elem_bytes, kp = wb::pad_kp(k), nP = S.d.nlev[S.primary];
+    const int64_t ns = __builtin_popcount(H.smask), wt = S.d.w.empty() ? 0 : 1;
+    return S.d.n * (4 * ns + e * wt) + (int64_t)(H.pcol.n + H.ocol.n) * (4 + e) + (nP + 1) * (8 + 4) +
+           (int64_t)H.rows.n * (4 + 8) + 2 * e * S.d.ndofs * kp;
+}
+
 int within_solver_obs_tune_times(const within_solver* s, int32_t k, int32_t elem_bytes, float* ms, int32_t n) {
     if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) || !ms || n < 0)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
