@@ -118,7 +118,10 @@ int within_solver_solve(within_solver *solver, const double *y, double *x, doubl
                         within_solve_stats *stats);
 
 /* Solver::solve_batch: ys (n_obs*k, RHS-major), x (n_dofs*k), demeaned (n_obs*k) host
- * buffers; stats has k entries; time_total of entry 0 is the batch total. */
+ * buffers; stats has k entries; time_total of entry 0 is the batch total.  Calls on one
+ * solver from several host threads are safe: each call has its own device buffers and
+ * copy stream, the solves take turns, and a call's upload and download overlap the other
+ * calls' solves (pinned host buffers make the copies asynchronous). */
 int within_solver_solve_batch(within_solver *solver, const double *ys, size_t k, double *x,
                               double *demeaned, within_solve_stats *stats);
 

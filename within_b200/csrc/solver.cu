@@ -437,6 +437,33 @@ struct Workspace {
     DArr<int32_t> sweep_err;                 // set when a barrier wait ran out
 };
 
+// The active-RHS count into the host's pinned status word, written by a kernel rather than
+// copied: a copy would wait in the copy engine's queue behind bulk transfers of other
+// calls (host-buffer solves overlap their uploads and downloads with other solves).
+__global__ void publish_active_kernel(const int32_t* __restrict__ n_active, volatile int32_t* host) {
+    *host = *n_active;
+    __threadfence_system();
+}
+
+// Small device-to-host reads of the solve loop (flags, per-RHS counters, partial sums)
+// go the same way: a kernel stores them into pinned host staging memory.
+__global__ void d2h_words_kernel(const uint32_t* __restrict__ src, volatile uint32_t* dst, size_t nwords) {
+    for (size_t i = threadIdx.x; i < nwords; i += blockDim.x) dst[i] = src[i];
+    __threadfence_system();
+}
+
+// Small host-to-device writes (per-RHS masks and tolerances, at most 32 each) travel as
+// kernel arguments, for the same reason.
+struct SmallI32 { int32_t v[32]; };
+struct SmallF64 { double v[32]; };
+__global__ void set_small_kernel(SmallI32 a, int32_t* __restrict__ da, SmallF64 b, double* __restrict__ db, int n) {
+    const int t = threadIdx.x;
+    if (t < n) {
+        if (da) da[t] = a.v[t];
+        if (db) db[t] = b.v[t];
+    }
+}
+
 // Resident blocks per SM of `kern` at kBlock threads without dynamic shared memory,
 // queried once per kernel (the instantiations of one template differ in registers, so
 // the count is kept per kernel, not per signature).
@@ -471,6 +498,16 @@ struct HybridDev {
     DArr<float> oval32;
     DArr<CsrChunk> ochunks;
     int64_t nochunks = 0, nnz = 0;
+};
+
+// Device buffers of one host-buffer solve (its inputs, outputs and copy stream).
+struct HostCall {
+    DArr<double> y, x, dem;
+    cudaStream_t stream = nullptr;
+    bool busy = false;
+    ~HostCall() {
+        if (stream) cudaStreamDestroy(stream);
+    }
 };
 
 struct SolverImpl {
@@ -529,7 +566,10 @@ struct SolverImpl {
     DArr<CsrChunk> g_chunks;
     int64_t g_nchunks = 0;
     Workspace ws;
-    DArr<double> host_y, host_x, host_dem;  // device side of the host-buffer entry points
+    // device side of the host-buffer entry points: one slot per call in flight (calls from
+    // several host threads upload and download concurrently; their solves take turns)
+    std::mutex calls_mu;
+    std::vector<std::unique_ptr<HostCall>> calls;
     std::shared_ptr<void> gmres;  // GmresBufs, created on first GMRES solve
     std::shared_ptr<void> lsmr;   // LsmrBufs, created on first LSMR solve
     std::shared_ptr<void> cn;     // CnState of the coarse-space network, kept while training
@@ -538,6 +578,8 @@ struct SolverImpl {
     int64_t sweep_cluster_chunks = 512;  // AC levels of at most this many chunks go to one cluster (0: none)
     std::vector<uint8_t> pc_bytes;  // serialized preconditioner, made on first request
     int32_t* h_active = nullptr;  // pinned
+    uint32_t* h_stage = nullptr;  // pinned staging of small reads (read_small)
+    size_t h_stage_words = 0;
     double setup_time = 0.0;
     int64_t gpu_launches = 0;
     // Optional event timing of selected launches (0: FP64 operator, 1: FP32 operator,
@@ -565,6 +607,7 @@ struct SolverImpl {
         for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         if (cg_exec) cudaGraphExecDestroy(cg_exec);
         if (h_active) cudaFreeHost(h_active);
+        if (h_stage) cudaFreeHost(h_stage);
         if (stream) cudaStreamDestroy(stream);
     }
     bool mixed() const { return params.precision == WITHIN_PRECISION_MIXED; }
@@ -626,6 +669,42 @@ namespace {
 // Lanes per row for kp RHS (kp a multiple of 4, <= 32): kp/4 rounded up to 1, 2, 4 or 8.
 // For kp in {12, 20, 24, 28} the extra lanes would own columns past kp, so those widths
 // are padded: kp is rounded to 16 or 32 by pad_kp below.
+// dst <- bytes (a multiple of 4) of device memory at src, after the work already on the
+// solver's stream (which this synchronizes).
+void read_small(SolverImpl& S, void* dst, const void* src, size_t bytes) {
+    const size_t words = bytes / 4;
+    if (words > S.h_stage_words) {
+        if (S.h_stage) WB_CUDA(cudaFreeHost(S.h_stage));
+        S.h_stage = nullptr;
+        S.h_stage_words = 0;
+        WB_CUDA(cudaMallocHost(&S.h_stage, std::max<size_t>(words, 1 << 16) * 4));
+        S.h_stage_words = std::max<size_t>(words, 1 << 16);
+    }
+    if (words > 0) {
+        d2h_words_kernel<<<1, 256, 0, S.stream>>>(static_cast<const uint32_t*>(src), S.h_stage, words);
+        WB_CUDA(cudaGetLastError());
+    }
+    WB_CUDA(cudaStreamSynchronize(S.stream));
+    std::memcpy(dst, S.h_stage, words * 4);
+}
+
+// da[0..n) <- a, db[0..n) <- b (either may be null; n <= 32), in order on the stream.
+void write_small(SolverImpl& S, int32_t* da, const int32_t* a, double* db, const double* b, int n) {
+    SmallI32 ai{};
+    SmallF64 bi{};
+    for (int i = 0; i < n; ++i) {
+        if (a) ai.v[i] = a[i];
+        if (b) bi.v[i] = b[i];
+    }
+    set_small_kernel<<<1, 32, 0, S.stream>>>(ai, a ? da : nullptr, bi, b ? db : nullptr, n);
+    WB_CUDA(cudaGetLastError());
+}
+
+void publish_active(SolverImpl& S, const int32_t* n_active) {
+    publish_active_kernel<<<1, 1, 0, S.stream>>>(n_active, S.h_active);
+    WB_CUDA(cudaGetLastError());
+}
+
 int group_for(int kp) { return kp / 4; }
 int pad_kp(int k) {
     const int kp = pad4(k);
@@ -1556,8 +1635,7 @@ void launch_sweep(SolverImpl& S, CsrDev<T>& c, const std::vector<int64_t>& lp, c
 bool sweeps_failed(SolverImpl& S) {
     if (!S.coop || !S.ws.sweep_err.p) return false;
     int32_t e = 0;
-    WB_CUDA(cudaStreamSynchronize(S.stream));
-    WB_CUDA(cudaMemcpy(&e, S.ws.sweep_err.p, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    read_small(S, &e, S.ws.sweep_err.p, sizeof(int32_t));
     if (e) WB_CUDA(cudaMemset(S.ws.sweep_err.p, 0, sizeof(int32_t)));
     return e != 0;
 }
@@ -1996,12 +2074,12 @@ void cg_device(SolverImpl& S, int kp, const T* b, T* x, T* r, T* z, T* p, T* ap,
         } else {
             body();
         }
-        WB_CUDA(cudaMemcpyAsync(S.h_active, w.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+        publish_active(S, w.n_active.p);
         WB_CUDA(cudaEventRecord(ev, S.stream));
     };
     // The host check of iteration `it` overlaps the device work of iteration it+1; an
     // iteration enqueued after every RHS stopped changes nothing (alpha = 0, masked p).
-    WB_CUDA(cudaMemcpyAsync(S.h_active, w.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+    publish_active(S, w.n_active.p);
     WB_CUDA(cudaStreamSynchronize(S.stream));
     if (*S.h_active > 0 && maxiter > 0) {
         cudaEvent_t evb;
@@ -2249,7 +2327,7 @@ void gmres_device(SolverImpl& S, GmresBufs& B, int kp, const double* rhs, double
         launch_dot<double, double>(S, B.r64.p, B.r64.p, m, kp, part, nb);
         launch_reduce(S, part, nb, kp, red);
         gm_restart_kernel<<<1, 32, 0, S.stream>>>(s, red, kp, maxiter);
-        WB_CUDA(cudaMemcpyAsync(S.h_active, B.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+        publish_active(S, B.n_active.p);
         WB_CUDA(cudaStreamSynchronize(S.stream));
         S.gpu_launches += 2;
         if (*S.h_active == 0) break;
@@ -2286,7 +2364,7 @@ void gmres_device(SolverImpl& S, GmresBufs& B, int kp, const double* rhs, double
             WB_CUDA(cudaGetLastError());
             S.gpu_launches += 2 * (j + 1) + 2;
             jmax = j + 1;
-            WB_CUDA(cudaMemcpyAsync(S.h_active, B.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+            publish_active(S, B.n_active.p);
             WB_CUDA(cudaStreamSynchronize(S.stream));
             if (*S.h_active == 0) break;
         }
@@ -2582,7 +2660,7 @@ void lsmr_device(SolverImpl& S, LsmrBufs& B, int kp, const double* yi, double* x
         WB_CUDA(cudaMemsetAsync(B.zeros.p, 0, 32 * sizeof(double), S.stream));
     }
     LsmrState s = lsmr_state(B, S.params.tol, S.params.maxiter, precond);
-    WB_CUDA(cudaMemcpyAsync(B.part_of.p, part_of.data(), sizeof(int32_t) * kp, cudaMemcpyHostToDevice, S.stream));
+    write_small(S, B.part_of.p, part_of.data(), nullptr, nullptr, kp);
     const int G = group_for(kp);
     const double* sw = B.sw.p;
     double* part = S.ws.part.p;
@@ -2662,7 +2740,7 @@ void lsmr_device(SolverImpl& S, LsmrBufs& B, int kp, const double* yi, double* x
     WB_CUDA(cudaMemcpyAsync(B.h.p, B.v.p, sizeof(double) * mk, cudaMemcpyDeviceToDevice, S.stream));
     WB_CUDA(cudaMemsetAsync(B.hb.p, 0, sizeof(double) * mk, S.stream));
     WB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * mk, S.stream));
-    WB_CUDA(cudaMemcpyAsync(S.h_active, B.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+    publish_active(S, B.n_active.p);
     WB_CUDA(cudaStreamSynchronize(S.stream));
     S.gpu_launches += 2;
     for (int itn = 1; itn <= S.params.maxiter && *S.h_active > 0; ++itn) {
@@ -2693,14 +2771,13 @@ void lsmr_device(SolverImpl& S, LsmrBufs& B, int kp, const double* yi, double* x
         WB_DISPATCH_G(G, lsmr_update_kernel<GV><<<gm, kBlock, 0, S.stream>>>(x, B.h.p, B.hb.p, B.v.p, B.coef.p, m, kp));
         WB_CUDA(cudaGetLastError());
         S.gpu_launches++;
-        WB_CUDA(cudaMemcpyAsync(S.h_active, B.n_active.p, sizeof(int32_t), cudaMemcpyDeviceToHost, S.stream));
+        publish_active(S, B.n_active.p);
         WB_CUDA(cudaStreamSynchronize(S.stream));
     }
     conv.assign(kp, 0);
     iters.assign(kp, 0);
-    WB_CUDA(cudaMemcpyAsync(conv.data(), B.conv.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
-    WB_CUDA(cudaMemcpyAsync(iters.data(), B.iters.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
-    WB_CUDA(cudaStreamSynchronize(S.stream));
+    read_small(S, conv.data(), B.conv.p, sizeof(int32_t) * kp);
+    read_small(S, iters.data(), B.iters.p, sizeof(int32_t) * kp);
 }
 
 }  // namespace
@@ -2718,8 +2795,7 @@ struct BatchOut {
 
 std::vector<double> host_reduce(SolverImpl& S, int nb, int kp) {
     std::vector<double> hpart((size_t)nb * kp), out(kp, 0.0);
-    WB_CUDA(cudaMemcpyAsync(hpart.data(), S.ws.part.p, sizeof(double) * nb * kp, cudaMemcpyDeviceToHost, S.stream));
-    WB_CUDA(cudaStreamSynchronize(S.stream));
+    read_small(S, hpart.data(), S.ws.part.p, sizeof(double) * nb * kp);
     for (int c = 0; c < kp; ++c)
         for (int b = 0; b < nb; ++b) out[c] += hpart[(size_t)b * kp + c];
     return out;
@@ -2779,8 +2855,7 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
         // then x += d on those RHS.
         auto run_inner = [&](const double* rhs, const std::vector<int32_t>& who, const std::vector<double>& tl,
                              std::vector<int32_t>& cv, std::vector<int32_t>& it) {
-            WB_CUDA(cudaMemcpyAsync(w.st_part.p, who.data(), sizeof(int32_t) * kp, cudaMemcpyHostToDevice, S.stream));
-            WB_CUDA(cudaMemcpyAsync(w.st_tol.p, tl.data(), sizeof(double) * kp, cudaMemcpyHostToDevice, S.stream));
+            write_small(S, w.st_part.p, who.data(), w.st_tol.p, tl.data(), kp);
             WB_CUDA(cudaMemsetAsync(w.st_conv.p, 0, sizeof(int32_t) * 32, S.stream));
             const int grid = S.nblk(m * kp, 1);
             if (S.params.krylov == WITHIN_KRYLOV_GMRES) {
@@ -2803,9 +2878,8 @@ void solve_chunk(SolverImpl& S, const double* ycol, int k, double* xcol, double*
             S.gpu_launches += 2;
             cv.assign(kp, 0);
             it.assign(kp, 0);
-            WB_CUDA(cudaMemcpyAsync(cv.data(), w.st_conv.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
-            WB_CUDA(cudaMemcpyAsync(it.data(), w.st_iters.p, sizeof(int32_t) * kp, cudaMemcpyDeviceToHost, S.stream));
-            WB_CUDA(cudaStreamSynchronize(S.stream));
+            read_small(S, cv.data(), w.st_conv.p, sizeof(int32_t) * kp);
+            read_small(S, it.data(), w.st_iters.p, sizeof(int32_t) * kp);
         };
         WB_CUDA(cudaMemsetAsync(w.x.p, 0, sizeof(double) * m * kp, S.stream));
         std::vector<int32_t> cv, it;
@@ -3266,6 +3340,7 @@ int guard(const std::function<int()>& f) {
     }
 }
 
+
 // Device attributes, the solver's stream and its pinned status word.
 void init_device(SolverImpl& S) {
     int dev = 0;
@@ -3606,25 +3681,65 @@ int within_solver_solve_batch(within_solver* s, const double* ys, size_t k, doub
                               within_solve_stats* stats) {
     if (!s) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "solver is null");
     SolverImpl& S = *s->impl;
-    std::lock_guard<std::mutex> lk(S.mu);
     return guard([&]() -> int {
         const double t0 = wb::now_s();
         if (k == 0) return WITHIN_OK;
         if (!ys || !x || !dem) return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "null buffer");
+        if (S.precond_only)
+            return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "this handle holds only a preconditioner; build a Solver to solve");
         const size_t n = (size_t)S.d.n, m = (size_t)S.d.ndofs;
-        // device copies of the host buffers, kept by the solver (grow-only)
-        wb::DArr<double>& dy = S.host_y;
-        wb::DArr<double>& dx = S.host_x;
-        wb::DArr<double>& dd = S.host_dem;
-        dy.alloc(n * k);
-        dx.alloc(m * k);
-        dd.alloc(n * k);
-        WB_CUDA(cudaMemcpyAsync(dy.p, ys, sizeof(double) * n * k, cudaMemcpyHostToDevice, S.stream));
-        const int rc = solve_device(S, dy.p, k, dx.p, dd.p, stats);
-        if (rc != WITHIN_OK) return rc;
-        WB_CUDA(cudaMemcpyAsync(x, dx.p, sizeof(double) * m * k, cudaMemcpyDeviceToHost, S.stream));
-        WB_CUDA(cudaMemcpyAsync(dem, dd.p, sizeof(double) * n * k, cudaMemcpyDeviceToHost, S.stream));
-        WB_CUDA(cudaStreamSynchronize(S.stream));
+        // this call's device buffers and copy stream (a slot kept by the solver); the
+        // upload and the download run outside the solver's lock, so that calls from other
+        // host threads overlap their copies with this solve and this one's with theirs
+        wb::HostCall* hc = nullptr;
+        {
+            std::lock_guard<std::mutex> lc(S.calls_mu);
+            for (auto& c : S.calls)
+                if (!c->busy) { hc = c.get(); break; }
+            if (!hc) {
+                S.calls.push_back(std::make_unique<wb::HostCall>());
+                hc = S.calls.back().get();
+            }
+            hc->busy = true;
+        }
+        struct Release {
+            wb::SolverImpl& S;
+            wb::HostCall* hc;
+            ~Release() {
+                std::lock_guard<std::mutex> lc(S.calls_mu);
+                hc->busy = false;
+            }
+        } release{S, hc};
+        if (!hc->stream) WB_CUDA(cudaStreamCreateWithFlags(&hc->stream, cudaStreamNonBlocking));
+        hc->y.alloc(n * k);
+        hc->x.alloc(m * k);
+        hc->dem.alloc(n * k);
+        cudaEvent_t up = nullptr, done = nullptr;
+        WB_CUDA(cudaEventCreateWithFlags(&up, cudaEventDisableTiming));
+        struct Events {
+            cudaEvent_t &a, &b;
+            ~Events() {
+                if (a) cudaEventDestroy(a);
+                if (b) cudaEventDestroy(b);
+            }
+        } evs{up, done};
+        WB_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        WB_CUDA(cudaMemcpyAsync(hc->y.p, ys, sizeof(double) * n * k, cudaMemcpyHostToDevice, hc->stream));
+        WB_CUDA(cudaEventRecord(up, hc->stream));
+        {
+            std::lock_guard<std::mutex> lk(S.mu);
+            WB_CUDA(cudaStreamWaitEvent(S.stream, up, 0));
+            const int rc = solve_device(S, hc->y.p, k, hc->x.p, hc->dem.p, stats);
+            if (rc != WITHIN_OK) {
+                WB_CUDA(cudaStreamSynchronize(S.stream));
+                return rc;
+            }
+            WB_CUDA(cudaEventRecord(done, S.stream));
+        }
+        WB_CUDA(cudaStreamWaitEvent(hc->stream, done, 0));
+        WB_CUDA(cudaMemcpyAsync(x, hc->x.p, sizeof(double) * m * k, cudaMemcpyDeviceToHost, hc->stream));
+        WB_CUDA(cudaMemcpyAsync(dem, hc->dem.p, sizeof(double) * n * k, cudaMemcpyDeviceToHost, hc->stream));
+        WB_CUDA(cudaStreamSynchronize(hc->stream));
         if (stats) stats[0].time_total = wb::now_s() - t0;
         return WITHIN_OK;
     });
