@@ -436,15 +436,26 @@ def uneven(args):
     import torch
     import within_b200 as wb
     from within_b200 import synthetic
-    torch.cuda.set_device(0)
-    probs = synthetic.config4(seed=0, n_problems=args.problems, max_obs=1_000_000)
-    n_rhs = sum(Y.shape[1] for _, Y in probs)
-    n_obs = sum(c.shape[0] for c, _ in probs)
+    rank, local, world = dist_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    all_probs = synthetic.config4(seed=0, n_problems=args.problems, max_obs=1_000_000)
+    n_rhs = sum(Y.shape[1] for _, Y in all_probs)
+    n_obs = sum(c.shape[0] for c, _ in all_probs)
+    # one shard of the problems per rank, balanced by observation count (no exchange)
+    mine = wb.shard_problems([c.shape[0] for c, _ in all_probs], world)[rank]
+    probs = [all_probs[i] for i in mine]
     cfg = wb.CG(precision=args.precision)
     for _ in range(max(1, args.warmup)):
         wb.solve_many(probs, cfg)
-    clocks = Clocks(0)
+    clocks = Clocks(local)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         res = wb.solve_many(probs, cfg)
@@ -452,11 +463,21 @@ def uneven(args):
     el = time.perf_counter() - t0
     clk = clocks.stop()
     conv = all(all(r.converged) for r in res)
-    worst = max(max(r.residual) for r in res)
+    worst = max(max(r.residual) for r in res) if res else 0.0
+    if dist:  # the job's time is its slowest rank's; every rank's problems must converge
+        el = max_over_ranks(dist, el)
+        ok = torch.tensor([1.0 if conv else 0.0], device="cuda")
+        dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+        conv = bool(ok.item() > 0.5)
+        worst = max_over_ranks(dist, worst)
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:
+            return
     # CPU baseline: the oracle on a sample of the problems, one after another, setup
     # included as in the GPU arm, the RHS of a problem in parallel over the host threads
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
         threads = max(1, min(16, os.cpu_count() or 1))
@@ -472,16 +493,19 @@ def uneven(args):
                "sample": f"{len(idx)} of the {len(probs)} problems (seeded choice, {rhs} RHS), setup included, "
                          f"one problem at a time"}
     line = {"metric": "RHS solved/sec at tol 1e-8, uneven batch of independent problems (setup included)",
-            "value": args.steps * n_rhs / el, "unit": "RHS/s", "n_gpus": 1, "steps": args.steps,
+            "value": args.steps * n_rhs / el, "unit": "RHS/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * el / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
             "dtype": "f32 inner / f64 refinement" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded log-uniform sizes, uniform codes)",
             "config": {"workload": f"{len(probs)} independent problems, n_obs log-uniform on [1e3, 1e6] "
                                    f"(total {n_obs}), 2-4 factors with levels log-uniform on [n/50, n/5], "
                                    f"1-8 RHS each (total {n_rhs}), CG + additive Schwarz, tol 1e-8, "
                                    f"{os.cpu_count()} problems in flight (one per host core)",
-                       "timing": "host wall clock, device synchronised"},
+                       "timing": "host wall clock, device synchronised" +
+                                 (", max over ranks" if world > 1 else ""),
+                       "sharding": "problems split over %d rank(s) by observation count (largest first to the "
+                                   "least-loaded rank), no exchange" % world},
             "clocks": clk, "accuracy": {"converged": conv, "max_final_residual": worst}}
     if cpu:
         line["cpu_baseline"] = cpu

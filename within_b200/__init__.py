@@ -612,3 +612,23 @@ def solve_batch(categories, Y, config=None, weights=None, preconditioner=None) -
     r = s.solve_batch(Y)
     r.time_total = time.perf_counter() - t0
     return r
+
+
+def shard_problems(sizes, world: int) -> list:
+    """Assignment of independent problems to ``world`` ranks (one GPU each), balanced by
+    observation count: the largest problem first, each to the rank with the least work
+    so far (ties: the lowest rank).  ``sizes`` are the problems' observation counts.
+    Returns one ascending index list per rank; together they hold every index once.
+
+    Independent problems share nothing, so ranks solve their shards with no exchange
+    (``solve_many`` on each); only the job's time is combined (its slowest rank's).
+    """
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda j: (-int(sizes[j]), j)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += int(sizes[i])
+    return [sorted(o) for o in out]
