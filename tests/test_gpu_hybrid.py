@@ -118,3 +118,25 @@ def test_autotuner_decides_and_the_decision_is_exact():
     GX = s.apply_gramian(X)  # FP32 operator of the mixed solver, as decided
     for c in range(3):
         assert rel(GX[:, c], o.apply_gramian(X[:, c])) < FP32_TOL
+
+
+def test_hybrid_decision_is_shared_by_a_shape_class():
+    """Solvers of one shape class (observation count within a factor of two, same factor
+    count and RHS width) take the first one's decision without timing it again."""
+    L = _lib.load()
+    cats, Y, w = synthetic.config2(seed=11, scale=0.08)
+    Y = np.asfortranarray(Y[:, :5])
+    s1 = wb.Solver(cats, weights=w)
+    s1.solve_batch(Y)
+    ms = C.c_float()
+    # timed here, or taken from an earlier solver of the class in this process
+    on1 = L.within_solver_hybrid(s1._h, 5, 8, C.byref(ms))
+    assert on1 in (0, 1)
+    cats2, Y2, w2 = synthetic.config2(seed=12, scale=0.08)
+    Y2 = np.asfortranarray(Y2[:, :5])
+    s2 = wb.Solver(cats2, weights=w2)
+    r2 = s2.solve_batch(Y2)
+    assert L.within_solver_hybrid(s2._h, 5, 8, C.byref(ms)) == on1 and ms.value == 0  # not timed again
+    o = oracle.OracleSolver(cats2, w2)
+    t = o.solve(Y2[:, 0])
+    assert rel(r2.demeaned[:, 0], t.demeaned) < 1e-8
