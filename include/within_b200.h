@@ -325,12 +325,17 @@ int32_t within_solver_obs_rhs_per_lane(const within_solver *solver, int32_t k, i
  * pass's lane-group tables stay implicit: one pass over the observations, with no code of
  * any other factor read.  Every other block is a factor-pair cross-tabulation of the
  * additive Schwarz setup, applied as CSR rows.  The autotuner times it against the
- * observation pass once per shape class and keeps the faster.  within_solver_set_hybrid
- * fixes the choice for k RHS in elem_bytes precision (1 builds its arrays here; outside
- * any stream capture): WITHIN_ERR_INVALID_ARGUMENT when the solver has no additive
- * Schwarz preconditioner, uses the assembled Gramian, or has no (or more than two) small
- * factors.  within_solver_hybrid returns 1 (on), 0 (off) or -1 (not decided yet), with
- * the autotuner's time per apply in *ms (0 when not timed; ms may be null). */
+ * observation pass once per shape class and keeps the faster.  Its primary-major part
+ * has two forms: lane-group tables of the small factors (prim_rows_kernel), and, for 16
+ * RHS and at most 48 small-factor levels (each factor padded to 8), products of per-warp
+ * weight tiles on the FP64 tensor cores (prim_mma_kernel).  within_solver_set_hybrid
+ * fixes the choice for k RHS in elem_bytes precision: 0 off, 1 tables, 2 tensor cores (1
+ * and 2 build the arrays here; outside any stream capture); WITHIN_ERR_INVALID_ARGUMENT
+ * when the solver has no additive Schwarz preconditioner, uses the assembled Gramian, or
+ * has no (or more than two) small factors, or for 2 where the tile does not apply.
+ * within_solver_hybrid returns the form in use (0, 1 or 2) or -1 (not decided yet), with
+ * the autotuner's time per apply of the faster form in *ms (0 when not timed; ms may be
+ * null). */
 int within_solver_set_hybrid(within_solver *solver, int32_t k, int32_t elem_bytes, int32_t on);
 int32_t within_solver_hybrid(const within_solver *solver, int32_t k, int32_t elem_bytes, float *ms);
 /* Algorithmic bytes of one hybrid apply for k RHS of elem_bytes per element (0 when the

@@ -29,7 +29,7 @@ def _set(s, k, elem, on):
 
 
 @pytest.mark.parametrize("name", ELIGIBLE)
-@pytest.mark.parametrize("k", [1, 5, 16, 32])
+@pytest.mark.parametrize("k", [1, 5, 13, 16, 32])
 def test_hybrid_apply_matches_oracle(name, k):
     cats, w = DESIGNS[name]()
     o = oracle.OracleSolver(cats, w)
@@ -53,6 +53,20 @@ def test_hybrid_apply_matches_oracle(name, k):
             assert rel(GX[:, c], want[c]) < FP32_TOL, c
             # no less accurate than the observation pass in the same precision
             assert rel(GX[:, c], want[c]) <= 2 * rel(GXi[:, c], want[c]) + 1e-7, c
+    if k in (16, 13):  # the tensor-core form (16 RHS columns)
+        assert _set(g64, k, 8, 2) == 0, _lib.last_error()
+        assert _lib.load().within_solver_hybrid(g64._h, k, 8, None) == 2
+        GX = g64.apply_gramian(X)
+        for c in range(k):
+            assert rel(GX[:, c], want[c]) < 1e-13, c
+        if rc == 0:
+            assert _set(g32, k, 4, 2) == 0, _lib.last_error()
+            GX = g32.apply_gramian(X)
+            for c in range(k):
+                assert rel(GX[:, c], want[c]) < FP32_TOL, c
+                assert rel(GX[:, c], want[c]) <= 2 * rel(GXi[:, c], want[c]) + 1e-7, c
+    else:
+        assert _set(g64, k, 8, 2) != 0  # no tensor-core form for this RHS width
     # and off again: the observation pass
     assert _set(g64, k, 8, 0) == 0
     GX = g64.apply_gramian(X)
@@ -70,14 +84,15 @@ def test_hybrid_rejected_where_it_does_not_apply():
     assert _set(wb.Solver(cats, weights=w), 16, 4, 1) != 0  # an FP64 solver has no FP32 operator
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_solve_with_hybrid_apply(precision):
+def test_solve_with_hybrid_apply(precision, form):
     cats, Y, w = synthetic.config3(seed=2, scale=0.01)
     k = Y.shape[1]
     s = wb.Solver(cats, wb.CG(precision=precision), weights=w)
-    assert _set(s, k, 8, 1) == 0, _lib.last_error()
+    assert _set(s, k, 8, form) == 0, _lib.last_error()
     if precision == "mixed":
-        assert _set(s, k, 4, 1) == 0, _lib.last_error()
+        assert _set(s, k, 4, form) == 0, _lib.last_error()
     r = s.solve_batch(Y)
     assert all(r.converged) and max(r.residual) <= 1e-8
     same_tol = oracle.OracleSolver(cats, w)
@@ -110,9 +125,9 @@ def test_autotuner_decides_and_the_decision_is_exact():
     assert all(r.converged) and max(r.residual) <= 1e-8
     ms = C.c_float()
     on32 = L.within_solver_hybrid(s._h, k, 4, C.byref(ms))
-    assert on32 in (0, 1) and ms.value > 0
+    assert on32 in (0, 1, 2) and ms.value > 0
     on64 = L.within_solver_hybrid(s._h, k, 8, C.byref(ms))
-    assert on64 in (0, 1)
+    assert on64 in (0, 1, 2)
     o = oracle.OracleSolver(cats, w)
     X = np.random.default_rng(7).standard_normal((s.n_dofs, 3))
     GX = s.apply_gramian(X)  # FP32 operator of the mixed solver, as decided
@@ -131,7 +146,7 @@ def test_hybrid_decision_is_shared_by_a_shape_class():
     ms = C.c_float()
     # timed here, or taken from an earlier solver of the class in this process
     on1 = L.within_solver_hybrid(s1._h, 5, 8, C.byref(ms))
-    assert on1 in (0, 1)
+    assert on1 in (0, 1)  # no tensor-core form at 5 RHS (kp 8)
     cats2, Y2, w2 = synthetic.config2(seed=12, scale=0.08)
     Y2 = np.asfortranarray(Y2[:, :5])
     s2 = wb.Solver(cats2, weights=w2)

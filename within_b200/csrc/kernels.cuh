@@ -709,6 +709,153 @@ __global__ void __launch_bounds__(obs_block<T>(), 2) prim_rows_kernel(PrimParams
         }
 }
 
+// ---------------------------------------------------------------------------
+// Primary-major pass of the hybrid apply on the FP64 tensor cores (16 RHS).  A warp
+// takes 8 pieces of primary levels at a time (a level of at most 64 observations, or a
+// 64-observation piece of a longer one), one per lane group.  Each group sums its
+// piece's weights by small-factor level into row g of an 8 x wcols tile W in shared
+// memory (the levels of up to two small factors side by side, each padded to 8), so that
+//   Y_P = W X_S     (the piece's sum_i w_i x_S[s_i]; 8 x 16, K = wcols)
+//   Y_S += W' X_P   (the small factors' sum_i w_i x_P[p_i]; wcols x 16, K = 8)
+// are products on the tensor cores (mma.sync m8n8k4, FP64, exact for FP32 inputs too)
+// instead of per-observation gathers and lane-group tables.  Y_S stays in the warp's
+// accumulator fragments until the end.  The piece's C_PO entries and its diagonal
+// (sum_i w_i) x_P[p] complete y_P[p] as in prim_rows_kernel.
+// ---------------------------------------------------------------------------
+constexpr int kMmaKP = 16;        // RHS columns (kp) of this kernel
+constexpr int kMmaMaxCols = 48;   // small-factor levels, padded to 8 per factor
+constexpr int kMmaPiece = 64;     // observations per piece at most
+
+struct PrimMmaParams {
+    int64_t off_p;
+    int32_t nsmall;                     // 1 or 2
+    const uint32_t* codes_s[kPrimMaxS];
+    int64_t off_s[kPrimMaxS];
+    int32_t nlev_s[kPrimMaxS];
+    int32_t col_s[kPrimMaxS];           // first column of each factor in W
+    int32_t wcols;                      // multiple of 8, <= kMmaMaxCols
+    const uint4* pieces;                // (level, first obs, end obs, first piece | split << 1)
+    int64_t npieces;
+    const int64_t* pptr;                // C_PO rows of the primary levels
+    const uint32_t* pcol;
+};
+
+// d = a b + c for an 8x4 by 4x8 FP64 product; per lane: a = A[lane/4][lane%4],
+// b = B[lane%4][lane/4], c and d = C[lane/4][2 (lane%4) + {0, 1}]
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) prim_mma_kernel(PrimMmaParams P, const T* __restrict__ w,
+                                                          const T* __restrict__ pval, const T* __restrict__ x,
+                                                          T* __restrict__ out) {
+    constexpr int KP = kMmaKP;
+    constexpr int MC = kMmaMaxCols;
+    __shared__ __align__(16) double XS[MC * KP];          // the small factors' rows of x
+    __shared__ __align__(16) double Wt[8][8 * MC];         // per warp: W, 8 x wcols (row stride MC)
+    __shared__ __align__(16) double XP[8][8 * KP];         // per warp: the pieces' rows of x_P
+    __shared__ __align__(16) double YP[8][8 * KP];         // per warp: W X_S
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, c = lane & 3;
+    const int wc = P.wcols;
+    for (int e = threadIdx.x; e < MC * KP; e += blockDim.x) {
+        const int col = e / KP, n = e % KP;
+        double v = 0.0;
+        for (int j = 0; j < P.nsmall; ++j)
+            if (col >= P.col_s[j] && col < P.col_s[j] + P.nlev_s[j])
+                v = (double)x[(size_t)(P.off_s[j] + (col - P.col_s[j])) * KP + n];
+        XS[e] = v;
+    }
+    __syncthreads();
+    double* W = Wt[warp];
+    double* xpw = XP[warp];
+    double* ypw = YP[warp];
+    double cs[MC / 8][2][2];  // Y_S fragments: rows 8 mt + g, columns 8 nt + 2 c + {0, 1}
+#pragma unroll
+    for (int mt = 0; mt < MC / 8; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) cs[mt][nt][0] = cs[mt][nt][1] = 0.0;
+    const T* const x0 = x + (size_t)P.off_p * KP + 4 * c;
+    T* const out0 = out + (size_t)P.off_p * KP + 4 * c;
+    const int64_t ntasks = (P.npieces + 7) / 8;
+    for (int64_t task = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; task < ntasks;
+         task += (int64_t)gridDim.x * (blockDim.x >> 5)) {
+        const int64_t pi = task * 8 + g;
+        const bool has = pi < P.npieces;
+        const uint4 pc = has ? __ldg(P.pieces + pi) : make_uint4(0u, 0u, 0u, 0u);
+        const uint32_t p = pc.x;
+        const V4<T> xp = has ? ldg4(x0 + (size_t)p * KP) : V4<T>(T(0));
+        xpw[g * KP + 4 * c + 0] = (double)xp.a;
+        xpw[g * KP + 4 * c + 1] = (double)xp.b;
+        xpw[g * KP + 4 * c + 2] = (double)xp.c;
+        xpw[g * KP + 4 * c + 3] = (double)xp.d;
+        for (int j = c; j < wc; j += 4) W[g * MC + j] = 0.0;
+        __syncwarp();
+        // row g of W: the piece's weights by small-factor level; the group's four lanes
+        // take every fourth observation (consecutive lanes, consecutive observations) and
+        // add with shared-memory reductions (two of them meet only on a repeated level)
+        double ws = 0.0;
+        for (uint32_t i = pc.y + c; i < pc.z; i += 4) {
+            const double wi = w ? (double)__ldg(w + i) : 1.0;
+            ws += wi;
+            for (int j = 0; j < P.nsmall; ++j) red_shared(W + g * MC + P.col_s[j] + __ldg(P.codes_s[j] + i), wi);
+        }
+        ws += __shfl_xor_sync(0xffffffffu, ws, 1);
+        ws += __shfl_xor_sync(0xffffffffu, ws, 2);
+        __syncwarp();
+        // Y_P = W X_S (8 x 16): two 8-column tiles, K = wcols in steps of 4
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+            double d0 = 0.0, d1 = 0.0;
+            for (int kk = 0; kk < wc; kk += 4)
+                dmma_8x8x4(d0, d1, W[g * MC + kk + c], XS[(kk + c) * KP + 8 * nt + g]);
+            ypw[g * KP + 8 * nt + 2 * c] = d0;
+            ypw[g * KP + 8 * nt + 2 * c + 1] = d1;
+        }
+        // Y_S += W' X_P (wcols x 16): rows in tiles of 8, K = the 8 pieces
+#pragma unroll
+        for (int mt = 0; mt < MC / 8; ++mt) {
+            if (8 * mt >= wc) break;
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+                for (int kk = 0; kk < 8; kk += 4)
+                    dmma_8x8x4(cs[mt][nt][0], cs[mt][nt][1], W[(kk + c) * MC + 8 * mt + g],
+                               xpw[(kk + c) * KP + 8 * nt + g]);
+        }
+        __syncwarp();
+        if (has) {
+            V4<double> acc(ypw[g * KP + 4 * c], ypw[g * KP + 4 * c + 1], ypw[g * KP + 4 * c + 2],
+                           ypw[g * KP + 4 * c + 3]);
+            acc += ws * to_d(xp);
+            if (pc.w & 1u)  // the level's first piece: its C_PO entries
+                for (int64_t e = __ldg(P.pptr + p), e1 = __ldg(P.pptr + p + 1); e < e1; ++e)
+                    acc += (double)__ldg(pval + e) * to_d(ldg4(x + (size_t)__ldg(P.pcol + e) * KP + 4 * c));
+            if (pc.w & 2u) atomic_add4(out0 + (size_t)p * KP, from_d<T>(acc));
+            else st4(out0 + (size_t)p * KP, from_d<T>(acc));
+        }
+        __syncwarp();  // W, XP and YP are rewritten by the next task
+    }
+    // the warp's Y_S into y_S
+#pragma unroll
+    for (int mt = 0; mt < MC / 8; ++mt) {
+        const int col = 8 * mt + g;
+        if (col >= wc) break;
+        for (int j = 0; j < P.nsmall; ++j) {
+            if (col < P.col_s[j] || col >= P.col_s[j] + P.nlev_s[j]) continue;
+            T* d = out + (size_t)(P.off_s[j] + (col - P.col_s[j])) * KP;
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                if (cs[mt][nt][0] != 0.0) atomicAdd(d + 8 * nt + 2 * c, (T)cs[mt][nt][0]);
+                if (cs[mt][nt][1] != 0.0) atomicAdd(d + 8 * nt + 2 * c + 1, (T)cs[mt][nt][1]);
+            }
+        }
+    }
+}
+
 // Column-major (RHS-major) user order <-> interleaved primary-sorted order with kp
 // columns (padding columns are zero).  perm[i] = user index of sorted row i (or identity).
 // Each warp transposes tiles of 32 rows through its own shared-memory tile (32 x kp+1):

@@ -498,6 +498,11 @@ struct HybridDev {
     DArr<float> oval32;
     DArr<CsrChunk> ochunks;
     int64_t nochunks = 0, nnz = 0;
+    // the primary levels in pieces of at most kMmaPiece observations (prim_mma_kernel):
+    // (level, first observation, end, first piece | split << 1)
+    DArr<uint4> pieces;
+    int64_t npieces = 0;
+    bool any_split = false;
 };
 
 // Device buffers of one host-buffer solve (its inputs, outputs and copy stream).
@@ -1162,6 +1167,23 @@ void build_hybrid(SolverImpl& S, uint32_t smask) {
     if (S.mixed()) H->oval32.upload_cast(oval);
     const std::vector<CsrChunk> ch = make_chunks(optr, 0, (int64_t)rows.size(), 256, 1, true);
     H->ochunks.upload(ch);
+    {
+        std::vector<uint4> pcs;
+        pcs.reserve((size_t)nP + 16);
+        for (int64_t l = 0; l < nP; ++l) {
+            const int64_t a = S.lvl_ptr_h[l], b = S.lvl_ptr_h[l + 1];
+            const bool split = b - a > kMmaPiece;
+            H->any_split = H->any_split || split;
+            int64_t at = a;
+            do {
+                const int64_t e = std::min(b, at + kMmaPiece);
+                pcs.push_back(make_uint4((uint32_t)l, (uint32_t)at, (uint32_t)e, (at == a ? 1u : 0u) | (split ? 2u : 0u)));
+                at = e;
+            } while (at < b);
+        }
+        H->pieces.upload(pcs);
+        H->npieces = (int64_t)pcs.size();
+    }
     H->nochunks = (int64_t)ch.size();
     H->nnz = (int64_t)pcol.size() + (int64_t)ocol.size();
     if (S.cg_exec) {  // a captured CG iteration may hold the old arrays
@@ -1180,12 +1202,64 @@ template <> const float* hyb_oval<float>(const HybridDev& H) { return H.oval32.p
 
 // y = G x by the hybrid apply (S.hyb built for the pass's small factors at this kp and
 // precision): zero the accumulated outputs, the primary-major pass, then the other rows.
+// The small factors' columns in prim_mma_kernel's tile (each padded to 8); false when the
+// tile does not apply (kp other than 16, or more than kMmaMaxCols columns).
+bool mma_layout(SolverImpl& S, int kp, size_t elem, PrimMmaParams& M) {
+    if (kp != kMmaKP) return false;
+    ObsParams O;
+    const int np = obs_params_for(S, kp, elem, O);
+    if (np < 1 || np > kPrimMaxS) return false;
+    M = PrimMmaParams{};
+    M.off_p = S.d.off[S.primary];
+    M.nsmall = np;
+    int j = 0, col = 0;
+    for (int sl = 1; sl < S.d.Q; ++sl) {
+        if (O.sink[sl] != SINK_PRIVATE) continue;
+        M.codes_s[j] = S.codes.p + (size_t)sl * O.ns;
+        M.off_s[j] = O.off[sl];
+        M.nlev_s[j] = (int32_t)S.d.nlev[S.dev_factor[sl]];
+        M.col_s[j] = col;
+        col += (M.nlev_s[j] + 7) / 8 * 8;
+        ++j;
+    }
+    M.wcols = col;
+    return col <= kMmaMaxCols;
+}
+
 template <typename T>
-void launch_hybrid(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
+void launch_hybrid(SolverImpl& S, int kp, const T* w, const T* x, T* y, bool mma = false) {
     const HybridDev& H = *S.hyb;
     ObsParams O;
     const int np = obs_params_for(S, kp, sizeof(T), O);
     const int G = group_for(kp);
+    PrimMmaParams M;
+    if (mma && mma_layout(S, kp, sizeof(T), M)) {
+        M.pieces = H.pieces.p;
+        M.npieces = H.npieces;
+        M.pptr = H.pptr.p;
+        M.pcol = H.pcol.p;
+        const size_t mrow = (size_t)S.d.ndofs;
+        if (H.any_split) {
+            WB_CUDA(cudaMemsetAsync(y, 0, mrow * kp * sizeof(T), S.stream));
+        } else {
+            const size_t a = (size_t)M.off_p * kp, b = (size_t)(M.off_p + S.d.nlev[S.primary]) * kp;
+            if (a > 0) WB_CUDA(cudaMemsetAsync(y, 0, a * sizeof(T), S.stream));
+            if (mrow * kp > b) WB_CUDA(cudaMemsetAsync(y + b, 0, (mrow * kp - b) * sizeof(T), S.stream));
+        }
+        const int64_t tasks = (H.npieces + 7) / 8;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((tasks + 7) / 8, (int64_t)S.n_sm * 2));
+        prim_mma_kernel<T><<<grid, 256, 0, S.stream>>>(M, w, hyb_pval<T>(H), x, y);
+        WB_CUDA(cudaGetLastError());
+        if (H.nochunks > 0) {
+            const int64_t need = (H.nochunks * 32 + kBlock - 1) / kBlock;
+            auto kern = csr_rows_kernel<T, 4, EPI_ACC>;
+            kern<<<S.fit(need, (const void*)kern), kBlock, 0, S.stream>>>(H.ochunks.p, H.nochunks, H.rows.p, H.optr.p,
+                                                                          H.ocol.p, hyb_oval<T>(H), nullptr, x, y, kp);
+            WB_CUDA(cudaGetLastError());
+        }
+        S.gpu_launches += 2;
+        return;
+    }
     const int ci = 1;  // 32 observations per chunk
     PrimParams P{};
     P.ns = O.ns;
@@ -1255,17 +1329,19 @@ void launch_hybrid(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
 // capture; x is read and y overwritten.
 std::mutex g_obs_tune_mu;
 std::map<std::array<int64_t, 4>, int32_t> g_obs_tune;
-std::map<std::array<int64_t, 4>, int32_t> g_hyb_tune;  // same classes: hybrid apply on (1) or off (0)
+// same classes: hybrid apply off (0), on with prim_rows_kernel (1) or with prim_mma_kernel (2)
+std::map<std::array<int64_t, 4>, int32_t> g_hyb_tune;
 
 bool hybrid_in_use(const SolverImpl& S) {
     for (const auto& c : S.hyb_on)
         for (int32_t v : c)
-            if (v == 1) return true;
+            if (v >= 1) return true;
     return false;
 }
 
-// Whether the operator apply for kp RHS in T runs as the hybrid apply: decided once per
-// shape class by timing it against the tuned observation pass (`best_ms`; < 0: take the
+// Whether the operator apply for kp RHS in T runs as the hybrid apply, and with which
+// primary-major kernel: decided once per shape class by timing both forms (the tensor-core
+// one where it applies) against the tuned observation pass (`best_ms`; < 0: take the
 // class's cached decision).  x is read and y overwritten.
 template <typename T>
 void hybrid_decide(SolverImpl& S, int kp, const T* w, const T* x, T* y, float best_ms,
@@ -1285,29 +1361,34 @@ void hybrid_decide(SolverImpl& S, int kp, const T* w, const T* x, T* y, float be
     if (best_ms < 0.f && cached == 0) return;
     if (S.hyb && S.hyb->smask != smask && hybrid_in_use(S)) return;  // one set of arrays per solver
     if (!S.hyb || S.hyb->smask != smask) build_hybrid(S, smask);
-    if (best_ms < 0.f && cached == 1) {
-        on = 1;
+    if (best_ms < 0.f && cached >= 1) {
+        on = cached;
         return;
     }
+    PrimMmaParams M;
+    const bool mma_ok = mma_layout(S, kp, sizeof(T), M);
     cudaEvent_t e0, e1;
     WB_CUDA(cudaEventCreate(&e0));
     WB_CUDA(cudaEventCreate(&e1));
-    float ms_best = 0.f;
-    for (int sweep = 0; sweep < 2; ++sweep) {
-        launch_hybrid<T>(S, kp, w, x, y);
-        WB_CUDA(cudaEventRecord(e0, S.stream));
-        for (int rep = 0; rep < 2; ++rep) launch_hybrid<T>(S, kp, w, x, y);
-        WB_CUDA(cudaEventRecord(e1, S.stream));
-        WB_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        WB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        ms *= 0.5f;
-        if (sweep == 0 || ms < ms_best) ms_best = ms;
-    }
+    float ms_v[3] = {0.f, 0.f, 0.f};
+    for (int sweep = 0; sweep < 2; ++sweep)
+        for (int v = 1; v <= (mma_ok ? 2 : 1); ++v) {
+            launch_hybrid<T>(S, kp, w, x, y, v == 2);
+            WB_CUDA(cudaEventRecord(e0, S.stream));
+            for (int rep = 0; rep < 2; ++rep) launch_hybrid<T>(S, kp, w, x, y, v == 2);
+            WB_CUDA(cudaEventRecord(e1, S.stream));
+            WB_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            WB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            ms *= 0.5f;
+            if (sweep == 0 || ms < ms_v[v]) ms_v[v] = ms;
+        }
     WB_CUDA(cudaEventDestroy(e0));
     WB_CUDA(cudaEventDestroy(e1));
+    const int vb = (mma_ok && ms_v[2] < ms_v[1]) ? 2 : 1;
+    const float ms_best = ms_v[vb];
     S.hyb_ms[kp_class(kp)][sizeof(T) == 8 ? 1 : 0] = ms_best;
-    on = (best_ms < 0.f || ms_best < best_ms) ? 1 : 0;
+    on = (best_ms < 0.f || ms_best < best_ms) ? vb : 0;
     if (!on && !hybrid_in_use(S)) S.hyb.reset();
     std::lock_guard<std::mutex> lk(g_obs_tune_mu);
     g_hyb_tune.emplace(key, on);
@@ -1469,8 +1550,9 @@ void launch_gram_acc(SolverImpl& S, int kp, const T* x, T* y);
 template <typename T>
 void launch_gram(SolverImpl& S, int kp, const T* w, const T* x, T* y) {
     if (!S.explicit_op) {
-        if (S.hyb_on[kp_class(kp)][sizeof(T) == 8 ? 1 : 0] == 1 && S.hyb) {
-            launch_hybrid<T>(S, kp, w, x, y);
+        const int32_t hv = S.hyb_on[kp_class(kp)][sizeof(T) == 8 ? 1 : 0];
+        if (hv >= 1 && S.hyb) {
+            launch_hybrid<T>(S, kp, w, x, y, hv == 2);
             return;
         }
         launch_obs<T, OBS_GRAM>(S, kp, w, x, nullptr, y, nullptr);
@@ -4074,7 +4156,7 @@ int32_t within_solver_obs_rhs_per_lane(const within_solver* s, int32_t k, int32_
 }
 
 int within_solver_set_hybrid(within_solver* s, int32_t k, int32_t elem_bytes, int32_t on) {
-    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) || on < 0 || on > 1)
+    if (!s || k <= 0 || k > 32 || (elem_bytes != 4 && elem_bytes != 8) || on < 0 || on > 2)
         return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "invalid argument");
     wb::SolverImpl& S = *s->impl;
     std::lock_guard<std::mutex> lk(S.mu);
@@ -4096,6 +4178,13 @@ int within_solver_set_hybrid(within_solver* s, int32_t k, int32_t elem_bytes, in
                     return wb::fail(WITHIN_ERR_INVALID_ARGUMENT, "the hybrid apply is in use with other small factors");
             }
             if (!S.hyb || S.hyb->smask != smask) wb::build_hybrid(S, smask);
+            wb::PrimMmaParams M;
+            if (on == 2 && !wb::mma_layout(S, kp, (size_t)elem_bytes, M)) {
+                cur = 0;
+                return wb::fail(WITHIN_ERR_INVALID_ARGUMENT,
+                                "no tensor-core form of the hybrid apply here (it needs 16 RHS columns and at most "
+                                "48 small-factor levels, each factor padded to 8)");
+            }
         }
         cur = on;
         if (S.cg_exec) {  // the captured CG iteration holds the old operator
@@ -4119,7 +4208,11 @@ int64_t within_solver_hybrid_bytes(const within_solver* s, int32_t k, int32_t el
     const wb::HybridDev& H = *S.hyb;
     const int64_t e = elem_bytes, kp = wb::pad_kp(k), nP = S.d.nlev[S.primary];
     const int64_t ns = __builtin_popcount(H.smask), wt = S.d.w.empty() ? 0 : 1;
-    return S.d.n * (4 * ns + e * wt) + (int64_t)(H.pcol.n + H.ocol.n) * (4 + e) + (nP + 1) * (8 + 4) +
+    const bool mma = S.hyb_on[wb::kp_class((int)kp)][elem_bytes == 8 ? 1 : 0] == 2;
+    // per primary level: its C_PO row pointer (8) and its observation offset (4), or its
+    // pieces (16 each) for the tensor-core form
+    const int64_t lvl = mma ? (nP + 1) * 8 + H.npieces * 16 : (nP + 1) * (8 + 4);
+    return S.d.n * (4 * ns + e * wt) + (int64_t)(H.pcol.n + H.ocol.n) * (4 + e) + lvl +
            (int64_t)H.rows.n * (4 + 8) + 2 * e * S.d.ndofs * kp;
 }
 
