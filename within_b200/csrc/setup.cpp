@@ -581,7 +581,8 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
     std::vector<std::vector<Edge>> fills;
     // vertices per task of the parallel phases (small: the late rounds pick few vertices
     // of high degree, whose lists and samples are the long ones)
-    constexpr size_t kCompactTask = 64, kSampleTask = 16;
+    constexpr size_t kCompactTask = 64, kSampleTask = 16, kColTask = 256;
+    std::vector<size_t> col_off;
     while (remaining > kAcCoreMax) {
         // compact the dirty lists (each list alone: independent across vertices)
         todo.clear();
@@ -632,18 +633,32 @@ AcFactor ac_factor(const SymCsr& s, uint64_t seed, uint32_t split) {
                 smp.sample(L.data(), (int32_t)L.size(), split, d, seed + (uint64_t)v, fills[a]);
             }
         });
-        for (size_t a = 0; a < picked.size(); ++a) {
-            const int32_t v = picked[a];
-            const std::vector<Nbr>& L = g[v];
-            double d = 0.0;
-            for (const Nbr& x : L) d += x.w;
-            f.col_vertex.push_back(v);
-            f.col_diag.push_back(L.empty() ? 0.0 : d);
-            f.col_ptr.push_back((int32_t)f.col_idx.size());
-            for (const Nbr& x : L) {
-                f.col_idx.push_back((int32_t)x.col);
-                f.col_coef.push_back(x.w / d);
-            }
+        // the picked vertices' columns: sized first, then written in parallel (each column
+        // at its offset, with the same arithmetic as an append in pick order)
+        {
+            const size_t c0 = f.col_vertex.size(), i0 = f.col_idx.size(), np = picked.size();
+            col_off.assign(np + 1, 0);
+            for (size_t a = 0; a < np; ++a) col_off[a + 1] = col_off[a] + g[picked[a]].size();
+            f.col_vertex.resize(c0 + np);
+            f.col_diag.resize(c0 + np);
+            f.col_ptr.resize(c0 + np);
+            f.col_idx.resize(i0 + col_off[np]);
+            f.col_coef.resize(i0 + col_off[np]);
+            parallel_tasks((np + kColTask - 1) / kColTask, [&](size_t t) {
+                for (size_t a = t * kColTask; a < std::min(np, (t + 1) * kColTask); ++a) {
+                    const int32_t v = picked[a];
+                    const std::vector<Nbr>& L = g[v];
+                    double d = 0.0;
+                    for (const Nbr& x : L) d += x.w;
+                    f.col_vertex[c0 + a] = v;
+                    f.col_diag[c0 + a] = L.empty() ? 0.0 : d;
+                    f.col_ptr[c0 + a] = (int32_t)(i0 + col_off[a]);
+                    for (size_t j = 0; j < L.size(); ++j) {
+                        f.col_idx[i0 + col_off[a] + j] = (int32_t)L[j].col;
+                        f.col_coef[i0 + col_off[a] + j] = L[j].w / d;
+                    }
+                }
+            });
         }
         // the fill, appended in emission order: worker w of nw owns the target vertices
         // u with u % nw == w and scans every edge, so each list receives its entries in
